@@ -1,0 +1,140 @@
+/*
+ * msbg_gpu.h — C ABI of the B200 sparse block-grid PDE solver.
+ *
+ * Drop-in GPU path for two MSBG entry points (reference = AkirA-fx/MSBG-Flip):
+ *   - MultiresSparseGrid::applyChannelPdeFast<float>(..., -(PDE_MEAN_CURVATURE +
+ *     OPT_8_COLOR_SCHEME), ...)                          src/msbg4.cpp:59-957
+ *   - MultiresSparseGrid::preparePressureSolveFLIP / solvePressureFLIP
+ *                                                       src/msbg3.cpp:3041-3271
+ *
+ * The host keeps owning the MSBG block pool; this library owns device pools and
+ * moves data only on explicit upload/download calls.  Every function returns an
+ * msbg_status; codes mirror the reference's MI_* codes (src/globdef.h:128-150).
+ * No function calls exit(); a failed call leaves a message for
+ * msbg_gpu_last_error().  One context = one host thread + one CUDA stream.
+ *
+ * Grid conventions (identical to the reference, src/sbg.h:1746-1822):
+ *   block id  bid = bx + by*nbx + bz*nbx*nby          (nbx = sx / bsx0, ...)
+ *   voxel id  vid = vx + vy*bsx + vz*bsx*bsx          (bsx = bsx0 >> level)
+ *   block colour (8-colour scheme) = (bx&1) + 2*(by&1) + 4*(bz&1)
+ *                                                       src/msbg.h:642-646
+ */
+#ifndef MSBG_GPU_H
+#define MSBG_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: same values as MI_OK .. MI_EINTERNAL (src/globdef.h:128-150). */
+typedef enum {
+  MSBG_OK = 0,
+  MSBG_ERROR = 1,
+  MSBG_ENOMEM = 2,
+  MSBG_ENOTIMPL = 4,
+  MSBG_EINVARG = 5,
+  MSBG_EMATH = 15,
+  MSBG_EINTERNAL = 20,
+  MSBG_ENODEV = 25, /* MI_ENOTAVAIL: no usable CUDA device */
+  MSBG_ETIMEOUT = 30
+} msbg_status;
+
+/* Per-block kind of a channel, as the reference's block map holds it
+ * (src/sbg.h:1906-2049): NULL entry, value block, const empty, const full. */
+enum {
+  MSBG_BLOCK_NULL = 0,
+  MSBG_BLOCK_VALUE = 1,
+  MSBG_BLOCK_EMPTY = 2,
+  MSBG_BLOCK_FULL = 3
+};
+
+/* Storage type of a channel's values. */
+enum { MSBG_F32 = 0, MSBG_F16 = 1, MSBG_BF16 = 2, MSBG_F64 = 3 };
+
+typedef struct msbg_gpu_ctx msbg_gpu_ctx;
+
+/* Grid topology: the block raster and the resolution level of every block at
+ * multigrid level 0 (the refinement map handed to
+ * MultiresSparseGrid::setRefinementMap, src/msbg.cpp:1428).  For a
+ * single-level grid pass blockLevel = NULL (all blocks at level 0). */
+typedef struct {
+  int sx, sy, sz;        /* finest-level resolution (multiples of bsx0) */
+  int bsx0;              /* base block size: 8, 16 or 32 */
+  int nLevels;           /* resolution levels (1..4) */
+  const int* blockLevel; /* [nbx*nby*nbz] level per block, or NULL */
+} msbg_topo_desc;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Replaces nothing in the reference (its state lives in MultiresSparseGrid);
+ * creates the device context (device memory, stream) on CUDA device `device`. */
+int msbg_gpu_init(int device, msbg_gpu_ctx** out);
+int msbg_gpu_destroy(msbg_gpu_ctx* ctx);
+const char* msbg_gpu_last_error(const msbg_gpu_ctx* ctx);
+/* Waits for all work issued on the context's stream. */
+int msbg_gpu_sync(msbg_gpu_ctx* ctx);
+
+/* Mirrors MultiresSparseGrid::create + setRefinementMap for the device side
+ * (src/msbg.cpp:131, 1428): stores the block raster; drops all channels. */
+int msbg_gpu_sync_topology(msbg_gpu_ctx* ctx, const msbg_topo_desc* desc);
+
+/* ---- channels ------------------------------------------------------------ */
+
+/* Uploads one FP32 channel of resolution level `level` (all blocks of the
+ * raster are of size bsx0>>level).  Replaces the host-side reads of
+ * SparseGrid<float>::getBlockDataPtr (src/sbg.h:913-979).
+ *   kind[nBlocks]      MSBG_BLOCK_* per block id
+ *   blockPtrs[nBlocks] host pointer of each value block (others ignored), as
+ *                      returned by getBlockDataPtr(bid); may be NULL when
+ *                      `packed` is given instead
+ *   packed             all value blocks' voxels back to back in ascending bid
+ *                      order (alternative to blockPtrs; one copy)
+ *   emptyVal/fullVal   values of const empty / full blocks (setEmptyValue /
+ *                      setFullValue, src/sbg.h)                           */
+int msbg_gpu_upload_channel(msbg_gpu_ctx* ctx, int chan, int level,
+                            const int8_t* kind, const float* const* blockPtrs,
+                            const float* packed, float emptyVal, float fullVal);
+
+/* Copies a channel's value blocks back to the host (same layouts as upload). */
+int msbg_gpu_download_channel(msbg_gpu_ctx* ctx, int chan, float* const* blockPtrs,
+                              float* packed);
+
+/* Number of value blocks of a channel (size of the packed layout / bsx^3). */
+int msbg_gpu_channel_num_value_blocks(msbg_gpu_ctx* ctx, int chan, int64_t* out);
+
+/* Device pointer to the packed value blocks of a channel (for callers that
+ * keep data resident and launch on the context stream). */
+int msbg_gpu_channel_device_ptr(msbg_gpu_ctx* ctx, int chan, void** out);
+
+/* ---- mean-curvature flow -------------------------------------------------- */
+
+/* Replaces MultiresSparseGrid::applyChannelPdeFast<float>(chan, CH_NULL, CH_NULL,
+ * &blockList, -(PDE_MEAN_CURVATURE+OPT_8_COLOR_SCHEME), clamp01, 0,0,0,
+ * numIter, 1.0f, dt)                        src/msbg4.cpp:59-957, msbg.h:2176
+ * In-place 8-colour block Gauss-Seidel (Jacobi inside a block) of the
+ * 19-point mean-curvature stencil, halo BC_NEUMANN.  numIter is rounded up
+ * to an even count as the reference does (src/msbg4.cpp:150-152).  Only
+ * blocks of `blockList` are updated; every value block is read as halo.
+ * Asynchronous on the context stream. */
+int msbg_gpu_pde_mcf(msbg_gpu_ctx* ctx, int chan, const int* blockList, int n,
+                     int numIter, float dt, int clamp01);
+
+/* Same smoother on caller-owned device memory, launched on `stream`
+ * (cudaStream_t as void*; NULL = the legacy default stream): pool = value blocks [nSlots][bsx^3] FP32,
+ * slotOf[nBlocks] = slot or -1 NULL / -2 empty / -3 full; colourList holds
+ * the updated blocks' ids grouped by colour with colourStart[9] offsets
+ * (device arrays).  For callers that keep the grid resident on the GPU. */
+int msbg_gpu_pde_mcf_device(msbg_gpu_ctx* ctx, float* pool, const int* slotOf,
+                            const int* colourList, const int* colourStartHost,
+                            int nbx, int nby, int nbz, int bsx, float emptyVal,
+                            float fullVal, int numIter, float dt, int clamp01,
+                            void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MSBG_GPU_H */

@@ -1,0 +1,99 @@
+// Shared definitions of the B200 sparse block-grid solver library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "msbg_gpu.h"
+
+namespace msbg {
+
+// Neighbour / block-map codes stored in slot tables (slot >= 0 = value block).
+enum : int {
+  SLOT_NULL = -1,   // no block in the map: BC_NEUMANN clamp to own block
+  SLOT_EMPTY = -2,  // const empty block
+  SLOT_FULL = -3,   // const full block
+  SLOT_OUT = -4     // outside the domain: BC_NEUMANN clamp to own block
+};
+
+struct DeviceBuffer {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&p, n ? n : 16);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+  }
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// One uploaded FP32 channel at one resolution level.
+struct Channel {
+  int level = 0;
+  int bsx = 0;
+  int64_t nValue = 0;
+  float emptyVal = 0.f, fullVal = 0.f;
+  std::vector<int> slotHost;   // [nb] slot or SLOT_* code
+  std::vector<int8_t> kindHost;
+  DeviceBuffer pool;           // [nValue][bsx^3] float
+  DeviceBuffer slot;           // [nb] int
+};
+
+}  // namespace msbg
+
+struct msbg_gpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sx = 0, sy = 0, sz = 0, bsx0 = 0, nLevels = 1;
+  int nbx = 0, nby = 0, nbz = 0;
+  std::vector<int> blockLevel;
+  std::map<int, std::unique_ptr<msbg::Channel>> channels;
+  std::string lastError;
+  // scratch for block lists (grouped by colour)
+  msbg::DeviceBuffer listBuf;
+  msbg::DeviceBuffer errBuf;  // int: set by kernels whose bounded wait gave up
+  std::vector<int> listHost;
+  void* pinned = nullptr;
+  size_t pinnedBytes = 0;
+  int64_t nb() const { return (int64_t)nbx * nby * nbz; }
+};
+
+namespace msbg {
+
+int set_error(msbg_gpu_ctx* ctx, int code, const char* fmt, ...);
+
+#define MSBG_CUDA_TRY(ctx, expr)                                                   \
+  do {                                                                             \
+    cudaError_t _e = (expr);                                                       \
+    if (_e != cudaSuccess)                                                         \
+      return ::msbg::set_error((ctx), _e == cudaErrorMemoryAllocation ? MSBG_ENOMEM \
+                                                                      : MSBG_ERROR, \
+                               "%s: %s (%s:%d)", #expr, cudaGetErrorString(_e),   \
+                               __FILE__, __LINE__);                                \
+  } while (0)
+
+// Launches of the 8-colour mean-curvature-flow passes (mcf.cu).
+cudaError_t launch_mcf(float* pool, const int* slotOf, const int* colourList,
+                       const int* colourStart, int nbx, int nby, int nbz, int bsx,
+                       float emptyVal, float fullVal, int nIter, float dt, int clamp01,
+                       int* errFlag, cudaStream_t stream);
+
+}  // namespace msbg

@@ -1,0 +1,186 @@
+"""Python binding (ctypes) of the C ABI in include/msbg_gpu.h.
+
+Thin: every call goes straight to libmsbg_gpu.so (the sm_100a kernels); there
+is no Python or CPU compute path.  If the library is missing the import of
+:func:`lib` raises, so nothing can silently fall back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "libmsbg_gpu.so")
+
+MSBG_OK = 0
+STATUS = {0: "MSBG_OK", 1: "MSBG_ERROR", 2: "MSBG_ENOMEM", 4: "MSBG_ENOTIMPL",
+          5: "MSBG_EINVARG", 15: "MSBG_EMATH", 20: "MSBG_EINTERNAL", 25: "MSBG_ENODEV",
+          30: "MSBG_ETIMEOUT"}
+
+BLOCK_NULL, BLOCK_VALUE, BLOCK_EMPTY, BLOCK_FULL = 0, 1, 2, 3
+
+_lib = None
+
+
+class MsbgError(RuntimeError):
+    def __init__(self, code, msg=""):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class TopoDesc(C.Structure):
+    _fields_ = [("sx", C.c_int), ("sy", C.c_int), ("sz", C.c_int), ("bsx0", C.c_int),
+                ("nLevels", C.c_int), ("blockLevel", C.POINTER(C.c_int))]
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct)) if a is not None else None
+
+
+def lib():
+    """Load libmsbg_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} missing: run msbg-flip_b200/build.py")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, f32 = C.c_void_p, C.c_int, C.c_float
+    pi32 = C.POINTER(C.c_int)
+    pi8 = C.POINTER(C.c_int8)
+    pf32 = C.POINTER(C.c_float)
+    sig = {
+        "msbg_gpu_init": (i32, [i32, C.POINTER(vp)]),
+        "msbg_gpu_destroy": (i32, [vp]),
+        "msbg_gpu_last_error": (C.c_char_p, [vp]),
+        "msbg_gpu_sync": (i32, [vp]),
+        "msbg_gpu_sync_topology": (i32, [vp, C.POINTER(TopoDesc)]),
+        "msbg_gpu_upload_channel": (i32, [vp, i32, i32, pi8, C.POINTER(pf32), pf32, f32, f32]),
+        "msbg_gpu_download_channel": (i32, [vp, i32, C.POINTER(pf32), pf32]),
+        "msbg_gpu_channel_num_value_blocks": (i32, [vp, i32, C.POINTER(C.c_int64)]),
+        "msbg_gpu_channel_device_ptr": (i32, [vp, i32, C.POINTER(vp)]),
+        "msbg_gpu_pde_mcf": (i32, [vp, i32, pi32, i32, i32, f32, i32]),
+        "msbg_gpu_pde_mcf_device": (i32, [vp, vp, vp, vp, pi32, i32, i32, i32, i32, f32, f32,
+                                          i32, f32, i32, vp]),
+        "msbg_scene_sphere_sdf": (i32, [i32, i32, i32, f32, f32, f32, i32, C.c_uint64, pi8, pf32,
+                                        C.POINTER(C.c_int64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def sphere_sdf_scene(res, bsx, n_spheres=64, rmin=20.0, rmax=60.0, band=4.0, dilate=1,
+                     seed=1234, with_values=True):
+    """Seeded union-of-spheres signed distance field on a single-level grid.
+
+    Returns (kind[nb] int8, values[nValue, bsx, bsx, bsx] float32 or None).
+    """
+    L = lib()
+    nb = (res // bsx) ** 3
+    kind = np.zeros(nb, np.int8)
+    nval = C.c_int64(0)
+    rc = L.msbg_scene_sphere_sdf(res, bsx, n_spheres, rmin, rmax, band, dilate, seed,
+                                 _p(kind, C.c_int8), None, C.byref(nval))
+    if rc:
+        raise MsbgError(rc, "scene generation")
+    if not with_values:
+        return kind, None
+    vals = np.empty((nval.value, bsx, bsx, bsx), np.float32)
+    rc = L.msbg_scene_sphere_sdf(res, bsx, n_spheres, rmin, rmax, band, dilate, seed,
+                                 _p(kind, C.c_int8), _p(vals, C.c_float), C.byref(nval))
+    if rc:
+        raise MsbgError(rc, "scene generation")
+    return kind, vals
+
+
+class Context:
+    """One device context (stream + device pools); mirrors the MSBG calls."""
+
+    def __init__(self, device=0):
+        L = lib()
+        h = C.c_void_p()
+        rc = L.msbg_gpu_init(device, C.byref(h))
+        if rc:
+            raise MsbgError(rc, "msbg_gpu_init")
+        self._h = h
+        self._L = L
+
+    def _check(self, rc, what):
+        if rc != MSBG_OK:
+            msg = self._L.msbg_gpu_last_error(self._h)
+            raise MsbgError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if self._h:
+            self._L.msbg_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        self._check(self._L.msbg_gpu_sync(self._h), "sync")
+
+    def set_topology(self, sx, sy, sz, bsx0, n_levels=1, block_level=None):
+        bl = None
+        if block_level is not None:
+            self._bl = np.ascontiguousarray(block_level, np.int32)
+            bl = _p(self._bl, C.c_int)
+        d = TopoDesc(sx, sy, sz, bsx0, n_levels, bl)
+        self._check(self._L.msbg_gpu_sync_topology(self._h, C.byref(d)), "sync_topology")
+
+    def upload_channel(self, chan, level, kind, packed, empty_val=0.0, full_val=0.0):
+        kind = np.ascontiguousarray(kind, np.int8)
+        packed = np.ascontiguousarray(packed, np.float32)
+        self._check(self._L.msbg_gpu_upload_channel(
+            self._h, chan, level, _p(kind, C.c_int8), None, _p(packed, C.c_float),
+            empty_val, full_val), "upload_channel")
+        self.sync()
+
+    def upload_channel_blocks(self, chan, level, kind, blocks, empty_val=0.0, full_val=0.0):
+        """Upload from per-block host arrays (blocks[bid] or None), as MSBG holds them."""
+        kind = np.ascontiguousarray(kind, np.int8)
+        ptrs = (C.POINTER(C.c_float) * len(kind))()
+        keep = []
+        for b, arr in enumerate(blocks):
+            if arr is not None:
+                a = np.ascontiguousarray(arr, np.float32)
+                keep.append(a)
+                ptrs[b] = _p(a, C.c_float)
+        self._check(self._L.msbg_gpu_upload_channel(
+            self._h, chan, level, _p(kind, C.c_int8), ptrs, None, empty_val, full_val),
+            "upload_channel")
+        self.sync()
+
+    def download_channel(self, chan, out):
+        self._check(self._L.msbg_gpu_download_channel(self._h, chan, None, _p(out, C.c_float)),
+                    "download_channel")
+        return out
+
+    def num_value_blocks(self, chan):
+        n = C.c_int64()
+        self._check(self._L.msbg_gpu_channel_num_value_blocks(self._h, chan, C.byref(n)), "nvb")
+        return n.value
+
+    def device_ptr(self, chan):
+        p = C.c_void_p()
+        self._check(self._L.msbg_gpu_channel_device_ptr(self._h, chan, C.byref(p)), "dptr")
+        return p.value
+
+    def apply_channel_pde_mcf(self, chan, block_list, num_iter, dt, clamp01=False, sync=True):
+        """msbg_gpu_pde_mcf: replaces applyChannelPdeFast<float>(MCF, 8-colour)."""
+        bl = np.ascontiguousarray(block_list, np.int32)
+        self._check(self._L.msbg_gpu_pde_mcf(self._h, chan, _p(bl, C.c_int), len(bl),
+                                             num_iter, dt, int(bool(clamp01))), "pde_mcf")
+        if sync:
+            self.sync()

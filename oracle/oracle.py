@@ -1,0 +1,108 @@
+"""ctypes loader of the oracle libraries (TEST INFRASTRUCTURE ONLY).
+
+- ``libmsbg_oracle.so``: the C restatement (oracle/msbg_oracle.c).
+- ``libmsbg_ref.so``: the reference MSBG core compiled from its own sources
+  plus oracle/ref/ref_harness.cpp (present only where it was built).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module; the GPU product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+ORACLE_SO = os.path.join(OUT, "libmsbg_oracle.so")
+REF_SO = os.path.join(OUT, "libmsbg_ref.so")
+
+_oracle = None
+_ref = None
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct)) if a is not None else None
+
+
+def build_oracle():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def build_ref(ref_root="/root/reference"):
+    if not os.path.isdir(os.path.join(ref_root, "src")):
+        return False
+    subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF_ROOT={ref_root}"], check=True)
+    return True
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build_oracle()
+        L = C.CDLL(ORACLE_SO)
+        L.oracle_mcf.restype = C.c_int
+        L.oracle_mcf.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int8), C.c_float, C.c_float,
+                                                 C.POINTER(C.c_float), C.POINTER(C.c_int),
+                                                 C.c_int, C.c_int, C.c_float, C.c_int, C.c_int]
+        _oracle = L
+    return _oracle
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError(REF_SO)
+        L = C.CDLL(REF_SO)
+        L.ref_init.restype = C.c_int
+        L.ref_init.argtypes = [C.c_int]
+        L.ref_mcf.restype = C.c_int
+        L.ref_mcf.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int8), C.c_float, C.c_float,
+                                              C.POINTER(C.c_float), C.POINTER(C.c_int), C.c_int,
+                                              C.c_int, C.c_float, C.c_int,
+                                              C.POINTER(C.c_double)]
+        L.ref_init(0)
+        _ref = L
+    return _ref
+
+
+def mcf_oracle(nb3, bsx, kind, values, update, num_iter, dt, clamp01=False, empty_val=4.0,
+               full_val=-4.0, exact_iter=False):
+    """C restatement of the 8-colour MCF smoother; returns the new values."""
+    nbx, nby, nbz = nb3
+    v = np.ascontiguousarray(values, np.float32).copy()
+    kind = np.ascontiguousarray(kind, np.int8)
+    up = np.ascontiguousarray(update, np.int32)
+    rc = oracle().oracle_mcf(nbx, nby, nbz, bsx, _p(kind, C.c_int8), empty_val, full_val,
+                             _p(v, C.c_float), _p(up, C.c_int), len(up), num_iter, dt,
+                             int(bool(clamp01)), int(bool(exact_iter)))
+    if rc:
+        raise RuntimeError(f"oracle_mcf rc={rc}")
+    return v
+
+
+def mcf_reference(res3, bsx, kind, values, update, num_iter, dt, clamp01=False, empty_val=4.0,
+                  full_val=-4.0, threads=0):
+    """Compiled reference applyChannelPdeFast<float>; returns (values, seconds)."""
+    L = ref()
+    if threads:
+        L.ref_init(threads)
+    sx, sy, sz = res3
+    v = np.ascontiguousarray(values, np.float32).copy()
+    kind = np.ascontiguousarray(kind, np.int8)
+    up = np.ascontiguousarray(update, np.int32)
+    secs = C.c_double(0)
+    rc = L.ref_mcf(sx, sy, sz, bsx, _p(kind, C.c_int8), empty_val, full_val, _p(v, C.c_float),
+                   _p(up, C.c_int), len(up), num_iter, dt, int(bool(clamp01)), C.byref(secs))
+    if rc:
+        raise RuntimeError(f"ref_mcf rc={rc}")
+    return v, secs.value
