@@ -133,6 +133,75 @@ int msbg_gpu_pde_mcf_device(msbg_gpu_ctx* ctx, float* pool, const int* slotOf,
                             float fullVal, int numIter, float dt, int clamp01,
                             void* stream);
 
+/* ---- FLIP pressure solve (MGPCG) ----------------------------------------- */
+
+/* Same callback contract as the reference's FlipPressureCallbacks
+ * (src/msbg.h:829-835; flip_sim.cpp:313-338 is its caller): cell type
+ * (0 liquid, CELL_SOLID 1, CELL_FIXED 2, CELL_VOID 0x1000), face coefficient
+ * of the LOWER face of cell (x,y,z) in direction dir, RHS per unit volume.
+ * Coordinates are fine-voxel coordinates.  The callbacks are called from
+ * several host threads at once and must be thread-safe. */
+typedef struct {
+  uint16_t (*sampleCellType)(void* user, int x, int y, int z);
+  float (*sampleFaceCoeff)(void* user, int dir, int x, int y, int z);
+  float (*sampleRhs)(void* user, int x, int y, int z);
+  void* user;
+} msbg_pressure_callbacks;
+
+/* Solver parameters.  The first five fields are the reference's
+ * FlipPressureSolveParams (src/msbg.h:837-844); the rest select the GPU
+ * variants.  msbg_gpu_solve_params_default() fills the defaults. */
+typedef struct {
+  int nPre, nPost, nCoarse, maxIter;
+  float tol;        /* stop when |r| <= tol*|b| */
+  int innerIter;    /* red-black sweeps inside a tile per smoother visit */
+  int storage;      /* MSBG_F32, MSBG_F16 or MSBG_BF16 vectors */
+  int maxRefine;    /* outer FP64 iterative-refinement steps (16-bit storage) */
+  int useGraph;     /* capture one PCG iteration in a CUDA graph */
+} msbg_gpu_solve_params;
+
+typedef struct {
+  int iterations;        /* PCG iterations (summed over refinement steps) */
+  int refinements;       /* outer refinement steps taken */
+  int status;            /* 0 converged, 1 maxIter, 2 breakdown, 3 non-finite */
+  double relResidual;    /* |b - A x| / |b|, recomputed in FP64 at the end */
+  double solveSeconds;   /* device time of the solve */
+  int64_t fineCells;     /* cells of MG level 0 (liquid) */
+  int nMgLevels;
+} msbg_gpu_solve_info;
+
+void msbg_gpu_solve_params_default(msbg_gpu_solve_params* p);
+
+/* Replaces MultiresSparseGrid::preparePressureSolveFLIP(cb)
+ * (src/msbg3.cpp:3041-3095): samples the callbacks on the block grid given by
+ * topo (refinement map = topo->blockLevel), builds the finite-volume operator
+ * of MG level 0 and the multigrid hierarchy, and uploads it. */
+int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
+                              const msbg_pressure_callbacks* cb);
+
+/* Replaces MultiresSparseGrid::solvePressureFLIP(params) (src/msbg3.cpp:3098-3271):
+ * MGPCG with a V-cycle preconditioner, FP64 inner products. */
+int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_params* p,
+                            msbg_gpu_solve_info* info);
+
+/* Pressure of MG level 0 in the reference's block layout: for every block in
+ * ascending bid order, (bsx0>>level)^3 values, vid = x + y*bs + z*bs*bs. */
+int msbg_gpu_pressure_download(msbg_gpu_ctx* ctx, float* packed, int64_t n);
+/* Same layout, the right-hand side b (volume-integrated) of MG level 0. */
+int msbg_gpu_pressure_download_rhs(msbg_gpu_ctx* ctx, float* packed, int64_t n);
+/* Number of values in that layout. */
+int msbg_gpu_pressure_packed_size(msbg_gpu_ctx* ctx, int64_t* n);
+
+/* Diagnostics without a GPU (no counterpart in the reference): builds the
+ * multigrid hierarchy as msbg_gpu_pressure_prepare does, then on the host
+ *   yPacked = A xPacked on MG level 0 (block layout; both may be NULL),
+ *   fluidPerLevel[m] = liquid cells of MG level m (m < 32),
+ *   galerkinErr[m] = max|P^T A_m P x - A_{m+1} x| / max|P^T A_m P x| for a
+ *                    random x (m < 32; NULL to skip). */
+int msbg_gpu_pressure_host_check(const msbg_topo_desc* topo, const msbg_pressure_callbacks* cb,
+                                 const float* xPacked, double* yPacked, int* nMgLevels,
+                                 int64_t* fluidPerLevel, double* galerkinErr);
+
 #ifdef __cplusplus
 }
 #endif

@@ -28,6 +28,35 @@ int msbg_scene_sphere_sdf(int res, int bsx, int nSpheres, float rmin, float rmax
                           float band, int dilate, uint64_t seed, int8_t* kind,
                           float* values, int64_t* nValueBlocks);
 
+/* Free-surface pressure problem (adaptive MSBG, FLIP pressure solve).
+ *   Domain res^3 (fine voxels), base blocks bsx0^3, nLevels resolution levels.
+ *   Liquid = {z < zLiquid*res} U nSpheres spheres (centres U[0,res)^3, radii
+ *   U[rMin,rMax]*res); nCuboids axis-aligned solid cuboids (sides
+ *   U[0.05,0.15]*res) override liquid; everything else is air.
+ *   Refinement map: level 0 for blocks whose centre lies within `band` fine
+ *   voxels (+ half a block diagonal) of the liquid surface, coarser levels in
+ *   further bands of width 2*band, 4*band ...; then 2:1 graded.
+ *   RHS = discrete MAC divergence (per unit volume) of
+ *   u = sum_k a_k sin(2 pi k.x/res + phi_k) over nModes modes, |k|_inf in
+ *   1..kMax, a_k ~ N(0,1) per component.
+ * The callbacks below sample it at fine-voxel coordinates like the
+ * reference's FlipPressureCallbacks (src/msbg.h:829-835, src/flip_sim.cpp:313-338):
+ *   cell type: 0 liquid, CELL_SOLID (1) solid or outside, CELL_VOID (0x1000) air;
+ *   face coefficient: 1 inside the box, 0 on faces touching a solid cell or a
+ *   box wall; rhs: divergence in liquid cells, 0 elsewhere. */
+typedef struct msbg_pressure_scene msbg_pressure_scene;
+
+msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, int nLevels, float zLiquid,
+                                                int nSpheres, float rMin, float rMax,
+                                                int nCuboids, int nModes, int kMax, float band,
+                                                uint64_t seed);
+void msbg_scene_pressure_destroy(msbg_pressure_scene* s);
+/* Refinement map (levels per base block, bid order). */
+int msbg_scene_pressure_block_levels(const msbg_pressure_scene* s, int* levels);
+uint16_t msbg_scene_cell_type(void* scene, int x, int y, int z);
+float msbg_scene_face_coeff(void* scene, int dir, int x, int y, int z);
+float msbg_scene_rhs(void* scene, int x, int y, int z);
+
 #ifdef __cplusplus
 }
 #endif

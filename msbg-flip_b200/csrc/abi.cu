@@ -57,6 +57,7 @@ extern "C" int msbg_gpu_destroy(msbg_gpu_ctx* ctx) {
   if (!ctx) return MSBG_EINVARG;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  pressure_release(ctx);
   ctx->channels.clear();
   ctx->listBuf.release();
   ctx->errBuf.release();

@@ -90,6 +90,9 @@ int set_error(msbg_gpu_ctx* ctx, int code, const char* fmt, ...);
                                __FILE__, __LINE__);                                \
   } while (0)
 
+// Releases the pressure solver state of a context (pressure.cu).
+void pressure_release(msbg_gpu_ctx* ctx);
+
 // Launches of the 8-colour mean-curvature-flow passes (mcf.cu).
 cudaError_t launch_mcf(float* pool, const int* slotOf, const int* colourList,
                        const int* colourStart, int nbx, int nby, int nbz, int bsx,

@@ -1,0 +1,786 @@
+// MGPCG pressure solve on the GPU: tile kernels, V-cycle, PCG driver, C ABI.
+//
+// Replaces MultiresSparseGrid::preparePressureSolveFLIP + solvePressureFLIP
+// (src/msbg3.cpp:3041-3271).  Structure of one PCG iteration as in the
+// reference (src/msbg3.cpp:3149-3236): q = A d, alpha = rho/(d.q),
+// x += alpha d, r -= alpha q, z = V(r), beta = (r.z)/rho, d = z + beta d;
+// stop when |r|^2 <= tol^2 |b|^2 or on breakdown.  Inner products and norms
+// are FP64 (two-stage deterministic reductions with warp shuffles).  The
+// V-cycle (src/msbg3.cpp:2412-2465) is pre-smooth, residual, restriction,
+// recursion, prolongation, post-smooth; the smoother is a tile-wise
+// red-black Gauss-Seidel with the tiles themselves visited in red-black
+// order per resolution level (the reference visits blocks red-black too,
+// src/msbg3.cpp:2185-2219); the post-smoother is the exact adjoint of the
+// pre-smoother so the preconditioner is symmetric.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "pressure.h"
+#include "pressure_kernels.cuh"
+
+namespace msbg {
+namespace ps {
+
+// ---------------------------------------------------------------------------
+// reductions
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum over the CTA; result valid in thread 0.
+__device__ double block_sum(double v) {
+  __shared__ double ws[32];
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? ws[threadIdx.x] : 0.0;
+  if (w == 0) v = warp_sum(v);
+  __syncthreads();
+  return v;
+}
+
+struct Scalars {
+  double bb, rho, rhoNew, dq, rr, alpha, beta;
+  int status;  // 0 ok, 2 breakdown, 3 non-finite
+  int pad;
+};
+
+enum { FIN_BB = 0, FIN_DQ_ALPHA = 1, FIN_RR = 2, FIN_RHO = 3, FIN_RHONEW_BETA = 4 };
+
+// Deterministic second stage: fixed-order sum of the CTA partials, then the
+// scalar step of PCG that depends on it.
+__global__ void __launch_bounds__(1024) k_finalize(const double* __restrict__ partial, int n,
+                                                   Scalars* s, int what) {
+  double v = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += partial[i];
+  v = block_sum(v);
+  if (threadIdx.x != 0) return;
+  switch (what) {
+    case FIN_BB: s->bb = v; break;
+    case FIN_RHO: s->rho = v; break;
+    case FIN_RR: s->rr = v; if (!isfinite(v)) s->status = 3; break;
+    case FIN_DQ_ALPHA:
+      s->dq = v;
+      if (!isfinite(v) || !isfinite(s->rho)) s->status = 3;
+      else if (!(v > 1e-300) || !(s->rho > 1e-300)) s->status = 2;
+      else s->alpha = s->rho / v;
+      break;
+    case FIN_RHONEW_BETA:
+      s->rhoNew = v;
+      if (!isfinite(v)) s->status = 3;
+      else if (!(v > 1e-300)) s->status = 2;
+      else {
+        s->beta = v / s->rho;
+        s->rho = v;
+      }
+      break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// level-0 vector kernels (grid-stride, fixed grid for deterministic partials)
+// ---------------------------------------------------------------------------
+constexpr int VEC_GRID = 148 * 4, VEC_BLOCK = 512;
+
+__global__ void __launch_bounds__(VEC_BLOCK) k_dot(const float* __restrict__ a,
+                                                   const float* __restrict__ b, int64_t n,
+                                                   double* __restrict__ partial) {
+  double acc = 0;
+  const int64_t n4 = n >> 2;
+  const float4* a4 = reinterpret_cast<const float4*>(a);
+  const float4* b4 = reinterpret_cast<const float4*>(b);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float4 u = a4[i], v = b4[i];
+    acc += (double)u.x * v.x + (double)u.y * v.y + (double)u.z * v.z + (double)u.w * v.w;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+// x += alpha d; r -= alpha q; partial |r|^2.  Skipped (norm only) after a breakdown.
+__global__ void __launch_bounds__(VEC_BLOCK) k_axpy_norm(float* __restrict__ x,
+                                                         float* __restrict__ r,
+                                                         const float* __restrict__ d,
+                                                         const float* __restrict__ q, int64_t n,
+                                                         const Scalars* __restrict__ s,
+                                                         double* __restrict__ partial) {
+  const bool ok = s->status == 0;
+  const float alpha = (float)s->alpha;
+  double acc = 0;
+  const int64_t n4 = n >> 2;
+  float4* x4 = reinterpret_cast<float4*>(x);
+  float4* r4 = reinterpret_cast<float4*>(r);
+  const float4* d4 = reinterpret_cast<const float4*>(d);
+  const float4* q4 = reinterpret_cast<const float4*>(q);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float4 rv = r4[i];
+    if (ok) {
+      float4 xv = x4[i], dv = d4[i], qv = q4[i];
+      xv.x = fmaf(alpha, dv.x, xv.x); xv.y = fmaf(alpha, dv.y, xv.y);
+      xv.z = fmaf(alpha, dv.z, xv.z); xv.w = fmaf(alpha, dv.w, xv.w);
+      rv.x = fmaf(-alpha, qv.x, rv.x); rv.y = fmaf(-alpha, qv.y, rv.y);
+      rv.z = fmaf(-alpha, qv.z, rv.z); rv.w = fmaf(-alpha, qv.w, rv.w);
+      x4[i] = xv;
+      r4[i] = rv;
+    }
+    acc += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+// d = z + beta d
+__global__ void __launch_bounds__(VEC_BLOCK) k_update_d(float* __restrict__ d,
+                                                        const float* __restrict__ z, int64_t n,
+                                                        const Scalars* __restrict__ s) {
+  if (s->status) return;
+  const float beta = (float)s->beta;
+  const int64_t n4 = n >> 2;
+  float4* d4 = reinterpret_cast<float4*>(d);
+  const float4* z4 = reinterpret_cast<const float4*>(z);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float4 dv = d4[i], zv = z4[i];
+    dv.x = fmaf(beta, dv.x, zv.x); dv.y = fmaf(beta, dv.y, zv.y);
+    dv.z = fmaf(beta, dv.z, zv.z); dv.w = fmaf(beta, dv.w, zv.w);
+    d4[i] = dv;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tile kernels
+// ---------------------------------------------------------------------------
+
+// In-tile neighbour sum S of cell (i,j,k) from a shared-memory tile, ghosts
+// from gs.  cxv etc. point at the tile's couplings (shared or global).
+template <int TS>
+__device__ __forceinline__ float nbr_sum(const float* xs, const float* cxv, const float* cyv,
+                                         const float* czv, const float (*gs)[TS * TS], int i,
+                                         int j, int k) {
+  const int e = tidx(TS, i, j, k);
+  float S = 0.f;
+  S += (i > 0) ? cxv[e] * xs[e - 1] : gs[0][j + TS * k];
+  S += (i < TS - 1) ? cxv[e + 1] * xs[e + 1] : gs[1][j + TS * k];
+  S += (j > 0) ? cyv[e] * xs[e - TS] : gs[2][i + TS * k];
+  S += (j < TS - 1) ? cyv[e + TS] * xs[e + TS] : gs[3][i + TS * k];
+  S += (k > 0) ? czv[e] * xs[e - TS * TS] : gs[4][i + TS * j];
+  S += (k < TS - 1) ? czv[e + TS * TS] * xs[e + TS * TS] : gs[5][i + TS * j];
+  return S;
+}
+
+// q = A d on the listed tiles, partial d.q per CTA.
+template <int TS>
+__global__ void __launch_bounds__(TS* TS) k_matvec_dot(LevelView L, const int* __restrict__ tiles,
+                                                       const float* __restrict__ d,
+                                                       float* __restrict__ q,
+                                                       double* __restrict__ partial) {
+  constexpr int N = TS * TS * TS, NT = TS * TS;
+  __shared__ float xs[N];
+  __shared__ float gs[6][NT];
+  const int ti = tiles[blockIdx.x];
+  const int64_t off = L.tileOff[ti];
+  const int t = threadIdx.x, i = t % TS, j = t / TS;
+  for (int e = t; e < N; e += NT) xs[e] = d[off + e];
+#pragma unroll
+  for (int f = 0; f < 6; f++) gs[f][t] = ghost_sum(L, d, ti, TS, f >> 1, f & 1, i, j);
+  __syncthreads();
+  double acc = 0;
+  const float* cxv = L.cx + off;
+  const float* cyv = L.cy + off;
+  const float* czv = L.cz + off;
+#pragma unroll 4
+  for (int k = 0; k < TS; k++) {
+    const int e = tidx(TS, i, j, k);
+    const float dg = L.diag[off + e];
+    float y = 0.f;
+    if (dg > 0.f) y = dg * xs[e] - nbr_sum<TS>(xs, cxv, cyv, czv, gs, i, j, k);
+    q[off + e] = y;
+    acc += (double)xs[e] * (double)y;
+  }
+  acc = block_sum(acc);
+  if (t == 0 && partial) partial[blockIdx.x] = acc;
+}
+
+// r = b - A x on the listed tiles, restricted (sum over the liquid children,
+// P^T) into the coarse right-hand side bc.
+template <int TS>
+__global__ void __launch_bounds__(TS* TS) k_residual_restrict(LevelView L,
+                                                              const int* __restrict__ tiles,
+                                                              const float* __restrict__ x,
+                                                              const float* __restrict__ b,
+                                                              float* __restrict__ bc,
+                                                              const int64_t* __restrict__ coarseOff) {
+  constexpr int N = TS * TS * TS, NT = TS * TS;
+  __shared__ float xs[N];
+  __shared__ float rs[N];
+  __shared__ float gs[6][NT];
+  const int ti = tiles[blockIdx.x];
+  const int64_t off = L.tileOff[ti];
+  const int t = threadIdx.x, i = t % TS, j = t / TS;
+  for (int e = t; e < N; e += NT) xs[e] = x[off + e];
+#pragma unroll
+  for (int f = 0; f < 6; f++) gs[f][t] = ghost_sum(L, x, ti, TS, f >> 1, f & 1, i, j);
+  __syncthreads();
+  const float* cxv = L.cx + off;
+  const float* cyv = L.cy + off;
+  const float* czv = L.cz + off;
+#pragma unroll 4
+  for (int k = 0; k < TS; k++) {
+    const int e = tidx(TS, i, j, k);
+    const float dg = L.diag[off + e];
+    float r = 0.f;
+    if (dg > 0.f) r = b[off + e] - (dg * xs[e] - nbr_sum<TS>(xs, cxv, cyv, czv, gs, i, j, k));
+    rs[e] = r;
+  }
+  __syncthreads();
+  const int* tc = L.toCoarse + (size_t)ti * 6;
+  const int ct = tc[0], ox = tc[1], oy = tc[2], oz = tc[3], agg = tc[4], cts = tc[5];
+  if (ct < 0) return;
+  float* dst = bc + coarseOff[ct];
+  if (agg) {
+    constexpr int H = TS / 2;
+    for (int c = t; c < H * H * H; c += NT) {
+      const int ci = c % H, cj = (c / H) % H, ck = c / (H * H);
+      const int e = tidx(TS, 2 * ci, 2 * cj, 2 * ck);
+      const float s = rs[e] + rs[e + 1] + rs[e + TS] + rs[e + TS + 1] + rs[e + TS * TS] +
+                      rs[e + TS * TS + 1] + rs[e + TS * TS + TS] + rs[e + TS * TS + TS + 1];
+      dst[tidx(cts, ox + ci, oy + cj, oz + ck)] = s;
+    }
+  } else {
+    for (int e = t; e < N; e += NT) {
+      const int ii = e % TS, jj = (e / TS) % TS, kk = e / (TS * TS);
+      dst[tidx(cts, ox + ii, oy + jj, oz + kk)] = rs[e];
+    }
+  }
+}
+
+// x += P xc (liquid cells only).
+template <int TS>
+__global__ void __launch_bounds__(TS* TS) k_prolong(LevelView L, const int* __restrict__ tiles,
+                                                    float* __restrict__ x,
+                                                    const float* __restrict__ xc,
+                                                    const int64_t* __restrict__ coarseOff) {
+  constexpr int N = TS * TS * TS, NT = TS * TS;
+  const int ti = tiles[blockIdx.x];
+  const int64_t off = L.tileOff[ti];
+  const int* tc = L.toCoarse + (size_t)ti * 6;
+  const int ct = tc[0], ox = tc[1], oy = tc[2], oz = tc[3], agg = tc[4], cts = tc[5];
+  if (ct < 0) return;
+  const float* src = xc + coarseOff[ct];
+  for (int e = threadIdx.x; e < N; e += NT) {
+    if (!(L.diag[off + e] > 0.f)) continue;
+    const int i = e % TS, j = (e / TS) % TS, k = e / (TS * TS);
+    const int sh = agg ? 1 : 0;
+    x[off + e] += src[tidx(cts, ox + (i >> sh), oy + (j >> sh), oz + (k >> sh))];
+  }
+}
+
+// Red-black Gauss-Seidel inside each listed tile, `inner` iterations, ghosts
+// frozen at their values when the tile is loaded.  reverse=0: red then black;
+// reverse=1: black then red (the adjoint order).  Optional partial b.x.
+template <int TS>
+__global__ void __launch_bounds__(TS* TS) k_smooth(LevelView L, const int* __restrict__ tiles,
+                                                   float* __restrict__ x,
+                                                   const float* __restrict__ b, int inner,
+                                                   int reverse, double* __restrict__ partial) {
+  constexpr int N = TS * TS * TS, NT = TS * TS;
+  extern __shared__ __align__(16) float sm[];
+  float* xs = sm;
+  float* cxs = sm + N;
+  float* cys = sm + 2 * N;
+  float* czs = sm + 3 * N;
+  float(*gs)[NT] = reinterpret_cast<float(*)[NT]>(sm + 4 * N);
+  const int ti = tiles[blockIdx.x];
+  const int64_t off = L.tileOff[ti];
+  const int t = threadIdx.x, i = t % TS, j = t / TS;
+  for (int e = t; e < N; e += NT) {
+    xs[e] = x[off + e];
+    cxs[e] = L.cx[off + e];
+    cys[e] = L.cy[off + e];
+    czs[e] = L.cz[off + e];
+  }
+  float bb[TS], inv[TS];
+#pragma unroll
+  for (int k = 0; k < TS; k++) {
+    const int e = tidx(TS, i, j, k);
+    const float dg = L.diag[off + e];
+    inv[k] = dg > 0.f ? 1.0f / dg : 0.f;
+    bb[k] = b[off + e];
+  }
+#pragma unroll
+  for (int f = 0; f < 6; f++) gs[f][t] = ghost_sum(L, x, ti, TS, f >> 1, f & 1, i, j);
+  __syncthreads();
+  for (int it = 0; it < inner; it++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int colour = reverse ? 1 - h : h;
+#pragma unroll
+      for (int k = 0; k < TS; k++) {
+        if (((i + j + k) & 1) != colour || inv[k] == 0.f) continue;
+        const float S = nbr_sum<TS>(xs, cxs, cys, czs, gs, i, j, k);
+        xs[tidx(TS, i, j, k)] = (bb[k] + S) * inv[k];
+      }
+      __syncthreads();
+    }
+  }
+  double acc = 0;
+  for (int e = t; e < N; e += NT) {
+    x[off + e] = xs[e];
+    if (partial) acc += (double)xs[e] * (double)b[off + e];
+  }
+  if (partial) {
+    acc = block_sum(acc);
+    if (t == 0) partial[blockIdx.x] = acc;
+  }
+}
+
+// Coarsest level: x = A^-1 b with the dense FP64 inverse (symmetric).
+__global__ void __launch_bounds__(512) k_coarse_solve(const double* __restrict__ Ainv, int n,
+                                                      const int64_t* __restrict__ cells,
+                                                      const float* __restrict__ b,
+                                                      float* __restrict__ x) {
+  __shared__ double bs[512];
+  const int t = threadIdx.x;
+  if (t < n) bs[t] = b[cells[t]];
+  __syncthreads();
+  if (t >= n) return;
+  double s = 0;
+  for (int j = 0; j < n; j++) s += Ainv[(size_t)j * n + t] * bs[j];
+  x[cells[t]] = (float)s;
+}
+
+template <int TS>
+size_t smooth_smem() {
+  return sizeof(float) * (4 * TS * TS * TS + 6 * TS * TS);
+}
+
+// ---------------------------------------------------------------------------
+// solver state
+// ---------------------------------------------------------------------------
+struct Solver {
+  Hierarchy H;
+  std::vector<std::unique_ptr<LevelDev>> dev;
+  std::vector<LevelView> views;
+  DeviceBuffer dCoarseInv, dCoarseCells;
+  DeviceBuffer rhs0, d0, q0, z0, r0, partial, scal;
+  int maxPartial = 0;
+  Scalars* hScal = nullptr;  // pinned
+  int bsx0 = 0, nbx = 0, nby = 0, nbz = 0;
+  std::vector<int> blockLevel;
+};
+
+template <int TS>
+void set_smooth_attr() {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(k_smooth<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smooth_smem<TS>());
+    done = true;
+  }
+}
+
+#define TS_DISPATCH(ts, CALL)        \
+  switch (ts) {                      \
+    case 16: { constexpr int T = 16; CALL; } break; \
+    case 8: { constexpr int T = 8; CALL; } break;   \
+    case 4: { constexpr int T = 4; CALL; } break;   \
+    case 2: { constexpr int T = 2; CALL; } break;   \
+    case 1: break;                   \
+    default: break;                  \
+  }
+
+struct Runner {
+  Solver& S;
+  cudaStream_t st;
+  int nPre, nPost, inner;
+
+  const int* passList(int m) { return S.dev[m]->passTiles.as<int>(); }
+  const int* groupList(int m) { return S.dev[m]->groupTiles.as<int>(); }
+
+  void smooth(int m, float* x, const float* b, bool post, double* partial) {
+    const Level& L = S.H.levels[m];
+    const int np = (int)L.passes.size();
+    for (int pi = 0; pi < np; pi++) {
+      const Level::Pass& P = L.passes[post ? np - 1 - pi : pi];
+      if (!P.count) continue;
+      const int* lst = passList(m) + P.start;
+      TS_DISPATCH(P.ts, (set_smooth_attr<T>(),
+                         k_smooth<T><<<P.count, T * T, smooth_smem<T>(), st>>>(
+                             S.views[m], lst, x, b, inner, post ? 1 : 0,
+                             (partial && pi == np - 1) ? partial : nullptr)));
+    }
+  }
+
+  void vcycle(int m, float* x, const float* b, double* rzPartial) {
+    const int last = (int)S.H.levels.size() - 1;
+    LevelDev& D = *S.dev[m];
+    const Level& L = S.H.levels[m];
+    cudaMemsetAsync(x, 0, sizeof(float) * L.nCells, st);
+    if (m == last) {
+      k_coarse_solve<<<1, 512, 0, st>>>(S.dCoarseInv.as<double>(), S.H.nCoarse,
+                                        S.dCoarseCells.as<int64_t>(), b, x);
+      return;
+    }
+    for (int s = 0; s < nPre; s++) smooth(m, x, b, false, nullptr);
+    LevelDev& C = *S.dev[m + 1];
+    for (const auto& g : L.groups) {
+      const int* lst = groupList(m) + g.start;
+      TS_DISPATCH(g.ts, (k_residual_restrict<T><<<g.count, T * T, 0, st>>>(
+                            S.views[m], lst, x, b, C.b.as<float>(), C.tileOff.as<int64_t>())));
+    }
+    vcycle(m + 1, C.x.as<float>(), C.b.as<float>(), nullptr);
+    for (const auto& g : L.groups) {
+      const int* lst = groupList(m) + g.start;
+      TS_DISPATCH(g.ts, (k_prolong<T><<<g.count, T * T, 0, st>>>(S.views[m], lst, x,
+                                                                  C.x.as<float>(),
+                                                                  C.tileOff.as<int64_t>())));
+    }
+    (void)D;
+    for (int s = 0; s < nPost; s++)
+      smooth(m, x, b, true, (rzPartial && s == nPost - 1) ? rzPartial : nullptr);
+  }
+
+  // q = A d with partial d.q (level 0)
+  int matvec_dot(const float* d, float* q, double* partial) {
+    const Level& L = S.H.levels[0];
+    int off = 0;
+    for (const auto& g : L.groups) {
+      const int* lst = groupList(0) + g.start;
+      TS_DISPATCH(g.ts, (k_matvec_dot<T><<<g.count, T * T, 0, st>>>(S.views[0], lst, d, q,
+                                                                     partial + off)));
+      off += g.count;
+    }
+    return off;
+  }
+};
+
+}  // namespace ps
+}  // namespace msbg
+
+using namespace msbg;
+using namespace msbg::ps;
+
+namespace {
+
+std::map<msbg_gpu_ctx*, std::unique_ptr<Solver>>& solvers() {
+  static std::map<msbg_gpu_ctx*, std::unique_ptr<Solver>> m;
+  return m;
+}
+
+std::unique_ptr<Solver>& solver_of(msbg_gpu_ctx* ctx) { return solvers()[ctx]; }
+
+template <typename T>
+cudaError_t upload(DeviceBuffer& buf, const std::vector<T>& v, cudaStream_t st) {
+  cudaError_t e = buf.ensure(sizeof(T) * std::max<size_t>(v.size(), 1));
+  if (e != cudaSuccess) return e;
+  if (v.empty()) return cudaSuccess;
+  return cudaMemcpyAsync(buf.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st);
+}
+
+}  // namespace
+
+namespace msbg {
+void pressure_release(msbg_gpu_ctx* ctx) {
+  auto it = solvers().find(ctx);
+  if (it == solvers().end()) return;
+  if (it->second && it->second->hScal) cudaFreeHost(it->second->hScal);
+  solvers().erase(it);
+}
+}  // namespace msbg
+
+extern "C" void msbg_gpu_solve_params_default(msbg_gpu_solve_params* p) {
+  if (!p) return;
+  p->nPre = 2;
+  p->nPost = 2;
+  p->nCoarse = 24;
+  p->maxIter = 500;
+  p->tol = 1e-6f;
+  p->innerIter = 2;
+  p->storage = MSBG_F32;
+  p->maxRefine = 4;
+  p->useGraph = 1;
+}
+
+extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
+                                         const msbg_pressure_callbacks* cb) {
+  if (!ctx || !topo || !cb || !cb->sampleCellType || !cb->sampleFaceCoeff || !cb->sampleRhs)
+    return MSBG_EINVARG;
+  int rc = msbg_gpu_sync_topology(ctx, topo);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  auto& sp = solver_of(ctx);
+  sp.reset(new Solver());
+  Solver& S = *sp;
+  std::string err;
+  rc = build_hierarchy(S.H, topo->sx, topo->sy, topo->sz, topo->bsx0, topo->nLevels,
+                       topo->blockLevel, cb, 512, &err);
+  if (rc) {
+    sp.reset();
+    return set_error(ctx, rc, "pressure prepare: %s", err.c_str());
+  }
+  for (size_t m = 0; m + 1 < S.H.levels.size(); m++)
+    for (const Tile& t : S.H.levels[m].tiles)
+      if (t.ts < 2 || t.ts > TS_MAX) {
+        sp.reset();
+        return set_error(ctx, MSBG_EINVARG, "grid dimensions give %d-cell tiles at MG level %d",
+                         t.ts, (int)m);
+      }
+  set_smooth_attr<16>();
+  set_smooth_attr<8>();
+  set_smooth_attr<4>();
+  set_smooth_attr<2>();
+  S.bsx0 = topo->bsx0;
+  S.nbx = ctx->nbx;
+  S.nby = ctx->nby;
+  S.nbz = ctx->nbz;
+  S.blockLevel = ctx->blockLevel;
+  cudaStream_t st = ctx->stream;
+  int maxPartial = VEC_GRID;
+  for (size_t m = 0; m < S.H.levels.size(); m++) {
+    const Level& L = S.H.levels[m];
+    auto D = std::make_unique<LevelDev>();
+    std::vector<int64_t> toff(L.tiles.size());
+    for (size_t i = 0; i < L.tiles.size(); i++) toff[i] = L.tiles[i].off;
+    MSBG_CUDA_TRY(ctx, upload(D->tileOff, toff, st));
+    MSBG_CUDA_TRY(ctx, upload(D->face, L.face, st));
+    MSBG_CUDA_TRY(ctx, upload(D->ifOff, L.ifOff, st));
+    MSBG_CUDA_TRY(ctx, upload(D->toCoarse, L.toCoarse, st));
+    MSBG_CUDA_TRY(ctx, upload(D->passTiles, L.passTiles, st));
+    MSBG_CUDA_TRY(ctx, upload(D->groupTiles, L.groupTiles, st));
+    MSBG_CUDA_TRY(ctx, upload(D->diag, L.diag, st));
+    MSBG_CUDA_TRY(ctx, upload(D->cx, L.cx, st));
+    MSBG_CUDA_TRY(ctx, upload(D->cy, L.cy, st));
+    MSBG_CUDA_TRY(ctx, upload(D->cz, L.cz, st));
+    MSBG_CUDA_TRY(ctx, upload(D->ifc, L.ifc, st));
+    const size_t nb = sizeof(float) * std::max<int64_t>(L.nCells, 4);
+    MSBG_CUDA_TRY(ctx, D->x.ensure(nb));
+    MSBG_CUDA_TRY(ctx, D->b.ensure(nb));
+    maxPartial = std::max(maxPartial, (int)L.tiles.size());
+    LevelView v;
+    v.tileOff = D->tileOff.as<int64_t>();
+    v.face = D->face.as<int>();
+    v.ifOff = D->ifOff.as<int64_t>();
+    v.toCoarse = D->toCoarse.as<int>();
+    v.diag = D->diag.as<float>();
+    v.cx = D->cx.as<float>();
+    v.cy = D->cy.as<float>();
+    v.cz = D->cz.as<float>();
+    v.ifc = D->ifc.as<float>();
+    S.views.push_back(v);
+    S.dev.push_back(std::move(D));
+  }
+  const Level& L0 = S.H.levels[0];
+  const size_t n0 = sizeof(float) * L0.nCells;
+  MSBG_CUDA_TRY(ctx, upload(S.rhs0, L0.rhs, st));
+  MSBG_CUDA_TRY(ctx, S.d0.ensure(n0));
+  MSBG_CUDA_TRY(ctx, S.q0.ensure(n0));
+  MSBG_CUDA_TRY(ctx, S.z0.ensure(n0));
+  MSBG_CUDA_TRY(ctx, S.r0.ensure(n0));
+  MSBG_CUDA_TRY(ctx, S.partial.ensure(sizeof(double) * maxPartial));
+  S.maxPartial = maxPartial;
+  MSBG_CUDA_TRY(ctx, S.scal.ensure(sizeof(Scalars)));
+  MSBG_CUDA_TRY(ctx, upload(S.dCoarseInv, S.H.coarseInv, st));
+  MSBG_CUDA_TRY(ctx, upload(S.dCoarseCells, S.H.coarseCells, st));
+  MSBG_CUDA_TRY(ctx, cudaMallocHost(&S.hScal, sizeof(Scalars)));
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return MSBG_OK;
+}
+
+extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_params* p,
+                                       msbg_gpu_solve_info* info) {
+  if (!ctx || !p) return MSBG_EINVARG;
+  auto& sp = solver_of(ctx);
+  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
+  if (p->nPre < 0 || p->nPost < 0 || p->maxIter < 0 || p->innerIter < 1 || !(p->tol >= 0))
+    return set_error(ctx, MSBG_EINVARG, "invalid solve parameters");
+  if (p->storage != MSBG_F32)
+    return set_error(ctx, MSBG_ENOTIMPL, "storage type %d not available", p->storage);
+  cudaSetDevice(ctx->device);
+  Solver& S = *sp;
+  cudaStream_t st = ctx->stream;
+  Runner R{S, st, p->nPre, p->nPost, p->innerIter};
+  const Level& L0 = S.H.levels[0];
+  const int64_t n = L0.nCells;
+  LevelDev& D0 = *S.dev[0];
+  float* x = D0.x.as<float>();
+  float* r = S.r0.as<float>();
+  float* d = S.d0.as<float>();
+  float* q = S.q0.as<float>();
+  float* z = S.z0.as<float>();
+  const float* b = S.rhs0.as<float>();
+  double* part = S.partial.as<double>();
+  Scalars* sc = S.scal.as<Scalars>();
+
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  // r = b, x = 0, bb = b.b, z = V(r), rho = r.z, d = z
+  cudaMemsetAsync(sc, 0, sizeof(Scalars), st);
+  cudaMemsetAsync(x, 0, sizeof(float) * n, st);
+  cudaMemcpyAsync(r, b, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+  k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(b, b, n, part);
+  k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_BB);
+  R.vcycle(0, z, r, nullptr);
+  k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
+  k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHO);
+  cudaMemcpyAsync(d, z, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  const double bb = S.hScal->bb;
+  int iters = 0, status = 1;
+  if (!(bb > 1e-30)) {
+    status = 0;
+  } else {
+    auto iteration = [&]() {
+      int nt = R.matvec_dot(d, q, part);
+      k_finalize<<<1, 1024, 0, st>>>(part, nt, sc, FIN_DQ_ALPHA);
+      k_axpy_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x, r, d, q, n, sc, part);
+      k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
+      R.vcycle(0, z, r, nullptr);
+      k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
+      k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHONEW_BETA);
+      k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, n, sc);
+      cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+    };
+    cudaGraphExec_t exec = nullptr;
+    if (p->useGraph) {
+      cudaGraph_t g;
+      MSBG_CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      iteration();
+      MSBG_CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
+      MSBG_CUDA_TRY(ctx, cudaGraphInstantiate(&exec, g, 0));
+      cudaGraphDestroy(g);
+    }
+    const double tol2 = (double)p->tol * (double)p->tol;
+    for (int it = 0; it < p->maxIter; it++) {
+      if (exec) {
+        MSBG_CUDA_TRY(ctx, cudaGraphLaunch(exec, st));
+      } else {
+        iteration();
+      }
+      MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+      iters = it + 1;
+      const Scalars hs = *S.hScal;
+      if (hs.status) {
+        // a breakdown found before the update leaves x, r unchanged
+        status = hs.status;
+        break;
+      }
+      if (hs.rr <= tol2 * bb) {
+        status = 0;
+        break;
+      }
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+  cudaEventRecord(e1, st);
+  // true residual |b - A x| (FP32 operator, FP64 norm)
+  int nt = R.matvec_dot(x, q, part);
+  (void)nt;
+  // q = A x; r_true = b - q -> reuse k_axpy_norm with alpha=-1 over (r=b copy)
+  cudaMemcpyAsync(z, b, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+  {
+    Scalars one{};
+    one.alpha = 1.0;
+    cudaMemcpyAsync(sc, &one, sizeof(Scalars), cudaMemcpyHostToDevice, st);
+    // z = b - 1*q (x argument gets d += q which is harmless: use q as x dummy)
+    k_axpy_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, q, q, n, sc, part);
+    k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
+    cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  }
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (info) {
+    info->iterations = iters;
+    info->refinements = 0;
+    info->status = status;
+    info->relResidual = bb > 0 ? std::sqrt(S.hScal->rr / bb) : 0.0;
+    info->solveSeconds = ms * 1e-3;
+    info->fineCells = L0.nFluid;
+    info->nMgLevels = (int)S.H.levels.size();
+  }
+  return MSBG_OK;
+}
+
+namespace {
+
+// Copy a level-0 vector (tile layout) into the reference's packed block layout.
+int to_packed(msbg_gpu_ctx* ctx, Solver& S, const float* dvec, float* packed, int64_t n) {
+  const Level& L = S.H.levels[0];
+  std::vector<float> h(L.nCells);
+  MSBG_CUDA_TRY(ctx, cudaMemcpy(h.data(), dvec, sizeof(float) * L.nCells, cudaMemcpyDeviceToHost));
+  // block offsets in the packed layout
+  const int64_t nb = (int64_t)S.nbx * S.nby * S.nbz;
+  std::vector<int64_t> boff(nb + 1, 0);
+  for (int64_t b = 0; b < nb; b++) {
+    const int bs = S.bsx0 >> S.blockLevel[b];
+    boff[b + 1] = boff[b] + (int64_t)bs * bs * bs;
+  }
+  if (n < boff[nb]) return set_error(ctx, MSBG_EINVARG, "packed buffer too small (%lld < %lld)",
+                                     (long long)n, (long long)boff[nb]);
+  std::memset(packed, 0, sizeof(float) * boff[nb]);
+  for (const Tile& t : L.tiles) {
+    for (int k = 0; k < t.ts; k++)
+      for (int j = 0; j < t.ts; j++)
+        for (int i = 0; i < t.ts; i++) {
+          const int X = t.ox + i, Y = t.oy + j, Z = t.oz + k;
+          const int bs = S.bsx0 >> t.level;
+          const int64_t b = (X / bs) + (int64_t)S.nbx * ((Y / bs) + (int64_t)S.nby * (Z / bs));
+          const int vx = X % bs, vy = Y % bs, vz = Z % bs;
+          packed[boff[b] + vx + (int64_t)bs * (vy + (int64_t)bs * vz)] =
+              h[t.off + i + (int64_t)t.ts * (j + (int64_t)t.ts * k)];
+        }
+  }
+  return MSBG_OK;
+}
+
+}  // namespace
+
+extern "C" int msbg_gpu_pressure_packed_size(msbg_gpu_ctx* ctx, int64_t* n) {
+  if (!ctx || !n) return MSBG_EINVARG;
+  auto& sp = solver_of(ctx);
+  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
+  int64_t s = 0;
+  for (int l : sp->blockLevel) {
+    const int bs = sp->bsx0 >> l;
+    s += (int64_t)bs * bs * bs;
+  }
+  *n = s;
+  return MSBG_OK;
+}
+
+extern "C" int msbg_gpu_pressure_download(msbg_gpu_ctx* ctx, float* packed, int64_t n) {
+  if (!ctx || !packed) return MSBG_EINVARG;
+  auto& sp = solver_of(ctx);
+  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
+  cudaSetDevice(ctx->device);
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return to_packed(ctx, *sp, sp->dev[0]->x.as<float>(), packed, n);
+}
+
+extern "C" int msbg_gpu_pressure_download_rhs(msbg_gpu_ctx* ctx, float* packed, int64_t n) {
+  if (!ctx || !packed) return MSBG_EINVARG;
+  auto& sp = solver_of(ctx);
+  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
+  cudaSetDevice(ctx->device);
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return to_packed(ctx, *sp, sp->rhs0.as<float>(), packed, n);
+}

@@ -1,0 +1,100 @@
+// Pressure solver internals: multigrid hierarchy of tiles on the MSBG block
+// grid (host description + device mirrors).  See pressure_host.cpp for the
+// construction and pressure.cu for the kernels and the MGPCG driver.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <vector>
+
+#include "common.cuh"
+#include "msbg_gpu.h"
+
+namespace msbg {
+namespace ps {
+
+constexpr int TS_MAX = 16;  // tile edge in cells (a 32^3 block is 8 tiles)
+
+// Face neighbour kinds of a tile face.
+enum : int {
+  FACE_NONE = 0,    // domain boundary, or a region whose tile holds no liquid
+  FACE_SAME = 1,    // same-level tile
+  FACE_COARSER = 2, // one level coarser tile (our face is part of its face)
+  FACE_FINER = 3    // one level finer tiles (1..4 of them cover our face)
+};
+
+// Per face: kind, t[4] neighbour tile ids, oa/ob offsets (FACE_COARSER: our
+// first face cell in neighbour cells; FACE_FINER: unused), cov (FACE_FINER:
+// our cells covered per fine tile along a/b), nts (neighbour tile size).
+constexpr int FACE_INTS = 9;
+enum { F_KIND = 0, F_T0 = 1, F_OA = 5, F_OB = 6, F_COV = 7, F_NTS = 8 };
+
+// Face order: -x,+x,-y,+y,-z,+z (face = 2*dir + side).  Tangential axes of a
+// face plane: dir 0 -> (y,z), dir 1 -> (x,z), dir 2 -> (x,y); plane index
+// a + ts*b.
+
+struct Tile {
+  int level;       // resolution level: cell edge = 2^level fine voxels
+  int ts;          // cells per edge
+  int ox, oy, oz;  // origin in level cells
+  int64_t off;     // first cell in the level pools
+};
+
+struct Level {
+  int m = 0;                       // multigrid level
+  std::vector<Tile> tiles;
+  std::vector<int> face;           // [nTiles*6*FACE_INTS]
+  std::vector<int64_t> ifOff;      // [nTiles*6] offset of the interface plane or -1
+  int64_t nCells = 0, nIf = 0;
+  // operator: a_ii, lower-face couplings to same-level neighbours, interface
+  // couplings (stored on the finer side, one per fine boundary cell)
+  std::vector<float> diag, cx, cy, cz, ifc, rhs;
+  // tile maps per resolution level: dense raster of tile ids (-1 = none)
+  std::vector<std::vector<int>> tmap = std::vector<std::vector<int>>(32);
+  std::vector<int> tmapN = std::vector<int>(32, 0);  // tiles per edge (0 = level absent)
+  std::vector<int> tsOf = std::vector<int>(32, 0);   // tile edge per level
+  // restriction map to level m+1: per tile coarse tile, offset, aggregated?
+  std::vector<int> toCoarse;       // [nTiles*6]: coarse tile, ox, oy, oz, aggregated, coarse ts
+  // smoothing passes: tile ids grouped by (level, colour), and per tile size
+  struct Pass {
+    int level, colour, ts;
+    int start, count;              // into passTiles
+  };
+  std::vector<Pass> passes;
+  std::vector<int> passTiles;
+  // all tiles grouped by tile size (for matvec/residual/restrict/prolong)
+  struct Group {
+    int ts, start, count;
+  };
+  std::vector<Group> groups;
+  std::vector<int> groupTiles;
+  int64_t nFluid = 0;
+};
+
+// Device mirror of one level.
+struct LevelDev {
+  DeviceBuffer tileOff, face, ifOff, toCoarse, passTiles, groupTiles;
+  DeviceBuffer diag, cx, cy, cz, ifc;
+  DeviceBuffer x, b, r;            // FP32 work vectors of this level
+};
+
+struct Hierarchy {
+  int res = 0, bsx0 = 0, nLevels = 0, nb1x = 0, nb1y = 0, nb1z = 0;
+  int sx = 0, sy = 0, sz = 0;
+  std::vector<int> blockLevel;     // refinement map (MG level 0)
+  std::vector<Level> levels;
+  // coarsest-level dense inverse (FP64), fluid cell indices
+  int nCoarse = 0;
+  std::vector<double> coarseInv;
+  std::vector<int64_t> coarseCells;
+};
+
+// Host construction (pressure_host.cpp).
+int build_hierarchy(Hierarchy& H, int sx, int sy, int sz, int bsx0, int nLevels,
+                    const int* blockLevel, const msbg_pressure_callbacks* cb,
+                    int maxCoarseCells, std::string* err);
+
+}  // namespace ps
+}  // namespace msbg

@@ -1,0 +1,744 @@
+// Host construction of the pressure multigrid hierarchy.
+//
+// MG level 0 is the reference's discretisation of the FLIP pressure equation
+// on the adaptive block grid (src/msbg3.cpp:564-1044 for the ghost couplings,
+// src/msbg3.cpp:2586-2779 for the diagonal), in finite-volume form:
+//   coupling across a same-level face of cells of edge h   = h * beta
+//   coupling across a fine(h)/coarse(2h) interface face    = (2/3) * h * beta
+//       (DPMR_GRAD_COEFF_FC, src/msbg.h:82-87; the reference's procNeighMixedRes2
+//        builds the same 2/3 weight, src/msbg3.cpp:59-161)
+//   a_ii = sum of the couplings of all faces of cell i (neighbours that are
+//       air/outside act as p = 0, solid faces have beta = 0)
+//   b_i  = rhs * h^3 (volume integral)
+// The diagonal differs from the reference only at level interfaces, where the
+// reference drops the interface coupling from a_ii and the resulting matrix is
+// not an M-matrix (see the design notes); here A is symmetric positive
+// definite.  Coarse MG levels are exact Galerkin products A_c = P^T A P with
+// piecewise-constant P over the liquid children, the same 2x2x2 aggregation
+// the reference's restriction uses (src/msbg4.cpp:1512-1914), on the block
+// hierarchy level(b, m) = max(map(b), m) of the reference (src/msbg.cpp:1650).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <tuple>
+
+#include "pressure.h"
+
+namespace msbg {
+namespace ps {
+namespace {
+
+constexpr uint16_t CELL_NONFLUID = 0x1 | 0x2 | 0x1000;  // SOLID | FIXED | VOID
+
+int pow2_divisor(int v, int cap) {
+  int p = 1;
+  while (p < cap && v % (p * 2) == 0) p *= 2;
+  return p;
+}
+
+struct Ctx {
+  Hierarchy& H;
+  const msbg_pressure_callbacks* cb;
+  int maxMap = 0;
+  explicit Ctx(Hierarchy& h) : H(h) {}
+
+  // level of the fine-voxel region (fx,fy,fz) at MG level m
+  int level_at(int m, int fx, int fy, int fz) const {
+    int b = (fx / H.bsx0) + H.nb1x * ((fy / H.bsx0) + H.nb1y * (fz / H.bsx0));
+    return std::max(H.blockLevel[b], m);
+  }
+  bool inside(int fx, int fy, int fz) const {
+    return fx >= 0 && fy >= 0 && fz >= 0 && fx < H.sx && fy < H.sy && fz < H.sz;
+  }
+  bool uniform(int m) const { return m >= maxMap; }
+  int ts_of(int m, int l) const {
+    if (uniform(m))
+      return pow2_divisor(std::gcd(std::gcd(H.sx >> l, H.sy >> l), H.sz >> l), TS_MAX);
+    return std::min(TS_MAX, H.bsx0 >> l);
+  }
+};
+
+inline void face_axes(int dir, int& a, int& b) {
+  a = dir == 0 ? 1 : 0;
+  b = dir == 2 ? 1 : 2;
+}
+
+// Tile lookup at resolution level l of MG level m for level-l cell coords.
+inline int tile_at(const Level& L, int l, int X, int Y, int Z) {
+  if (l < 0 || l >= 32) return -1;
+  const int n = L.tmapN[l];
+  if (!n || X < 0 || Y < 0 || Z < 0) return -1;
+  const int ts = L.tsOf[l];
+  int tx = X / ts, ty = Y / ts, tz = Z / ts;
+  if (tx >= n || ty >= n || tz >= n) return -1;
+  return L.tmap[l][tx + (size_t)n * (ty + (size_t)n * tz)];
+}
+
+// Create the candidate tiles of MG level m (regions whose level equals the
+// tile's level); fluid filtering happens later.
+void enumerate_tiles(const Ctx& C, int m, Level& L, std::vector<Tile>& cand) {
+  const Hierarchy& H = C.H;
+  std::vector<int> present;
+  for (int l = m; l <= std::max(m, C.maxMap); l++) present.push_back(l);
+  for (int l : present) {
+    if ((H.sx >> l) << l != H.sx || (H.sy >> l) << l != H.sy || (H.sz >> l) << l != H.sz) continue;
+    const int ts = C.ts_of(m, l);
+    const int nx = (H.sx >> l) / ts, ny = (H.sy >> l) / ts, nz = (H.sz >> l) / ts;
+    if (nx <= 0 || ny <= 0 || nz <= 0) continue;
+    L.tsOf[l] = ts;
+    L.tmapN[l] = std::max({nx, ny, nz});
+    const int n = L.tmapN[l];
+    L.tmap[l].assign((size_t)n * n * n, -1);
+    for (int tz = 0; tz < nz; tz++)
+      for (int ty = 0; ty < ny; ty++)
+        for (int tx = 0; tx < nx; tx++) {
+          const int fx = (tx * ts) << l, fy = (ty * ts) << l, fz = (tz * ts) << l;
+          if (C.level_at(m, fx, fy, fz) != l) continue;
+          Tile t;
+          t.level = l;
+          t.ts = ts;
+          t.ox = tx * ts;
+          t.oy = ty * ts;
+          t.oz = tz * ts;
+          t.off = 0;
+          cand.push_back(t);
+        }
+  }
+}
+
+void register_tiles(Level& L, std::vector<Tile>& tiles) {
+  // order by (level, colour) so each smoothing pass is a contiguous range
+  std::stable_sort(tiles.begin(), tiles.end(), [&](const Tile& a, const Tile& b) {
+    if (a.level != b.level) return a.level < b.level;
+    int ca = ((a.ox / a.ts) + (a.oy / a.ts) + (a.oz / a.ts)) & 1;
+    int cb = ((b.ox / b.ts) + (b.oy / b.ts) + (b.oz / b.ts)) & 1;
+    return ca < cb;
+  });
+  int64_t off = 0;
+  for (auto& t : tiles) {
+    t.off = off;
+    off += (int64_t)t.ts * t.ts * t.ts;
+  }
+  L.tiles = tiles;
+  L.nCells = off;
+  for (size_t i = 0; i < tiles.size(); i++) {
+    const Tile& t = tiles[i];
+    const int n = L.tmapN[t.level];
+    L.tmap[t.level][(t.ox / t.ts) + (size_t)n * ((t.oy / t.ts) + (size_t)n * (t.oz / t.ts))] = (int)i;
+  }
+  // passes: (level, colour) ranges; groups: by tile size
+  L.passes.clear();
+  L.passTiles.resize(tiles.size());
+  for (size_t i = 0; i < tiles.size(); i++) L.passTiles[i] = (int)i;
+  for (size_t i = 0; i < tiles.size();) {
+    const Tile& t = tiles[i];
+    int col = ((t.ox / t.ts) + (t.oy / t.ts) + (t.oz / t.ts)) & 1;
+    size_t j = i;
+    while (j < tiles.size() && tiles[j].level == t.level &&
+           (((tiles[j].ox / tiles[j].ts) + (tiles[j].oy / tiles[j].ts) + (tiles[j].oz / tiles[j].ts)) & 1) == col)
+      j++;
+    L.passes.push_back({t.level, col, t.ts, (int)i, (int)(j - i)});
+    i = j;
+  }
+  L.groups.clear();
+  L.groupTiles.clear();
+  std::map<int, std::vector<int>> byTs;
+  for (size_t i = 0; i < tiles.size(); i++) byTs[tiles[i].ts].push_back((int)i);
+  for (auto& kv : byTs) {
+    L.groups.push_back({kv.first, (int)L.groupTiles.size(), (int)kv.second.size()});
+    L.groupTiles.insert(L.groupTiles.end(), kv.second.begin(), kv.second.end());
+  }
+}
+
+// Face descriptors and interface-plane offsets.
+void build_faces(const Ctx& C, Level& L) {
+  const int nT = (int)L.tiles.size();
+  L.face.assign((size_t)nT * 6 * FACE_INTS, 0);
+  L.ifOff.assign((size_t)nT * 6, -1);
+  int64_t nIf = 0;
+  for (int ti = 0; ti < nT; ti++) {
+    const Tile& t = L.tiles[ti];
+    const int l = t.level, ts = t.ts;
+    const int o[3] = {t.ox, t.oy, t.oz};
+    for (int dir = 0; dir < 3; dir++)
+      for (int side = 0; side < 2; side++) {
+        int* F = &L.face[((size_t)ti * 6 + dir * 2 + side) * FACE_INTS];
+        for (int k = 0; k < 4; k++) F[F_T0 + k] = -1;
+        F[F_KIND] = FACE_NONE;
+        // first fine voxel just outside the face
+        int cell[3] = {o[0], o[1], o[2]};
+        cell[dir] = side ? o[dir] + ts : o[dir] - 1;
+        int fv[3];
+        for (int k = 0; k < 3; k++) fv[k] = cell[k] << l;
+        if (side == 0) fv[dir] = (o[dir] << l) - 1;
+        if (!C.inside(fv[0], fv[1], fv[2])) continue;
+        const int l2 = C.level_at(L.m, fv[0], fv[1], fv[2]);
+        int ax, bx;
+        face_axes(dir, ax, bx);
+        if (l2 == l) {
+          int nb = tile_at(L, l, cell[0], cell[1], cell[2]);
+          if (nb < 0) continue;
+          F[F_KIND] = FACE_SAME;
+          F[F_T0] = nb;
+          F[F_NTS] = ts;
+        } else if (l2 == l + 1) {
+          int cc[3];
+          for (int k = 0; k < 3; k++) cc[k] = fv[k] >> (l + 1);
+          int nb = tile_at(L, l + 1, cc[0], cc[1], cc[2]);
+          // interface plane is needed for the coupling even if the coarse
+          // side holds no liquid (it is zero then; kept for uniformity)
+          L.ifOff[(size_t)ti * 6 + dir * 2 + side] = nIf;
+          nIf += (int64_t)ts * ts;
+          if (nb < 0) continue;
+          const Tile& tn = L.tiles[nb];
+          const int no[3] = {tn.ox, tn.oy, tn.oz};
+          F[F_KIND] = FACE_COARSER;
+          F[F_T0] = nb;
+          F[F_OA] = (o[ax] >> 1) - no[ax];
+          F[F_OB] = (o[bx] >> 1) - no[bx];
+          F[F_NTS] = tn.ts;
+        } else if (l2 == l - 1) {
+          // fine cells just outside, level l-1 coordinates
+          const int tsf = L.tsOf[l - 1];
+          const int cov = tsf / 2;  // our cells per fine tile along a/b
+          const int per = ts / cov;  // fine tiles per axis (1 or 2)
+          int fc[3];
+          fc[dir] = side ? (o[dir] + ts) * 2 : o[dir] * 2 - 1;
+          bool any = false;
+          for (int qb = 0; qb < per; qb++)
+            for (int qa = 0; qa < per; qa++) {
+              fc[ax] = (o[ax] + qa * cov) * 2;
+              fc[bx] = (o[bx] + qb * cov) * 2;
+              int nb = tile_at(L, l - 1, fc[0], fc[1], fc[2]);
+              F[F_T0 + qa + per * qb] = nb;
+              any |= nb >= 0;
+            }
+          if (!any) continue;
+          F[F_KIND] = FACE_FINER;
+          F[F_COV] = cov;
+          F[F_NTS] = tsf;
+        }
+      }
+  }
+  L.nIf = nIf;
+}
+
+// Fine-side coupling across a face of a level-l cell (h = 2^l) whose
+// neighbour region is coarser: (2/3) h beta, beta sampled on the shared face.
+inline double interface_coupling(const msbg_pressure_callbacks* cb, int l, int dir, int side,
+                                 int X, int Y, int Z) {
+  int c[3] = {X, Y, Z};
+  if (side) c[dir] += 1;
+  const double h = (double)(1 << l);
+  return (2.0 / 3.0) * h * cb->sampleFaceCoeff(cb->user, dir, c[0] << l, c[1] << l, c[2] << l);
+}
+
+// Level 0 operator from the callbacks.
+void sample_level0(const Ctx& C, Level& L, std::vector<uint8_t>& fluid) {
+  const msbg_pressure_callbacks* cb = C.cb;
+  const int nT = (int)L.tiles.size();
+  L.diag.assign(L.nCells, 0.f);
+  L.cx.assign(L.nCells, 0.f);
+  L.cy.assign(L.nCells, 0.f);
+  L.cz.assign(L.nCells, 0.f);
+  L.rhs.assign(L.nCells, 0.f);
+  L.ifc.assign(L.nIf, 0.f);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int ti = 0; ti < nT; ti++) {
+    const Tile& t = L.tiles[ti];
+    const int l = t.level, ts = t.ts;
+    const double h = (double)(1 << l);
+    float* cdir[3] = {&L.cx[t.off], &L.cy[t.off], &L.cz[t.off]};
+    for (int k = 0; k < ts; k++)
+      for (int j = 0; j < ts; j++)
+        for (int i = 0; i < ts; i++) {
+          const int64_t ci = i + (int64_t)ts * (j + (int64_t)ts * k);
+          const int X = t.ox + i, Y = t.oy + j, Z = t.oz + k;
+          const int p[3] = {X, Y, Z}, loc[3] = {i, j, k};
+          const bool isFluid = !fluid.empty() ? fluid[t.off + ci] : false;
+          double diag = 0;
+          for (int dir = 0; dir < 3; dir++)
+            for (int side = 0; side < 2; side++) {
+              // neighbour region level
+              int fv[3] = {p[0] << l, p[1] << l, p[2] << l};
+              fv[dir] = side ? (p[dir] + 1) << l : (p[dir] << l) - 1;
+              int q[3] = {p[0], p[1], p[2]};
+              if (side) q[dir] += 1;
+              double c;
+              if (!C.inside(fv[0], fv[1], fv[2])) {
+                c = h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
+                if (side == 0) cdir[dir][ci] = (float)c;
+              } else {
+                const int l2 = C.level_at(L.m, fv[0], fv[1], fv[2]);
+                if (l2 == l) {
+                  c = h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
+                  if (side == 0) cdir[dir][ci] = (float)c;
+                } else if (l2 == l + 1) {
+                  c = interface_coupling(cb, l, dir, side, X, Y, Z);
+                  const bool onFace = side ? loc[dir] == ts - 1 : loc[dir] == 0;
+                  if (onFace) {
+                    int64_t io = L.ifOff[(size_t)ti * 6 + dir * 2 + side];
+                    int ax, bx;
+                    face_axes(dir, ax, bx);
+                    if (io >= 0) L.ifc[io + loc[ax] + (int64_t)ts * loc[bx]] = (float)c;
+                  }
+                } else {
+                  // finer neighbours: 4 fine cells share this face
+                  int ax, bx;
+                  face_axes(dir, ax, bx);
+                  c = 0;
+                  for (int u = 0; u < 2; u++)
+                    for (int v = 0; v < 2; v++) {
+                      int f[3];
+                      f[dir] = side ? (p[dir] + 1) * 2 : p[dir] * 2 - 1;
+                      f[ax] = p[ax] * 2 + u;
+                      f[bx] = p[bx] * 2 + v;
+                      c += interface_coupling(cb, l - 1, dir, 1 - side, f[0], f[1], f[2]);
+                    }
+                }
+              }
+              diag += c;
+            }
+          if (isFluid) {
+            L.diag[t.off + ci] = (float)diag;
+            L.rhs[t.off + ci] =
+                (float)(cb->sampleRhs(cb->user, X << l, Y << l, Z << l) * h * h * h);
+          }
+        }
+  }
+}
+
+// Exact Galerkin coarsening: level m (fine) -> level m+1 (coarse).
+// fineFluid/coarseFluid: per-cell liquid flags.
+void galerkin(const Ctx& C, const Level& F, const std::vector<uint8_t>& fineFluid, Level& G,
+              const std::vector<uint8_t>& coarseFluid) {
+  const int nT = (int)G.tiles.size();
+  G.diag.assign(G.nCells, 0.f);
+  G.cx.assign(G.nCells, 0.f);
+  G.cy.assign(G.nCells, 0.f);
+  G.cz.assign(G.nCells, 0.f);
+  G.ifc.assign(G.nIf, 0.f);
+  // fine cell lookup: (level, cell coords) -> global fine cell index or -1
+  auto fine_cell = [&](int l, int X, int Y, int Z) -> int64_t {
+    int t = tile_at(F, l, X, Y, Z);
+    if (t < 0) return -1;
+    const Tile& ft = F.tiles[t];
+    return ft.off + (X - ft.ox) + (int64_t)ft.ts * ((Y - ft.oy) + (int64_t)ft.ts * (Z - ft.oz));
+  };
+  auto fine_fluid = [&](int64_t c) { return c >= 0 && fineFluid[c]; };
+  // coupling between fine cell c (level l, coords p) and its neighbour across
+  // face (dir, side), if both are liquid; 0 otherwise.
+  auto fine_pair = [&](int l, const int p[3], int dir, int side) -> double {
+    int64_t c0 = fine_cell(l, p[0], p[1], p[2]);
+    if (!fine_fluid(c0)) return 0;
+    int fv[3] = {p[0] << l, p[1] << l, p[2] << l};
+    fv[dir] = side ? (p[dir] + 1) << l : (p[dir] << l) - 1;
+    if (!C.inside(fv[0], fv[1], fv[2])) return 0;
+    const int l2 = C.level_at(F.m, fv[0], fv[1], fv[2]);
+    if (l2 == l) {
+      int q[3] = {p[0], p[1], p[2]};
+      q[dir] += side ? 1 : -1;
+      int64_t c1 = fine_cell(l, q[0], q[1], q[2]);
+      if (!fine_fluid(c1)) return 0;
+      const float* cd = dir == 0 ? F.cx.data() : dir == 1 ? F.cy.data() : F.cz.data();
+      return side ? cd[c1] : cd[c0];
+    }
+    if (l2 == l + 1) {
+      int cc[3];
+      for (int k = 0; k < 3; k++) cc[k] = fv[k] >> (l + 1);
+      int64_t c1 = fine_cell(l + 1, cc[0], cc[1], cc[2]);
+      if (!fine_fluid(c1)) return 0;
+      int t = tile_at(F, l, p[0], p[1], p[2]);
+      const Tile& ft = F.tiles[t];
+      int64_t io = F.ifOff[(size_t)t * 6 + dir * 2 + side];
+      int ax, bx;
+      face_axes(dir, ax, bx);
+      const int loc[3] = {p[0] - ft.ox, p[1] - ft.oy, p[2] - ft.oz};
+      return io >= 0 ? F.ifc[io + loc[ax] + (int64_t)ft.ts * loc[bx]] : 0.0;
+    }
+    // finer neighbour: sum over the 4 fine cells facing us
+    int ax, bx;
+    face_axes(dir, ax, bx);
+    double s = 0;
+    for (int u = 0; u < 2; u++)
+      for (int v = 0; v < 2; v++) {
+        int f[3];
+        f[dir] = side ? (p[dir] + 1) * 2 : p[dir] * 2 - 1;
+        f[ax] = p[ax] * 2 + u;
+        f[bx] = p[bx] * 2 + v;
+        int64_t c1 = fine_cell(l - 1, f[0], f[1], f[2]);
+        if (!fine_fluid(c1)) continue;
+        int t = tile_at(F, l - 1, f[0], f[1], f[2]);
+        const Tile& ft = F.tiles[t];
+        int64_t io = F.ifOff[(size_t)t * 6 + dir * 2 + (1 - side)];
+        const int loc[3] = {f[0] - ft.ox, f[1] - ft.oy, f[2] - ft.oz};
+        if (io >= 0) s += F.ifc[io + loc[ax] + (int64_t)ft.ts * loc[bx]];
+      }
+    return s;
+  };
+  // is the coarse cell (level lc, coords P) an aggregate of level lc-1 cells?
+  auto aggregated = [&](int lc, const int P[3]) {
+    int fv[3] = {P[0] << lc, P[1] << lc, P[2] << lc};
+    return C.level_at(F.m, fv[0], fv[1], fv[2]) == lc - 1;
+  };
+  // coupling between coarse cell P and its neighbour across (dir, side):
+  // sum of the fine liquid pairs across that coarse face.
+  auto coarse_face = [&](int lc, const int P[3], int dir, int side) -> double {
+    if (!aggregated(lc, P)) return fine_pair(lc, P, dir, side);
+    int ax, bx;
+    face_axes(dir, ax, bx);
+    double s = 0;
+    for (int u = 0; u < 2; u++)
+      for (int v = 0; v < 2; v++) {
+        int f[3];
+        f[dir] = P[dir] * 2 + side;
+        f[ax] = P[ax] * 2 + u;
+        f[bx] = P[bx] * 2 + v;
+        s += fine_pair(lc - 1, f, dir, side);
+      }
+    return s;
+  };
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int ti = 0; ti < nT; ti++) {
+    const Tile& t = G.tiles[ti];
+    const int lc = t.level, ts = t.ts;
+    float* cdir[3] = {&G.cx[t.off], &G.cy[t.off], &G.cz[t.off]};
+    for (int k = 0; k < ts; k++)
+      for (int j = 0; j < ts; j++)
+        for (int i = 0; i < ts; i++) {
+          const int64_t ci = i + (int64_t)ts * (j + (int64_t)ts * k);
+          const int P[3] = {t.ox + i, t.oy + j, t.oz + k};
+          const int loc[3] = {i, j, k};
+          if (!coarseFluid[t.off + ci]) continue;
+          // diagonal
+          double d = 0;
+          if (aggregated(lc, P)) {
+            for (int c = 0; c < 8; c++) {
+              int f[3] = {P[0] * 2 + (c & 1), P[1] * 2 + ((c >> 1) & 1), P[2] * 2 + (c >> 2)};
+              int64_t fc = fine_cell(lc - 1, f[0], f[1], f[2]);
+              if (!fine_fluid(fc)) continue;
+              d += F.diag[fc];
+              // internal pairs: count each once (the upper child of each pair)
+              for (int dir = 0; dir < 3; dir++) {
+                const int bit = dir == 0 ? (c & 1) : dir == 1 ? ((c >> 1) & 1) : (c >> 2);
+                if (bit) d -= 2.0 * fine_pair(lc - 1, f, dir, 0);
+              }
+            }
+          } else {
+            int64_t fc = fine_cell(lc, P[0], P[1], P[2]);
+            d = F.diag[fc];
+          }
+          G.diag[t.off + ci] = (float)d;
+          // couplings on the lower faces / interface planes
+          for (int dir = 0; dir < 3; dir++)
+            for (int side = 0; side < 2; side++) {
+              int fv[3] = {P[0] << lc, P[1] << lc, P[2] << lc};
+              fv[dir] = side ? (P[dir] + 1) << lc : (P[dir] << lc) - 1;
+              if (!C.inside(fv[0], fv[1], fv[2])) continue;
+              const int l2 = C.level_at(G.m, fv[0], fv[1], fv[2]);
+              if (l2 == lc && side == 0) {
+                cdir[dir][ci] = (float)coarse_face(lc, P, dir, side);
+              } else if (l2 == lc + 1) {
+                const bool onFace = side ? loc[dir] == ts - 1 : loc[dir] == 0;
+                int64_t io = G.ifOff[(size_t)ti * 6 + dir * 2 + side];
+                if (onFace && io >= 0) {
+                  int ax, bx;
+                  face_axes(dir, ax, bx);
+                  G.ifc[io + loc[ax] + (int64_t)ts * loc[bx]] = (float)coarse_face(lc, P, dir, side);
+                }
+              }
+            }
+        }
+  }
+}
+
+// Coarse tile of every fine tile: (coarse tile, offset x,y,z in coarse cells, aggregated).
+void build_restriction(const Ctx& C, Level& F, const Level& G) {
+  F.toCoarse.assign(F.tiles.size() * 6, -1);
+  for (size_t ti = 0; ti < F.tiles.size(); ti++) {
+    const Tile& t = F.tiles[ti];
+    const int fv[3] = {t.ox << t.level, t.oy << t.level, t.oz << t.level};
+    const int lc = C.level_at(G.m, fv[0], fv[1], fv[2]);
+    const bool agg = lc == t.level + 1;
+    const int sh = agg ? 1 : 0;
+    int P[3] = {t.ox >> sh, t.oy >> sh, t.oz >> sh};
+    int ct = tile_at(G, lc, P[0], P[1], P[2]);
+    int* r = &F.toCoarse[ti * 6];
+    r[0] = ct;
+    if (ct >= 0) {
+      const Tile& g = G.tiles[ct];
+      r[1] = P[0] - g.ox;
+      r[2] = P[1] - g.oy;
+      r[3] = P[2] - g.oz;
+    }
+    r[4] = agg ? 1 : 0;
+    r[5] = ct >= 0 ? G.tiles[ct].ts : 0;
+  }
+}
+
+// Cholesky of a dense SPD matrix (lower), then its inverse.  Returns false if
+// the matrix is not positive definite.
+bool dense_spd_inverse(std::vector<double>& A, int n, std::vector<double>& inv) {
+  std::vector<double> Lm(A);
+  for (int j = 0; j < n; j++) {
+    double s = Lm[(size_t)j * n + j];
+    for (int k = 0; k < j; k++) s -= Lm[(size_t)j * n + k] * Lm[(size_t)j * n + k];
+    if (!(s > 0)) return false;
+    const double d = std::sqrt(s);
+    Lm[(size_t)j * n + j] = d;
+    for (int i = j + 1; i < n; i++) {
+      double v = Lm[(size_t)i * n + j];
+      for (int k = 0; k < j; k++) v -= Lm[(size_t)i * n + k] * Lm[(size_t)j * n + k];
+      Lm[(size_t)i * n + j] = v / d;
+    }
+  }
+  inv.assign((size_t)n * n, 0.0);
+  std::vector<double> e(n), y(n);
+  for (int c = 0; c < n; c++) {
+    std::fill(e.begin(), e.end(), 0.0);
+    e[c] = 1;
+    for (int i = 0; i < n; i++) {
+      double v = e[i];
+      for (int k = 0; k < i; k++) v -= Lm[(size_t)i * n + k] * y[k];
+      y[i] = v / Lm[(size_t)i * n + i];
+    }
+    for (int i = n - 1; i >= 0; i--) {
+      double v = y[i];
+      for (int k = i + 1; k < n; k++) v -= Lm[(size_t)k * n + i] * inv[(size_t)k * n + c];
+      inv[(size_t)i * n + c] = v / Lm[(size_t)i * n + i];
+    }
+  }
+  return true;
+}
+
+}  // namespace
+
+int build_hierarchy(Hierarchy& H, int sx, int sy, int sz, int bsx0, int nLevels,
+                    const int* blockLevel, const msbg_pressure_callbacks* cb,
+                    int maxCoarseCells, std::string* err) {
+  H = Hierarchy();
+  H.sx = sx;
+  H.sy = sy;
+  H.sz = sz;
+  H.res = std::max({sx, sy, sz});
+  H.bsx0 = bsx0;
+  H.nLevels = nLevels;
+  H.nb1x = sx / bsx0;
+  H.nb1y = sy / bsx0;
+  H.nb1z = sz / bsx0;
+  const int64_t nb = (int64_t)H.nb1x * H.nb1y * H.nb1z;
+  H.blockLevel.assign(nb, 0);
+  if (blockLevel) std::copy(blockLevel, blockLevel + nb, H.blockLevel.begin());
+  Ctx C(H);
+  C.cb = cb;
+  for (int v : H.blockLevel) C.maxMap = std::max(C.maxMap, v);
+
+  // ---- MG level 0 ----
+  std::vector<uint8_t> fluid;
+  {
+    Level L;
+    L.m = 0;
+    std::vector<Tile> cand;
+    enumerate_tiles(C, 0, L, cand);
+    // keep tiles that hold liquid
+    std::vector<uint8_t> keep(cand.size(), 0);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t i = 0; i < (int64_t)cand.size(); i++) {
+      const Tile& t = cand[i];
+      bool any = false;
+      for (int k = 0; k < t.ts && !any; k++)
+        for (int j = 0; j < t.ts && !any; j++)
+          for (int ii = 0; ii < t.ts; ii++) {
+            uint16_t ct = cb->sampleCellType(cb->user, (t.ox + ii) << t.level,
+                                             (t.oy + j) << t.level, (t.oz + k) << t.level);
+            if (!(ct & CELL_NONFLUID)) {
+              any = true;
+              break;
+            }
+          }
+      keep[i] = any;
+    }
+    std::vector<Tile> tiles;
+    for (size_t i = 0; i < cand.size(); i++)
+      if (keep[i]) tiles.push_back(cand[i]);
+    register_tiles(L, tiles);
+    build_faces(C, L);
+    fluid.assign(L.nCells, 0);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t ti = 0; ti < (int64_t)L.tiles.size(); ti++) {
+      const Tile& t = L.tiles[ti];
+      for (int k = 0; k < t.ts; k++)
+        for (int j = 0; j < t.ts; j++)
+          for (int i = 0; i < t.ts; i++) {
+            uint16_t ct = cb->sampleCellType(cb->user, (t.ox + i) << t.level,
+                                             (t.oy + j) << t.level, (t.oz + k) << t.level);
+            fluid[t.off + i + (int64_t)t.ts * (j + (int64_t)t.ts * k)] = !(ct & CELL_NONFLUID);
+          }
+    }
+    sample_level0(C, L, fluid);
+    int64_t nf = 0;
+    for (auto f : fluid) nf += f;
+    L.nFluid = nf;
+    H.levels.push_back(std::move(L));
+  }
+  if (H.levels[0].nFluid == 0) {
+    if (err) *err = "no liquid cells";
+    return MSBG_EINVARG;
+  }
+
+  // ---- coarser MG levels (Galerkin) ----
+  std::vector<uint8_t> fineFluid = fluid;
+  for (int m = 1;; m++) {
+    Level& F = H.levels.back();
+    if (F.nFluid <= maxCoarseCells) break;
+    // can we coarsen once more?
+    const int lmin = m;  // finest level present at MG level m
+    if ((sx >> lmin) << lmin != sx || (sy >> lmin) << lmin != sy || (sz >> lmin) << lmin != sz ||
+        (sx >> lmin) < 1 || (sy >> lmin) < 1 || (sz >> lmin) < 1) {
+      if (err) *err = "grid cannot be coarsened to the direct-solve size";
+      return MSBG_EINVARG;
+    }
+    Level G;
+    G.m = m;
+    std::vector<Tile> cand;
+    enumerate_tiles(C, m, G, cand);
+    // coarse liquid flags: any liquid child (aggregates) or same cell
+    auto fine_cell = [&](int l, int X, int Y, int Z) -> int64_t {
+      int t = tile_at(F, l, X, Y, Z);
+      if (t < 0) return -1;
+      const Tile& ft = F.tiles[t];
+      return ft.off + (X - ft.ox) + (int64_t)ft.ts * ((Y - ft.oy) + (int64_t)ft.ts * (Z - ft.oz));
+    };
+    std::vector<std::vector<uint8_t>> candFluid(cand.size());
+    std::vector<uint8_t> keep(cand.size(), 0);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t i = 0; i < (int64_t)cand.size(); i++) {
+      const Tile& t = cand[i];
+      auto& cf = candFluid[i];
+      cf.assign((size_t)t.ts * t.ts * t.ts, 0);
+      bool any = false;
+      for (int k = 0; k < t.ts; k++)
+        for (int j = 0; j < t.ts; j++)
+          for (int ii = 0; ii < t.ts; ii++) {
+            const int P[3] = {t.ox + ii, t.oy + j, t.oz + k};
+            const int fv[3] = {P[0] << t.level, P[1] << t.level, P[2] << t.level};
+            bool f = false;
+            if (C.level_at(F.m, fv[0], fv[1], fv[2]) == t.level - 1) {
+              for (int c = 0; c < 8 && !f; c++) {
+                int64_t fc = fine_cell(t.level - 1, P[0] * 2 + (c & 1), P[1] * 2 + ((c >> 1) & 1),
+                                       P[2] * 2 + (c >> 2));
+                f = fc >= 0 && fineFluid[fc];
+              }
+            } else {
+              int64_t fc = fine_cell(t.level, P[0], P[1], P[2]);
+              f = fc >= 0 && fineFluid[fc];
+            }
+            cf[ii + (size_t)t.ts * (j + (size_t)t.ts * k)] = f;
+            any |= f;
+          }
+      keep[i] = any;
+    }
+    std::vector<Tile> tiles;
+    std::vector<int> order;
+    for (size_t i = 0; i < cand.size(); i++)
+      if (keep[i]) {
+        tiles.push_back(cand[i]);
+        order.push_back((int)i);
+      }
+    // register_tiles sorts; recover each tile's fluid flags by origin
+    std::map<std::tuple<int, int, int, int>, int> byOrigin;
+    for (size_t i = 0; i < tiles.size(); i++)
+      byOrigin[{tiles[i].level, tiles[i].ox, tiles[i].oy, tiles[i].oz}] = order[i];
+    register_tiles(G, tiles);
+    build_faces(C, G);
+    std::vector<uint8_t> coarseFluid(G.nCells, 0);
+    int64_t nf = 0;
+    for (const Tile& t : G.tiles) {
+      const auto& cf = candFluid[byOrigin[{t.level, t.ox, t.oy, t.oz}]];
+      std::copy(cf.begin(), cf.end(), coarseFluid.begin() + t.off);
+      for (auto f : cf) nf += f;
+    }
+    G.nFluid = nf;
+    galerkin(C, F, fineFluid, G, coarseFluid);
+    build_restriction(C, F, G);
+    H.levels.push_back(std::move(G));
+    fineFluid.swap(coarseFluid);
+    if (m > 24) {
+      if (err) *err = "too many multigrid levels";
+      return MSBG_EINTERNAL;
+    }
+  }
+
+  // ---- coarsest: dense FP64 inverse over the liquid cells ----
+  {
+    const Level& L = H.levels.back();
+    std::vector<int64_t> cells;
+    std::vector<int> idx(L.nCells, -1);
+    for (int64_t c = 0; c < L.nCells; c++)
+      if (fineFluid[c]) {
+        idx[c] = (int)cells.size();
+        cells.push_back(c);
+      }
+    const int n = (int)cells.size();
+    std::vector<double> A((size_t)n * n, 0.0);
+    for (int r = 0; r < n; r++) A[(size_t)r * n + r] = L.diag[cells[r]];
+    // off-diagonals: same-level lower faces and interface planes
+    for (size_t ti = 0; ti < L.tiles.size(); ti++) {
+      const Tile& t = L.tiles[ti];
+      const int ts = t.ts;
+      for (int k = 0; k < ts; k++)
+        for (int j = 0; j < ts; j++)
+          for (int i = 0; i < ts; i++) {
+            const int64_t c = t.off + i + (int64_t)ts * (j + (int64_t)ts * k);
+            if (idx[c] < 0) continue;
+            const int P[3] = {t.ox + i, t.oy + j, t.oz + k};
+            const float* cd[3] = {L.cx.data(), L.cy.data(), L.cz.data()};
+            for (int dir = 0; dir < 3; dir++) {
+              int q[3] = {P[0], P[1], P[2]};
+              q[dir] -= 1;
+              int nt = q[dir] >= 0 ? tile_at(L, t.level, q[0], q[1], q[2]) : -1;
+              if (nt < 0) continue;
+              const Tile& u = L.tiles[nt];
+              int64_t c2 = u.off + (q[0] - u.ox) + (int64_t)u.ts * ((q[1] - u.oy) + (int64_t)u.ts * (q[2] - u.oz));
+              if (idx[c2] < 0) continue;
+              const double w = cd[dir][c];
+              A[(size_t)idx[c] * n + idx[c2]] -= w;
+              A[(size_t)idx[c2] * n + idx[c]] -= w;
+            }
+            // interface couplings (this cell on the finer side)
+            for (int dir = 0; dir < 3; dir++)
+              for (int side = 0; side < 2; side++) {
+                int64_t io = L.ifOff[ti * 6 + dir * 2 + side];
+                const int loc[3] = {i, j, k};
+                if (io < 0 || (side ? loc[dir] != ts - 1 : loc[dir] != 0)) continue;
+                int fv[3] = {P[0] << t.level, P[1] << t.level, P[2] << t.level};
+                fv[dir] = side ? (P[dir] + 1) << t.level : (P[dir] << t.level) - 1;
+                int cc[3];
+                for (int kk = 0; kk < 3; kk++) cc[kk] = fv[kk] >> (t.level + 1);
+                int nt = tile_at(L, t.level + 1, cc[0], cc[1], cc[2]);
+                if (nt < 0) continue;
+                const Tile& u = L.tiles[nt];
+                int64_t c2 = u.off + (cc[0] - u.ox) + (int64_t)u.ts * ((cc[1] - u.oy) + (int64_t)u.ts * (cc[2] - u.oz));
+                if (idx[c2] < 0) continue;
+                int ax, bx;
+                face_axes(dir, ax, bx);
+                const double w = L.ifc[io + loc[ax] + (int64_t)ts * loc[bx]];
+                A[(size_t)idx[c] * n + idx[c2]] -= w;
+                A[(size_t)idx[c2] * n + idx[c]] -= w;
+              }
+          }
+    }
+    if (!dense_spd_inverse(A, n, H.coarseInv)) {
+      if (err) *err = "coarsest operator is not positive definite";
+      return MSBG_EMATH;
+    }
+    H.nCoarse = n;
+    H.coarseCells = cells;
+  }
+  return MSBG_OK;
+}
+
+}  // namespace ps
+}  // namespace msbg

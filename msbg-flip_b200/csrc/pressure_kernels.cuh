@@ -1,0 +1,87 @@
+// Device kernels of the MGPCG pressure solver (tile-based, sm_100a).
+//
+// Data of one MG level: tiles of TS^3 cells stored back to back (cell index
+// i + TS*(j + TS*k) inside a tile); operator diag (a_ii), cx/cy/cz (coupling
+// to the same-level -x/-y/-z neighbour), ifc (interface couplings on the finer
+// side of a level jump, one per fine boundary cell).  One CTA per tile, thread
+// (i,j) owns the z column of the tile.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pressure.h"
+
+namespace msbg {
+namespace ps {
+
+struct LevelView {
+  const int64_t* tileOff;
+  const int* face;
+  const int64_t* ifOff;
+  const int* toCoarse;
+  const float* diag;
+  const float* cx;
+  const float* cy;
+  const float* cz;
+  const float* ifc;
+};
+
+__host__ __device__ __forceinline__ int tidx(int ts, int i, int j, int k) { return i + ts * (j + ts * k); }
+
+// Cell of a tile addressed by its face plane: position along dir = p, face
+// coordinates (a,b).
+__host__ __device__ __forceinline__ int plane_idx(int ts, int dir, int p, int a, int b) {
+  return dir == 0 ? tidx(ts, p, a, b) : dir == 1 ? tidx(ts, a, p, b) : tidx(ts, a, b, p);
+}
+
+// Sum over the neighbours across face (dir, side) of face cell (a,b) of tile
+// ti: coupling * x(neighbour).  x = vector of this level.
+template <typename XT>
+__host__ __device__ __forceinline__ float ghost_sum(const LevelView& L, const XT* __restrict__ x, int ti,
+                                           int ts, int dir, int side, int a, int b) {
+  const int* F = L.face + ((size_t)ti * 6 + dir * 2 + side) * FACE_INTS;
+  const int kind = F[F_KIND];
+  if (kind == FACE_NONE) return 0.f;
+  const float* cd = dir == 0 ? L.cx : dir == 1 ? L.cy : L.cz;
+  if (kind == FACE_SAME) {
+    const int nb = F[F_T0];
+    const int64_t no = L.tileOff[nb];
+    const int pn = side ? 0 : ts - 1;
+    const float xn = (float)x[no + plane_idx(ts, dir, pn, a, b)];
+    const float c = side ? cd[no + plane_idx(ts, dir, 0, a, b)]
+                         : cd[L.tileOff[ti] + plane_idx(ts, dir, 0, a, b)];
+    return c * xn;
+  }
+  if (kind == FACE_COARSER) {
+    const int nb = F[F_T0], nts = F[F_NTS];
+    const int64_t no = L.tileOff[nb];
+    const int pn = side ? 0 : nts - 1;
+    const float xn = (float)x[no + plane_idx(nts, dir, pn, F[F_OA] + (a >> 1), F[F_OB] + (b >> 1))];
+    const float c = L.ifc[L.ifOff[(size_t)ti * 6 + dir * 2 + side] + a + ts * b];
+    return c * xn;
+  }
+  // FACE_FINER
+  const int cov = F[F_COV], nts = F[F_NTS];
+  const int per = ts / cov;
+  const int nb = F[F_T0 + (a / cov) + per * (b / cov)];
+  if (nb < 0) return 0.f;
+  const int64_t no = L.tileOff[nb];
+  const int64_t io = L.ifOff[(size_t)nb * 6 + dir * 2 + (1 - side)];
+  if (io < 0) return 0.f;
+  const int pn = side ? 0 : nts - 1;
+  const int fa0 = 2 * (a % cov), fb0 = 2 * (b % cov);
+  float s = 0.f;
+#pragma unroll
+  for (int v = 0; v < 2; v++)
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int fa = fa0 + u, fb = fb0 + v;
+      s += L.ifc[io + fa + nts * fb] * (float)x[no + plane_idx(nts, dir, pn, fa, fb)];
+    }
+  return s;
+}
+
+}  // namespace ps
+}  // namespace msbg

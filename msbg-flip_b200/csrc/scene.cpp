@@ -162,3 +162,165 @@ extern "C" int msbg_scene_sphere_sdf(int res, int bsx, int nSpheres, float rmin,
   }
   return MSBG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Free-surface pressure problem (see include/msbg_scene.h).
+// ---------------------------------------------------------------------------
+struct msbg_pressure_scene {
+  int res, bsx0, nLevels;
+  float zLiquid, band;
+  std::vector<Sphere> spheres;
+  struct Box { double lo[3], hi[3]; };
+  std::vector<Box> boxes;
+  struct Mode { int k[3]; double a[3], phi; double coef; };  // div = coef*cos(theta)
+  std::vector<Mode> modes;
+  std::vector<int> levels;
+
+  double liquid_sdf(double x, double y, double z) const {
+    double d = z - zLiquid * res;
+    for (const auto& s : spheres) {
+      double dx = x - s.cx, dy = y - s.cy, dz = z - s.cz;
+      d = std::min(d, std::sqrt(dx * dx + dy * dy + dz * dz) - s.r);
+    }
+    return d;
+  }
+  bool solid(int x, int y, int z) const {
+    const double p[3] = {x + 0.5, y + 0.5, z + 0.5};
+    for (const auto& b : boxes)
+      if (p[0] >= b.lo[0] && p[0] < b.hi[0] && p[1] >= b.lo[1] && p[1] < b.hi[1] &&
+          p[2] >= b.lo[2] && p[2] < b.hi[2])
+        return true;
+    return false;
+  }
+  bool inside(int x, int y, int z) const {
+    return x >= 0 && y >= 0 && z >= 0 && x < res && y < res && z < res;
+  }
+  uint16_t cell_type(int x, int y, int z) const {
+    if (!inside(x, y, z) || solid(x, y, z)) return 1;  // CELL_SOLID
+    return liquid_sdf(x + 0.5, y + 0.5, z + 0.5) < 0 ? 0 : 0x1000;  // CELL_VOID
+  }
+  float face(int dir, int x, int y, int z) const {
+    int xm = x - (dir == 0), ym = y - (dir == 1), zm = z - (dir == 2);
+    if (!inside(x, y, z) || !inside(xm, ym, zm)) return 0.f;
+    if (solid(x, y, z) || solid(xm, ym, zm)) return 0.f;
+    return 1.f;
+  }
+  float rhs(int x, int y, int z) const {
+    if (cell_type(x, y, z) != 0) return 0.f;
+    const double w = 2.0 * M_PI / res;
+    double s = 0;
+    for (const auto& m : modes)
+      s += m.coef * std::cos(w * (m.k[0] * (x + 0.5) + m.k[1] * (y + 0.5) + m.k[2] * (z + 0.5)) + m.phi);
+    return (float)s;
+  }
+};
+
+extern "C" msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, int nLevels,
+                                                           float zLiquid, int nSpheres,
+                                                           float rMin, float rMax, int nCuboids,
+                                                           int nModes, int kMax, float band,
+                                                           uint64_t seed) {
+  if (res <= 0 || bsx0 <= 0 || res % bsx0 || nLevels < 1 || nLevels > 4) return nullptr;
+  auto* s = new msbg_pressure_scene();
+  s->res = res;
+  s->bsx0 = bsx0;
+  s->nLevels = nLevels;
+  s->zLiquid = zLiquid;
+  s->band = band;
+  SplitMix64 rng(seed);
+  for (int i = 0; i < nSpheres; i++) {
+    Sphere sp;
+    sp.cx = rng.uniform() * res;
+    sp.cy = rng.uniform() * res;
+    sp.cz = rng.uniform() * res;
+    sp.r = (rMin + rng.uniform() * (rMax - rMin)) * res;
+    s->spheres.push_back(sp);
+  }
+  for (int i = 0; i < nCuboids; i++) {
+    msbg_pressure_scene::Box b;
+    for (int k = 0; k < 3; k++) {
+      double side = (0.05 + 0.10 * rng.uniform()) * res;
+      double c = rng.uniform() * res;
+      b.lo[k] = c - side / 2;
+      b.hi[k] = c + side / 2;
+    }
+    s->boxes.push_back(b);
+  }
+  // Box-Muller normals for the amplitudes.
+  auto normal = [&]() {
+    double u1 = std::max(rng.uniform(), 1e-300), u2 = rng.uniform();
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(2 * M_PI * u2);
+  };
+  for (int i = 0; i < nModes; i++) {
+    msbg_pressure_scene::Mode m;
+    do {
+      for (int k = 0; k < 3; k++) m.k[k] = (int)(rng.uniform() * (2 * kMax + 1)) - kMax;
+    } while (std::max({std::abs(m.k[0]), std::abs(m.k[1]), std::abs(m.k[2])}) < 1);
+    for (int k = 0; k < 3; k++) m.a[k] = normal();
+    m.phi = rng.uniform() * 2 * M_PI;
+    // Discrete MAC divergence of a_d sin(w k.x + phi) sampled on faces:
+    // sum_d a_d [sin(theta + pi k_d/res) - sin(theta - pi k_d/res)]
+    //   = 2 cos(theta) sum_d a_d sin(pi k_d / res).
+    double c = 0;
+    for (int k = 0; k < 3; k++) c += m.a[k] * std::sin(M_PI * m.k[k] / res);
+    m.coef = 2 * c;
+    s->modes.push_back(m);
+  }
+  // Refinement map.
+  const int nb1 = res / bsx0;
+  const int64_t nb = (int64_t)nb1 * nb1 * nb1;
+  s->levels.assign(nb, nLevels - 1);
+  const double halfDiag = bsx0 * std::sqrt(3.0) / 2;
+#pragma omp parallel for schedule(static)
+  for (int64_t b = 0; b < nb; b++) {
+    int bx = (int)(b % nb1), by = (int)((b / nb1) % nb1), bz = (int)(b / ((int64_t)nb1 * nb1));
+    double d = std::fabs(s->liquid_sdf((bx + 0.5) * bsx0, (by + 0.5) * bsx0, (bz + 0.5) * bsx0));
+    int l = nLevels - 1;
+    double w = band;
+    for (int k = 0; k < nLevels - 1; k++) {
+      if (d <= w + halfDiag) { l = k; break; }
+      w += band * (2 << k);
+    }
+    s->levels[b] = l;
+  }
+  // 2:1 grading over the 26-neighbourhood (src/msbg.cpp:1202-1423 enforces the same).
+  for (bool changed = true; changed;) {
+    changed = false;
+    std::vector<int> nl = s->levels;
+    for (int64_t b = 0; b < nb; b++) {
+      int bx = (int)(b % nb1), by = (int)((b / nb1) % nb1), bz = (int)(b / ((int64_t)nb1 * nb1));
+      int lm = s->levels[b];
+      for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+          for (int dx = -1; dx <= 1; dx++) {
+            int x = bx + dx, y = by + dy, z = bz + dz;
+            if (x < 0 || y < 0 || z < 0 || x >= nb1 || y >= nb1 || z >= nb1) continue;
+            lm = std::min(lm, s->levels[x + (int64_t)nb1 * (y + (int64_t)nb1 * z)] + 1);
+          }
+      if (lm < nl[b]) {
+        nl[b] = lm;
+        changed = true;
+      }
+    }
+    s->levels.swap(nl);
+  }
+  return s;
+}
+
+extern "C" void msbg_scene_pressure_destroy(msbg_pressure_scene* s) { delete s; }
+
+extern "C" int msbg_scene_pressure_block_levels(const msbg_pressure_scene* s, int* levels) {
+  if (!s || !levels) return MSBG_EINVARG;
+  std::memcpy(levels, s->levels.data(), sizeof(int) * s->levels.size());
+  return MSBG_OK;
+}
+
+extern "C" uint16_t msbg_scene_cell_type(void* p, int x, int y, int z) {
+  return static_cast<msbg_pressure_scene*>(p)->cell_type(x, y, z);
+}
+extern "C" float msbg_scene_face_coeff(void* p, int dir, int x, int y, int z) {
+  return static_cast<msbg_pressure_scene*>(p)->face(dir, x, y, z);
+}
+extern "C" float msbg_scene_rhs(void* p, int x, int y, int z) {
+  return static_cast<msbg_pressure_scene*>(p)->rhs(x, y, z);
+}

@@ -184,3 +184,128 @@ class Context:
                                              num_iter, dt, int(bool(clamp01))), "pde_mcf")
         if sync:
             self.sync()
+
+
+# ---------------------------------------------------------------------------
+# FLIP pressure solve
+# ---------------------------------------------------------------------------
+CELL_TYPE_FN = C.CFUNCTYPE(C.c_uint16, C.c_void_p, C.c_int, C.c_int, C.c_int)
+FACE_FN = C.CFUNCTYPE(C.c_float, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int)
+RHS_FN = C.CFUNCTYPE(C.c_float, C.c_void_p, C.c_int, C.c_int, C.c_int)
+
+
+class PressureCallbacks(C.Structure):
+    _fields_ = [("sampleCellType", C.c_void_p), ("sampleFaceCoeff", C.c_void_p),
+                ("sampleRhs", C.c_void_p), ("user", C.c_void_p)]
+
+
+class SolveParams(C.Structure):
+    _fields_ = [("nPre", C.c_int), ("nPost", C.c_int), ("nCoarse", C.c_int),
+                ("maxIter", C.c_int), ("tol", C.c_float), ("innerIter", C.c_int),
+                ("storage", C.c_int), ("maxRefine", C.c_int), ("useGraph", C.c_int)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("status", C.c_int),
+                ("relResidual", C.c_double), ("solveSeconds", C.c_double),
+                ("fineCells", C.c_int64), ("nMgLevels", C.c_int)]
+
+
+def _pressure_sigs(L):
+    vp, i32 = C.c_void_p, C.c_int
+    sig = {
+        "msbg_scene_pressure_create": (vp, [i32, i32, i32, C.c_float, i32, C.c_float, C.c_float,
+                                            i32, i32, i32, C.c_float, C.c_uint64]),
+        "msbg_scene_pressure_destroy": (None, [vp]),
+        "msbg_scene_pressure_block_levels": (i32, [vp, C.POINTER(C.c_int)]),
+        "msbg_gpu_solve_params_default": (None, [C.POINTER(SolveParams)]),
+        "msbg_gpu_pressure_prepare": (i32, [vp, C.POINTER(TopoDesc), C.POINTER(PressureCallbacks)]),
+        "msbg_gpu_pressure_solve": (i32, [vp, C.POINTER(SolveParams), C.POINTER(SolveInfo)]),
+        "msbg_gpu_pressure_download": (i32, [vp, C.POINTER(C.c_float), C.c_int64]),
+        "msbg_gpu_pressure_download_rhs": (i32, [vp, C.POINTER(C.c_float), C.c_int64]),
+        "msbg_gpu_pressure_packed_size": (i32, [vp, C.POINTER(C.c_int64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+class PressureScene:
+    """Seeded free-surface pressure problem (include/msbg_scene.h)."""
+
+    def __init__(self, res, bsx0, n_levels, z_liquid=0.4, n_spheres=32, r_min=0.03, r_max=0.1,
+                 n_cuboids=8, n_modes=16, k_max=8, band=64.0, seed=2024):
+        L = lib()
+        _pressure_sigs(L)
+        self._L = L
+        self.res, self.bsx0, self.n_levels = res, bsx0, n_levels
+        self.h = L.msbg_scene_pressure_create(res, bsx0, n_levels, z_liquid, n_spheres, r_min,
+                                              r_max, n_cuboids, n_modes, k_max, band, seed)
+        if not self.h:
+            raise MsbgError(5, "scene")
+        nb = (res // bsx0) ** 3
+        self.block_levels = np.zeros(nb, np.int32)
+        L.msbg_scene_pressure_block_levels(self.h, _p(self.block_levels, C.c_int))
+
+    def callbacks(self):
+        L = self._L
+        return PressureCallbacks(C.cast(L.msbg_scene_cell_type, C.c_void_p).value,
+                                 C.cast(L.msbg_scene_face_coeff, C.c_void_p).value,
+                                 C.cast(L.msbg_scene_rhs, C.c_void_p).value, self.h)
+
+    def packed_size(self):
+        return int(sum((self.bsx0 >> int(l)) ** 3 for l in self.block_levels))
+
+    def close(self):
+        if self.h:
+            self._L.msbg_scene_pressure_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_params(**kw):
+    L = lib()
+    _pressure_sigs(L)
+    p = SolveParams()
+    L.msbg_gpu_solve_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _ctx_pressure_prepare(self, scene):
+    _pressure_sigs(self._L)
+    self._bl_p = np.ascontiguousarray(scene.block_levels, np.int32)
+    d = TopoDesc(scene.res, scene.res, scene.res, scene.bsx0, scene.n_levels,
+                 _p(self._bl_p, C.c_int))
+    cb = scene.callbacks()
+    self._check(self._L.msbg_gpu_pressure_prepare(self._h, C.byref(d), C.byref(cb)),
+                "pressure_prepare")
+
+
+def _ctx_pressure_solve(self, params=None, **kw):
+    p = params or solve_params(**kw)
+    info = SolveInfo()
+    self._check(self._L.msbg_gpu_pressure_solve(self._h, C.byref(p), C.byref(info)),
+                "pressure_solve")
+    return info
+
+
+def _ctx_pressure_download(self, rhs=False):
+    n = C.c_int64()
+    self._check(self._L.msbg_gpu_pressure_packed_size(self._h, C.byref(n)), "packed_size")
+    out = np.zeros(n.value, np.float32)
+    fn = self._L.msbg_gpu_pressure_download_rhs if rhs else self._L.msbg_gpu_pressure_download
+    self._check(fn(self._h, _p(out, C.c_float), n.value), "pressure_download")
+    return out
+
+
+Context.pressure_prepare = _ctx_pressure_prepare
+Context.pressure_solve = _ctx_pressure_solve
+Context.pressure_download = _ctx_pressure_download

@@ -31,6 +31,31 @@ int oracle_mcf(int nbx, int nby, int nbz, int bsx, const int8_t* kind,
                float emptyVal, float fullVal, float* values, const int* update,
                int nUpdate, int numIter, float dt, int clamp01, int exactIter);
 
+/* FP64 reference solution of the FLIP pressure system on an adaptive block
+ * grid (the system the GPU MGPCG solves):
+ *   cells: every block b holds (bsx0>>L)^3 cells of edge h = 2^L, L = map[b];
+ *   cell type, face coefficient beta and rhs come from the callbacks at the
+ *   fine-voxel coordinates of the cell's lowest corner voxel;
+ *   coupling across a face: same level h*beta; level jump (2/3)*h_fine*beta
+ *   with beta of the fine cell's face (src/msbg.h:82-87, src/msbg3.cpp:59-161);
+ *   a_ii = sum of the face couplings of cell i (air / outside = p 0);
+ *   b_i = rhs * h^3.
+ * Solved with Jacobi-preconditioned CG in FP64 to |r| <= tol |b|.
+ * x, b: outputs in the reference block layout (blocks in bid order, each
+ * (bsx0>>L)^3 values, vid = x + y*bs + z*bs*bs).  Returns 0 on success. */
+typedef unsigned short (*oracle_cell_type_fn)(void*, int, int, int);
+typedef float (*oracle_face_fn)(void*, int, int, int, int);
+typedef float (*oracle_rhs_fn)(void*, int, int, int);
+int oracle_pressure_solve(int sx, int sy, int sz, int bsx0, const int* blockLevel,
+                          oracle_cell_type_fn cellType, oracle_face_fn face, oracle_rhs_fn rhs,
+                          void* user, double tol, int maxIter, double* x, double* b,
+                          int* itersOut, double* relResOut);
+
+/* y = A x for the same system (x, y in the block layout, FP64). */
+int oracle_pressure_apply(int sx, int sy, int sz, int bsx0, const int* blockLevel,
+                          oracle_cell_type_fn cellType, oracle_face_fn face, void* user,
+                          const double* x, double* y);
+
 #ifdef __cplusplus
 }
 #endif

@@ -106,3 +106,51 @@ def mcf_reference(res3, bsx, kind, values, update, num_iter, dt, clamp01=False, 
     if rc:
         raise RuntimeError(f"ref_mcf rc={rc}")
     return v, secs.value
+
+
+def pressure_oracle(scene, tol=1e-12, max_iter=20000):
+    """FP64 CG solution of the pressure system of a msbg_gpu.PressureScene.
+
+    Returns (x, b, iterations, true relative residual); x, b in the
+    reference block layout."""
+    L = oracle()
+    if not hasattr(L, "_ps_sig"):
+        L.oracle_pressure_solve.restype = C.c_int
+        L.oracle_pressure_solve.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int)] + [C.c_void_p] * 4 + [
+            C.c_double, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+            C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.oracle_pressure_apply.restype = C.c_int
+        L.oracle_pressure_apply.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int)] + [C.c_void_p] * 3 + [
+            C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L._ps_sig = True
+    n = scene.packed_size()
+    x = np.zeros(n, np.float64)
+    b = np.zeros(n, np.float64)
+    it = C.c_int()
+    rr = C.c_double()
+    cb = scene.callbacks()
+    bl = np.ascontiguousarray(scene.block_levels, np.int32)
+    rc = L.oracle_pressure_solve(scene.res, scene.res, scene.res, scene.bsx0, _p(bl, C.c_int),
+                                 cb.sampleCellType, cb.sampleFaceCoeff, cb.sampleRhs, cb.user,
+                                 tol, max_iter, _p(x, C.c_double), _p(b, C.c_double),
+                                 C.byref(it), C.byref(rr))
+    if rc:
+        raise RuntimeError(f"oracle_pressure_solve rc={rc}")
+    return x, b, it.value, rr.value
+
+
+def pressure_apply_oracle(scene, x):
+    L = oracle()
+    pressure_oracle  # signatures are set on first solve
+    if not hasattr(L, "_ps_sig"):
+        pressure_oracle(scene, tol=1.0, max_iter=0)
+    cb = scene.callbacks()
+    bl = np.ascontiguousarray(scene.block_levels, np.int32)
+    xx = np.ascontiguousarray(x, np.float64)
+    y = np.zeros_like(xx)
+    rc = L.oracle_pressure_apply(scene.res, scene.res, scene.res, scene.bsx0, _p(bl, C.c_int),
+                                 cb.sampleCellType, cb.sampleFaceCoeff, cb.user,
+                                 _p(xx, C.c_double), _p(y, C.c_double))
+    if rc:
+        raise RuntimeError(f"oracle_pressure_apply rc={rc}")
+    return y

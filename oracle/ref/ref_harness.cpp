@@ -14,6 +14,24 @@
 #include <cstring>
 #include <vector>
 
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <functional>
+#include <iostream>
+#include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <omp.h>
+#include "tbb/tbb.h"
+#include <vectorclass/vectorclass.h>
+// Test-only access to the solver internals the harness drives.
+#define private public
+#define protected public
 #include "common_headers.h"
 #include "msbg.h"
 #include "thread.h"
@@ -106,4 +124,192 @@ extern "C" int ref_mcf(int sx, int sy, int sz, int bsx, const int8_t* kind,
   }
   MultiresSparseGrid::destroy(msbg);
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// FLIP pressure solver (src/msbg3.cpp:2467-3271) driven from arrays.
+//
+// The callbacks sample dense fine-resolution arrays at the coordinates the
+// reference passes (it passes unscaled block-local coordinates for coarse
+// blocks, src/msbg3.cpp:2494-2503); out-of-range reads return CELL_SOLID / 0.
+// Channel data move in a packed layout: for every block id in ascending order,
+// the block's (bsx0>>level)^3 values at its level for the given MG level.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct PsArrays {
+  int sx, sy, sz;
+  const uint16_t* cellType;  // [sz][sy][sx]
+  const float* face;         // [3][sz][sy][sx]
+  const float* rhs;          // [sz][sy][sx]
+  bool in(int x, int y, int z) const {
+    return x >= 0 && y >= 0 && z >= 0 && x < sx && y < sy && z < sz;
+  }
+  size_t idx(int x, int y, int z) const { return (size_t)x + (size_t)sx * (y + (size_t)sy * z); }
+};
+
+CellFlags psCellType(void* u, int x, int y, int z) {
+  auto* a = (PsArrays*)u;
+  return a->in(x, y, z) ? (CellFlags)a->cellType[a->idx(x, y, z)] : (CellFlags)CELL_SOLID;
+}
+float psFace(void* u, int dir, int x, int y, int z) {
+  auto* a = (PsArrays*)u;
+  return a->in(x, y, z) ? a->face[(size_t)dir * a->sx * a->sy * a->sz + a->idx(x, y, z)] : 0.f;
+}
+float psRhs(void* u, int x, int y, int z) {
+  auto* a = (PsArrays*)u;
+  return a->in(x, y, z) ? a->rhs[a->idx(x, y, z)] : 0.f;
+}
+
+struct PsHandle {
+  MultiresSparseGrid* msbg;
+  PsArrays arr;
+};
+
+// Channel ids understood by ref_ps_get/set: the reference's channel ids, plus
+//   -1,-2,-3 = face coefficients dir 0,1,2 (CH_FACE_AREA), -10 = cell flags.
+SparseGrid<float>* ps_float_grid(MultiresSparseGrid* m, int ch, int level, int levelMg) {
+  if (ch <= -1 && ch >= -3) return m->getFaceAreaChannel(-ch - 1, level, levelMg);
+  if (ch == CH_DIAGONAL) return m->getPSFloatChannel(CH_DIAGONAL, level, levelMg);
+  return m->getFloatChannel(ch, level, levelMg);
+}
+
+}  // namespace
+
+extern "C" void* ref_ps_create(int sx, int sy, int sz, int bsx0, int nLevels,
+                               const int* blockLevel, const int* domBc,
+                               const uint16_t* cellType, const float* face,
+                               const float* rhs) {
+  MultiresSparseGrid* m = MultiresSparseGrid::create("PS", sx, sy, sz, bsx0, -1, 0, -1, 0,
+                                                     NULL, NULL, nLevels);
+  if (!m) return nullptr;
+  const int nb = m->nBlocks();
+  std::vector<int> levels(blockLevel, blockLevel + nb);
+  m->setRefinementMap(levels.data(), NULL, -1, NULL, false, true);
+  m->setDomainBoundarySpec_(domBc[0], domBc[1], domBc[2], domBc[3], domBc[4], domBc[5]);
+  auto* h = new PsHandle{m, {sx, sy, sz, cellType, face, rhs}};
+  FlipPressureCallbacks cb;
+  cb.sampleCellType = &psCellType;
+  cb.sampleFaceCoeff = &psFace;
+  cb.sampleRhs = &psRhs;
+  cb.user = &h->arr;
+  m->preparePressureSolveFLIP(cb);
+  return h;
+}
+
+extern "C" void ref_ps_destroy(void* hp) {
+  auto* h = (PsHandle*)hp;
+  MultiresSparseGrid::destroy(h->msbg);
+  delete h;
+}
+
+extern "C" float ref_ps_omega(void* hp) { return ((PsHandle*)hp)->msbg->_mgSmOmega; }
+extern "C" int ref_ps_num_levels(void* hp) { return ((PsHandle*)hp)->msbg->getNumLevels(); }
+
+// Block level and flags per block at MG level levelMg.
+extern "C" int ref_ps_block_info(void* hp, int levelMg, int* level, int* flags) {
+  auto* m = ((PsHandle*)hp)->msbg;
+  for (int b = 0; b < m->nBlocks(); b++) {
+    BlockInfo* bi = m->getBlockInfo(b, levelMg);
+    level[b] = bi ? bi->level : -1;
+    flags[b] = bi ? bi->flags : 0;
+  }
+  return 0;
+}
+
+// Packed size (number of values) of a channel at MG level levelMg.
+extern "C" long long ref_ps_packed_size(void* hp, int levelMg) {
+  auto* m = ((PsHandle*)hp)->msbg;
+  long long n = 0;
+  const int bsx0 = m->sg0()->bsx();
+  for (int b = 0; b < m->nBlocks(); b++) {
+    int l = m->getBlockInfo(b, levelMg)->level;
+    int bs = bsx0 >> l;
+    n += (long long)bs * bs * bs;
+  }
+  return n;
+}
+
+// Copy a channel out (get=1) or in (get=0).  Missing blocks read as 0 and
+// are skipped on write (written with allocation when alloc != 0).
+extern "C" int ref_ps_channel(void* hp, int ch, int levelMg, float* data, int get, int alloc) {
+  auto* m = ((PsHandle*)hp)->msbg;
+  const int bsx0 = m->sg0()->bsx();
+  size_t off = 0;
+  for (int b = 0; b < m->nBlocks(); b++) {
+    int l = m->getBlockInfo(b, levelMg)->level;
+    int bs = bsx0 >> l, nv = bs * bs * bs;
+    if (ch == -10) {
+      SparseGrid<CellFlags>* sg = m->getFlagsChannel(CH_CELL_FLAGS, l, levelMg);
+      CellFlags* d = sg ? sg->getBlockDataPtr(b) : nullptr;
+      for (int i = 0; i < nv; i++) {
+        if (get) data[off + i] = d ? (float)d[i] : -1.f;
+      }
+    } else {
+      SparseGrid<float>* sg = ps_float_grid(m, ch, l, levelMg);
+      float* d = sg ? sg->getBlockDataPtr(b, (!get && alloc) ? 1 : 0, 0) : nullptr;
+      if (get) {
+        for (int i = 0; i < nv; i++) data[off + i] = d ? d[i] : 0.f;
+      } else if (d) {
+        std::memcpy(d, data + off, sizeof(float) * nv);
+      }
+    }
+    off += nv;
+  }
+  return 0;
+}
+
+// q = A x (residual=0) or r = b - A x (residual=1) on MG level levelMg
+// (src/msbg3.cpp:1757-1912).
+extern "C" int ref_ps_multiply(void* hp, int levelMg, int chX, int chB, int chDst,
+                               int residual) {
+  auto* m = ((PsHandle*)hp)->msbg;
+  m->multiplyLaplacianMatrixOpt(residual ? OPT_CALC_RESIDUAL : 0, levelMg, chX,
+                                residual ? chB : CH_NULL, 0.0f, chDst, nullptr, nullptr);
+  return 0;
+}
+
+// nIter block red-black sweeps of the smoother on MG level levelMg
+// (src/msbg3.cpp:2245-2369).
+extern "C" int ref_ps_relax(void* hp, int levelMg, int chX, int chB, int chTmp, int nIter,
+                            int reverse) {
+  auto* m = ((PsHandle*)hp)->msbg;
+  m->relax(0, reverse, levelMg, chX, chB, chTmp, nIter, 0);
+  return 0;
+}
+
+extern "C" int ref_ps_downsample(void* hp, int levelMgCoarse, int chSrc, int chDst) {
+  auto* m = ((PsHandle*)hp)->msbg;
+  m->downsampleChannel<float, float>(levelMgCoarse, chSrc, chDst,
+                                     OPT_SIMPLE_AVERAGE | OPT_ALL_CELLS);
+  return 0;
+}
+
+extern "C" int ref_ps_prolongate(void* hp, int levelMgFine, int chSrc, int chDst) {
+  auto* m = ((PsHandle*)hp)->msbg;
+  m->prolongateChannel<float>(levelMgFine, chSrc, chDst, 0, MG_CONST_PROLONGATION_ALPHA);
+  return 0;
+}
+
+extern "C" int ref_ps_vcycle(void* hp, int chX, int chB, int chR, int chTmp, int nPre,
+                             int nPost, int nCoarse) {
+  auto* m = ((PsHandle*)hp)->msbg;
+  m->vCycle(0, chX, chB, chR, chTmp, nPre, nPost, nCoarse);
+  return 0;
+}
+
+extern "C" int ref_ps_solve(void* hp, int nPre, int nPost, int nCoarse, int maxIter, float tol,
+                            float* relRes, double* seconds) {
+  auto* m = ((PsHandle*)hp)->msbg;
+  FlipPressureSolveParams p;
+  p.nPre = nPre;
+  p.nPost = nPost;
+  p.nCoarse = nCoarse;
+  p.maxIter = maxIter;
+  p.tol = tol;
+  auto t0 = std::chrono::steady_clock::now();
+  int it = m->solvePressureFLIP(p, relRes);
+  auto t1 = std::chrono::steady_clock::now();
+  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+  return it;
 }
