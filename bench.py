@@ -1,22 +1,29 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 sparse block-grid solver.
+"""Benchmark of the B200 sparse block-grid PDE solver.
 
-Workload ``mcf`` (smoother at the 512^3 sphere-band configuration): one step =
-one MultiresSparseGrid::applyChannelPdeFast-equivalent call, i.e. 20
-iterations x 8 colour passes of the mean-curvature-flow smoother over every
-value block (512^3, 16^3 blocks, band +-4 around 64 seeded spheres,
-dt = 0.1), data resident in HBM.
+Default workload ``mgpcg`` — the FLIP pressure solve on a 2-level adaptive
+MSBG at 1024^3 effective resolution: 32^3 base blocks, level 0 within 64
+voxels of the liquid surface and 2x coarser elsewhere, liquid = half-space
+z < 0.4 plus 32 seeded spheres, 8 seeded solid cuboids, Dirichlet p = 0 in
+air, Neumann at walls and solids, RHS = MAC divergence of 16 random Fourier
+modes (|k|_inf 1..8, N(0,1) amplitudes).  One step = one plain FP32 MGPCG
+solve from p = 0 to relative residual 1e-6 (V(2,2) preconditioner) on the
+resident operator.  value = liquid cells x PCG iterations / solve time
+(Gvoxel/s per iteration); the time to 1e-6 is reported beside it.
 
-Prints one JSON line (rank 0).  ``--impl reference`` times the reference's own
-CPU implementation instead (compiled from the reference sources into
-oracle/_ref/libmsbg_ref.so) on the same configuration.
+Workload ``mcf``: the 8-colour mean-curvature-flow smoother at 512^3
+(16^3 blocks, band +-4 around 64 seeded spheres, 20 iterations, dt 0.1).
 
-Multi-GPU: the smoother runs as independent replicas, one per rank (no data
-path collective); value = all ranks' voxel updates / max-over-ranks time.
+``--impl reference`` times the reference's own CPU implementation (compiled
+from its sources into oracle/_ref/libmsbg_ref.so) with all host threads.
+
+Multi-GPU: independent replicas, one per rank (the solve does not shard in
+this build); value = all ranks' work / max-over-ranks time.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -31,6 +38,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "msbg-flip_b200"))
 
 METRIC = "MGPCG time-to-1e-6 & Gvoxel/s/iter: learned+mixed vs plain FP32, one B200"
+
+PS_CFG = dict(res=1024, bsx0=32, n_levels=2, z_liquid=0.4, n_spheres=32, r_min=0.03, r_max=0.1,
+              n_cuboids=8, n_modes=16, k_max=8, band=64.0, seed=2024, tol=1e-6, n_pre=2,
+              n_post=2, inner=2)
+# bounded analogue of the pressure workload the reference CPU solver can run:
+# it aborts for 32^3 base blocks (src/msbg3.cpp:1692-1749), so 16^3 blocks,
+# a quarter of the resolution and the band scaled alike.
+PS_REF_CFG = dict(res=256, bsx0=16, n_levels=2, band=16.0, iters=10)
 
 MCF_CFG = dict(res=512, bsx=16, n_spheres=64, rmin=20.0, rmax=60.0, band=4.0, dilate=1,
                seed=1234, iters=20, dt=0.1)
@@ -96,13 +111,13 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(mhz)}
 
 
-def read_traffic(name):
-    """Per-cell DRAM traffic of a kernel from its committed ncu summary."""
+def read_profile_value(name, key):
+    """A `key=value` line of a committed ncu summary under profiles/."""
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_cell="):
+        if line.startswith(key + "="):
             return float(line.split("=")[1])
     return None
 
@@ -114,6 +129,203 @@ def dist_env():
     return ws, rank, local
 
 
+def init_dist(ws):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def max_over_ranks(dist, v, dev):
+    if not dist:
+        return v
+    import torch
+    t = torch.tensor([v], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# pressure workload
+# ---------------------------------------------------------------------------
+def ps_scene(cfg):
+    import msbg_gpu
+    return msbg_gpu.PressureScene(cfg["res"], cfg["bsx0"], cfg["n_levels"], cfg["z_liquid"],
+                                  cfg["n_spheres"], cfg["r_min"], cfg["r_max"], cfg["n_cuboids"],
+                                  cfg["n_modes"], cfg["k_max"], cfg["band"], cfg["seed"])
+
+
+def ps_stats(ctx):
+    import msbg_gpu
+    L = msbg_gpu.lib()
+    st = msbg_gpu.PressureStats()
+    ctx._check(L.msbg_gpu_pressure_stats(ctx._h, C.byref(st)), "stats")
+    return st
+
+
+def cpu_reference_ps(max_seconds=60.0):
+    """Reference solvePressureFLIP (all host threads) on the bounded analogue."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    c = dict(PS_CFG)
+    c.update(PS_REF_CFG)
+    cores = os.cpu_count() or 1
+    if not oracle.ref_available():
+        return {"value": None, "unit": "Gvoxel/s/iter", "cores": cores, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/libmsbg_ref.so not built"}
+    import ref_pressure
+    oracle.ref().ref_init(cores)
+    scene = ps_scene(c)
+    r = ref_pressure.RefPressure(scene)
+    # liquid cells of the analogue (from our FP64 oracle's assembly of the same scene)
+    import msbg_gpu
+    nfl = msbg_gpu.count_liquid_cells(scene)
+    r.solve(max_iter=1)  # warm-up (allocations inside the first V-cycle)
+    times, iters = [], []
+    t0 = time.perf_counter()
+    while True:
+        it, rr, secs = r.solve(max_iter=c["iters"])
+        times.append(secs)
+        iters.append(it)
+        if time.perf_counter() - t0 > max_seconds * 0.5 or len(times) >= 3:
+            break
+    r.close()
+    rate = nfl * sum(iters) / sum(times) / 1e9
+    return {"value": rate, "unit": "Gvoxel/s/iter", "cores": cores, "kind": "reference",
+            "sample": (f"reference solvePressureFLIP (V(2,2)-PCG, src/msbg3.cpp:3098) on the "
+                       f"{c['res']}^3, {c['bsx0']}^3-block, 2-level analogue of the workload "
+                       f"(band {c['band']:.0f}), {c['iters']} iterations per call, "
+                       f"{len(times)} calls; {nfl} liquid cells; prepare {r.prep_seconds:.1f}s "
+                       f"not counted; its |r|/|b| after {c['iters']} its: {rr:.2e} "
+                       f"(it does not reach 1e-6)")}
+
+
+def bench_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    if args.workload == "mcf":
+        return bench_reference_mcf(args)
+    cb = cpu_reference_ps(max_seconds=120.0)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "Gvoxel/s/iter", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded free-surface pressure problem)", "impl": "reference",
+            "config": {"workload": "flip_pressure_mgpcg_analogue_256_b16_2lvl",
+                       "time_to_1e-6": "not reached (reference MGPCG stalls)",
+                       "parallelism": "cpu"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "Gvoxel/s/iter", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def bench_mgpcg(args):
+    import torch
+    import msbg_gpu
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = init_dist(ws)
+    dev = torch.device("cuda", local)
+    c = dict(PS_CFG)
+    if args.res:
+        c["res"] = args.res
+        c["band"] = PS_CFG["band"] * args.res / PS_CFG["res"]
+    ctx = msbg_gpu.Context(local)
+    scene = ps_scene(c)
+    ctx.pressure_prepare(scene)
+    st = ps_stats(ctx)
+    params = msbg_gpu.solve_params(nPre=c["n_pre"], nPost=c["n_post"], tol=c["tol"],
+                                   innerIter=c["inner"], useGraph=1)
+    for _ in range(args.warmup):
+        ctx.pressure_solve(params)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    infos = []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            infos.append(ctx.pressure_solve(params))
+        torch.cuda.synchronize()
+    clocks = clk.summary()
+    solve_s = sum(i.solveSeconds for i in infos)
+    solve_s = max_over_ranks(dist, solve_s, dev)
+    iters = [i.iterations for i in infos]
+    fluid = int(st.fluid[0])
+    ms_step = solve_s / args.steps * 1e3
+    rate = fluid * sum(iters) / solve_s / 1e9 * ws
+    if args.profile:
+        ctx.close()
+        return
+    # dominant kernel: the level-0 tile smoother, timed on its own (same stream)
+    hbm, _, pk_kind = peaks()
+    ms_sw, bytes_sw = ctx.pressure_profile(0, 20, c["inner"])
+    ms_vc, bytes_vc = ctx.pressure_profile(2, 5, c["inner"])
+    cells0 = int(st.cells[0])
+    dpc = read_profile_value("k_smooth_16_mgpcg_1024_b32.txt", "dram_bytes_per_cell")
+    launches_sweep = None
+    roof = {"bound": "hbm", "achieved": bytes_sw / (ms_sw * 1e-3) / 1e9, "peak": hbm,
+            "unit": "GB/s", "frac": bytes_sw / (ms_sw * 1e-3) / 1e9 / hbm, "peak_kind": pk_kind,
+            "traffic": dpc * cells0 if dpc else None, "alg_bytes_per_sweep": bytes_sw,
+            "kernel": "k_smooth<16> (one level-0 pre-smoothing sweep, 4 launches)",
+            "vcycle_achieved_gbs": bytes_vc / (ms_vc * 1e-3) / 1e9,
+            "vcycle_frac": bytes_vc / (ms_vc * 1e-3) / 1e9 / hbm}
+    del launches_sweep
+    # end to end through the C ABI: prepare from the host callbacks (host
+    # sampling + hierarchy + upload), solve, download the pressure
+    n_e2e = max(1, min(args.steps, 2))
+    t0 = time.perf_counter()
+    e2e_iters = 0
+    for _ in range(n_e2e):
+        ctx.pressure_prepare(scene)
+        inf = ctx.pressure_solve(params)
+        e2e_iters += inf.iterations
+        out = ctx.pressure_download()
+    e2e_s = (time.perf_counter() - t0) / n_e2e
+    e2e_s = max_over_ranks(dist, e2e_s, dev)
+    e2e_rate = fluid * (e2e_iters / n_e2e) / e2e_s / 1e9 * ws
+    st2 = ps_stats(ctx)
+    cb = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cb = cpu_reference_ps()
+    if rank == 0:
+        line = {"metric": METRIC, "value": rate, "unit": "Gvoxel/s/iter", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded free-surface pressure problem)",
+                "config": {"workload": f"flip_pressure_mgpcg_{c['res']}_b{c['bsx0']}_2lvl",
+                           "mode": "plain FP32 MGPCG (V(2,2), FP64 dots, FP64 coarsest solve)",
+                           "time_to_1e-6_ms": ms_step, "pcg_iterations": iters,
+                           "true_rel_residual": infos[-1].relResidual,
+                           "liquid_cells": fluid, "stored_cells_level0": cells0,
+                           "mg_levels": int(st.nMgLevels),
+                           "prepare_s": st.prepareSeconds, "host_build_s": st.buildSeconds,
+                           "l2": "inputs larger than L2 (%.1f GB operator+vectors)" %
+                                 (st.deviceBytesUsed / 1e9),
+                           "parallelism": f"replicas{ws}"},
+                "gpu_launches": None,
+                "roofline": roof, "clocks": clocks,
+                "e2e": {"value": e2e_rate, "unit": "Gvoxel/s/iter",
+                        "h2d_bytes_per_step": int(st2.h2dBytes),
+                        "d2h_bytes_per_step": int(out.nbytes),
+                        "seconds_per_step": e2e_s},
+                "cpu_baseline": cb}
+        launches = ctx.last_solve_launches()
+        line["gpu_launches"] = launches * args.steps if launches else None
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# mean-curvature-flow workload
+# ---------------------------------------------------------------------------
 def mcf_scene():
     import msbg_gpu
     c = MCF_CFG
@@ -124,56 +336,32 @@ def mcf_scene():
 
 
 def cpu_reference_mcf(kind, vals, upd, max_seconds=20.0):
-    """Time the compiled reference smoother (all host threads) on a bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     c = MCF_CFG
     cores = os.cpu_count() or 1
     nvox = len(upd) * c["bsx"] ** 3
-    if oracle.ref_available():
-        try:
-            oracle.ref()
-            kind_s = "reference"
-        except OSError:
-            kind_s = "port"
-    else:
-        kind_s = "port"
-    if kind_s == "reference":
-        oracle.ref().ref_init(cores)
-        # warm-up: 2 iterations
-        oracle.mcf_reference((c["res"],) * 3, c["bsx"], kind, vals, upd, 2, c["dt"])
-        times, it_done = [], 0
-        t_start = time.perf_counter()
-        while True:
-            _, secs = oracle.mcf_reference((c["res"],) * 3, c["bsx"], kind, vals, upd, 4, c["dt"])
-            times.append(secs)
-            it_done += 4
-            if time.perf_counter() - t_start > max_seconds * 0.5 or len(times) >= 5:
-                break
-        secs = statistics.median(times)
-        rate = nvox * 4 / secs / 1e9
-        sample = (f"reference applyChannelPdeFast<float> MCF 8-colour on the full 512^3 workload, "
-                  f"4 iterations per call, median of {len(times)} calls")
-    else:
-        t = time.perf_counter()
-        oracle.mcf_oracle((c["res"] // c["bsx"],) * 3, c["bsx"], kind, vals, upd, 2, c["dt"])
-        secs = time.perf_counter() - t
-        rate = nvox * 2 / secs / 1e9
-        sample = "C restatement (oracle) of the smoother, full 512^3 workload, 2 iterations"
-    return {"value": rate, "unit": "Gvoxel/s/iter", "cores": cores, "kind": kind_s,
-            "sample": sample}
+    oracle.ref().ref_init(cores)
+    oracle.mcf_reference((c["res"],) * 3, c["bsx"], kind, vals, upd, 2, c["dt"])
+    times = []
+    t_start = time.perf_counter()
+    while True:
+        _, secs = oracle.mcf_reference((c["res"],) * 3, c["bsx"], kind, vals, upd, 4, c["dt"])
+        times.append(secs)
+        if time.perf_counter() - t_start > max_seconds * 0.5 or len(times) >= 5:
+            break
+    secs = statistics.median(times)
+    return {"value": nvox * 4 / secs / 1e9, "unit": "Gvoxel/s/iter", "cores": cores,
+            "kind": "reference",
+            "sample": (f"reference applyChannelPdeFast<float> MCF 8-colour on the full 512^3 "
+                       f"workload, 4 iterations per call, median of {len(times)} calls")}
 
 
-def bench_reference(args):
-    ws, rank, _ = dist_env()
-    if rank != 0:
-        return
+def bench_reference_mcf(args):
     kind, vals, upd = mcf_scene()
     cb = cpu_reference_mcf(kind, vals, upd, max_seconds=60.0)
     c = MCF_CFG
     nvox = len(upd) * c["bsx"] ** 3
-    # steps: each a full 20-iteration call would take minutes on few cores;
-    # the per-iteration rate is the metric, measured over 4-iteration calls.
     line = {"metric": METRIC, "value": cb["value"], "unit": "Gvoxel/s/iter", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": nvox * c["iters"] / (cb["value"] * 1e9) * 1e3,
@@ -192,32 +380,24 @@ def bench_mcf(args):
     import msbg_gpu
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dist = init_dist(ws)
+    dev = torch.device("cuda", local)
     c = MCF_CFG
     kind, vals, upd = mcf_scene()
     nb1 = c["res"] // c["bsx"]
     nvox = len(upd) * c["bsx"] ** 3
     ctx = msbg_gpu.Context(local)
     L = msbg_gpu.lib()
-
-    # --- resident-data timing through the device entry point -----------------
-    ctx.set_topology(c["res"], c["res"], c["res"], c["bsx"])
-    ctx.upload_channel(1, 0, kind, vals, c["band"], -c["band"])
-    slot = np.where(kind == 1, np.cumsum(kind == 1) - 1, np.where(kind == 2, -2, np.where(kind == 3, -3, -1))).astype(np.int32)
+    slot = np.where(kind == 1, np.cumsum(kind == 1) - 1,
+                    np.where(kind == 2, -2, np.where(kind == 3, -3, -1))).astype(np.int32)
     bx, by, bz = upd % nb1, (upd // nb1) % nb1, upd // (nb1 * nb1)
     col = (bx & 1) + 2 * (by & 1) + 4 * (bz & 1)
-    order = np.argsort(col, kind="stable")
-    clist = upd[order]
+    clist = upd[np.argsort(col, kind="stable")]
     cstart = np.zeros(9, np.int32)
     cstart[1:] = np.cumsum(np.bincount(col, minlength=8))
-    dev = torch.device("cuda", local)
     pool = torch.from_numpy(vals).to(dev)
     slot_t = torch.from_numpy(slot).to(dev)
     clist_t = torch.from_numpy(clist.astype(np.int32)).to(dev)
-    import ctypes as C
     stream = torch.cuda.current_stream()
 
     def step():
@@ -244,31 +424,22 @@ def bench_mcf(args):
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
-    ctx.sync()  # raises if a kernel reported a bounded wait that gave up
+    ctx.sync()
     if args.profile:
         ctx.close()
         return
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
-    torch.cuda.synchronize()
+    ms = max_over_ranks(dist, ms, dev)
     clocks = clk.summary()
     ms_step = ms / args.steps
-    rate = nvox * c["iters"] / (ms_step * 1e-3) / 1e9 * ws  # whole job
+    rate = nvox * c["iters"] / (ms_step * 1e-3) / 1e9 * ws
     hbm, _, pk_kind = peaks()
-    alg_bytes_step = 8.0 * nvox * c["iters"]
-    achieved = alg_bytes_step / (ms_step * 1e-3) / 1e9
-    tpc = read_traffic("mcf_colour_kernel_512_b16.txt")
-    cells_per_launch = nvox / 8.0
+    alg = 8.0 * nvox * c["iters"]
+    achieved = alg / (ms_step * 1e-3) / 1e9
+    dpc = read_profile_value("mcf_colour_kernel_512_b16.txt", "dram_bytes_per_cell")
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "peak_kind": pk_kind,
-            "traffic": tpc * cells_per_launch if tpc else None,
-            "alg_bytes_per_launch": 8.0 * cells_per_launch,
-            "kernel": "mcf_colour_kernel<16>"}
-
-    # --- end to end through the C ABI with pinned host buffers ----------------
+            "traffic": dpc * nvox / 8.0 if dpc else None,
+            "alg_bytes_per_launch": 8.0 * nvox / 8.0, "kernel": "mcf_colour_kernel<16>"}
     host_in = torch.from_numpy(vals).pin_memory()
     host_out = torch.empty_like(host_in).pin_memory()
     kind_c = np.ascontiguousarray(kind)
@@ -285,24 +456,15 @@ def bench_mcf(args):
                                                C.cast(C.c_void_p(host_out.data_ptr()), pf))
         rc = rc or L.msbg_gpu_sync(ctx._h)
         if rc:
-            raise RuntimeError(f"e2e rc={rc}: {L.msbg_gpu_last_error(ctx._h)}")
+            raise RuntimeError(f"e2e rc={rc}")
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
+    e2e_step()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_rate = nvox * c["iters"] / e2e_s / 1e9 * ws
-    h2d = vals.nbytes + kind.nbytes * 4 + upd.nbytes  # values + slot map + block list
-    d2h = vals.nbytes
-
+    e2e_s = max_over_ranks(dist, (time.perf_counter() - t0) / args.steps, dev)
     cb = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cb = cpu_reference_mcf(kind, vals, upd)
@@ -315,32 +477,37 @@ def bench_mcf(args):
                            "value_blocks": int(len(upd)), "iters_per_step": c["iters"],
                            "l2": "inputs larger than L2 (%.0f MB)" % (vals.nbytes / 1e6),
                            "parallelism": f"replicas{ws}"},
-                "gpu_launches": launches_per_step * args.steps,
-                "roofline": roof, "clocks": clocks,
-                "e2e": {"value": e2e_rate, "unit": "Gvoxel/s/iter", "h2d_bytes_per_step": int(h2d),
-                        "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": launches_per_step * args.steps, "roofline": roof,
+                "clocks": clocks,
+                "e2e": {"value": nvox * c["iters"] / e2e_s / 1e9 * ws, "unit": "Gvoxel/s/iter",
+                        "h2d_bytes_per_step": int(vals.nbytes + kind.nbytes * 4 + upd.nbytes),
+                        "d2h_bytes_per_step": int(vals.nbytes)},
                 "cpu_baseline": cb}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
+        dist.barrier()
         dist.destroy_process_group()
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mcf", choices=["mcf"])
+    ap.add_argument("--workload", default="mgpcg", choices=["mgpcg", "mcf"])
+    ap.add_argument("--res", type=int, default=0, help="override the pressure resolution")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--profile", action="store_true",
                     help="only the resident-data steps (for ncu captures); prints nothing")
     args = ap.parse_args()
     if args.impl == "reference":
         bench_reference(args)
-    else:
+    elif args.workload == "mcf":
         bench_mcf(args)
+    else:
+        bench_mgpcg(args)
 
 
 if __name__ == "__main__":

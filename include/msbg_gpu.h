@@ -168,6 +168,7 @@ typedef struct {
   double solveSeconds;   /* device time of the solve */
   int64_t fineCells;     /* cells of MG level 0 (liquid) */
   int nMgLevels;
+  int64_t kernelLaunches; /* kernels launched inside the timed solve */
 } msbg_gpu_solve_info;
 
 void msbg_gpu_solve_params_default(msbg_gpu_solve_params* p);
@@ -191,6 +192,31 @@ int msbg_gpu_pressure_download(msbg_gpu_ctx* ctx, float* packed, int64_t n);
 int msbg_gpu_pressure_download_rhs(msbg_gpu_ctx* ctx, float* packed, int64_t n);
 /* Number of values in that layout. */
 int msbg_gpu_pressure_packed_size(msbg_gpu_ctx* ctx, int64_t* n);
+
+/* Sizes and costs of the prepared problem (no counterpart in the reference;
+ * the reference logs similar figures through TRC, src/msbg3.cpp:2340-2348). */
+typedef struct {
+  int nMgLevels;
+  int coarseCells;          /* unknowns of the dense FP64 coarsest solve */
+  int64_t cells[32];        /* stored cells per MG level (tiles holding liquid) */
+  int64_t fluid[32];        /* liquid cells per MG level */
+  int64_t tiles[32];
+  int64_t h2dBytes;         /* bytes uploaded by msbg_gpu_pressure_prepare */
+  int64_t deviceBytesUsed;  /* device memory in use after prepare */
+  double prepareSeconds;    /* wall time of msbg_gpu_pressure_prepare */
+  double buildSeconds;      /* of which host sampling + hierarchy build */
+} msbg_gpu_pressure_stats_t;
+
+int msbg_gpu_pressure_stats(msbg_gpu_ctx* ctx, msbg_gpu_pressure_stats_t* out);
+
+/* Times `reps` calls of one solver part on the context stream with CUDA
+ * events: what = 0 one pre-smoothing sweep of MG level 0 (innerIter sweeps
+ * inside each tile), 1 the level-0 matrix-vector product with its dot
+ * product, 2 one V-cycle (2 pre, 2 post sweeps).  *algBytesPerCall is the
+ * algorithmic DRAM traffic of one call (28 B/cell per smoothing sweep, 24 B/cell
+ * per matvec, summed over the MG levels for a V-cycle). */
+int msbg_gpu_pressure_profile(msbg_gpu_ctx* ctx, int what, int reps, int innerIter,
+                              double* msPerCall, double* algBytesPerCall);
 
 /* Diagnostics without a GPU (no counterpart in the reference): builds the
  * multigrid hierarchy as msbg_gpu_pressure_prepare does, then on the host

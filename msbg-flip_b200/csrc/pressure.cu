@@ -373,6 +373,8 @@ size_t smooth_smem() {
 // ---------------------------------------------------------------------------
 struct Solver {
   Hierarchy H;
+  int64_t h2dBytes = 0;
+  double prepareSeconds = 0, buildSeconds = 0;
   std::vector<std::unique_ptr<LevelDev>> dev;
   std::vector<LevelView> views;
   DeviceBuffer dCoarseInv, dCoarseCells;
@@ -407,54 +409,56 @@ struct Runner {
   Solver& S;
   cudaStream_t st;
   int nPre, nPost, inner;
+  int64_t launches = 0;  // kernels launched through this runner
 
   const int* passList(int m) { return S.dev[m]->passTiles.as<int>(); }
   const int* groupList(int m) { return S.dev[m]->groupTiles.as<int>(); }
 
-  void smooth(int m, float* x, const float* b, bool post, double* partial) {
+  // One smoothing sweep of MG level m: the (level, colour) passes in order
+  // (pre) or in reverse order with the adjoint colour order inside (post).
+  void smooth(int m, float* x, const float* b, bool post) {
     const Level& L = S.H.levels[m];
     const int np = (int)L.passes.size();
     for (int pi = 0; pi < np; pi++) {
       const Level::Pass& P = L.passes[post ? np - 1 - pi : pi];
       if (!P.count) continue;
       const int* lst = passList(m) + P.start;
-      TS_DISPATCH(P.ts, (set_smooth_attr<T>(),
-                         k_smooth<T><<<P.count, T * T, smooth_smem<T>(), st>>>(
-                             S.views[m], lst, x, b, inner, post ? 1 : 0,
-                             (partial && pi == np - 1) ? partial : nullptr)));
+      TS_DISPATCH(P.ts, (k_smooth<T><<<P.count, T * T, smooth_smem<T>(), st>>>(
+                             S.views[m], lst, x, b, inner, post ? 1 : 0, nullptr)));
+      launches++;
     }
   }
 
-  void vcycle(int m, float* x, const float* b, double* rzPartial) {
+  void vcycle(int m, float* x, const float* b) {
     const int last = (int)S.H.levels.size() - 1;
-    LevelDev& D = *S.dev[m];
     const Level& L = S.H.levels[m];
     cudaMemsetAsync(x, 0, sizeof(float) * L.nCells, st);
     if (m == last) {
       k_coarse_solve<<<1, 512, 0, st>>>(S.dCoarseInv.as<double>(), S.H.nCoarse,
                                         S.dCoarseCells.as<int64_t>(), b, x);
+      launches++;
       return;
     }
-    for (int s = 0; s < nPre; s++) smooth(m, x, b, false, nullptr);
+    for (int s = 0; s < nPre; s++) smooth(m, x, b, false);
     LevelDev& C = *S.dev[m + 1];
     for (const auto& g : L.groups) {
       const int* lst = groupList(m) + g.start;
       TS_DISPATCH(g.ts, (k_residual_restrict<T><<<g.count, T * T, 0, st>>>(
                             S.views[m], lst, x, b, C.b.as<float>(), C.tileOff.as<int64_t>())));
+      launches++;
     }
-    vcycle(m + 1, C.x.as<float>(), C.b.as<float>(), nullptr);
+    vcycle(m + 1, C.x.as<float>(), C.b.as<float>());
     for (const auto& g : L.groups) {
       const int* lst = groupList(m) + g.start;
       TS_DISPATCH(g.ts, (k_prolong<T><<<g.count, T * T, 0, st>>>(S.views[m], lst, x,
                                                                   C.x.as<float>(),
                                                                   C.tileOff.as<int64_t>())));
+      launches++;
     }
-    (void)D;
-    for (int s = 0; s < nPost; s++)
-      smooth(m, x, b, true, (rzPartial && s == nPost - 1) ? rzPartial : nullptr);
+    for (int s = 0; s < nPost; s++) smooth(m, x, b, true);
   }
 
-  // q = A d with partial d.q (level 0)
+  // q = A d with partial d.q (level 0); returns the number of partials.
   int matvec_dot(const float* d, float* q, double* partial) {
     const Level& L = S.H.levels[0];
     int off = 0;
@@ -462,6 +466,7 @@ struct Runner {
       const int* lst = groupList(0) + g.start;
       TS_DISPATCH(g.ts, (k_matvec_dot<T><<<g.count, T * T, 0, st>>>(S.views[0], lst, d, q,
                                                                      partial + off)));
+      launches++;
       off += g.count;
     }
     return off;
@@ -526,8 +531,11 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
   sp.reset(new Solver());
   Solver& S = *sp;
   std::string err;
+  auto tp0 = std::chrono::steady_clock::now();
   rc = build_hierarchy(S.H, topo->sx, topo->sy, topo->sz, topo->bsx0, topo->nLevels,
                        topo->blockLevel, cb, 512, &err);
+  S.buildSeconds =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - tp0).count();
   if (rc) {
     sp.reset();
     return set_error(ctx, rc, "pressure prepare: %s", err.c_str());
@@ -597,6 +605,14 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
   MSBG_CUDA_TRY(ctx, upload(S.dCoarseCells, S.H.coarseCells, st));
   MSBG_CUDA_TRY(ctx, cudaMallocHost(&S.hScal, sizeof(Scalars)));
   MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  for (const auto& D : S.dev)
+    S.h2dBytes += (int64_t)(D->tileOff.bytes + D->face.bytes + D->ifOff.bytes +
+                            D->toCoarse.bytes + D->passTiles.bytes + D->groupTiles.bytes +
+                            D->diag.bytes + D->cx.bytes + D->cy.bytes + D->cz.bytes +
+                            D->ifc.bytes);
+  S.h2dBytes += (int64_t)(S.rhs0.bytes + S.dCoarseInv.bytes + S.dCoarseCells.bytes);
+  S.prepareSeconds =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - tp0).count();
   return MSBG_OK;
 }
 
@@ -635,7 +651,7 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
   cudaMemcpyAsync(r, b, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
   k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(b, b, n, part);
   k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_BB);
-  R.vcycle(0, z, r, nullptr);
+  R.vcycle(0, z, r);
   k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
   k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHO);
   cudaMemcpyAsync(d, z, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
@@ -647,22 +663,28 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
     status = 0;
   } else {
     auto iteration = [&]() {
+      R.launches += 6;  // finalize x3, axpy_norm, dot, update_d
       int nt = R.matvec_dot(d, q, part);
       k_finalize<<<1, 1024, 0, st>>>(part, nt, sc, FIN_DQ_ALPHA);
       k_axpy_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x, r, d, q, n, sc, part);
       k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
-      R.vcycle(0, z, r, nullptr);
+      R.vcycle(0, z, r);
       k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
       k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHONEW_BETA);
       k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, n, sc);
       cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
     };
+    R.launches += 4;  // initial dot/finalize pairs
     cudaGraphExec_t exec = nullptr;
+    int64_t perIter = 0;
     if (p->useGraph) {
+      const int64_t before = R.launches;
       cudaGraph_t g;
       MSBG_CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       iteration();
       MSBG_CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
+      perIter = R.launches - before;
+      R.launches = before;
       MSBG_CUDA_TRY(ctx, cudaGraphInstantiate(&exec, g, 0));
       cudaGraphDestroy(g);
     }
@@ -670,6 +692,7 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
     for (int it = 0; it < p->maxIter; it++) {
       if (exec) {
         MSBG_CUDA_TRY(ctx, cudaGraphLaunch(exec, st));
+        R.launches += perIter;
       } else {
         iteration();
       }
@@ -716,7 +739,87 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
     info->solveSeconds = ms * 1e-3;
     info->fineCells = L0.nFluid;
     info->nMgLevels = (int)S.H.levels.size();
+    info->kernelLaunches = R.launches;
   }
+  return MSBG_OK;
+}
+
+extern "C" int msbg_gpu_pressure_stats(msbg_gpu_ctx* ctx, msbg_gpu_pressure_stats_t* out) {
+  if (!ctx || !out) return MSBG_EINVARG;
+  auto& sp = solver_of(ctx);
+  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
+  Solver& S = *sp;
+  std::memset(out, 0, sizeof(*out));
+  out->nMgLevels = (int)S.H.levels.size();
+  for (size_t m = 0; m < S.H.levels.size() && m < 32; m++) {
+    out->cells[m] = S.H.levels[m].nCells;
+    out->fluid[m] = S.H.levels[m].nFluid;
+    out->tiles[m] = (int64_t)S.H.levels[m].tiles.size();
+  }
+  out->h2dBytes = S.h2dBytes;
+  out->prepareSeconds = S.prepareSeconds;
+  out->buildSeconds = S.buildSeconds;
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  out->deviceBytesUsed = (int64_t)(tot - fr);
+  out->coarseCells = S.H.nCoarse;
+  return MSBG_OK;
+}
+
+extern "C" int msbg_gpu_pressure_profile(msbg_gpu_ctx* ctx, int what, int reps, int innerIter,
+                                         double* msPerCall, double* algBytesPerCall) {
+  if (!ctx || reps <= 0 || innerIter < 1) return MSBG_EINVARG;
+  auto& sp = solver_of(ctx);
+  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
+  cudaSetDevice(ctx->device);
+  Solver& S = *sp;
+  cudaStream_t st = ctx->stream;
+  Runner R{S, st, 2, 2, innerIter};
+  const Level& L0 = S.H.levels[0];
+  LevelDev& D0 = *S.dev[0];
+  float* x = D0.x.as<float>();
+  double* part = S.partial.as<double>();
+  const float* b = S.rhs0.as<float>();
+  // algorithmic bytes per cell: smoother reads x,b,diag,cx,cy,cz and writes x
+  const double smoothB = 28.0, mvB = 24.0, resB = 28.0 + 0.5, prolB = 12.5;
+  auto vcycle_bytes = [&]() {
+    double s = 0;
+    for (size_t m = 0; m + 1 < S.H.levels.size(); m++) {
+      const double n = (double)S.H.levels[m].nCells;
+      s += n * (4.0 /*zero x*/ + (R.nPre + R.nPost) * smoothB + resB + prolB);
+    }
+    return s;
+  };
+  double bytes = 0;
+  auto body = [&]() {
+    switch (what) {
+      case 0: R.smooth(0, x, b, false); break;
+      case 1: R.matvec_dot(x, S.q0.as<float>(), part); break;
+      case 2: R.vcycle(0, S.z0.as<float>(), b); break;
+      default: break;
+    }
+  };
+  switch (what) {
+    case 0: bytes = smoothB * L0.nCells; break;
+    case 1: bytes = mvB * L0.nCells; break;
+    case 2: bytes = vcycle_bytes(); break;
+    default: return set_error(ctx, MSBG_EINVARG, "profile target %d", what);
+  }
+  MSBG_CUDA_TRY(ctx, cudaMemsetAsync(x, 0, sizeof(float) * L0.nCells, st));
+  body();  // warm-up
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  for (int i = 0; i < reps; i++) body();
+  cudaEventRecord(e1, st);
+  MSBG_CUDA_TRY(ctx, cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (msPerCall) *msPerCall = ms / reps;
+  if (algBytesPerCall) *algBytesPerCall = bytes;
   return MSBG_OK;
 }
 

@@ -208,7 +208,15 @@ class SolveParams(C.Structure):
 class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("status", C.c_int),
                 ("relResidual", C.c_double), ("solveSeconds", C.c_double),
-                ("fineCells", C.c_int64), ("nMgLevels", C.c_int)]
+                ("fineCells", C.c_int64), ("nMgLevels", C.c_int),
+                ("kernelLaunches", C.c_int64)]
+
+
+class PressureStats(C.Structure):
+    _fields_ = [("nMgLevels", C.c_int), ("coarseCells", C.c_int),
+                ("cells", C.c_int64 * 32), ("fluid", C.c_int64 * 32), ("tiles", C.c_int64 * 32),
+                ("h2dBytes", C.c_int64), ("deviceBytesUsed", C.c_int64),
+                ("prepareSeconds", C.c_double), ("buildSeconds", C.c_double)]
 
 
 def _pressure_sigs(L):
@@ -224,6 +232,13 @@ def _pressure_sigs(L):
         "msbg_gpu_pressure_download": (i32, [vp, C.POINTER(C.c_float), C.c_int64]),
         "msbg_gpu_pressure_download_rhs": (i32, [vp, C.POINTER(C.c_float), C.c_int64]),
         "msbg_gpu_pressure_packed_size": (i32, [vp, C.POINTER(C.c_int64)]),
+        "msbg_gpu_pressure_stats": (i32, [vp, C.POINTER(PressureStats)]),
+        "msbg_gpu_pressure_profile": (i32, [vp, i32, i32, i32, C.POINTER(C.c_double),
+                                            C.POINTER(C.c_double)]),
+        "msbg_gpu_pressure_host_check": (i32, [C.POINTER(TopoDesc), C.POINTER(PressureCallbacks),
+                                               C.POINTER(C.c_float), C.POINTER(C.c_double),
+                                               C.POINTER(C.c_int), C.POINTER(C.c_int64),
+                                               C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -294,7 +309,33 @@ def _ctx_pressure_solve(self, params=None, **kw):
     info = SolveInfo()
     self._check(self._L.msbg_gpu_pressure_solve(self._h, C.byref(p), C.byref(info)),
                 "pressure_solve")
+    self._last_launches = info.kernelLaunches
     return info
+
+
+def _ctx_pressure_profile(self, what, reps, inner=2):
+    ms = C.c_double()
+    by = C.c_double()
+    self._check(self._L.msbg_gpu_pressure_profile(self._h, what, reps, inner, C.byref(ms),
+                                                  C.byref(by)), "pressure_profile")
+    return ms.value, by.value
+
+
+def count_liquid_cells(scene):
+    """Liquid cells of MG level 0 of a scene (host-side hierarchy build, no GPU)."""
+    L = lib()
+    _pressure_sigs(L)
+    bl = np.ascontiguousarray(scene.block_levels, np.int32)
+    d = TopoDesc(scene.res, scene.res, scene.res, scene.bsx0, scene.n_levels,
+                 _p(bl, C.c_int))
+    cb = scene.callbacks()
+    nm = C.c_int()
+    fluid = np.zeros(32, np.int64)
+    rc = L.msbg_gpu_pressure_host_check(C.byref(d), C.byref(cb), None, None, C.byref(nm),
+                                        _p(fluid, C.c_int64), None)
+    if rc:
+        raise MsbgError(rc, "host check")
+    return int(fluid[0])
 
 
 def _ctx_pressure_download(self, rhs=False):
@@ -309,3 +350,5 @@ def _ctx_pressure_download(self, rhs=False):
 Context.pressure_prepare = _ctx_pressure_prepare
 Context.pressure_solve = _ctx_pressure_solve
 Context.pressure_download = _ctx_pressure_download
+Context.pressure_profile = _ctx_pressure_profile
+Context.last_solve_launches = lambda self: getattr(self, "_last_launches", None)

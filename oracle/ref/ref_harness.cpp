@@ -129,41 +129,20 @@ extern "C" int ref_mcf(int sx, int sy, int sz, int bsx, const int8_t* kind,
 // ---------------------------------------------------------------------------
 // FLIP pressure solver (src/msbg3.cpp:2467-3271) driven from arrays.
 //
-// The callbacks sample dense fine-resolution arrays at the coordinates the
-// reference passes (it passes unscaled block-local coordinates for coarse
-// blocks, src/msbg3.cpp:2494-2503); out-of-range reads return CELL_SOLID / 0.
+// The callbacks are the caller's (the same seeded scene the GPU path samples);
+// the reference calls them with unscaled coordinates for coarse blocks
+// (src/msbg3.cpp:2494-2503), exactly as it does in its own FLIP driver.
 // Channel data move in a packed layout: for every block id in ascending order,
 // the block's (bsx0>>level)^3 values at its level for the given MG level.
 // ---------------------------------------------------------------------------
 namespace {
 
-struct PsArrays {
-  int sx, sy, sz;
-  const uint16_t* cellType;  // [sz][sy][sx]
-  const float* face;         // [3][sz][sy][sx]
-  const float* rhs;          // [sz][sy][sx]
-  bool in(int x, int y, int z) const {
-    return x >= 0 && y >= 0 && z >= 0 && x < sx && y < sy && z < sz;
-  }
-  size_t idx(int x, int y, int z) const { return (size_t)x + (size_t)sx * (y + (size_t)sy * z); }
-};
-
-CellFlags psCellType(void* u, int x, int y, int z) {
-  auto* a = (PsArrays*)u;
-  return a->in(x, y, z) ? (CellFlags)a->cellType[a->idx(x, y, z)] : (CellFlags)CELL_SOLID;
-}
-float psFace(void* u, int dir, int x, int y, int z) {
-  auto* a = (PsArrays*)u;
-  return a->in(x, y, z) ? a->face[(size_t)dir * a->sx * a->sy * a->sz + a->idx(x, y, z)] : 0.f;
-}
-float psRhs(void* u, int x, int y, int z) {
-  auto* a = (PsArrays*)u;
-  return a->in(x, y, z) ? a->rhs[a->idx(x, y, z)] : 0.f;
-}
+typedef CellFlags (*PsCellTypeFn)(void*, int, int, int);
+typedef float (*PsFaceFn)(void*, int, int, int, int);
+typedef float (*PsRhsFn)(void*, int, int, int);
 
 struct PsHandle {
   MultiresSparseGrid* msbg;
-  PsArrays arr;
 };
 
 // Channel ids understood by ref_ps_get/set: the reference's channel ids, plus
@@ -177,9 +156,8 @@ SparseGrid<float>* ps_float_grid(MultiresSparseGrid* m, int ch, int level, int l
 }  // namespace
 
 extern "C" void* ref_ps_create(int sx, int sy, int sz, int bsx0, int nLevels,
-                               const int* blockLevel, const int* domBc,
-                               const uint16_t* cellType, const float* face,
-                               const float* rhs) {
+                               const int* blockLevel, const int* domBc, PsCellTypeFn cellType,
+                               PsFaceFn face, PsRhsFn rhs, void* user, double* prepSeconds) {
   MultiresSparseGrid* m = MultiresSparseGrid::create("PS", sx, sy, sz, bsx0, -1, 0, -1, 0,
                                                      NULL, NULL, nLevels);
   if (!m) return nullptr;
@@ -187,13 +165,16 @@ extern "C" void* ref_ps_create(int sx, int sy, int sz, int bsx0, int nLevels,
   std::vector<int> levels(blockLevel, blockLevel + nb);
   m->setRefinementMap(levels.data(), NULL, -1, NULL, false, true);
   m->setDomainBoundarySpec_(domBc[0], domBc[1], domBc[2], domBc[3], domBc[4], domBc[5]);
-  auto* h = new PsHandle{m, {sx, sy, sz, cellType, face, rhs}};
+  auto* h = new PsHandle{m};
   FlipPressureCallbacks cb;
-  cb.sampleCellType = &psCellType;
-  cb.sampleFaceCoeff = &psFace;
-  cb.sampleRhs = &psRhs;
-  cb.user = &h->arr;
+  cb.sampleCellType = cellType;
+  cb.sampleFaceCoeff = face;
+  cb.sampleRhs = rhs;
+  cb.user = user;
+  auto t0 = std::chrono::steady_clock::now();
   m->preparePressureSolveFLIP(cb);
+  auto t1 = std::chrono::steady_clock::now();
+  if (prepSeconds) *prepSeconds = std::chrono::duration<double>(t1 - t0).count();
   return h;
 }
 
