@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -273,7 +274,8 @@ template <int TS>
 __global__ void __launch_bounds__(TS* TS) k_prolong(LevelView L, const int* __restrict__ tiles,
                                                     float* __restrict__ x,
                                                     const float* __restrict__ xc,
-                                                    const int64_t* __restrict__ coarseOff) {
+                                                    const int64_t* __restrict__ coarseOff,
+                                                    float scale) {
   constexpr int N = TS * TS * TS, NT = TS * TS;
   const int ti = tiles[blockIdx.x];
   const int64_t off = L.tileOff[ti];
@@ -285,7 +287,7 @@ __global__ void __launch_bounds__(TS* TS) k_prolong(LevelView L, const int* __re
     if (!(L.diag[off + e] > 0.f)) continue;
     const int i = e % TS, j = (e / TS) % TS, k = e / (TS * TS);
     const int sh = agg ? 1 : 0;
-    x[off + e] += src[tidx(cts, ox + (i >> sh), oy + (j >> sh), oz + (k >> sh))];
+    x[off + e] += scale * src[tidx(cts, ox + (i >> sh), oy + (j >> sh), oz + (k >> sh))];
   }
 }
 
@@ -298,7 +300,7 @@ __global__ void __launch_bounds__(TS* TS) k_smooth(LevelView L, const int* __res
                                                    const float* __restrict__ b, int inner,
                                                    int reverse, double* __restrict__ partial) {
   constexpr int N = TS * TS * TS, NT = TS * TS;
-  extern __shared__ __align__(16) float sm[];
+  extern __shared__ __align__(128) float sm[];
   float* xs = sm;
   float* cxs = sm + N;
   float* cys = sm + 2 * N;
@@ -348,6 +350,8 @@ __global__ void __launch_bounds__(TS* TS) k_smooth(LevelView L, const int* __res
   }
 }
 
+#include "smooth_pipe.cuh"
+
 // Coarsest level: x = A^-1 b with the dense FP64 inverse (symmetric).
 __global__ void __launch_bounds__(512) k_coarse_solve(const double* __restrict__ Ainv, int n,
                                                       const int64_t* __restrict__ cells,
@@ -374,6 +378,7 @@ size_t smooth_smem() {
 struct Solver {
   Hierarchy H;
   int64_t h2dBytes = 0;
+  int numSMs = 148;
   double prepareSeconds = 0, buildSeconds = 0;
   std::vector<std::unique_ptr<LevelDev>> dev;
   std::vector<LevelView> views;
@@ -409,6 +414,10 @@ struct Runner {
   Solver& S;
   cudaStream_t st;
   int nPre, nPost, inner;
+  float coarseScale = 1.0f;
+  int* err = nullptr;     // device flag set by kernels whose bounded wait gave up
+  int numSMs = 148;
+  bool usePipe = true;
   int64_t launches = 0;  // kernels launched through this runner
 
   const int* passList(int m) { return S.dev[m]->passTiles.as<int>(); }
@@ -423,8 +432,15 @@ struct Runner {
       const Level::Pass& P = L.passes[post ? np - 1 - pi : pi];
       if (!P.count) continue;
       const int* lst = passList(m) + P.start;
-      TS_DISPATCH(P.ts, (k_smooth<T><<<P.count, T * T, smooth_smem<T>(), st>>>(
-                             S.views[m], lst, x, b, inner, post ? 1 : 0, nullptr)));
+      if (P.ts == 16 && usePipe) {
+        const int grid = std::min(P.count, numSMs);
+        // passes are contiguous tile-id ranges (register_tiles sorts by pass)
+        k_smooth_pipe16<<<grid, pipe::NT, pipe::SMEM, st>>>(S.views[m], P.start, P.count, x,
+                                                            b, inner, post ? 1 : 0, err);
+      } else {
+        TS_DISPATCH(P.ts, (k_smooth<T><<<P.count, T * T, smooth_smem<T>(), st>>>(
+                               S.views[m], lst, x, b, inner, post ? 1 : 0, nullptr)));
+      }
       launches++;
     }
   }
@@ -452,7 +468,8 @@ struct Runner {
       const int* lst = groupList(m) + g.start;
       TS_DISPATCH(g.ts, (k_prolong<T><<<g.count, T * T, 0, st>>>(S.views[m], lst, x,
                                                                   C.x.as<float>(),
-                                                                  C.tileOff.as<int64_t>())));
+                                                                  C.tileOff.as<int64_t>(),
+                                                                  coarseScale)));
       launches++;
     }
     for (int s = 0; s < nPost; s++) smooth(m, x, b, true);
@@ -518,6 +535,7 @@ extern "C" void msbg_gpu_solve_params_default(msbg_gpu_solve_params* p) {
   p->storage = MSBG_F32;
   p->maxRefine = 4;
   p->useGraph = 1;
+  p->coarseScale = 1.0f;
 }
 
 extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
@@ -548,6 +566,9 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
                          t.ts, (int)m);
       }
   set_smooth_attr<16>();
+  cudaFuncSetAttribute(k_smooth_pipe16, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pipe::SMEM);
+  cudaDeviceGetAttribute(&S.numSMs, cudaDevAttrMultiProcessorCount, ctx->device);
   set_smooth_attr<8>();
   set_smooth_attr<4>();
   set_smooth_attr<2>();
@@ -570,6 +591,18 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
     MSBG_CUDA_TRY(ctx, upload(D->passTiles, L.passTiles, st));
     MSBG_CUDA_TRY(ctx, upload(D->groupTiles, L.groupTiles, st));
     MSBG_CUDA_TRY(ctx, upload(D->diag, L.diag, st));
+    {
+      std::vector<float> inv(L.diag.size());
+      for (size_t c = 0; c < inv.size(); c++)
+        inv[c] = L.diag[c] > 0.f ? (float)(1.0 / (double)L.diag[c]) : 0.f;
+      MSBG_CUDA_TRY(ctx, upload(D->invdiag, inv, st));
+      MSBG_CUDA_TRY(ctx, upload(D->tileRec, build_tile_records(L), st));
+      // the hot-path kernels address passes as contiguous tile-id ranges
+      for (size_t i = 0; i < L.passTiles.size(); i++)
+        if (L.passTiles[i] != (int)i)
+          return set_error(ctx, MSBG_EINTERNAL, "pass tiles are not contiguous");
+      MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));  // host vectors above are temporaries
+    }
     MSBG_CUDA_TRY(ctx, upload(D->cx, L.cx, st));
     MSBG_CUDA_TRY(ctx, upload(D->cy, L.cy, st));
     MSBG_CUDA_TRY(ctx, upload(D->cz, L.cz, st));
@@ -584,6 +617,8 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
     v.ifOff = D->ifOff.as<int64_t>();
     v.toCoarse = D->toCoarse.as<int>();
     v.diag = D->diag.as<float>();
+    v.invdiag = D->invdiag.as<float>();
+    v.tileRec = D->tileRec.p;
     v.cx = D->cx.as<float>();
     v.cy = D->cy.as<float>();
     v.cz = D->cz.as<float>();
@@ -629,6 +664,9 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
   Solver& S = *sp;
   cudaStream_t st = ctx->stream;
   Runner R{S, st, p->nPre, p->nPost, p->innerIter};
+  R.coarseScale = p->coarseScale > 0 ? p->coarseScale : 1.0f;
+  R.err = ctx->errBuf.as<int>();
+  R.numSMs = S.numSMs;
   const Level& L0 = S.H.levels[0];
   const int64_t n = L0.nCells;
   LevelDev& D0 = *S.dev[0];
@@ -775,6 +813,8 @@ extern "C" int msbg_gpu_pressure_profile(msbg_gpu_ctx* ctx, int what, int reps, 
   Solver& S = *sp;
   cudaStream_t st = ctx->stream;
   Runner R{S, st, 2, 2, innerIter};
+  R.err = ctx->errBuf.as<int>();
+  R.numSMs = S.numSMs;
   const Level& L0 = S.H.levels[0];
   LevelDev& D0 = *S.dev[0];
   float* x = D0.x.as<float>();
@@ -794,13 +834,15 @@ extern "C" int msbg_gpu_pressure_profile(msbg_gpu_ctx* ctx, int what, int reps, 
   auto body = [&]() {
     switch (what) {
       case 0: R.smooth(0, x, b, false); break;
+      case 3: R.usePipe = false; R.smooth(0, x, b, false); R.usePipe = true; break;
       case 1: R.matvec_dot(x, S.q0.as<float>(), part); break;
       case 2: R.vcycle(0, S.z0.as<float>(), b); break;
       default: break;
     }
   };
   switch (what) {
-    case 0: bytes = smoothB * L0.nCells; break;
+    case 0:
+    case 3: bytes = smoothB * L0.nCells; break;
     case 1: bytes = mvB * L0.nCells; break;
     case 2: bytes = vcycle_bytes(); break;
     default: return set_error(ctx, MSBG_EINVARG, "profile target %d", what);

@@ -76,7 +76,8 @@ struct Level {
 // Device mirror of one level.
 struct LevelDev {
   DeviceBuffer tileOff, face, ifOff, toCoarse, passTiles, groupTiles;
-  DeviceBuffer diag, cx, cy, cz, ifc;
+  DeviceBuffer diag, invdiag, cx, cy, cz, ifc;
+  DeviceBuffer tileRec;            // 256-byte per-tile records (smooth_pipe.cuh)
   DeviceBuffer x, b, r;            // FP32 work vectors of this level
 };
 

@@ -22,6 +22,8 @@ struct LevelView {
   const int64_t* ifOff;
   const int* toCoarse;
   const float* diag;
+  const float* invdiag;  // 1/a_ii (0 for cells that are not liquid)
+  const void* tileRec;   // per-tile records of the pipelined smoother
   const float* cx;
   const float* cy;
   const float* cz;

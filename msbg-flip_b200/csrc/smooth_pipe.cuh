@@ -1,0 +1,320 @@
+// Persistent, TMA-pipelined red-black tile smoother for 16^3 tiles (the
+// level-0 hot path of the pressure V-cycle).  Included inside namespace
+// msbg::ps of pressure.cu.
+//
+// One CTA per SM walks a pass (a contiguous range of tile ids of one level and
+// colour) with a stride of gridDim.x.  Per tile:
+//   * the six contiguous 16 KB arrays (x, b, 1/a_ii, cx, cy, cz) arrive by bulk
+//     asynchronous copies (cp.async.bulk, completion on an mbarrier) into one
+//     of two shared-memory stages, issued one tile ahead;
+//   * the tile's 256-byte record (its offset and the resolved data of its six
+//     faces) arrives the same way two tiles ahead, so no dependent global load
+//     sits on the critical path;
+//   * the halo values of the next tile are loaded into registers before the
+//     current tile is smoothed and summed afterwards;
+//   * the smoothed x leaves by one bulk store.
+// 512 threads; per colour each thread owns 4 cells whose couplings, 1/a_ii
+// and right-hand side (with the constant halo sums folded in) sit in
+// registers, laid out so a warp's shared-memory accesses hit 32 banks.
+
+namespace pipe {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Bounded wait on the given phase parity; false if the copies never landed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done = 0;
+  for (int i = 0; i < (1 << 24); i++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+               "r"(smem_u32(src)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// Wait until the bulk stores issued so far have finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+constexpr int TS = 16, N = TS * TS * TS, NT = 512;
+
+// Per-face data of a tile needed to gather its halo.
+struct FaceRes {
+  int kind, nts, oa, ob, cov, pad;
+  int64_t nOff;   // SAME/COARSER: neighbour tile offset
+  int64_t ifOwn;  // COARSER: our interface-coupling plane
+};
+struct __align__(16) TileRec {
+  int64_t off;
+  int64_t pad;
+  FaceRes f[6];
+};
+static_assert(sizeof(TileRec) == 256, "tile record is one 256-byte bulk copy");
+
+// A zeroed guard band in front of the first stage keeps the neighbour reads
+// of boundary cells (whose couplings are zero) inside shared memory.
+constexpr int GUARD = TS * TS;
+constexpr int ZERO_FLOATS = GUARD + 12 * N + 2 * 6 * TS * TS;
+constexpr size_t SMEM = sizeof(float) * ZERO_FLOATS + 3 * sizeof(TileRec) + 3 * sizeof(uint64_t);
+
+// Issue the global loads of one halo cell of a SAME/COARSER face; the own
+// lower-face coupling of a SAME face is taken later from shared memory.
+__device__ __forceinline__ void halo_load(const LevelView& L, const float* __restrict__ x,
+                                          const FaceRes& r, int dir, int side, int a, int b,
+                                          float& xv, float& cv) {
+  const float* cd = dir == 0 ? L.cx : dir == 1 ? L.cy : L.cz;
+  xv = 0.f;
+  cv = 0.f;
+  if (r.kind == FACE_SAME) {
+    xv = __ldg(x + r.nOff + plane_idx(TS, dir, side ? 0 : TS - 1, a, b));
+    if (side) cv = __ldg(cd + r.nOff + plane_idx(TS, dir, 0, a, b));
+  } else if (r.kind == FACE_COARSER) {
+    xv = __ldg(x + r.nOff +
+               plane_idx(r.nts, dir, side ? 0 : r.nts - 1, r.oa + (a >> 1), r.ob + (b >> 1)));
+    cv = __ldg(L.ifc + r.ifOwn + a + TS * b);
+  }
+}
+
+}  // namespace pipe
+
+__global__ void __launch_bounds__(pipe::NT, 1)
+    k_smooth_pipe16(LevelView L, int tileBase, int count, float* __restrict__ x,
+                    const float* __restrict__ b, int inner, int reverse, int* __restrict__ err) {
+  using namespace pipe;
+  extern __shared__ __align__(128) float sm[];
+  float* stages[2] = {sm + GUARD, sm + GUARD + 6 * N};
+  float(*gsb)[6][TS * TS] = reinterpret_cast<float(*)[6][TS * TS]>(sm + GUARD + 12 * N);
+  TileRec* recs = reinterpret_cast<TileRec*>(sm + ZERO_FLOATS);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(recs + 3);  // [0],[1] stages, [2] prologue
+  const TileRec* grec = reinterpret_cast<const TileRec*>(L.tileRec) + tileBase;
+  const int tid = threadIdx.x;
+  const int G = gridDim.x;
+  int t = blockIdx.x;
+  if (t >= count) return;
+  // every float of shared memory holds 0 or a value of our (finite) arrays
+  for (int q = tid; q < ZERO_FLOATS / 4; q += NT)
+    reinterpret_cast<float4*>(sm)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init(&bar[2], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue_arrays = [&](const TileRec& r, float* st, uint64_t* br, int tRec, int slot) {
+    fence_proxy_async();
+    const bool rec = tRec < count;
+    mbar_expect_tx(br, 6 * N * sizeof(float) + (rec ? sizeof(TileRec) : 0));
+    const int64_t off = r.off;
+    bulk_g2s(st + 0 * N, x + off, N * sizeof(float), br);
+    bulk_g2s(st + 1 * N, b + off, N * sizeof(float), br);
+    bulk_g2s(st + 2 * N, L.invdiag + off, N * sizeof(float), br);
+    bulk_g2s(st + 3 * N, L.cx + off, N * sizeof(float), br);
+    bulk_g2s(st + 4 * N, L.cy + off, N * sizeof(float), br);
+    bulk_g2s(st + 5 * N, L.cz + off, N * sizeof(float), br);
+    if (rec) bulk_g2s(&recs[slot], grec + tRec, sizeof(TileRec), br);
+  };
+  float hx[3], hc[3];
+  auto halo_issue = [&](const TileRec& r) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const int g = tid + NT * q, f = g >> 8, c = g & 255;
+      halo_load(L, x, r.f[f], f >> 1, f & 1, c & 15, c >> 4, hx[q], hc[q]);
+    }
+  };
+  auto halo_combine = [&](const TileRec& r, int ti, int u) {
+    const float* st = stages[u];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const int g = tid + NT * q, f = g >> 8, c = g & 255;
+      const int dir = f >> 1, side = f & 1, a = c & 15, bb = c >> 4;
+      const int kind = r.f[f].kind;
+      float v = 0.f;
+      if (kind == FACE_SAME) {
+        const float cown = st[(3 + dir) * N + plane_idx(TS, dir, 0, a, bb)];
+        v = (side ? hc[q] : cown) * hx[q];
+      } else if (kind == FACE_COARSER) {
+        v = hc[q] * hx[q];
+      } else if (kind == FACE_FINER) {
+        v = ghost_sum(L, x, ti, TS, dir, side, a, bb);
+      }
+      gsb[u][f][c] = v;
+    }
+  };
+  // prologue: the first tile's record, then its arrays (which bring the
+  // second tile's record along: the arrays of tile m carry record m+1)
+  if (tid == 0) {
+    mbar_expect_tx(&bar[2], sizeof(TileRec));
+    bulk_g2s(&recs[0], grec + t, sizeof(TileRec), &bar[2]);
+  }
+  if (!__syncthreads_and(mbar_wait(&bar[2], 0))) {
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  if (tid == 0) issue_arrays(recs[0], stages[0], &bar[0], t + G, 1);
+  halo_issue(recs[0]);
+  if (!__syncthreads_and(mbar_wait(&bar[0], 0))) {
+    if (tid == 0) {
+      atomicExch(err, 1);
+      mbar_wait(&bar[0], 0);  // one more bounded wait for the copies in flight
+    }
+    return;
+  }
+  halo_combine(recs[0], tileBase + t, 0);
+  __syncthreads();
+  const int ip = tid & 7, jj = 2 * ((tid >> 5) & 7) + ((tid >> 3) & 1);
+  const int kb = ((tid >> 4) & 1) + 2 * (tid >> 8);
+  for (int n = 0; t < count; n++, t += G) {
+    const int s = n & 1, u = s ^ 1;
+    const int tn = t + G;
+    const bool hasNext = tn < count;
+    const TileRec& rc = recs[n % 3];
+    const TileRec& rn = recs[(n + 1) % 3];
+    // 1: prefetch the next tile (arrays + the record two ahead), halo loads
+    if (hasNext) {
+      if (tid == 0) {
+        bulk_wait_read();  // the store from stage u (tile n-1) has read it
+        issue_arrays(rn, stages[u], &bar[u], tn + G, (n + 2) % 3);
+      }
+      halo_issue(rn);
+    }
+    // 2: registers: couplings, 1/a_ii, b with the halo sums folded in
+    float* X = stages[s];
+    const float* B = X + N;
+    const float* IV = X + 2 * N;
+    const float* CX = X + 3 * N;
+    const float* CY = X + 4 * N;
+    const float* CZ = X + 5 * N;
+    const float(*gs)[TS * TS] = gsb[s];
+    float R[2][4], I[2][4], Cm[2][4][3], Cp[2][4][3];
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) {
+        const int k = kb + 4 * kk, ii = 2 * ip + ((jj + k + c) & 1);
+        const int e = tidx(TS, ii, jj, k);
+        const float iv = IV[e];
+        const bool fl = iv > 0.f;
+        I[c][kk] = iv;
+        float r = B[e];
+        if (ii == 0) r += gs[0][jj + TS * k];
+        if (ii == TS - 1) r += gs[1][jj + TS * k];
+        if (jj == 0) r += gs[2][ii + TS * k];
+        if (jj == TS - 1) r += gs[3][ii + TS * k];
+        if (k == 0) r += gs[4][ii + TS * jj];
+        if (k == TS - 1) r += gs[5][ii + TS * jj];
+        R[c][kk] = r;
+        Cm[c][kk][0] = (fl && ii > 0) ? CX[e] : 0.f;
+        Cp[c][kk][0] = (fl && ii < TS - 1) ? CX[e + 1] : 0.f;
+        Cm[c][kk][1] = (fl && jj > 0) ? CY[e] : 0.f;
+        Cp[c][kk][1] = (fl && jj < TS - 1) ? CY[e + TS] : 0.f;
+        Cm[c][kk][2] = (fl && k > 0) ? CZ[e] : 0.f;
+        Cp[c][kk][2] = (fl && k < TS - 1) ? CZ[e + TS * TS] : 0.f;
+      }
+    // 3: red-black sweeps (colour compile-time so the arrays stay in registers)
+    auto half = [&](auto cc) {
+      constexpr int c = decltype(cc)::value;
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) {
+        const int k = kb + 4 * kk, ii = 2 * ip + ((jj + k + c) & 1);
+        const int e = tidx(TS, ii, jj, k);
+        // out-of-tile neighbours have zero coupling; their reads stay inside
+        // shared memory (guard band / adjacent arrays, all finite)
+        float S = R[c][kk];
+        S = fmaf(Cm[c][kk][0], X[e - 1], S);
+        S = fmaf(Cp[c][kk][0], X[e + 1], S);
+        S = fmaf(Cm[c][kk][1], X[e - TS], S);
+        S = fmaf(Cp[c][kk][1], X[e + TS], S);
+        S = fmaf(Cm[c][kk][2], X[e - TS * TS], S);
+        S = fmaf(Cp[c][kk][2], X[e + TS * TS], S);
+        X[e] = S * I[c][kk];
+      }
+      __syncthreads();
+    };
+    for (int it = 0; it < inner; it++) {
+      if (reverse) {
+        half(std::integral_constant<int, 1>());
+        half(std::integral_constant<int, 0>());
+      } else {
+        half(std::integral_constant<int, 0>());
+        half(std::integral_constant<int, 1>());
+      }
+    }
+    // 4: the tile leaves by one bulk store
+    if (tid == 0) {
+      fence_proxy_async();
+      bulk_s2g(x + rc.off, X, N * sizeof(float));
+    }
+    // 5: next tile's arrays landed -> its halo sums
+    if (hasNext) {
+      if (!__syncthreads_and(mbar_wait(&bar[u], ((n + 1) >> 1) & 1))) {
+        if (tid == 0) {
+          atomicExch(err, 1);
+          bulk_wait_all();
+        }
+        return;
+      }
+      halo_combine(rn, tileBase + tn, u);
+    }
+    __syncthreads();  // stage s, gsb[s] and record slot n%3 are free again
+  }
+  if (tid == 0) bulk_wait_all();
+}
+
+// Host side: the 256-byte tile records of one level (offset + resolved faces).
+inline std::vector<pipe::TileRec> build_tile_records(const Level& L) {
+  std::vector<pipe::TileRec> recs(L.tiles.size());
+  for (size_t ti = 0; ti < L.tiles.size(); ti++) {
+    pipe::TileRec& r = recs[ti];
+    std::memset(&r, 0, sizeof(r));
+    r.off = L.tiles[ti].off;
+    for (int f = 0; f < 6; f++) {
+      const int* F = &L.face[(ti * 6 + f) * FACE_INTS];
+      pipe::FaceRes& fr = r.f[f];
+      fr.kind = F[F_KIND];
+      fr.nts = F[F_NTS];
+      fr.oa = F[F_OA];
+      fr.ob = F[F_OB];
+      fr.cov = F[F_COV];
+      fr.nOff = (fr.kind == FACE_SAME || fr.kind == FACE_COARSER) ? L.tiles[F[F_T0]].off : 0;
+      fr.ifOwn = fr.kind == FACE_COARSER ? L.ifOff[ti * 6 + f] : 0;
+    }
+  }
+  return recs;
+}

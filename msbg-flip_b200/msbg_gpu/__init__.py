@@ -202,7 +202,8 @@ class PressureCallbacks(C.Structure):
 class SolveParams(C.Structure):
     _fields_ = [("nPre", C.c_int), ("nPost", C.c_int), ("nCoarse", C.c_int),
                 ("maxIter", C.c_int), ("tol", C.c_float), ("innerIter", C.c_int),
-                ("storage", C.c_int), ("maxRefine", C.c_int), ("useGraph", C.c_int)]
+                ("storage", C.c_int), ("maxRefine", C.c_int), ("useGraph", C.c_int),
+                ("coarseScale", C.c_float)]
 
 
 class SolveInfo(C.Structure):
