@@ -158,7 +158,7 @@ typedef struct {
   int storage;      /* MSBG_F32, MSBG_F16 or MSBG_BF16 vectors */
   int maxRefine;    /* outer FP64 iterative-refinement steps (16-bit storage) */
   int useGraph;     /* capture one PCG iteration in a CUDA graph */
-  float coarseScale; /* coarse-grid correction over-correction factor (1 = plain) */
+  float coarseScale; /* coarse-grid correction factor (default 1.8; 1 = plain) */
 } msbg_gpu_solve_params;
 
 typedef struct {

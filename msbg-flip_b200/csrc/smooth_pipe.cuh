@@ -318,3 +318,204 @@ inline std::vector<pipe::TileRec> build_tile_records(const Level& L) {
   }
   return recs;
 }
+
+// ---------------------------------------------------------------------------
+// Persistent, TMA-pipelined operator application on 16^3 tiles (same
+// pipeline as the smoother, read-only on x, no colouring):
+//   APPLY_MATVEC:   q = A d, per-CTA partial d.q           (b unused)
+//   APPLY_RESIDUAL: r = b - A x, restricted into the coarse right-hand side
+//                   (sum over the liquid children, or copy for cells that do
+//                   not coarsen) through the tile's coarse map.
+// Thread (i, j, half) marches 8 cells of the z column (i, j) with a register
+// window; warps read shared memory without bank conflicts.
+// ---------------------------------------------------------------------------
+enum { APPLY_MATVEC = 0, APPLY_RESIDUAL = 1 };
+
+template <int MODE>
+__global__ void __launch_bounds__(pipe::NT, 1)
+    k_apply_pipe16(LevelView L, int tileBase, int count, const float* __restrict__ x,
+                   const float* __restrict__ b, float* __restrict__ y,
+                   float* __restrict__ bc, const int64_t* __restrict__ coarseOff,
+                   double* __restrict__ partial, int* __restrict__ err) {
+  using namespace pipe;
+  constexpr int NARR = MODE == APPLY_RESIDUAL ? 6 : 5;  // x, [b], a, cx, cy, cz
+  extern __shared__ __align__(128) float sm[];
+  float* stages[2] = {sm + GUARD, sm + GUARD + 6 * N};
+  float(*gsb)[6][TS * TS] = reinterpret_cast<float(*)[6][TS * TS]>(sm + GUARD + 12 * N);
+  TileRec* recs = reinterpret_cast<TileRec*>(sm + ZERO_FLOATS);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(recs + 3);
+  __shared__ int cmap[2][6];  // coarse tile, ox, oy, oz, aggregated, coarse ts
+  const TileRec* grec = reinterpret_cast<const TileRec*>(L.tileRec) + tileBase;
+  const int tid = threadIdx.x;
+  const int G = gridDim.x;
+  int t = blockIdx.x;
+  double acc = 0;
+  if (t < count) {
+    if (tid == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      mbar_init(&bar[2], 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    // stage arrays: 0 x, 1 b (residual), 2 a_ii, 3..5 couplings
+    auto issue_arrays = [&](const TileRec& r, float* st, uint64_t* br, int tRec, int slot) {
+      fence_proxy_async();
+      const bool rec = tRec < count;
+      mbar_expect_tx(br, NARR * N * sizeof(float) + (rec ? sizeof(TileRec) : 0));
+      const int64_t off = r.off;
+      bulk_g2s(st + 0 * N, x + off, N * sizeof(float), br);
+      if (MODE == APPLY_RESIDUAL) bulk_g2s(st + 1 * N, b + off, N * sizeof(float), br);
+      bulk_g2s(st + 2 * N, L.diag + off, N * sizeof(float), br);
+      bulk_g2s(st + 3 * N, L.cx + off, N * sizeof(float), br);
+      bulk_g2s(st + 4 * N, L.cy + off, N * sizeof(float), br);
+      bulk_g2s(st + 5 * N, L.cz + off, N * sizeof(float), br);
+      if (rec) bulk_g2s(&recs[slot], grec + tRec, sizeof(TileRec), br);
+    };
+    float hx[3], hc[3];
+    auto halo_issue = [&](const TileRec& r, int ti, int u) {
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const int g = tid + NT * q, f = g >> 8, c = g & 255;
+        halo_load(L, x, r.f[f], f >> 1, f & 1, c & 15, c >> 4, hx[q], hc[q]);
+      }
+      if (MODE == APPLY_RESIDUAL && tid < 6) cmap[u][tid] = L.toCoarse[(size_t)ti * 6 + tid];
+    };
+    auto halo_combine = [&](const TileRec& r, int ti, int u) {
+      const float* st = stages[u];
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const int g = tid + NT * q, f = g >> 8, c = g & 255;
+        const int dir = f >> 1, side = f & 1, a = c & 15, bb = c >> 4;
+        const int kind = r.f[f].kind;
+        float v = 0.f;
+        if (kind == FACE_SAME) {
+          const float cown = st[(3 + dir) * N + plane_idx(TS, dir, 0, a, bb)];
+          v = (side ? hc[q] : cown) * hx[q];
+        } else if (kind == FACE_COARSER) {
+          v = hc[q] * hx[q];
+        } else if (kind == FACE_FINER) {
+          v = ghost_sum(L, x, ti, TS, dir, side, a, bb);
+        }
+        gsb[u][f][c] = v;
+      }
+    };
+    if (tid == 0) {
+      mbar_expect_tx(&bar[2], sizeof(TileRec));
+      bulk_g2s(&recs[0], grec + t, sizeof(TileRec), &bar[2]);
+    }
+    bool ok = __syncthreads_and(mbar_wait(&bar[2], 0));
+    if (ok) {
+      if (tid == 0) issue_arrays(recs[0], stages[0], &bar[0], t + G, 1);
+      halo_issue(recs[0], tileBase + t, 0);
+      ok = __syncthreads_and(mbar_wait(&bar[0], 0));
+      if (!ok && tid == 0) mbar_wait(&bar[0], 0);
+    }
+    if (!ok) {
+      if (tid == 0) atomicExch(err, 1);
+      t = count;  // skip the loop, still write this CTA's partial
+    } else {
+      halo_combine(recs[0], tileBase + t, 0);
+      __syncthreads();
+    }
+    const int i = tid & 15, j = (tid >> 4) & 15, kh = tid >> 8;
+    for (int n = 0; t < count; n++, t += G) {
+      const int s = n & 1, u = s ^ 1;
+      const int tn = t + G;
+      const bool hasNext = tn < count;
+      const TileRec& rc = recs[n % 3];
+      const TileRec& rn = recs[(n + 1) % 3];
+      if (hasNext) {
+        if (tid == 0) {
+          bulk_wait_read();
+          issue_arrays(rn, stages[u], &bar[u], tn + G, (n + 2) % 3);
+        }
+        halo_issue(rn, tileBase + tn, u);
+      }
+      float* X = stages[s];
+      const float* B = X + N;
+      const float* D = X + 2 * N;
+      const float* CX = X + 3 * N;
+      const float* CY = X + 4 * N;
+      const float* CZ = X + 5 * N;
+      const float(*gs)[TS * TS] = gsb[s];
+      float* Y = X + 2 * N;  // results overwrite the a_ii array in place (each
+                             // thread reads its own a_ii before writing it)
+      const int k0 = 8 * kh;
+      float xm = k0 > 0 ? X[tidx(TS, i, j, k0 - 1)] : 0.f;
+      float xc = X[tidx(TS, i, j, k0)];
+      float yv[8];
+#pragma unroll
+      for (int kk = 0; kk < 8; kk++) {
+        const int k = k0 + kk, e = tidx(TS, i, j, k);
+        const float xp = k < TS - 1 ? X[e + TS * TS] : 0.f;
+        const float dg = D[e];
+        float S = 0.f;
+        S += i > 0 ? CX[e] * X[e - 1] : gs[0][j + TS * k];
+        S += i < TS - 1 ? CX[e + 1] * X[e + 1] : gs[1][j + TS * k];
+        S += j > 0 ? CY[e] * X[e - TS] : gs[2][i + TS * k];
+        S += j < TS - 1 ? CY[e + TS] * X[e + TS] : gs[3][i + TS * k];
+        S += k > 0 ? CZ[e] * xm : gs[4][i + TS * j];
+        S += k < TS - 1 ? CZ[e + TS * TS] * xp : gs[5][i + TS * j];
+        float v = 0.f;
+        if (dg > 0.f) v = dg * xc - S;
+        if (MODE == APPLY_RESIDUAL) {
+          if (dg > 0.f) v = B[e] - v;
+        } else {
+          acc += (double)xc * (double)v;
+        }
+        yv[kk] = v;
+        xm = xc;
+        xc = xp;
+      }
+      __syncthreads();  // every thread has read its D / neighbours before Y is written
+#pragma unroll
+      for (int kk = 0; kk < 8; kk++) Y[tidx(TS, i, j, k0 + kk)] = yv[kk];
+      __syncthreads();
+      if (MODE == APPLY_MATVEC) {
+        if (tid == 0) {
+          fence_proxy_async();
+          bulk_s2g(y + rc.off, Y, N * sizeof(float));
+        }
+      } else {
+        const int* tc = cmap[s];
+        const int ct = tc[0];
+        if (ct >= 0) {
+          float* dst = bc + coarseOff[ct];
+          const int ox = tc[1], oy = tc[2], oz = tc[3], cts = tc[5];
+          if (tc[4]) {
+            constexpr int H = TS / 2;
+            const int c = tid;  // 512 coarse cells, one per thread
+            const int ci = c % H, cj = (c / H) % H, ck = c / (H * H);
+            const int e = tidx(TS, 2 * ci, 2 * cj, 2 * ck);
+            const float sum = Y[e] + Y[e + 1] + Y[e + TS] + Y[e + TS + 1] + Y[e + TS * TS] +
+                              Y[e + TS * TS + 1] + Y[e + TS * TS + TS] +
+                              Y[e + TS * TS + TS + 1];
+            dst[tidx(cts, ox + ci, oy + cj, oz + ck)] = sum;
+          } else {
+            for (int e = tid; e < N; e += NT) {
+              const int ii = e % TS, jj = (e / TS) % TS, kk = e / (TS * TS);
+              dst[tidx(cts, ox + ii, oy + jj, oz + kk)] = Y[e];
+            }
+          }
+        }
+      }
+      if (hasNext) {
+        if (!__syncthreads_and(mbar_wait(&bar[u], ((n + 1) >> 1) & 1))) {
+          if (tid == 0) {
+            atomicExch(err, 1);
+            bulk_wait_all();
+          }
+          break;
+        }
+        halo_combine(rn, tileBase + tn, u);
+      }
+      __syncthreads();
+    }
+    if (tid == 0) bulk_wait_all();
+  }
+  if (MODE == APPLY_MATVEC && partial) {
+    acc = block_sum(acc);
+    if (tid == 0) partial[blockIdx.x] = acc;
+  }
+}
