@@ -156,7 +156,10 @@ typedef struct {
   float tol;        /* stop when |r| <= tol*|b| */
   int innerIter;    /* red-black sweeps inside a tile per smoother visit */
   int storage;      /* MSBG_F32, MSBG_F16 or MSBG_BF16 vectors */
-  int maxRefine;    /* outer FP64 iterative-refinement steps (16-bit storage) */
+  int maxRefine;    /* 0: plain MGPCG stopping on the recursive residual (as the
+                       reference); >0: up to maxRefine outer steps of FP64
+                       iterative refinement (FP64 solution and residual, FP32
+                       inner MGPCG) stopping on the true FP64 residual */
   int useGraph;     /* capture one PCG iteration in a CUDA graph */
   float coarseScale; /* coarse-grid correction factor (default 1.8; 1 = plain) */
 } msbg_gpu_solve_params;
@@ -165,7 +168,9 @@ typedef struct {
   int iterations;        /* PCG iterations (summed over refinement steps) */
   int refinements;       /* outer refinement steps taken */
   int status;            /* 0 converged, 1 maxIter, 2 breakdown, 3 non-finite */
-  double relResidual;    /* |b - A x| / |b|, recomputed in FP64 at the end */
+  double relResidual;    /* true |b - A x| / |b| of the delivered iterate: FP32
+                            operator and iterate for maxRefine = 0, FP64 for
+                            the refined solve */
   double solveSeconds;   /* device time of the solve */
   int64_t fineCells;     /* cells of MG level 0 (liquid) */
   int nMgLevels;
@@ -189,6 +194,9 @@ int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_params* p,
 /* Pressure of MG level 0 in the reference's block layout: for every block in
  * ascending bid order, (bsx0>>level)^3 values, vid = x + y*bs + z*bs*bs. */
 int msbg_gpu_pressure_download(msbg_gpu_ctx* ctx, float* packed, int64_t n);
+/* Same layout in FP64: the refined solution (available after a solve with
+ * maxRefine > 0; the FP32 download then holds it rounded to FP32). */
+int msbg_gpu_pressure_download64(msbg_gpu_ctx* ctx, double* packed, int64_t n);
 /* Same layout, the right-hand side b (volume-integrated) of MG level 0. */
 int msbg_gpu_pressure_download_rhs(msbg_gpu_ctx* ctx, float* packed, int64_t n);
 /* Number of values in that layout. */

@@ -351,6 +351,7 @@ __global__ void __launch_bounds__(TS* TS) k_smooth(LevelView L, const int* __res
 }
 
 #include "smooth_pipe.cuh"
+#include "refine.cuh"
 
 // Coarsest level: x = A^-1 b with the dense FP64 inverse (symmetric).
 __global__ void __launch_bounds__(512) k_coarse_solve(const double* __restrict__ Ainv, int n,
@@ -384,6 +385,7 @@ struct Solver {
   std::vector<LevelView> views;
   DeviceBuffer dCoarseInv, dCoarseCells;
   DeviceBuffer rhs0, d0, q0, z0, r0, partial, scal;
+  DeviceBuffer x64, rin;  // FP64 solution and inner right-hand side of the refinement
   int maxPartial = 0;
   Scalars* hScal = nullptr;  // pinned
   int bsx0 = 0, nbx = 0, nby = 0, nbz = 0;
@@ -558,7 +560,7 @@ extern "C" void msbg_gpu_solve_params_default(msbg_gpu_solve_params* p) {
   p->tol = 1e-6f;
   p->innerIter = 2;
   p->storage = MSBG_F32;
-  p->maxRefine = 4;
+  p->maxRefine = 0;  // plain MGPCG on the recursive residual, as the reference
   p->useGraph = 1;
   // Piecewise-constant transfers with Galerkin coarse operators under-correct
   // smooth errors; scaling the coarse correction by 1.8 restores
@@ -683,12 +685,127 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
   return MSBG_OK;
 }
 
+namespace {
+
+struct PcgResult {
+  int iters = 0;
+  int status = 1;  // 0 converged, 1 maxIter, 2 breakdown, 3 non-finite
+  double bb = 0;
+};
+
+// MGPCG on MG level 0 for A e = bin from e = 0 (e in the level-0 x vector),
+// stopping at |r| <= tolRel |bin| (recursive residual, as the reference).
+// One iteration is one CUDA graph launch; the graph is captured on the first
+// call and reused (all buffers are fixed).
+int run_pcg(msbg_gpu_ctx* ctx, Solver& S, Runner& R, const float* bin, double tolRel, int maxIter,
+            bool useGraph, cudaGraphExec_t& exec, int64_t& perIter, PcgResult& out) {
+  cudaStream_t st = R.st;
+  const int64_t n = S.H.levels[0].nCells;
+  float* x = S.dev[0]->x.as<float>();
+  float* r = S.r0.as<float>();
+  float* d = S.d0.as<float>();
+  float* q = S.q0.as<float>();
+  float* z = S.z0.as<float>();
+  double* part = S.partial.as<double>();
+  Scalars* sc = S.scal.as<Scalars>();
+  // r = b, x = 0, bb = b.b, z = V(r), rho = r.z, d = z
+  cudaMemsetAsync(sc, 0, sizeof(Scalars), st);
+  cudaMemsetAsync(x, 0, sizeof(float) * n, st);
+  cudaMemcpyAsync(r, bin, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+  k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(bin, bin, n, part);
+  k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_BB);
+  R.vcycle(0, z, r);
+  k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
+  k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHO);
+  cudaMemcpyAsync(d, z, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  R.launches += 4;
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  out = PcgResult();
+  out.bb = S.hScal->bb;
+  if (!(out.bb > 1e-300)) {
+    out.status = 0;
+    return MSBG_OK;
+  }
+  auto iteration = [&]() {
+    R.launches += 6;  // finalize x3, axpy_norm, dot, update_d
+    int nt = R.matvec_dot(d, q, part);
+    k_finalize<<<1, 1024, 0, st>>>(part, nt, sc, FIN_DQ_ALPHA);
+    k_axpy_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x, r, d, q, n, sc, part);
+    k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
+    R.vcycle(0, z, r);
+    k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
+    k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHONEW_BETA);
+    k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, n, sc);
+    cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  };
+  if (useGraph && !exec) {
+    const int64_t before = R.launches;
+    cudaGraph_t g;
+    MSBG_CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    iteration();
+    MSBG_CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
+    perIter = R.launches - before;
+    R.launches = before;
+    MSBG_CUDA_TRY(ctx, cudaGraphInstantiate(&exec, g, 0));
+    cudaGraphDestroy(g);
+  }
+  const double tol2 = tolRel * tolRel;
+  for (int it = 0; it < maxIter; it++) {
+    if (exec) {
+      MSBG_CUDA_TRY(ctx, cudaGraphLaunch(exec, st));
+      R.launches += perIter;
+    } else {
+      iteration();
+    }
+    MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    out.iters = it + 1;
+    const Scalars hs = *S.hScal;
+    if (hs.status) {
+      // a breakdown found before the update leaves x, r unchanged
+      out.status = hs.status;
+      break;
+    }
+    if (hs.rr <= tol2 * out.bb) {
+      out.status = 0;
+      break;
+    }
+  }
+  return MSBG_OK;
+}
+
+// r32 = b - A x64 (FP64) on level 0; returns |r|^2 in *rr.
+int residual64(msbg_gpu_ctx* ctx, Solver& S, Runner& R, const float* b, float* r32,
+               double* rr) {
+  cudaStream_t st = R.st;
+  const Level& L = S.H.levels[0];
+  double* part = S.partial.as<double>();
+  int off = 0;
+  for (const auto& g : L.groups) {
+    const int* lst = S.dev[0]->groupTiles.as<int>() + g.start;
+    TS_DISPATCH(g.ts, (k_residual64<T><<<g.count, T * T, 0, st>>>(
+                          S.views[0], lst, S.x64.as<double>(), b, r32, part + off)));
+    off += g.count;
+    R.launches++;
+  }
+  Scalars* sc = S.scal.as<Scalars>();
+  k_finalize<<<1, 1024, 0, st>>>(part, off, sc, FIN_RR);
+  cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  R.launches++;
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  *rr = S.hScal->rr;
+  return MSBG_OK;
+}
+
+}  // namespace
+
 extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_params* p,
                                        msbg_gpu_solve_info* info) {
   if (!ctx || !p) return MSBG_EINVARG;
   auto& sp = solver_of(ctx);
   if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
-  if (p->nPre < 0 || p->nPost < 0 || p->maxIter < 0 || p->innerIter < 1 || !(p->tol >= 0))
+  if (p->nPre < 0 || p->nPost < 0 || p->maxIter < 0 || p->innerIter < 1 || !(p->tol >= 0) ||
+      p->maxRefine < 0)
     return set_error(ctx, MSBG_EINVARG, "invalid solve parameters");
   if (p->storage != MSBG_F32)
     return set_error(ctx, MSBG_ENOTIMPL, "storage type %d not available", p->storage);
@@ -701,111 +818,98 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
   R.numSMs = S.numSMs;
   const Level& L0 = S.H.levels[0];
   const int64_t n = L0.nCells;
-  LevelDev& D0 = *S.dev[0];
-  float* x = D0.x.as<float>();
-  float* r = S.r0.as<float>();
-  float* d = S.d0.as<float>();
-  float* q = S.q0.as<float>();
-  float* z = S.z0.as<float>();
+  float* x = S.dev[0]->x.as<float>();
   const float* b = S.rhs0.as<float>();
-  double* part = S.partial.as<double>();
-  Scalars* sc = S.scal.as<Scalars>();
-
+  if (p->maxRefine > 0) {
+    MSBG_CUDA_TRY(ctx, S.x64.ensure(sizeof(double) * n));
+    MSBG_CUDA_TRY(ctx, S.rin.ensure(sizeof(float) * n));
+  }
+  cudaGraphExec_t exec = nullptr;
+  int64_t perIter = 0;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
-  // r = b, x = 0, bb = b.b, z = V(r), rho = r.z, d = z
-  cudaMemsetAsync(sc, 0, sizeof(Scalars), st);
-  cudaMemsetAsync(x, 0, sizeof(float) * n, st);
-  cudaMemcpyAsync(r, b, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
-  k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(b, b, n, part);
-  k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_BB);
-  R.vcycle(0, z, r);
-  k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
-  k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHO);
-  cudaMemcpyAsync(d, z, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
-  cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
-  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  const double bb = S.hScal->bb;
-  int iters = 0, status = 1;
-  if (!(bb > 1e-30)) {
-    status = 0;
-  } else {
-    auto iteration = [&]() {
-      R.launches += 6;  // finalize x3, axpy_norm, dot, update_d
-      int nt = R.matvec_dot(d, q, part);
-      k_finalize<<<1, 1024, 0, st>>>(part, nt, sc, FIN_DQ_ALPHA);
-      k_axpy_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x, r, d, q, n, sc, part);
+  int iters = 0, status = 1, refinements = 0;
+  double relres = 0;
+  int rc = MSBG_OK;
+  if (p->maxRefine == 0) {
+    PcgResult pr;
+    rc = run_pcg(ctx, S, R, b, p->tol, p->maxIter, p->useGraph, exec, perIter, pr);
+    iters = pr.iters;
+    status = pr.status;
+    cudaEventRecord(e1, st);
+    if (rc == MSBG_OK) {
+      // true residual of the FP32 iterate, FP32 operator, FP64 norm
+      float* q = S.q0.as<float>();
+      float* z = S.z0.as<float>();
+      float* d = S.d0.as<float>();
+      double* part = S.partial.as<double>();
+      Scalars* sc = S.scal.as<Scalars>();
+      R.matvec_dot(x, q, part);
+      cudaMemcpyAsync(z, b, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+      Scalars one{};
+      one.alpha = 1.0;
+      cudaMemcpyAsync(sc, &one, sizeof(Scalars), cudaMemcpyHostToDevice, st);
+      k_axpy_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, q, q, n, sc, part);  // z = b - q
       k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
-      R.vcycle(0, z, r);
-      k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
-      k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHONEW_BETA);
-      k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, n, sc);
       cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
-    };
-    R.launches += 4;  // initial dot/finalize pairs
-    cudaGraphExec_t exec = nullptr;
-    int64_t perIter = 0;
-    if (p->useGraph) {
-      const int64_t before = R.launches;
-      cudaGraph_t g;
-      MSBG_CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      iteration();
-      MSBG_CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
-      perIter = R.launches - before;
-      R.launches = before;
-      MSBG_CUDA_TRY(ctx, cudaGraphInstantiate(&exec, g, 0));
-      cudaGraphDestroy(g);
+      cudaStreamSynchronize(st);
+      relres = pr.bb > 0 ? std::sqrt(S.hScal->rr / pr.bb) : 0.0;
     }
-    const double tol2 = (double)p->tol * (double)p->tol;
-    for (int it = 0; it < p->maxIter; it++) {
-      if (exec) {
-        MSBG_CUDA_TRY(ctx, cudaGraphLaunch(exec, st));
-        R.launches += perIter;
-      } else {
-        iteration();
-      }
-      MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-      iters = it + 1;
-      const Scalars hs = *S.hScal;
-      if (hs.status) {
-        // a breakdown found before the update leaves x, r unchanged
-        status = hs.status;
-        break;
-      }
-      if (hs.rr <= tol2 * bb) {
+  } else {
+    // FP64 iterative refinement around the FP32 MGPCG
+    double* x64 = S.x64.as<double>();
+    float* rin = S.rin.as<float>();
+    cudaMemsetAsync(x64, 0, sizeof(double) * n, st);
+    double bb = 0, rr = 0;
+    for (int outer = 0;; outer++) {
+      rc = residual64(ctx, S, R, b, rin, &rr);
+      if (rc) break;
+      if (outer == 0) bb = rr;
+      relres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+      if (!(bb > 1e-300) || relres <= p->tol) {
         status = 0;
         break;
       }
+      if (!std::isfinite(rr)) {
+        status = 3;
+        break;
+      }
+      if (outer >= p->maxRefine || iters >= p->maxIter) {
+        status = 1;
+        break;
+      }
+      // inner tolerance: what is still missing, not below the FP32 floor
+      const double need = p->tol / std::max(relres, 1e-300);
+      const double tolIn = std::min(0.5, std::max(need * 0.5, 1e-5));
+      PcgResult pr;
+      rc = run_pcg(ctx, S, R, rin, tolIn, p->maxIter - iters, p->useGraph, exec, perIter, pr);
+      if (rc) break;
+      iters += pr.iters;
+      refinements++;
+      if (pr.status >= 2) {
+        status = pr.status;
+        break;
+      }
+      k_add64<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, x, n);
+      R.launches++;
     }
-    if (exec) cudaGraphExecDestroy(exec);
+    k_narrow<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x, x64, n);
+    cudaEventRecord(e1, st);
   }
-  cudaEventRecord(e1, st);
-  // true residual |b - A x| (FP32 operator, FP64 norm)
-  int nt = R.matvec_dot(x, q, part);
-  (void)nt;
-  // q = A x; r_true = b - q -> reuse k_axpy_norm with alpha=-1 over (r=b copy)
-  cudaMemcpyAsync(z, b, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
-  {
-    Scalars one{};
-    one.alpha = 1.0;
-    cudaMemcpyAsync(sc, &one, sizeof(Scalars), cudaMemcpyHostToDevice, st);
-    // z = b - 1*q (x argument gets d += q which is harmless: use q as x dummy)
-    k_axpy_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, q, q, n, sc, part);
-    k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
-    cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
-  }
+  if (exec) cudaGraphExecDestroy(exec);
   MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (rc) return rc;
   if (info) {
     info->iterations = iters;
-    info->refinements = 0;
+    info->refinements = refinements;
     info->status = status;
-    info->relResidual = bb > 0 ? std::sqrt(S.hScal->rr / bb) : 0.0;
+    info->relResidual = relres;
     info->solveSeconds = ms * 1e-3;
     info->fineCells = L0.nFluid;
     info->nMgLevels = (int)S.H.levels.size();
@@ -951,6 +1055,39 @@ extern "C" int msbg_gpu_pressure_download(msbg_gpu_ctx* ctx, float* packed, int6
   cudaSetDevice(ctx->device);
   MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return to_packed(ctx, *sp, sp->dev[0]->x.as<float>(), packed, n);
+}
+
+extern "C" int msbg_gpu_pressure_download64(msbg_gpu_ctx* ctx, double* packed, int64_t n) {
+  if (!ctx || !packed) return MSBG_EINVARG;
+  auto& sp = solver_of(ctx);
+  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
+  Solver& S = *sp;
+  if (!S.x64.p) return set_error(ctx, MSBG_EINVARG, "no FP64 solution (solve with maxRefine > 0)");
+  cudaSetDevice(ctx->device);
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  const Level& L = S.H.levels[0];
+  std::vector<double> h(L.nCells);
+  MSBG_CUDA_TRY(ctx, cudaMemcpy(h.data(), S.x64.p, sizeof(double) * L.nCells,
+                                cudaMemcpyDeviceToHost));
+  const int64_t nb = (int64_t)S.nbx * S.nby * S.nbz;
+  std::vector<int64_t> boff(nb + 1, 0);
+  for (int64_t b = 0; b < nb; b++) {
+    const int bs = S.bsx0 >> S.blockLevel[b];
+    boff[b + 1] = boff[b] + (int64_t)bs * bs * bs;
+  }
+  if (n < boff[nb]) return set_error(ctx, MSBG_EINVARG, "packed buffer too small");
+  std::memset(packed, 0, sizeof(double) * boff[nb]);
+  for (const Tile& t : L.tiles)
+    for (int k = 0; k < t.ts; k++)
+      for (int j = 0; j < t.ts; j++)
+        for (int i = 0; i < t.ts; i++) {
+          const int X = t.ox + i, Y = t.oy + j, Z = t.oz + k;
+          const int bs = S.bsx0 >> t.level;
+          const int64_t b = (X / bs) + (int64_t)S.nbx * ((Y / bs) + (int64_t)S.nby * (Z / bs));
+          packed[boff[b] + (X % bs) + (int64_t)bs * ((Y % bs) + (int64_t)bs * (Z % bs))] =
+              h[t.off + i + (int64_t)t.ts * (j + (int64_t)t.ts * k)];
+        }
+  return MSBG_OK;
 }
 
 extern "C" int msbg_gpu_pressure_download_rhs(msbg_gpu_ctx* ctx, float* packed, int64_t n) {

@@ -39,48 +39,49 @@ __host__ __device__ __forceinline__ int plane_idx(int ts, int dir, int p, int a,
 }
 
 // Sum over the neighbours across face (dir, side) of face cell (a,b) of tile
-// ti: coupling * x(neighbour).  x = vector of this level.
-template <typename XT>
-__host__ __device__ __forceinline__ float ghost_sum(const LevelView& L, const XT* __restrict__ x, int ti,
-                                           int ts, int dir, int side, int a, int b) {
+// ti: coupling * x(neighbour), accumulated in AT.  x = vector of this level.
+template <typename XT, typename AT = float>
+__host__ __device__ __forceinline__ AT ghost_sum(const LevelView& L, const XT* __restrict__ x,
+                                                 int ti, int ts, int dir, int side, int a,
+                                                 int b) {
   const int* F = L.face + ((size_t)ti * 6 + dir * 2 + side) * FACE_INTS;
   const int kind = F[F_KIND];
-  if (kind == FACE_NONE) return 0.f;
+  if (kind == FACE_NONE) return AT(0);
   const float* cd = dir == 0 ? L.cx : dir == 1 ? L.cy : L.cz;
   if (kind == FACE_SAME) {
     const int nb = F[F_T0];
     const int64_t no = L.tileOff[nb];
     const int pn = side ? 0 : ts - 1;
-    const float xn = (float)x[no + plane_idx(ts, dir, pn, a, b)];
-    const float c = side ? cd[no + plane_idx(ts, dir, 0, a, b)]
-                         : cd[L.tileOff[ti] + plane_idx(ts, dir, 0, a, b)];
+    const AT xn = (AT)x[no + plane_idx(ts, dir, pn, a, b)];
+    const AT c = side ? (AT)cd[no + plane_idx(ts, dir, 0, a, b)]
+                      : (AT)cd[L.tileOff[ti] + plane_idx(ts, dir, 0, a, b)];
     return c * xn;
   }
   if (kind == FACE_COARSER) {
     const int nb = F[F_T0], nts = F[F_NTS];
     const int64_t no = L.tileOff[nb];
     const int pn = side ? 0 : nts - 1;
-    const float xn = (float)x[no + plane_idx(nts, dir, pn, F[F_OA] + (a >> 1), F[F_OB] + (b >> 1))];
-    const float c = L.ifc[L.ifOff[(size_t)ti * 6 + dir * 2 + side] + a + ts * b];
+    const AT xn = (AT)x[no + plane_idx(nts, dir, pn, F[F_OA] + (a >> 1), F[F_OB] + (b >> 1))];
+    const AT c = (AT)L.ifc[L.ifOff[(size_t)ti * 6 + dir * 2 + side] + a + ts * b];
     return c * xn;
   }
   // FACE_FINER
   const int cov = F[F_COV], nts = F[F_NTS];
   const int per = ts / cov;
   const int nb = F[F_T0 + (a / cov) + per * (b / cov)];
-  if (nb < 0) return 0.f;
+  if (nb < 0) return AT(0);
   const int64_t no = L.tileOff[nb];
   const int64_t io = L.ifOff[(size_t)nb * 6 + dir * 2 + (1 - side)];
-  if (io < 0) return 0.f;
+  if (io < 0) return AT(0);
   const int pn = side ? 0 : nts - 1;
   const int fa0 = 2 * (a % cov), fb0 = 2 * (b % cov);
-  float s = 0.f;
+  AT s = AT(0);
 #pragma unroll
   for (int v = 0; v < 2; v++)
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       const int fa = fa0 + u, fb = fb0 + v;
-      s += L.ifc[io + fa + nts * fb] * (float)x[no + plane_idx(nts, dir, pn, fa, fb)];
+      s += (AT)L.ifc[io + fa + nts * fb] * (AT)x[no + plane_idx(nts, dir, pn, fa, fb)];
     }
   return s;
 }

@@ -1,0 +1,67 @@
+// FP64 outer iterative refinement of the pressure solve (included inside
+// namespace msbg::ps of pressure.cu after the reduction helpers).
+//
+// The solution is accumulated in FP64; each outer step recomputes
+// r = b - A x in FP64 (FP32 operator entries widened exactly, FP64 sums),
+// hands r to the inner MGPCG as its right-hand side and adds the inner
+// correction to x in FP64.  This is what lets the true residual reach 1e-6
+// where an FP32 iterate cannot represent it.
+
+// r32 = b - A x64 on MG level 0 (one CTA per tile, thread (i,j) owns the z
+// column), per-CTA partial |r|^2 in FP64.
+template <int TS>
+__global__ void __launch_bounds__(TS* TS) k_residual64(LevelView L, const int* __restrict__ tiles,
+                                                       const double* __restrict__ x,
+                                                       const float* __restrict__ b,
+                                                       float* __restrict__ r,
+                                                       double* __restrict__ partial) {
+  constexpr int N = TS * TS * TS, NT = TS * TS;
+  __shared__ double xs[N];
+  __shared__ double gs[6][NT];
+  const int ti = tiles[blockIdx.x];
+  const int64_t off = L.tileOff[ti];
+  const int t = threadIdx.x, i = t % TS, j = t / TS;
+  for (int e = t; e < N; e += NT) xs[e] = x[off + e];
+#pragma unroll
+  for (int f = 0; f < 6; f++) gs[f][t] = ghost_sum<double, double>(L, x, ti, TS, f >> 1, f & 1, i, j);
+  __syncthreads();
+  const float* cx = L.cx + off;
+  const float* cy = L.cy + off;
+  const float* cz = L.cz + off;
+  double acc = 0;
+  for (int k = 0; k < TS; k++) {
+    const int e = tidx(TS, i, j, k);
+    const double dg = L.diag[off + e];
+    double rv = 0;
+    if (dg > 0) {
+      double S = 0;
+      S += (i > 0) ? (double)cx[e] * xs[e - 1] : gs[0][j + TS * k];
+      S += (i < TS - 1) ? (double)cx[e + 1] * xs[e + 1] : gs[1][j + TS * k];
+      S += (j > 0) ? (double)cy[e] * xs[e - TS] : gs[2][i + TS * k];
+      S += (j < TS - 1) ? (double)cy[e + TS] * xs[e + TS] : gs[3][i + TS * k];
+      S += (k > 0) ? (double)cz[e] * xs[e - TS * TS] : gs[4][i + TS * j];
+      S += (k < TS - 1) ? (double)cz[e + TS * TS] * xs[e + TS * TS] : gs[5][i + TS * j];
+      rv = (double)b[off + e] - (dg * xs[e] - S);
+    }
+    r[off + e] = (float)rv;
+    acc += rv * rv;
+  }
+  acc = block_sum(acc);
+  if (t == 0) partial[blockIdx.x] = acc;
+}
+
+// x64 += e (all cells; e is 0 off the liquid)
+__global__ void __launch_bounds__(512) k_add64(double* __restrict__ x, const float* __restrict__ e,
+                                               int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += (double)e[i];
+}
+
+// x32 = (float) x64
+__global__ void __launch_bounds__(512) k_narrow(float* __restrict__ y, const double* __restrict__ x,
+                                                int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = (float)x[i];
+}

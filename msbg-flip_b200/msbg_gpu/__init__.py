@@ -232,6 +232,7 @@ def _pressure_sigs(L):
         "msbg_gpu_pressure_solve": (i32, [vp, C.POINTER(SolveParams), C.POINTER(SolveInfo)]),
         "msbg_gpu_pressure_download": (i32, [vp, C.POINTER(C.c_float), C.c_int64]),
         "msbg_gpu_pressure_download_rhs": (i32, [vp, C.POINTER(C.c_float), C.c_int64]),
+        "msbg_gpu_pressure_download64": (i32, [vp, C.POINTER(C.c_double), C.c_int64]),
         "msbg_gpu_pressure_packed_size": (i32, [vp, C.POINTER(C.c_int64)]),
         "msbg_gpu_pressure_stats": (i32, [vp, C.POINTER(PressureStats)]),
         "msbg_gpu_pressure_profile": (i32, [vp, i32, i32, i32, C.POINTER(C.c_double),
@@ -339,9 +340,14 @@ def count_liquid_cells(scene):
     return int(fluid[0])
 
 
-def _ctx_pressure_download(self, rhs=False):
+def _ctx_pressure_download(self, rhs=False, fp64=False):
     n = C.c_int64()
     self._check(self._L.msbg_gpu_pressure_packed_size(self._h, C.byref(n)), "packed_size")
+    if fp64:
+        out = np.zeros(n.value, np.float64)
+        self._check(self._L.msbg_gpu_pressure_download64(self._h, _p(out, C.c_double), n.value),
+                    "pressure_download64")
+        return out
     out = np.zeros(n.value, np.float32)
     fn = self._L.msbg_gpu_pressure_download_rhs if rhs else self._L.msbg_gpu_pressure_download
     self._check(fn(self._h, _p(out, C.c_float), n.value), "pressure_download")

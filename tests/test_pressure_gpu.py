@@ -58,3 +58,23 @@ def test_solve_without_prepare_is_an_error():
     with pytest.raises(msbg_gpu.MsbgError):
         ctx.pressure_solve(tol=1e-6)
     ctx.close()
+
+
+@pytest.mark.parametrize("res,bsx0,nl,band", [(128, 16, 2, 8.0), (128, 32, 2, 8.0),
+                                              (128, 16, 3, 4.0)])
+def test_fp64_refinement_reaches_true_residual_and_oracle(gpu_ctx, res, bsx0, nl, band):
+    """Outer FP64 refinement: true residual <= 1e-6, error vs FP64 oracle <= 1e-5."""
+    s = msbg_gpu.PressureScene(res, bsx0, nl, band=band, seed=11)
+    gpu_ctx.pressure_prepare(s)
+    info = gpu_ctx.pressure_solve(tol=1e-6, maxRefine=4)
+    assert info.status == 0
+    assert info.relResidual <= 1e-6, info.relResidual
+    assert info.refinements >= 1
+    xo, bo, it, rr = oracle.pressure_oracle(s, tol=1e-12)
+    x64 = gpu_ctx.pressure_download(fp64=True)
+    x32 = gpu_ctx.pressure_download()
+    assert rel_err(x64, xo) <= 1e-5, rel_err(x64, xo)
+    assert rel_err(x32, xo) <= 1e-5, rel_err(x32, xo)
+    # the FP64 iterate's residual, recomputed by the oracle's own matrix
+    r = bo - oracle.pressure_apply_oracle(s, x64)
+    assert np.linalg.norm(r) <= 1.5e-6 * np.linalg.norm(bo)
