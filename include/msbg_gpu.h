@@ -133,6 +133,30 @@ int msbg_gpu_pde_mcf_device(msbg_gpu_ctx* ctx, float* pool, const int* slotOf,
                             float fullVal, int numIter, float dt, int clamp01,
                             void* stream);
 
+/* Same smoother for callers that cannot let this library allocate device
+ * memory.  No counterpart in the reference (its smoother runs on host memory).
+ * Who needs it: simulation codes that reserve all device memory up front with
+ * their own pool allocator, where a cudaMalloc from a library fails or
+ * fragments that pool, and host threads that must not block in the CUDA
+ * allocator's device-wide synchronisation during a time step.
+ *   pool, slotOf   caller-owned device arrays, as for msbg_gpu_pde_mcf_device
+ *   blockList, n   host array of the block ids to update (value blocks only)
+ *   stream         cudaStream_t as void* (NULL = legacy default stream)
+ *   timedOut       NULL: return right after the launches; non-NULL: wait for
+ *                  the stream and report whether a bounded wait gave up
+ * No context, no cudaMalloc/cudaFree: the colour-grouped block list and the
+ * error flag live in a fixed device array of 2*MSBG_MCF_NOALLOC_MAX_BLOCKS+16
+ * ints (2 MB) that every device using this library keeps until the process
+ * exits.  n > MSBG_MCF_NOALLOC_MAX_BLOCKS is rejected with MSBG_EINVARG.
+ * The first call on a device looks up that array's device address; make
+ * that first call before any stream capture.  All calls on a device share
+ * the array (each call resets what must start at zero), so calls whose work
+ * overlaps on the GPU race: serialise them on one stream. */
+#define MSBG_MCF_NOALLOC_MAX_BLOCKS 262144
+int msbg_gpu_pde_mcf_noalloc(float* pool, const int* slotOf, const int* blockList, int n,
+                             int nbx, int nby, int nbz, int bsx, float emptyVal, float fullVal,
+                             int numIter, float dt, int clamp01, void* stream, int* timedOut);
+
 /* ---- FLIP pressure solve (MGPCG) ----------------------------------------- */
 
 /* Same callback contract as the reference's FlipPressureCallbacks
