@@ -223,6 +223,31 @@ def bench_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def bench_part(args):
+    """One solver part (a level-0 smoothing sweep, the level-0 matvec or a
+    V-cycle) of the pressure workload, timed through msbg_gpu_pressure_profile:
+    one warm-up call, then --steps calls.  Prints the level-0 cell count so a
+    capture's DRAM bytes can be put per cell."""
+    import torch
+    import msbg_gpu
+    torch.cuda.set_device(0)
+    c = dict(PS_CFG)
+    if args.res:
+        c["res"] = args.res
+        c["band"] = PS_CFG["band"] * args.res / PS_CFG["res"]
+    ctx = msbg_gpu.Context(0)
+    ctx.pressure_prepare(ps_scene(c))
+    st = ps_stats(ctx)
+    what = {"smooth": 0, "matvec": 1, "vcycle": 2}[args.part]
+    storage = {"f32": msbg_gpu.F32, "f16": msbg_gpu.F16, "bf16": msbg_gpu.BF16}[args.storage]
+    ms, by = ctx.pressure_profile(what | (storage << 4), max(1, args.steps), c["inner"])
+    print(json.dumps({"part": args.part, "storage": args.storage, "res": c["res"],
+                      "cells_level0": int(st.cells[0]), "ms_per_call": ms,
+                      "alg_bytes_per_call": by, "achieved_gbs": by / (ms * 1e-3) / 1e9}),
+          flush=True)
+    ctx.close()
+
+
 def bench_mgpcg(args):
     import torch
     import msbg_gpu
@@ -271,10 +296,23 @@ def bench_mgpcg(args):
     roof = {"bound": "hbm", "achieved": bytes_sw / (ms_sw * 1e-3) / 1e9, "peak": hbm,
             "unit": "GB/s", "frac": bytes_sw / (ms_sw * 1e-3) / 1e9 / hbm, "peak_kind": pk_kind,
             "traffic": dpc * cells0 if dpc else None, "alg_bytes_per_sweep": bytes_sw,
-            "kernel": "k_smooth<16> (one level-0 pre-smoothing sweep, 4 launches)",
+            "kernel": "k_smooth_pipe16 (one level-0 pre-smoothing sweep, one launch per pass)",
             "vcycle_achieved_gbs": bytes_vc / (ms_vc * 1e-3) / 1e9,
             "vcycle_frac": bytes_vc / (ms_vc * 1e-3) / 1e9 / hbm}
     del launches_sweep
+    # the same solve to a true FP64 residual of 1e-6 with the FP64 outer
+    # refinement, level-0 vectors in FP32, FP16 and BF16 (one warm-up each)
+    variants = {}
+    for name, storage in (("f32", msbg_gpu.F32), ("f16", msbg_gpu.F16), ("bf16", msbg_gpu.BF16)):
+        vp = msbg_gpu.solve_params(nPre=c["n_pre"], nPost=c["n_post"], tol=c["tol"],
+                                   innerIter=c["inner"], useGraph=1, storage=storage,
+                                   maxRefine=30)
+        ctx.pressure_solve(vp)
+        vi = ctx.pressure_solve(vp)
+        variants[name + "_vectors_fp64_refined"] = {
+            "ms": vi.solveSeconds * 1e3, "pcg_iterations": vi.iterations,
+            "refinements": vi.refinements, "status": vi.status,
+            "true_rel_residual_fp64": vi.relResidual}
     # end to end through the C ABI: prepare from the host callbacks (host
     # sampling + hierarchy + upload), solve, download the pressure
     n_e2e = max(1, min(args.steps, 2))
@@ -301,6 +339,7 @@ def bench_mgpcg(args):
                            "mode": "plain FP32 MGPCG (V(2,2), FP64 dots, FP64 coarsest solve)",
                            "time_to_1e-6_ms": ms_step, "pcg_iterations": iters,
                            "true_rel_residual": infos[-1].relResidual,
+                           "refined_variants": variants,
                            "liquid_cells": fluid, "stored_cells_level0": cells0,
                            "mg_levels": int(st.nMgLevels),
                            "prepare_s": st.prepareSeconds, "host_build_s": st.buildSeconds,
@@ -501,8 +540,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--profile", action="store_true",
                     help="only the resident-data steps (for ncu captures); prints nothing")
+    ap.add_argument("--part", default="", choices=["", "smooth", "matvec", "vcycle"],
+                    help="time one solver part of the pressure workload (ncu captures); "
+                         "--steps calls after one warm-up call")
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"],
+                    help="level-0 vector storage of --part")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.part:
+        bench_part(args)
+    elif args.impl == "reference":
         bench_reference(args)
     elif args.workload == "mcf":
         bench_mcf(args)

@@ -179,11 +179,14 @@ typedef struct {
   int nPre, nPost, nCoarse, maxIter;
   float tol;        /* stop when |r| <= tol*|b| */
   int innerIter;    /* red-black sweeps inside a tile per smoother visit */
-  int storage;      /* MSBG_F32, MSBG_F16 or MSBG_BF16 vectors */
+  int storage;      /* MSBG_F32, MSBG_F16 or MSBG_BF16: storage of the MG
+                       level-0 vectors (coarser levels, the operator and all
+                       arithmetic stay FP32; dots FP64) */
   int maxRefine;    /* 0: plain MGPCG stopping on the recursive residual (as the
                        reference); >0: up to maxRefine outer steps of FP64
-                       iterative refinement (FP64 solution and residual, FP32
-                       inner MGPCG) stopping on the true FP64 residual */
+                       iterative refinement (FP64 solution and residual, inner
+                       MGPCG in the storage type) stopping on the true FP64
+                       residual.  16-bit storage always refines (0 = 30). */
   int useGraph;     /* capture one PCG iteration in a CUDA graph */
   float coarseScale; /* coarse-grid correction factor (default 1.8; 1 = plain) */
 } msbg_gpu_solve_params;
@@ -245,9 +248,12 @@ int msbg_gpu_pressure_stats(msbg_gpu_ctx* ctx, msbg_gpu_pressure_stats_t* out);
 /* Times `reps` calls of one solver part on the context stream with CUDA
  * events: what = 0 one pre-smoothing sweep of MG level 0 (innerIter sweeps
  * inside each tile), 1 the level-0 matrix-vector product with its dot
- * product, 2 one V-cycle (2 pre, 2 post sweeps).  *algBytesPerCall is the
- * algorithmic DRAM traffic of one call (28 B/cell per smoothing sweep, 24 B/cell
- * per matvec, summed over the MG levels for a V-cycle). */
+ * product, 2 one V-cycle (2 pre, 2 post sweeps), 3 the smoothing sweep
+ * through the one-CTA-per-tile kernel.  what | (storage << 4) times the
+ * same part with level-0 vectors of that storage type (MSBG_F16/MSBG_BF16).
+ * *algBytesPerCall is the algorithmic DRAM traffic of one call (per level-0
+ * cell: 16 B of operator plus 3 vector values per smoothing sweep, 16 B plus
+ * 2 vector values per matvec; summed over the MG levels for a V-cycle). */
 int msbg_gpu_pressure_profile(msbg_gpu_ctx* ctx, int what, int reps, int innerIter,
                               double* msPerCall, double* algBytesPerCall);
 

@@ -25,353 +25,14 @@
 #include "common.cuh"
 #include "pressure.h"
 #include "pressure_kernels.cuh"
+#include "vec_types.cuh"
 
 namespace msbg {
 namespace ps {
 
-// ---------------------------------------------------------------------------
-// reductions
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Sum over the CTA; result valid in thread 0.
-__device__ double block_sum(double v) {
-  __shared__ double ws[32];
-  v = warp_sum(v);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) ws[w] = v;
-  __syncthreads();
-  const int nw = (blockDim.x + 31) >> 5;
-  v = (threadIdx.x < nw) ? ws[threadIdx.x] : 0.0;
-  if (w == 0) v = warp_sum(v);
-  __syncthreads();
-  return v;
-}
-
-struct Scalars {
-  double bb, rho, rhoNew, dq, rr, alpha, beta;
-  int status;  // 0 ok, 2 breakdown, 3 non-finite
-  int pad;
-};
-
-enum { FIN_BB = 0, FIN_DQ_ALPHA = 1, FIN_RR = 2, FIN_RHO = 3, FIN_RHONEW_BETA = 4 };
-
-// Deterministic second stage: fixed-order sum of the CTA partials, then the
-// scalar step of PCG that depends on it.
-__global__ void __launch_bounds__(1024) k_finalize(const double* __restrict__ partial, int n,
-                                                   Scalars* s, int what) {
-  double v = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) v += partial[i];
-  v = block_sum(v);
-  if (threadIdx.x != 0) return;
-  switch (what) {
-    case FIN_BB: s->bb = v; break;
-    case FIN_RHO: s->rho = v; break;
-    case FIN_RR: s->rr = v; if (!isfinite(v)) s->status = 3; break;
-    case FIN_DQ_ALPHA:
-      s->dq = v;
-      if (!isfinite(v) || !isfinite(s->rho)) s->status = 3;
-      else if (!(v > 1e-300) || !(s->rho > 1e-300)) s->status = 2;
-      else s->alpha = s->rho / v;
-      break;
-    case FIN_RHONEW_BETA:
-      s->rhoNew = v;
-      if (!isfinite(v)) s->status = 3;
-      else if (!(v > 1e-300)) s->status = 2;
-      else {
-        s->beta = v / s->rho;
-        s->rho = v;
-      }
-      break;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// level-0 vector kernels (grid-stride, fixed grid for deterministic partials)
-// ---------------------------------------------------------------------------
-constexpr int VEC_GRID = 148 * 4, VEC_BLOCK = 512;
-
-__global__ void __launch_bounds__(VEC_BLOCK) k_dot(const float* __restrict__ a,
-                                                   const float* __restrict__ b, int64_t n,
-                                                   double* __restrict__ partial) {
-  double acc = 0;
-  const int64_t n4 = n >> 2;
-  const float4* a4 = reinterpret_cast<const float4*>(a);
-  const float4* b4 = reinterpret_cast<const float4*>(b);
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    float4 u = a4[i], v = b4[i];
-    acc += (double)u.x * v.x + (double)u.y * v.y + (double)u.z * v.z + (double)u.w * v.w;
-  }
-  acc = block_sum(acc);
-  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
-}
-
-// x += alpha d; r -= alpha q; partial |r|^2.  Skipped (norm only) after a breakdown.
-__global__ void __launch_bounds__(VEC_BLOCK) k_axpy_norm(float* __restrict__ x,
-                                                         float* __restrict__ r,
-                                                         const float* __restrict__ d,
-                                                         const float* __restrict__ q, int64_t n,
-                                                         const Scalars* __restrict__ s,
-                                                         double* __restrict__ partial) {
-  const bool ok = s->status == 0;
-  const float alpha = (float)s->alpha;
-  double acc = 0;
-  const int64_t n4 = n >> 2;
-  float4* x4 = reinterpret_cast<float4*>(x);
-  float4* r4 = reinterpret_cast<float4*>(r);
-  const float4* d4 = reinterpret_cast<const float4*>(d);
-  const float4* q4 = reinterpret_cast<const float4*>(q);
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    float4 rv = r4[i];
-    if (ok) {
-      float4 xv = x4[i], dv = d4[i], qv = q4[i];
-      xv.x = fmaf(alpha, dv.x, xv.x); xv.y = fmaf(alpha, dv.y, xv.y);
-      xv.z = fmaf(alpha, dv.z, xv.z); xv.w = fmaf(alpha, dv.w, xv.w);
-      rv.x = fmaf(-alpha, qv.x, rv.x); rv.y = fmaf(-alpha, qv.y, rv.y);
-      rv.z = fmaf(-alpha, qv.z, rv.z); rv.w = fmaf(-alpha, qv.w, rv.w);
-      x4[i] = xv;
-      r4[i] = rv;
-    }
-    acc += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
-  }
-  acc = block_sum(acc);
-  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
-}
-
-// d = z + beta d
-__global__ void __launch_bounds__(VEC_BLOCK) k_update_d(float* __restrict__ d,
-                                                        const float* __restrict__ z, int64_t n,
-                                                        const Scalars* __restrict__ s) {
-  if (s->status) return;
-  const float beta = (float)s->beta;
-  const int64_t n4 = n >> 2;
-  float4* d4 = reinterpret_cast<float4*>(d);
-  const float4* z4 = reinterpret_cast<const float4*>(z);
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    float4 dv = d4[i], zv = z4[i];
-    dv.x = fmaf(beta, dv.x, zv.x); dv.y = fmaf(beta, dv.y, zv.y);
-    dv.z = fmaf(beta, dv.z, zv.z); dv.w = fmaf(beta, dv.w, zv.w);
-    d4[i] = dv;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// tile kernels
-// ---------------------------------------------------------------------------
-
-// In-tile neighbour sum S of cell (i,j,k) from a shared-memory tile, ghosts
-// from gs.  cxv etc. point at the tile's couplings (shared or global).
-template <int TS>
-__device__ __forceinline__ float nbr_sum(const float* xs, const float* cxv, const float* cyv,
-                                         const float* czv, const float (*gs)[TS * TS], int i,
-                                         int j, int k) {
-  const int e = tidx(TS, i, j, k);
-  float S = 0.f;
-  S += (i > 0) ? cxv[e] * xs[e - 1] : gs[0][j + TS * k];
-  S += (i < TS - 1) ? cxv[e + 1] * xs[e + 1] : gs[1][j + TS * k];
-  S += (j > 0) ? cyv[e] * xs[e - TS] : gs[2][i + TS * k];
-  S += (j < TS - 1) ? cyv[e + TS] * xs[e + TS] : gs[3][i + TS * k];
-  S += (k > 0) ? czv[e] * xs[e - TS * TS] : gs[4][i + TS * j];
-  S += (k < TS - 1) ? czv[e + TS * TS] * xs[e + TS * TS] : gs[5][i + TS * j];
-  return S;
-}
-
-// q = A d on the listed tiles, partial d.q per CTA.
-template <int TS>
-__global__ void __launch_bounds__(TS* TS) k_matvec_dot(LevelView L, const int* __restrict__ tiles,
-                                                       const float* __restrict__ d,
-                                                       float* __restrict__ q,
-                                                       double* __restrict__ partial) {
-  constexpr int N = TS * TS * TS, NT = TS * TS;
-  __shared__ float xs[N];
-  __shared__ float gs[6][NT];
-  const int ti = tiles[blockIdx.x];
-  const int64_t off = L.tileOff[ti];
-  const int t = threadIdx.x, i = t % TS, j = t / TS;
-  for (int e = t; e < N; e += NT) xs[e] = d[off + e];
-#pragma unroll
-  for (int f = 0; f < 6; f++) gs[f][t] = ghost_sum(L, d, ti, TS, f >> 1, f & 1, i, j);
-  __syncthreads();
-  double acc = 0;
-  const float* cxv = L.cx + off;
-  const float* cyv = L.cy + off;
-  const float* czv = L.cz + off;
-#pragma unroll 4
-  for (int k = 0; k < TS; k++) {
-    const int e = tidx(TS, i, j, k);
-    const float dg = L.diag[off + e];
-    float y = 0.f;
-    if (dg > 0.f) y = dg * xs[e] - nbr_sum<TS>(xs, cxv, cyv, czv, gs, i, j, k);
-    q[off + e] = y;
-    acc += (double)xs[e] * (double)y;
-  }
-  acc = block_sum(acc);
-  if (t == 0 && partial) partial[blockIdx.x] = acc;
-}
-
-// r = b - A x on the listed tiles, restricted (sum over the liquid children,
-// P^T) into the coarse right-hand side bc.
-template <int TS>
-__global__ void __launch_bounds__(TS* TS) k_residual_restrict(LevelView L,
-                                                              const int* __restrict__ tiles,
-                                                              const float* __restrict__ x,
-                                                              const float* __restrict__ b,
-                                                              float* __restrict__ bc,
-                                                              const int64_t* __restrict__ coarseOff) {
-  constexpr int N = TS * TS * TS, NT = TS * TS;
-  __shared__ float xs[N];
-  __shared__ float rs[N];
-  __shared__ float gs[6][NT];
-  const int ti = tiles[blockIdx.x];
-  const int64_t off = L.tileOff[ti];
-  const int t = threadIdx.x, i = t % TS, j = t / TS;
-  for (int e = t; e < N; e += NT) xs[e] = x[off + e];
-#pragma unroll
-  for (int f = 0; f < 6; f++) gs[f][t] = ghost_sum(L, x, ti, TS, f >> 1, f & 1, i, j);
-  __syncthreads();
-  const float* cxv = L.cx + off;
-  const float* cyv = L.cy + off;
-  const float* czv = L.cz + off;
-#pragma unroll 4
-  for (int k = 0; k < TS; k++) {
-    const int e = tidx(TS, i, j, k);
-    const float dg = L.diag[off + e];
-    float r = 0.f;
-    if (dg > 0.f) r = b[off + e] - (dg * xs[e] - nbr_sum<TS>(xs, cxv, cyv, czv, gs, i, j, k));
-    rs[e] = r;
-  }
-  __syncthreads();
-  const int* tc = L.toCoarse + (size_t)ti * 6;
-  const int ct = tc[0], ox = tc[1], oy = tc[2], oz = tc[3], agg = tc[4], cts = tc[5];
-  if (ct < 0) return;
-  float* dst = bc + coarseOff[ct];
-  if (agg) {
-    constexpr int H = TS / 2;
-    for (int c = t; c < H * H * H; c += NT) {
-      const int ci = c % H, cj = (c / H) % H, ck = c / (H * H);
-      const int e = tidx(TS, 2 * ci, 2 * cj, 2 * ck);
-      const float s = rs[e] + rs[e + 1] + rs[e + TS] + rs[e + TS + 1] + rs[e + TS * TS] +
-                      rs[e + TS * TS + 1] + rs[e + TS * TS + TS] + rs[e + TS * TS + TS + 1];
-      dst[tidx(cts, ox + ci, oy + cj, oz + ck)] = s;
-    }
-  } else {
-    for (int e = t; e < N; e += NT) {
-      const int ii = e % TS, jj = (e / TS) % TS, kk = e / (TS * TS);
-      dst[tidx(cts, ox + ii, oy + jj, oz + kk)] = rs[e];
-    }
-  }
-}
-
-// x += P xc (liquid cells only).
-template <int TS>
-__global__ void __launch_bounds__(TS* TS) k_prolong(LevelView L, const int* __restrict__ tiles,
-                                                    float* __restrict__ x,
-                                                    const float* __restrict__ xc,
-                                                    const int64_t* __restrict__ coarseOff,
-                                                    float scale) {
-  constexpr int N = TS * TS * TS, NT = TS * TS;
-  const int ti = tiles[blockIdx.x];
-  const int64_t off = L.tileOff[ti];
-  const int* tc = L.toCoarse + (size_t)ti * 6;
-  const int ct = tc[0], ox = tc[1], oy = tc[2], oz = tc[3], agg = tc[4], cts = tc[5];
-  if (ct < 0) return;
-  const float* src = xc + coarseOff[ct];
-  for (int e = threadIdx.x; e < N; e += NT) {
-    if (!(L.diag[off + e] > 0.f)) continue;
-    const int i = e % TS, j = (e / TS) % TS, k = e / (TS * TS);
-    const int sh = agg ? 1 : 0;
-    x[off + e] += scale * src[tidx(cts, ox + (i >> sh), oy + (j >> sh), oz + (k >> sh))];
-  }
-}
-
-// Red-black Gauss-Seidel inside each listed tile, `inner` iterations, ghosts
-// frozen at their values when the tile is loaded.  reverse=0: red then black;
-// reverse=1: black then red (the adjoint order).  Optional partial b.x.
-template <int TS>
-__global__ void __launch_bounds__(TS* TS) k_smooth(LevelView L, const int* __restrict__ tiles,
-                                                   float* __restrict__ x,
-                                                   const float* __restrict__ b, int inner,
-                                                   int reverse, double* __restrict__ partial) {
-  constexpr int N = TS * TS * TS, NT = TS * TS;
-  extern __shared__ __align__(128) float sm[];
-  float* xs = sm;
-  float* cxs = sm + N;
-  float* cys = sm + 2 * N;
-  float* czs = sm + 3 * N;
-  float(*gs)[NT] = reinterpret_cast<float(*)[NT]>(sm + 4 * N);
-  const int ti = tiles[blockIdx.x];
-  const int64_t off = L.tileOff[ti];
-  const int t = threadIdx.x, i = t % TS, j = t / TS;
-  for (int e = t; e < N; e += NT) {
-    xs[e] = x[off + e];
-    cxs[e] = L.cx[off + e];
-    cys[e] = L.cy[off + e];
-    czs[e] = L.cz[off + e];
-  }
-  float bb[TS], inv[TS];
-#pragma unroll
-  for (int k = 0; k < TS; k++) {
-    const int e = tidx(TS, i, j, k);
-    const float dg = L.diag[off + e];
-    inv[k] = dg > 0.f ? 1.0f / dg : 0.f;
-    bb[k] = b[off + e];
-  }
-#pragma unroll
-  for (int f = 0; f < 6; f++) gs[f][t] = ghost_sum(L, x, ti, TS, f >> 1, f & 1, i, j);
-  __syncthreads();
-  for (int it = 0; it < inner; it++) {
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int colour = reverse ? 1 - h : h;
-#pragma unroll
-      for (int k = 0; k < TS; k++) {
-        if (((i + j + k) & 1) != colour || inv[k] == 0.f) continue;
-        const float S = nbr_sum<TS>(xs, cxs, cys, czs, gs, i, j, k);
-        xs[tidx(TS, i, j, k)] = (bb[k] + S) * inv[k];
-      }
-      __syncthreads();
-    }
-  }
-  double acc = 0;
-  for (int e = t; e < N; e += NT) {
-    x[off + e] = xs[e];
-    if (partial) acc += (double)xs[e] * (double)b[off + e];
-  }
-  if (partial) {
-    acc = block_sum(acc);
-    if (t == 0) partial[blockIdx.x] = acc;
-  }
-}
-
+#include "tile_kernels.cuh"
 #include "smooth_pipe.cuh"
 #include "refine.cuh"
-
-// Coarsest level: x = A^-1 b with the dense FP64 inverse (symmetric).
-__global__ void __launch_bounds__(512) k_coarse_solve(const double* __restrict__ Ainv, int n,
-                                                      const int64_t* __restrict__ cells,
-                                                      const float* __restrict__ b,
-                                                      float* __restrict__ x) {
-  __shared__ double bs[512];
-  const int t = threadIdx.x;
-  if (t < n) bs[t] = b[cells[t]];
-  __syncthreads();
-  if (t >= n) return;
-  double s = 0;
-  for (int j = 0; j < n; j++) s += Ainv[(size_t)j * n + t] * bs[j];
-  x[cells[t]] = (float)s;
-}
-
-template <int TS>
-size_t smooth_smem() {
-  return sizeof(float) * (4 * TS * TS * TS + 6 * TS * TS);
-}
 
 // ---------------------------------------------------------------------------
 // solver state
@@ -386,20 +47,31 @@ struct Solver {
   DeviceBuffer dCoarseInv, dCoarseCells;
   DeviceBuffer rhs0, d0, q0, z0, r0, partial, scal;
   DeviceBuffer x64, rin;  // FP64 solution and inner right-hand side of the refinement
+  DeviceBuffer rinv;      // the inner right-hand side scaled and stored in 16 bits
   int maxPartial = 0;
   Scalars* hScal = nullptr;  // pinned
   int bsx0 = 0, nbx = 0, nby = 0, nbz = 0;
   std::vector<int> blockLevel;
 };
 
-template <int TS>
-void set_smooth_attr() {
+// Dynamic shared-memory limits of the kernels a level-0 vector type needs
+// (coarse levels always run in FP32).
+template <typename VT>
+void set_kernel_attrs() {
   static bool done = false;
-  if (!done) {
-    cudaFuncSetAttribute(k_smooth<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smooth_smem<TS>());
-    done = true;
-  }
+  if (done) return;
+  const int pipeSmem = (int)pipe::SMEM;
+  cudaFuncSetAttribute(k_smooth<16, VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smooth_smem<16>());
+  cudaFuncSetAttribute(k_smooth<8, VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smooth_smem<8>());
+  cudaFuncSetAttribute(k_smooth_pipe16<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       pipeSmem);
+  cudaFuncSetAttribute(k_apply_pipe16<APPLY_MATVEC, VT, VT>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, pipeSmem);
+  cudaFuncSetAttribute(k_apply_pipe16<APPLY_RESIDUAL, VT, float>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, pipeSmem);
+  done = true;
 }
 
 #define TS_DISPATCH(ts, CALL)        \
@@ -412,6 +84,10 @@ void set_smooth_attr() {
     default: break;                  \
   }
 
+// Launches the V-cycle and operator kernels.  VT is the storage type of the
+// level-0 vectors; the coarser levels hold FP32 vectors (they carry 1/8 of
+// the cells and the restricted right-hand sides grow by up to 8x per level).
+template <typename VT>
 struct Runner {
   Solver& S;
   cudaStream_t st;
@@ -422,12 +98,13 @@ struct Runner {
   bool usePipe = true;
   int64_t launches = 0;  // kernels launched through this runner
 
-  const int* passList(int m) { return S.dev[m]->passTiles.as<int>(); }
-  const int* groupList(int m) { return S.dev[m]->groupTiles.as<int>(); }
+  const int* passList(int m) { return S.dev[m]->passTiles.template as<int>(); }
+  const int* groupList(int m) { return S.dev[m]->groupTiles.template as<int>(); }
 
   // One smoothing sweep of MG level m: the (level, colour) passes in order
   // (pre) or in reverse order with the adjoint colour order inside (post).
-  void smooth(int m, float* x, const float* b, bool post) {
+  template <typename V>
+  void smooth(int m, V* x, const V* b, bool post) {
     const Level& L = S.H.levels[m];
     const int np = (int)L.passes.size();
     for (int pi = 0; pi < np; pi++) {
@@ -437,36 +114,37 @@ struct Runner {
       if (P.ts == 16 && usePipe) {
         const int grid = std::min(P.count, numSMs);
         // passes are contiguous tile-id ranges (register_tiles sorts by pass)
-        k_smooth_pipe16<<<grid, pipe::NT, pipe::SMEM, st>>>(S.views[m], P.start, P.count, x,
-                                                            b, inner, post ? 1 : 0, err);
+        k_smooth_pipe16<V><<<grid, pipe::NT, pipe::SMEM, st>>>(S.views[m], P.start, P.count, x,
+                                                               b, inner, post ? 1 : 0, err);
       } else {
-        TS_DISPATCH(P.ts, (k_smooth<T><<<P.count, T * T, smooth_smem<T>(), st>>>(
-                               S.views[m], lst, x, b, inner, post ? 1 : 0, nullptr)));
+        TS_DISPATCH(P.ts, (k_smooth<T, V><<<P.count, T * T, smooth_smem<T>(), st>>>(
+                               S.views[m], lst, x, b, inner, post ? 1 : 0)));
       }
       launches++;
     }
   }
 
-  void vcycle(int m, float* x, const float* b) {
+  template <typename V>
+  void vcycle(int m, V* x, const V* b) {
     const int last = (int)S.H.levels.size() - 1;
     const Level& L = S.H.levels[m];
-    cudaMemsetAsync(x, 0, sizeof(float) * L.nCells, st);
+    cudaMemsetAsync(x, 0, sizeof(V) * L.nCells, st);
     if (m == last) {
-      k_coarse_solve<<<1, 512, 0, st>>>(S.dCoarseInv.as<double>(), S.H.nCoarse,
-                                        S.dCoarseCells.as<int64_t>(), b, x);
+      k_coarse_solve<V><<<1, 512, 0, st>>>(S.dCoarseInv.template as<double>(), S.H.nCoarse,
+                                           S.dCoarseCells.template as<int64_t>(), b, x);
       launches++;
       return;
     }
     for (int s = 0; s < nPre; s++) smooth(m, x, b, false);
     LevelDev& C = *S.dev[m + 1];
     residual_restrict(m, x, b);
-    vcycle(m + 1, C.x.as<float>(), C.b.as<float>());
+    float* xc = C.x.template as<float>();
+    vcycle<float>(m + 1, xc, C.b.template as<float>());
     for (const auto& g : L.groups) {
       const int* lst = groupList(m) + g.start;
-      TS_DISPATCH(g.ts, (k_prolong<T><<<g.count, T * T, 0, st>>>(S.views[m], lst, x,
-                                                                  C.x.as<float>(),
-                                                                  C.tileOff.as<int64_t>(),
-                                                                  coarseScale)));
+      TS_DISPATCH(g.ts, (k_prolong<T, V, float><<<g.count, T * T, 0, st>>>(
+                            S.views[m], lst, x, xc, C.tileOff.template as<int64_t>(),
+                            coarseScale)));
       launches++;
     }
     for (int s = 0; s < nPost; s++) smooth(m, x, b, true);
@@ -475,20 +153,20 @@ struct Runner {
   // q = A d with partial d.q (level 0); returns the number of partials.
   // Passes are contiguous tile ranges of one tile size; 16^3 passes go
   // through the pipelined kernel, the others through the per-tile kernel.
-  int matvec_dot(const float* d, float* q, double* partial) {
+  int matvec_dot(const VT* d, VT* q, double* partial) {
     const Level& L = S.H.levels[0];
     int off = 0;
     for (const auto& P : L.passes) {
       if (!P.count) continue;
       if (P.ts == 16 && usePipe) {
         const int grid = std::min(P.count, numSMs);
-        k_apply_pipe16<APPLY_MATVEC><<<grid, pipe::NT, pipe::SMEM, st>>>(
+        k_apply_pipe16<APPLY_MATVEC, VT, VT><<<grid, pipe::NT, pipe::SMEM, st>>>(
             S.views[0], P.start, P.count, d, nullptr, q, nullptr, nullptr, partial + off, err);
         off += grid;
       } else {
         const int* lst = passList(0) + P.start;
-        TS_DISPATCH(P.ts, (k_matvec_dot<T><<<P.count, T * T, 0, st>>>(S.views[0], lst, d, q,
-                                                                       partial + off)));
+        TS_DISPATCH(P.ts, (k_matvec_dot<T, VT><<<P.count, T * T, 0, st>>>(S.views[0], lst, d, q,
+                                                                           partial + off)));
         off += P.count;
       }
       launches++;
@@ -496,21 +174,23 @@ struct Runner {
     return off;
   }
 
-  // r = b - A x on MG level m, restricted into the right-hand side of m+1.
-  void residual_restrict(int m, const float* x, const float* b) {
+  // r = b - A x on MG level m, restricted into the (FP32) right-hand side of m+1.
+  template <typename V>
+  void residual_restrict(int m, const V* x, const V* b) {
     const Level& L = S.H.levels[m];
     LevelDev& C = *S.dev[m + 1];
+    float* bc = C.b.template as<float>();
+    const int64_t* coff = C.tileOff.template as<int64_t>();
     for (const auto& P : L.passes) {
       if (!P.count) continue;
       if (P.ts == 16 && usePipe) {
         const int grid = std::min(P.count, numSMs);
-        k_apply_pipe16<APPLY_RESIDUAL><<<grid, pipe::NT, pipe::SMEM, st>>>(
-            S.views[m], P.start, P.count, x, b, nullptr, C.b.as<float>(),
-            C.tileOff.as<int64_t>(), nullptr, err);
+        k_apply_pipe16<APPLY_RESIDUAL, V, float><<<grid, pipe::NT, pipe::SMEM, st>>>(
+            S.views[m], P.start, P.count, x, b, nullptr, bc, coff, nullptr, err);
       } else {
         const int* lst = passList(m) + P.start;
-        TS_DISPATCH(P.ts, (k_residual_restrict<T><<<P.count, T * T, 0, st>>>(
-                              S.views[m], lst, x, b, C.b.as<float>(), C.tileOff.as<int64_t>())));
+        TS_DISPATCH(P.ts, (k_residual_restrict<T, V, float><<<P.count, T * T, 0, st>>>(
+                              S.views[m], lst, x, b, bc, coff)));
       }
       launches++;
     }
@@ -595,17 +275,10 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
         return set_error(ctx, MSBG_EINVARG, "grid dimensions give %d-cell tiles at MG level %d",
                          t.ts, (int)m);
       }
-  set_smooth_attr<16>();
-  cudaFuncSetAttribute(k_apply_pipe16<APPLY_MATVEC>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe::SMEM);
-  cudaFuncSetAttribute(k_apply_pipe16<APPLY_RESIDUAL>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe::SMEM);
-  cudaFuncSetAttribute(k_smooth_pipe16, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)pipe::SMEM);
+  set_kernel_attrs<float>();
+  set_kernel_attrs<__half>();
+  set_kernel_attrs<__nv_bfloat16>();
   cudaDeviceGetAttribute(&S.numSMs, cudaDevAttrMultiProcessorCount, ctx->device);
-  set_smooth_attr<8>();
-  set_smooth_attr<4>();
-  set_smooth_attr<2>();
   S.bsx0 = topo->bsx0;
   S.nbx = ctx->nbx;
   S.nby = ctx->nby;
@@ -644,6 +317,10 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
     const size_t nb = sizeof(float) * std::max<int64_t>(L.nCells, 4);
     MSBG_CUDA_TRY(ctx, D->x.ensure(nb));
     MSBG_CUDA_TRY(ctx, D->b.ensure(nb));
+    // Coarse cells whose finer tiles do not exist are never written by the
+    // restriction; they must read as 0 (not as recycled device memory).
+    MSBG_CUDA_TRY(ctx, cudaMemsetAsync(D->x.p, 0, nb, st));
+    MSBG_CUDA_TRY(ctx, cudaMemsetAsync(D->b.p, 0, nb, st));
     maxPartial = std::max(maxPartial, (int)L.tiles.size());
     LevelView v;
     v.tileOff = D->tileOff.as<int64_t>();
@@ -697,32 +374,38 @@ struct PcgResult {
 // stopping at |r| <= tolRel |bin| (recursive residual, as the reference).
 // One iteration is one CUDA graph launch; the graph is captured on the first
 // call and reused (all buffers are fixed).
-int run_pcg(msbg_gpu_ctx* ctx, Solver& S, Runner& R, const float* bin, double tolRel, int maxIter,
-            bool useGraph, cudaGraphExec_t& exec, int64_t& perIter, PcgResult& out) {
+template <typename VT>
+int run_pcg(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const VT* bin, double tolRel,
+            int maxIter, bool useGraph, cudaGraphExec_t& exec, int64_t& perIter,
+            PcgResult& out) {
   cudaStream_t st = R.st;
   const int64_t n = S.H.levels[0].nCells;
-  float* x = S.dev[0]->x.as<float>();
-  float* r = S.r0.as<float>();
-  float* d = S.d0.as<float>();
-  float* q = S.q0.as<float>();
-  float* z = S.z0.as<float>();
+  VT* x = S.dev[0]->x.as<VT>();
+  VT* r = S.r0.as<VT>();
+  VT* d = S.d0.as<VT>();
+  VT* q = S.q0.as<VT>();
+  VT* z = S.z0.as<VT>();
   double* part = S.partial.as<double>();
   Scalars* sc = S.scal.as<Scalars>();
   // r = b, x = 0, bb = b.b, z = V(r), rho = r.z, d = z
   cudaMemsetAsync(sc, 0, sizeof(Scalars), st);
-  cudaMemsetAsync(x, 0, sizeof(float) * n, st);
-  cudaMemcpyAsync(r, bin, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+  cudaMemsetAsync(x, 0, sizeof(VT) * n, st);
+  cudaMemcpyAsync(r, bin, sizeof(VT) * n, cudaMemcpyDeviceToDevice, st);
   k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(bin, bin, n, part);
   k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_BB);
   R.vcycle(0, z, r);
   k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
   k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHO);
-  cudaMemcpyAsync(d, z, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(d, z, sizeof(VT) * n, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
   R.launches += 4;
   MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   out = PcgResult();
   out.bb = S.hScal->bb;
+  if (!std::isfinite(out.bb) || !std::isfinite(S.hScal->rho)) {
+    out.status = 3;
+    return MSBG_OK;
+  }
   if (!(out.bb > 1e-300)) {
     out.status = 0;
     return MSBG_OK;
@@ -775,7 +458,8 @@ int run_pcg(msbg_gpu_ctx* ctx, Solver& S, Runner& R, const float* bin, double to
 }
 
 // r32 = b - A x64 (FP64) on level 0; returns |r|^2 in *rr.
-int residual64(msbg_gpu_ctx* ctx, Solver& S, Runner& R, const float* b, float* r32,
+template <typename VT>
+int residual64(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const float* b, float* r32,
                double* rr) {
   cudaStream_t st = R.st;
   const Level& L = S.H.levels[0];
@@ -797,6 +481,190 @@ int residual64(msbg_gpu_ctx* ctx, Solver& S, Runner& R, const float* b, float* r
   return MSBG_OK;
 }
 
+// max |v| over the n level-0 values of v.
+template <typename VT, typename V>
+int absmax(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const V* v, int64_t n, double* m) {
+  cudaStream_t st = R.st;
+  Scalars* sc = S.scal.as<Scalars>();
+  k_absmax<<<VEC_GRID, VEC_BLOCK, 0, st>>>(v, n, S.partial.as<double>());
+  k_finalize_max<<<1, 32, 0, st>>>(S.partial.as<double>(), VEC_GRID, sc);
+  cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  R.launches += 2;
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  *m = S.hScal->amax;
+  return MSBG_OK;
+}
+
+struct SolveOut {
+  int iters = 0, status = 1, refinements = 0;
+  double relres = 0;
+};
+
+// Plain MGPCG on the FP32 right-hand side, stopping on the recursive
+// residual (the reference's criterion); relres is the true FP32 residual.
+int solve_plain(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gpu_solve_params* p,
+                cudaGraphExec_t& exec, int64_t& perIter, cudaEvent_t e1, SolveOut& o) {
+  cudaStream_t st = R.st;
+  const int64_t n = S.H.levels[0].nCells;
+  float* x = S.dev[0]->x.as<float>();
+  const float* b = S.rhs0.as<float>();
+  PcgResult pr;
+  int rc = run_pcg(ctx, S, R, b, p->tol, p->maxIter, p->useGraph, exec, perIter, pr);
+  o.iters = pr.iters;
+  o.status = pr.status;
+  cudaEventRecord(e1, st);
+  if (rc) return rc;
+  // true residual of the FP32 iterate, FP32 operator, FP64 norm
+  float* q = S.q0.as<float>();
+  float* z = S.z0.as<float>();
+  float* d = S.d0.as<float>();
+  double* part = S.partial.as<double>();
+  Scalars* sc = S.scal.as<Scalars>();
+  R.matvec_dot(x, q, part);
+  cudaMemcpyAsync(z, b, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+  Scalars one{};
+  one.alpha = 1.0;
+  cudaMemcpyAsync(sc, &one, sizeof(Scalars), cudaMemcpyHostToDevice, st);
+  k_axpy_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, q, q, n, sc, part);  // z = b - q
+  k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
+  cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  o.relres = pr.bb > 0 ? std::sqrt(S.hScal->rr / pr.bb) : 0.0;
+  return MSBG_OK;
+}
+
+// Inner relative tolerance floor per storage type: a few unit roundoffs of
+// the stored vectors (FP32 2^-24, FP16 2^-11, BF16 2^-8).
+template <typename VT> constexpr double inner_floor() { return 1e-5; }
+template <> constexpr double inner_floor<__half>() { return 2e-3; }
+template <> constexpr double inner_floor<__nv_bfloat16>() { return 1.5e-2; }
+
+// FP64 iterative refinement: x64 += s^-1 MGPCG_VT(s (b - A x64)).  For
+// 16-bit vectors the inner right-hand side is scaled by a power of two s that
+// keeps the inner solution inside the FP16 range: the first step aims at
+// max|s r| = 2^-4, later steps at max|e| = 2^10 through the measured gain
+// max|e| / max|s r| of the previous inner solve (the gain moves by up to
+// about 20x between steps, the FP16 range leaves 64x).  An inner solve whose
+// residual or solution is non-finite (an FP16 overflow) is repeated with s
+// reduced by 2^8, at most twice.  Inner solves of 16-bit vectors stop at 40
+// iterations or at a breakdown: their recursive residual stagnates near the
+// rounding level, and the outer step then recomputes the true residual in
+// FP64 and continues from the iterate reached.
+template <typename VT>
+int solve_refined(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const msbg_gpu_solve_params* p,
+                  int maxRefine, cudaGraphExec_t& exec, int64_t& perIter, SolveOut& o) {
+  cudaStream_t st = R.st;
+  const int64_t n = S.H.levels[0].nCells;
+  constexpr bool WIDE = std::is_same<VT, float>::value;
+  constexpr int INNER_MAX_16 = 40;
+  double* x64 = S.x64.as<double>();
+  float* rin = S.rin.as<float>();
+  VT* rinV = WIDE ? reinterpret_cast<VT*>(rin) : S.rinv.as<VT>();
+  VT* e = S.dev[0]->x.as<VT>();
+  const float* b = S.rhs0.as<float>();
+  cudaMemsetAsync(x64, 0, sizeof(double) * n, st);
+  double bb = 0, rr = 0, gain = 0;
+  int rc = MSBG_OK;
+  for (int outer = 0;; outer++) {
+    rc = residual64(ctx, S, R, b, rin, &rr);
+    if (rc) return rc;
+    if (outer == 0) bb = rr;
+    o.relres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+    if (!(bb > 1e-300) || o.relres <= p->tol) {
+      o.status = 0;
+      break;
+    }
+    if (!std::isfinite(rr)) {
+      o.status = 3;
+      break;
+    }
+    if (outer >= maxRefine || o.iters >= p->maxIter) {
+      o.status = 1;
+      break;
+    }
+    // inner tolerance: what is still missing, not below the storage floor
+    const double need = p->tol / std::max(o.relres, 1e-300);
+    const double tolIn = std::min(0.5, std::max(need * 0.5, inner_floor<VT>()));
+    double scale = 1.0, rmax = 0, emax = 0;
+    if (!WIDE) {
+      rc = absmax(ctx, S, R, rin, n, &rmax);
+      if (rc) return rc;
+      if (!(rmax > 0) || !std::isfinite(rmax)) {
+        o.status = std::isfinite(rmax) ? 0 : 3;
+        break;
+      }
+      const double target = gain > 0 ? std::ldexp(1.0, 10) / gain : std::ldexp(1.0, -4);
+      scale = std::ldexp(1.0, (int)std::floor(std::log2(target / rmax)));
+    }
+    PcgResult pr;
+    const int budget = p->maxIter - o.iters;
+    for (int attempt = 0;; attempt++) {
+      if (!WIDE) {
+        k_convert<<<VEC_GRID, VEC_BLOCK, 0, st>>>(rinV, rin, n, (float)scale);
+        R.launches++;
+      }
+      rc = run_pcg(ctx, S, R, (const VT*)rinV, tolIn,
+                   WIDE ? budget : std::min(budget, INNER_MAX_16), p->useGraph, exec, perIter,
+                   pr);
+      if (rc) return rc;
+      o.iters += pr.iters;
+      if (WIDE) break;
+      rc = absmax(ctx, S, R, e, n, &emax);
+      if (rc) return rc;
+      const bool overflow = pr.status == 3 || !std::isfinite(emax);
+      if (!overflow || attempt == 2) {
+        if (overflow) pr.status = 3;
+        break;
+      }
+      scale = std::ldexp(scale, -8);
+    }
+    o.refinements++;
+    if (pr.status == 3 || (pr.status == 2 && WIDE)) {
+      o.status = pr.status;
+      break;
+    }
+    if (!WIDE) gain = emax > 0 ? emax / (rmax * scale) : 0.0;
+    k_add64<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, e, n, 1.0 / scale);
+    R.launches++;
+  }
+  k_narrow<<<VEC_GRID, VEC_BLOCK, 0, st>>>(S.dev[0]->x.as<float>(), x64, n);
+  R.launches++;
+  return MSBG_OK;
+}
+
+template <typename VT>
+int solve_typed(msbg_gpu_ctx* ctx, Solver& S, const msbg_gpu_solve_params* p, cudaEvent_t e0,
+                cudaEvent_t e1, SolveOut& o, int64_t* launches) {
+  cudaStream_t st = ctx->stream;
+  Runner<VT> R{S, st, p->nPre, p->nPost, p->innerIter};
+  R.coarseScale = p->coarseScale > 0 ? p->coarseScale : 1.0f;
+  R.err = ctx->errBuf.as<int>();
+  R.numSMs = S.numSMs;
+  const int64_t n = S.H.levels[0].nCells;
+  constexpr bool WIDE = std::is_same<VT, float>::value;
+  // 16-bit vectors always run under the FP64 refinement
+  const int maxRefine = p->maxRefine > 0 ? p->maxRefine : (WIDE ? 0 : 30);
+  if (maxRefine > 0) {
+    MSBG_CUDA_TRY(ctx, S.x64.ensure(sizeof(double) * n));
+    MSBG_CUDA_TRY(ctx, S.rin.ensure(sizeof(float) * n));
+    if (!WIDE) MSBG_CUDA_TRY(ctx, S.rinv.ensure(sizeof(VT) * n));
+  }
+  cudaGraphExec_t exec = nullptr;
+  int64_t perIter = 0;
+  cudaEventRecord(e0, st);
+  int rc = MSBG_OK;
+  if constexpr (WIDE) {
+    if (maxRefine == 0) rc = solve_plain(ctx, S, R, p, exec, perIter, e1, o);
+  }
+  if (maxRefine > 0) {
+    rc = solve_refined(ctx, S, R, p, maxRefine, exec, perIter, o);
+    cudaEventRecord(e1, st);
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  *launches = R.launches;
+  return rc;
+}
+
 }  // namespace
 
 extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_params* p,
@@ -807,113 +675,38 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
   if (p->nPre < 0 || p->nPost < 0 || p->maxIter < 0 || p->innerIter < 1 || !(p->tol >= 0) ||
       p->maxRefine < 0)
     return set_error(ctx, MSBG_EINVARG, "invalid solve parameters");
-  if (p->storage != MSBG_F32)
+  if (p->storage != MSBG_F32 && p->storage != MSBG_F16 && p->storage != MSBG_BF16)
     return set_error(ctx, MSBG_ENOTIMPL, "storage type %d not available", p->storage);
   cudaSetDevice(ctx->device);
   Solver& S = *sp;
-  cudaStream_t st = ctx->stream;
-  Runner R{S, st, p->nPre, p->nPost, p->innerIter};
-  R.coarseScale = p->coarseScale > 0 ? p->coarseScale : 1.0f;
-  R.err = ctx->errBuf.as<int>();
-  R.numSMs = S.numSMs;
-  const Level& L0 = S.H.levels[0];
-  const int64_t n = L0.nCells;
-  float* x = S.dev[0]->x.as<float>();
-  const float* b = S.rhs0.as<float>();
-  if (p->maxRefine > 0) {
-    MSBG_CUDA_TRY(ctx, S.x64.ensure(sizeof(double) * n));
-    MSBG_CUDA_TRY(ctx, S.rin.ensure(sizeof(float) * n));
-  }
-  cudaGraphExec_t exec = nullptr;
-  int64_t perIter = 0;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  cudaEventRecord(e0, st);
-  int iters = 0, status = 1, refinements = 0;
-  double relres = 0;
-  int rc = MSBG_OK;
-  if (p->maxRefine == 0) {
-    PcgResult pr;
-    rc = run_pcg(ctx, S, R, b, p->tol, p->maxIter, p->useGraph, exec, perIter, pr);
-    iters = pr.iters;
-    status = pr.status;
-    cudaEventRecord(e1, st);
-    if (rc == MSBG_OK) {
-      // true residual of the FP32 iterate, FP32 operator, FP64 norm
-      float* q = S.q0.as<float>();
-      float* z = S.z0.as<float>();
-      float* d = S.d0.as<float>();
-      double* part = S.partial.as<double>();
-      Scalars* sc = S.scal.as<Scalars>();
-      R.matvec_dot(x, q, part);
-      cudaMemcpyAsync(z, b, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
-      Scalars one{};
-      one.alpha = 1.0;
-      cudaMemcpyAsync(sc, &one, sizeof(Scalars), cudaMemcpyHostToDevice, st);
-      k_axpy_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, q, q, n, sc, part);  // z = b - q
-      k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
-      cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
-      cudaStreamSynchronize(st);
-      relres = pr.bb > 0 ? std::sqrt(S.hScal->rr / pr.bb) : 0.0;
-    }
-  } else {
-    // FP64 iterative refinement around the FP32 MGPCG
-    double* x64 = S.x64.as<double>();
-    float* rin = S.rin.as<float>();
-    cudaMemsetAsync(x64, 0, sizeof(double) * n, st);
-    double bb = 0, rr = 0;
-    for (int outer = 0;; outer++) {
-      rc = residual64(ctx, S, R, b, rin, &rr);
-      if (rc) break;
-      if (outer == 0) bb = rr;
-      relres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
-      if (!(bb > 1e-300) || relres <= p->tol) {
-        status = 0;
-        break;
-      }
-      if (!std::isfinite(rr)) {
-        status = 3;
-        break;
-      }
-      if (outer >= p->maxRefine || iters >= p->maxIter) {
-        status = 1;
-        break;
-      }
-      // inner tolerance: what is still missing, not below the FP32 floor
-      const double need = p->tol / std::max(relres, 1e-300);
-      const double tolIn = std::min(0.5, std::max(need * 0.5, 1e-5));
-      PcgResult pr;
-      rc = run_pcg(ctx, S, R, rin, tolIn, p->maxIter - iters, p->useGraph, exec, perIter, pr);
-      if (rc) break;
-      iters += pr.iters;
-      refinements++;
-      if (pr.status >= 2) {
-        status = pr.status;
-        break;
-      }
-      k_add64<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, x, n);
-      R.launches++;
-    }
-    k_narrow<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x, x64, n);
-    cudaEventRecord(e1, st);
+  SolveOut o;
+  int64_t launches = 0;
+  int rc;
+  switch (p->storage) {
+    case MSBG_F16: rc = solve_typed<__half>(ctx, S, p, e0, e1, o, &launches); break;
+    case MSBG_BF16: rc = solve_typed<__nv_bfloat16>(ctx, S, p, e0, e1, o, &launches); break;
+    default: rc = solve_typed<float>(ctx, S, p, e0, e1, o, &launches); break;
   }
-  if (exec) cudaGraphExecDestroy(exec);
-  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  const cudaError_t se = cudaStreamSynchronize(ctx->stream);
   float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
+  if (rc == MSBG_OK && se == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
+  MSBG_CUDA_TRY(ctx, se);
   if (info) {
-    info->iterations = iters;
-    info->refinements = refinements;
-    info->status = status;
-    info->relResidual = relres;
+    const Level& L0 = S.H.levels[0];
+    info->iterations = o.iters;
+    info->refinements = o.refinements;
+    info->status = o.status;
+    info->relResidual = o.relres;
     info->solveSeconds = ms * 1e-3;
     info->fineCells = L0.nFluid;
     info->nMgLevels = (int)S.H.levels.size();
-    info->kernelLaunches = R.launches;
+    info->kernelLaunches = launches;
   }
   return MSBG_OK;
 }
@@ -940,50 +733,57 @@ extern "C" int msbg_gpu_pressure_stats(msbg_gpu_ctx* ctx, msbg_gpu_pressure_stat
   return MSBG_OK;
 }
 
-extern "C" int msbg_gpu_pressure_profile(msbg_gpu_ctx* ctx, int what, int reps, int innerIter,
-                                         double* msPerCall, double* algBytesPerCall) {
-  if (!ctx || reps <= 0 || innerIter < 1) return MSBG_EINVARG;
-  auto& sp = solver_of(ctx);
-  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
-  cudaSetDevice(ctx->device);
-  Solver& S = *sp;
+namespace {
+
+template <typename VT>
+int profile_typed(msbg_gpu_ctx* ctx, Solver& S, int what, int reps, int innerIter,
+                  double* msPerCall, double* algBytesPerCall) {
   cudaStream_t st = ctx->stream;
-  Runner R{S, st, 2, 2, innerIter};
+  Runner<VT> R{S, st, 2, 2, innerIter};
   R.err = ctx->errBuf.as<int>();
   R.numSMs = S.numSMs;
   const Level& L0 = S.H.levels[0];
   LevelDev& D0 = *S.dev[0];
-  float* x = D0.x.as<float>();
+  VT* x = D0.x.as<VT>();
   double* part = S.partial.as<double>();
-  const float* b = S.rhs0.as<float>();
-  // algorithmic bytes per cell: smoother reads x,b,diag,cx,cy,cz and writes x
-  const double smoothB = 28.0, mvB = 24.0, resB = 28.0 + 0.5, prolB = 12.5;
+  // a VT copy of the right-hand side (FP32 storage reads it in place)
+  VT* b = std::is_same<VT, float>::value ? (VT*)S.rhs0.as<float>() : S.r0.as<VT>();
+  if (!std::is_same<VT, float>::value)
+    k_convert<<<VEC_GRID, VEC_BLOCK, 0, st>>>(b, S.rhs0.as<float>(), L0.nCells, 1.0f);
+  // algorithmic bytes per cell: the smoother reads x, b, 1/a_ii, cx, cy, cz
+  // and writes x; the matvec reads d, a_ii, cx, cy, cz and writes q
+  const double v = sizeof(VT);
+  const double smooth0 = 16.0 + 3 * v, smoothC = 28.0, mvB = 16.0 + 2 * v;
   auto vcycle_bytes = [&]() {
     double s = 0;
     for (size_t m = 0; m + 1 < S.H.levels.size(); m++) {
       const double n = (double)S.H.levels[m].nCells;
-      s += n * (4.0 /*zero x*/ + (R.nPre + R.nPost) * smoothB + resB + prolB);
+      const double vs = m == 0 ? v : 4.0;
+      const double sm = m == 0 ? smooth0 : smoothC;
+      // zero x, sweeps, residual (x, b, operator, 1/8 restricted write),
+      // prolongation (a_ii mask, x read + write, 1/8 coarse read)
+      s += n * (vs + (R.nPre + R.nPost) * sm + (16.0 + 2 * vs + 0.5) + (4.0 + 2 * vs + 0.5));
     }
     return s;
   };
   double bytes = 0;
   auto body = [&]() {
     switch (what) {
-      case 0: R.smooth(0, x, b, false); break;
-      case 3: R.usePipe = false; R.smooth(0, x, b, false); R.usePipe = true; break;
-      case 1: R.matvec_dot(x, S.q0.as<float>(), part); break;
-      case 2: R.vcycle(0, S.z0.as<float>(), b); break;
+      case 0: R.smooth(0, x, (const VT*)b, false); break;
+      case 3: R.usePipe = false; R.smooth(0, x, (const VT*)b, false); R.usePipe = true; break;
+      case 1: R.matvec_dot(x, S.q0.as<VT>(), part); break;
+      case 2: R.vcycle(0, S.z0.as<VT>(), (const VT*)b); break;
       default: break;
     }
   };
   switch (what) {
     case 0:
-    case 3: bytes = smoothB * L0.nCells; break;
+    case 3: bytes = smooth0 * L0.nCells; break;
     case 1: bytes = mvB * L0.nCells; break;
     case 2: bytes = vcycle_bytes(); break;
     default: return set_error(ctx, MSBG_EINVARG, "profile target %d", what);
   }
-  MSBG_CUDA_TRY(ctx, cudaMemsetAsync(x, 0, sizeof(float) * L0.nCells, st));
+  MSBG_CUDA_TRY(ctx, cudaMemsetAsync(x, 0, sizeof(VT) * L0.nCells, st));
   body();  // warm-up
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -991,14 +791,36 @@ extern "C" int msbg_gpu_pressure_profile(msbg_gpu_ctx* ctx, int what, int reps, 
   cudaEventRecord(e0, st);
   for (int i = 0; i < reps; i++) body();
   cudaEventRecord(e1, st);
-  MSBG_CUDA_TRY(ctx, cudaEventSynchronize(e1));
+  const cudaError_t se = cudaEventSynchronize(e1);
   float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
+  if (se == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  MSBG_CUDA_TRY(ctx, se);
   if (msPerCall) *msPerCall = ms / reps;
   if (algBytesPerCall) *algBytesPerCall = bytes;
   return MSBG_OK;
+}
+
+}  // namespace
+
+extern "C" int msbg_gpu_pressure_profile(msbg_gpu_ctx* ctx, int what, int reps, int innerIter,
+                                         double* msPerCall, double* algBytesPerCall) {
+  if (!ctx || reps <= 0 || innerIter < 1) return MSBG_EINVARG;
+  auto& sp = solver_of(ctx);
+  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
+  cudaSetDevice(ctx->device);
+  Solver& S = *sp;
+  const int target = what & 15, storage = what >> 4;
+  switch (storage) {
+    case MSBG_F32: return profile_typed<float>(ctx, S, target, reps, innerIter, msPerCall,
+                                               algBytesPerCall);
+    case MSBG_F16: return profile_typed<__half>(ctx, S, target, reps, innerIter, msPerCall,
+                                                algBytesPerCall);
+    case MSBG_BF16: return profile_typed<__nv_bfloat16>(ctx, S, target, reps, innerIter,
+                                                        msPerCall, algBytesPerCall);
+    default: return set_error(ctx, MSBG_ENOTIMPL, "storage type %d not available", storage);
+  }
 }
 
 namespace {

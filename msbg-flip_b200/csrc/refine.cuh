@@ -50,12 +50,13 @@ __global__ void __launch_bounds__(TS* TS) k_residual64(LevelView L, const int* _
   if (t == 0) partial[blockIdx.x] = acc;
 }
 
-// x64 += e (all cells; e is 0 off the liquid)
-__global__ void __launch_bounds__(512) k_add64(double* __restrict__ x, const float* __restrict__ e,
-                                               int64_t n) {
+// x64 += e * unscale (all cells; e is 0 off the liquid)
+template <typename VT>
+__global__ void __launch_bounds__(512) k_add64(double* __restrict__ x, const VT* __restrict__ e,
+                                               int64_t n, double unscale) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
-    x[i] += (double)e[i];
+    x[i] += (double)to_f(e[i]) * unscale;
 }
 
 // x32 = (float) x64
@@ -64,4 +65,34 @@ __global__ void __launch_bounds__(512) k_narrow(float* __restrict__ y, const dou
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     y[i] = (float)x[i];
+}
+
+// Per-CTA partial max |v| (grid-stride over groups of 4).
+template <typename VT>
+__global__ void __launch_bounds__(VEC_BLOCK) k_absmax(const VT* __restrict__ v, int64_t n,
+                                                      double* __restrict__ partial) {
+  __shared__ float ws[32];
+  float m = 0.f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n >> 2);
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const F4 u = load4(v + 4 * i);
+    m = fmaxf(m, fmaxf(fmaxf(fabsf(u.x), fabsf(u.y)), fmaxf(fabsf(u.z), fabsf(u.w))));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = fmaxf(m, ws[w]);
+    partial[blockIdx.x] = m;
+  }
+}
+
+// Max of the partials into s->amax.
+__global__ void __launch_bounds__(32) k_finalize_max(const double* __restrict__ partial, int n,
+                                                     Scalars* s) {
+  if (threadIdx.x != 0) return;
+  double m = 0;
+  for (int i = 0; i < n; i++) m = (partial[i] != partial[i] || m != m) ? NAN : fmax(m, partial[i]);
+  s->amax = m;
 }

@@ -16,6 +16,11 @@
 // 512 threads; per colour each thread owns 4 cells whose couplings, 1/a_ii
 // and right-hand side (with the constant halo sums folded in) sit in
 // registers, laid out so a warp's shared-memory accesses hit 32 banks.
+//
+// Vectors may be stored in 16 bits (VT = __half / __nv_bfloat16): x and b
+// then arrive together in stage slot 1 and x is widened into the FP32
+// working slot 0; the smoothed tile is narrowed back into slot 1 for the
+// bulk store.  The operator arrays are always FP32.
 
 namespace pipe {
 
@@ -95,27 +100,48 @@ constexpr size_t SMEM = sizeof(float) * ZERO_FLOATS + 3 * sizeof(TileRec) + 3 * 
 
 // Issue the global loads of one halo cell of a SAME/COARSER face; the own
 // lower-face coupling of a SAME face is taken later from shared memory.
-__device__ __forceinline__ void halo_load(const LevelView& L, const float* __restrict__ x,
+template <typename VT>
+__device__ __forceinline__ void halo_load(const LevelView& L, const VT* __restrict__ x,
                                           const FaceRes& r, int dir, int side, int a, int b,
                                           float& xv, float& cv) {
   const float* cd = dir == 0 ? L.cx : dir == 1 ? L.cy : L.cz;
   xv = 0.f;
   cv = 0.f;
   if (r.kind == FACE_SAME) {
-    xv = __ldg(x + r.nOff + plane_idx(TS, dir, side ? 0 : TS - 1, a, b));
+    xv = to_f(__ldg(x + r.nOff + plane_idx(TS, dir, side ? 0 : TS - 1, a, b)));
     if (side) cv = __ldg(cd + r.nOff + plane_idx(TS, dir, 0, a, b));
   } else if (r.kind == FACE_COARSER) {
-    xv = __ldg(x + r.nOff +
-               plane_idx(r.nts, dir, side ? 0 : r.nts - 1, r.oa + (a >> 1), r.ob + (b >> 1)));
+    xv = to_f(__ldg(x + r.nOff + plane_idx(r.nts, dir, side ? 0 : r.nts - 1, r.oa + (a >> 1),
+                                           r.ob + (b >> 1))));
     cv = __ldg(L.ifc + r.ifOwn + a + TS * b);
   }
 }
 
+// Where the x and b vectors of a tile land in a stage: FP32 x straight into
+// the working slot 0 and b into slot 1; 16-bit x and b both into slot 1.
+template <typename VT>
+__device__ __forceinline__ VT* raw_x(float* st) {
+  return std::is_same<VT, float>::value ? reinterpret_cast<VT*>(st)
+                                        : reinterpret_cast<VT*>(st + N);
+}
+template <typename VT>
+__device__ __forceinline__ VT* raw_b(float* st) {
+  return reinterpret_cast<VT*>(st + N) + (std::is_same<VT, float>::value ? 0 : N);
+}
+// Widen a 16-bit x tile into the FP32 working slot (no-op for FP32).
+template <typename VT>
+__device__ __forceinline__ void widen_x(float* st, int tid) {
+  if (std::is_same<VT, float>::value) return;
+  const VT* xr = raw_x<VT>(st);
+  for (int e = tid; e < N; e += NT) st[e] = to_f(xr[e]);
+}
+
 }  // namespace pipe
 
+template <typename VT>
 __global__ void __launch_bounds__(pipe::NT, 1)
-    k_smooth_pipe16(LevelView L, int tileBase, int count, float* __restrict__ x,
-                    const float* __restrict__ b, int inner, int reverse, int* __restrict__ err) {
+    k_smooth_pipe16(LevelView L, int tileBase, int count, VT* __restrict__ x,
+                    const VT* __restrict__ b, int inner, int reverse, int* __restrict__ err) {
   using namespace pipe;
   extern __shared__ __align__(128) float sm[];
   float* stages[2] = {sm + GUARD, sm + GUARD + 6 * N};
@@ -140,10 +166,10 @@ __global__ void __launch_bounds__(pipe::NT, 1)
   auto issue_arrays = [&](const TileRec& r, float* st, uint64_t* br, int tRec, int slot) {
     fence_proxy_async();
     const bool rec = tRec < count;
-    mbar_expect_tx(br, 6 * N * sizeof(float) + (rec ? sizeof(TileRec) : 0));
+    mbar_expect_tx(br, 2 * N * sizeof(VT) + 4 * N * sizeof(float) + (rec ? sizeof(TileRec) : 0));
     const int64_t off = r.off;
-    bulk_g2s(st + 0 * N, x + off, N * sizeof(float), br);
-    bulk_g2s(st + 1 * N, b + off, N * sizeof(float), br);
+    bulk_g2s(raw_x<VT>(st), x + off, N * sizeof(VT), br);
+    bulk_g2s(raw_b<VT>(st), b + off, N * sizeof(VT), br);
     bulk_g2s(st + 2 * N, L.invdiag + off, N * sizeof(float), br);
     bulk_g2s(st + 3 * N, L.cx + off, N * sizeof(float), br);
     bulk_g2s(st + 4 * N, L.cy + off, N * sizeof(float), br);
@@ -159,6 +185,7 @@ __global__ void __launch_bounds__(pipe::NT, 1)
     }
   };
   auto halo_combine = [&](const TileRec& r, int ti, int u) {
+    widen_x<VT>(stages[u], tid);
     const float* st = stages[u];
 #pragma unroll
     for (int q = 0; q < 3; q++) {
@@ -216,7 +243,7 @@ __global__ void __launch_bounds__(pipe::NT, 1)
     }
     // 2: registers: couplings, 1/a_ii, b with the halo sums folded in
     float* X = stages[s];
-    const float* B = X + N;
+    const VT* B = raw_b<VT>(X);
     const float* IV = X + 2 * N;
     const float* CX = X + 3 * N;
     const float* CY = X + 4 * N;
@@ -232,7 +259,7 @@ __global__ void __launch_bounds__(pipe::NT, 1)
         const float iv = IV[e];
         const bool fl = iv > 0.f;
         I[c][kk] = iv;
-        float r = B[e];
+        float r = to_f(B[e]);
         if (ii == 0) r += gs[0][jj + TS * k];
         if (ii == TS - 1) r += gs[1][jj + TS * k];
         if (jj == 0) r += gs[2][ii + TS * k];
@@ -276,10 +303,16 @@ __global__ void __launch_bounds__(pipe::NT, 1)
         half(std::integral_constant<int, 1>());
       }
     }
-    // 4: the tile leaves by one bulk store
+    // 4: the tile leaves by one bulk store (narrowed into slot 1 first when
+    // the vectors are 16-bit; slot 1's b is no longer read)
+    if (!std::is_same<VT, float>::value) {
+      VT* xr = raw_x<VT>(X);
+      for (int e = tid; e < N; e += NT) xr[e] = from_f<VT>(X[e]);
+      __syncthreads();
+    }
     if (tid == 0) {
       fence_proxy_async();
-      bulk_s2g(x + rc.off, X, N * sizeof(float));
+      bulk_s2g(x + rc.off, raw_x<VT>(X), N * sizeof(VT));
     }
     // 5: next tile's arrays landed -> its halo sums
     if (hasNext) {
@@ -331,14 +364,14 @@ inline std::vector<pipe::TileRec> build_tile_records(const Level& L) {
 // ---------------------------------------------------------------------------
 enum { APPLY_MATVEC = 0, APPLY_RESIDUAL = 1 };
 
-template <int MODE>
+template <int MODE, typename VT, typename VC>
 __global__ void __launch_bounds__(pipe::NT, 1)
-    k_apply_pipe16(LevelView L, int tileBase, int count, const float* __restrict__ x,
-                   const float* __restrict__ b, float* __restrict__ y,
-                   float* __restrict__ bc, const int64_t* __restrict__ coarseOff,
+    k_apply_pipe16(LevelView L, int tileBase, int count, const VT* __restrict__ x,
+                   const VT* __restrict__ b, VT* __restrict__ y,
+                   VC* __restrict__ bc, const int64_t* __restrict__ coarseOff,
                    double* __restrict__ partial, int* __restrict__ err) {
   using namespace pipe;
-  constexpr int NARR = MODE == APPLY_RESIDUAL ? 6 : 5;  // x, [b], a, cx, cy, cz
+  constexpr int NVEC = MODE == APPLY_RESIDUAL ? 2 : 1;  // x, [b]
   extern __shared__ __align__(128) float sm[];
   float* stages[2] = {sm + GUARD, sm + GUARD + 6 * N};
   float(*gsb)[6][TS * TS] = reinterpret_cast<float(*)[6][TS * TS]>(sm + GUARD + 12 * N);
@@ -362,10 +395,11 @@ __global__ void __launch_bounds__(pipe::NT, 1)
     auto issue_arrays = [&](const TileRec& r, float* st, uint64_t* br, int tRec, int slot) {
       fence_proxy_async();
       const bool rec = tRec < count;
-      mbar_expect_tx(br, NARR * N * sizeof(float) + (rec ? sizeof(TileRec) : 0));
+      mbar_expect_tx(br, NVEC * N * sizeof(VT) + 4 * N * sizeof(float) +
+                             (rec ? sizeof(TileRec) : 0));
       const int64_t off = r.off;
-      bulk_g2s(st + 0 * N, x + off, N * sizeof(float), br);
-      if (MODE == APPLY_RESIDUAL) bulk_g2s(st + 1 * N, b + off, N * sizeof(float), br);
+      bulk_g2s(raw_x<VT>(st), x + off, N * sizeof(VT), br);
+      if (MODE == APPLY_RESIDUAL) bulk_g2s(raw_b<VT>(st), b + off, N * sizeof(VT), br);
       bulk_g2s(st + 2 * N, L.diag + off, N * sizeof(float), br);
       bulk_g2s(st + 3 * N, L.cx + off, N * sizeof(float), br);
       bulk_g2s(st + 4 * N, L.cy + off, N * sizeof(float), br);
@@ -382,6 +416,7 @@ __global__ void __launch_bounds__(pipe::NT, 1)
       if (MODE == APPLY_RESIDUAL && tid < 6) cmap[u][tid] = L.toCoarse[(size_t)ti * 6 + tid];
     };
     auto halo_combine = [&](const TileRec& r, int ti, int u) {
+      widen_x<VT>(stages[u], tid);
       const float* st = stages[u];
 #pragma unroll
       for (int q = 0; q < 3; q++) {
@@ -433,7 +468,7 @@ __global__ void __launch_bounds__(pipe::NT, 1)
         halo_issue(rn, tileBase + tn, u);
       }
       float* X = stages[s];
-      const float* B = X + N;
+      const VT* B = raw_b<VT>(X);
       const float* D = X + 2 * N;
       const float* CX = X + 3 * N;
       const float* CY = X + 4 * N;
@@ -460,8 +495,9 @@ __global__ void __launch_bounds__(pipe::NT, 1)
         float v = 0.f;
         if (dg > 0.f) v = dg * xc - S;
         if (MODE == APPLY_RESIDUAL) {
-          if (dg > 0.f) v = B[e] - v;
+          if (dg > 0.f) v = to_f(B[e]) - v;
         } else {
+          v = to_f(from_f<VT>(v));  // the dot product sees the stored q
           acc += (double)xc * (double)v;
         }
         yv[kk] = v;
@@ -469,19 +505,25 @@ __global__ void __launch_bounds__(pipe::NT, 1)
         xc = xp;
       }
       __syncthreads();  // every thread has read its D / neighbours before Y is written
+      if (MODE == APPLY_MATVEC) {
+        VT* Yv = reinterpret_cast<VT*>(Y);
 #pragma unroll
-      for (int kk = 0; kk < 8; kk++) Y[tidx(TS, i, j, k0 + kk)] = yv[kk];
+        for (int kk = 0; kk < 8; kk++) Yv[tidx(TS, i, j, k0 + kk)] = from_f<VT>(yv[kk]);
+      } else {
+#pragma unroll
+        for (int kk = 0; kk < 8; kk++) Y[tidx(TS, i, j, k0 + kk)] = yv[kk];
+      }
       __syncthreads();
       if (MODE == APPLY_MATVEC) {
         if (tid == 0) {
           fence_proxy_async();
-          bulk_s2g(y + rc.off, Y, N * sizeof(float));
+          bulk_s2g(y + rc.off, Y, N * sizeof(VT));
         }
       } else {
         const int* tc = cmap[s];
         const int ct = tc[0];
         if (ct >= 0) {
-          float* dst = bc + coarseOff[ct];
+          VC* dst = bc + coarseOff[ct];
           const int ox = tc[1], oy = tc[2], oz = tc[3], cts = tc[5];
           if (tc[4]) {
             constexpr int H = TS / 2;
@@ -491,11 +533,11 @@ __global__ void __launch_bounds__(pipe::NT, 1)
             const float sum = Y[e] + Y[e + 1] + Y[e + TS] + Y[e + TS + 1] + Y[e + TS * TS] +
                               Y[e + TS * TS + 1] + Y[e + TS * TS + TS] +
                               Y[e + TS * TS + TS + 1];
-            dst[tidx(cts, ox + ci, oy + cj, oz + ck)] = sum;
+            dst[tidx(cts, ox + ci, oy + cj, oz + ck)] = from_f<VC>(sum);
           } else {
             for (int e = tid; e < N; e += NT) {
               const int ii = e % TS, jj = (e / TS) % TS, kk = e / (TS * TS);
-              dst[tidx(cts, ox + ii, oy + jj, oz + kk)] = Y[e];
+              dst[tidx(cts, ox + ii, oy + jj, oz + kk)] = from_f<VC>(Y[e]);
             }
           }
         }

@@ -22,6 +22,9 @@ STATUS = {0: "MSBG_OK", 1: "MSBG_ERROR", 2: "MSBG_ENOMEM", 4: "MSBG_ENOTIMPL",
 
 BLOCK_NULL, BLOCK_VALUE, BLOCK_EMPTY, BLOCK_FULL = 0, 1, 2, 3
 
+# storage types of the solver vectors (msbg_gpu_solve_params.storage)
+F32, F16, BF16, F64 = 0, 1, 2, 3
+
 _lib = None
 
 

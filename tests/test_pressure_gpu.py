@@ -78,3 +78,74 @@ def test_fp64_refinement_reaches_true_residual_and_oracle(gpu_ctx, res, bsx0, nl
     # the FP64 iterate's residual, recomputed by the oracle's own matrix
     r = bo - oracle.pressure_apply_oracle(s, x64)
     assert np.linalg.norm(r) <= 1.5e-6 * np.linalg.norm(bo)
+
+
+@pytest.mark.parametrize("storage", [msbg_gpu.F16, msbg_gpu.BF16])
+@pytest.mark.parametrize("res,bsx0,nl,band", [(128, 16, 2, 8.0), (128, 32, 2, 8.0),
+                                              (128, 16, 3, 4.0)])
+def test_16bit_vectors_under_fp64_refinement_reach_oracle(gpu_ctx, storage, res, bsx0, nl, band):
+    """FP16 / BF16 level-0 vectors, FP32 arithmetic, FP64 refinement: the same
+    true residual (1e-6) and the same distance to the FP64 oracle (1e-5) as the
+    FP32 solve; the inner solves stop near the 16-bit rounding level, so more
+    refinement steps are taken."""
+    s = msbg_gpu.PressureScene(res, bsx0, nl, band=band, seed=11)
+    gpu_ctx.pressure_prepare(s)
+    ref = gpu_ctx.pressure_solve(tol=1e-6, maxRefine=4)
+    assert ref.status == 0, ref.status
+    info = gpu_ctx.pressure_solve(tol=1e-6, storage=storage, maxRefine=30)
+    assert info.status == 0, info.status
+    assert info.relResidual <= 1e-6, info.relResidual
+    assert info.refinements >= 2
+    assert info.iterations <= 4 * ref.iterations + 10, (info.iterations, ref.iterations)
+    xo, bo, it, rr = oracle.pressure_oracle(s, tol=1e-12)
+    x64 = gpu_ctx.pressure_download(fp64=True)
+    assert rel_err(x64, xo) <= 1e-5, rel_err(x64, xo)
+    r = bo - oracle.pressure_apply_oracle(s, x64)
+    assert np.linalg.norm(r) <= 1.5e-6 * np.linalg.norm(bo)
+
+
+def test_16bit_vectors_always_refine(gpu_ctx):
+    """maxRefine = 0 with 16-bit storage still runs the FP64 refinement."""
+    s = msbg_gpu.PressureScene(64, 16, 2, band=4.0, seed=3)
+    gpu_ctx.pressure_prepare(s)
+    info = gpu_ctx.pressure_solve(tol=1e-6, storage=msbg_gpu.F16, maxRefine=0)
+    assert info.status == 0 and info.refinements >= 1
+    assert info.relResidual <= 1e-6
+
+
+def test_16bit_solves_are_deterministic(gpu_ctx):
+    s = msbg_gpu.PressureScene(64, 16, 2, band=4.0, seed=8)
+    gpu_ctx.pressure_prepare(s)
+    out = []
+    for _ in range(2):
+        gpu_ctx.pressure_solve(tol=1e-6, storage=msbg_gpu.BF16, maxRefine=30)
+        out.append(gpu_ctx.pressure_download(fp64=True))
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_unsupported_storage_is_rejected(gpu_ctx):
+    s = msbg_gpu.PressureScene(64, 16, 2, band=4.0, seed=3)
+    gpu_ctx.pressure_prepare(s)
+    with pytest.raises(msbg_gpu.MsbgError):
+        gpu_ctx.pressure_solve(tol=1e-6, storage=msbg_gpu.F64)
+
+
+def test_uncovered_coarse_cells_read_as_zero():
+    """Coarse cells under finer tiles that do not exist are never written by
+    the restriction.  Here the context first fills and frees block tables of a
+    smoother channel, so the pressure buffers allocated next start on recycled
+    memory; the solve must still converge (it did not while those cells were
+    left uninitialised and the recycled bits happened to be NaN patterns)."""
+    ctx = msbg_gpu.Context(0)
+    for _ in range(3):
+        kind, vals = msbg_gpu.sphere_sdf_scene(256, 8, n_spheres=4, rmin=8, rmax=16, seed=5)
+        ctx.set_topology(256, 256, 256, 8)
+        ctx.upload_channel(1, 0, kind, vals[: int((kind == 1).sum())], 4.0, -4.0)
+    ctx.set_topology(64, 64, 64, 8)  # frees the channel above
+    s = msbg_gpu.PressureScene(128, 16, 2, band=8.0, seed=11)
+    ctx.pressure_prepare(s)
+    for storage in (msbg_gpu.F32, msbg_gpu.F16):
+        info = ctx.pressure_solve(tol=1e-6, storage=storage, maxRefine=30)
+        assert info.status == 0, (storage, info.status)
+        assert info.relResidual <= 1e-6
+    ctx.close()
