@@ -291,7 +291,7 @@ def bench_mgpcg(args):
     ms_sw, bytes_sw = ctx.pressure_profile(0, 20, c["inner"])
     ms_vc, bytes_vc = ctx.pressure_profile(2, 5, c["inner"])
     cells0 = int(st.cells[0])
-    dpc = read_profile_value("k_smooth_16_mgpcg_1024_b32.txt", "dram_bytes_per_cell")
+    dpc = read_profile_value("k_smooth_pipe16_mgpcg_b32.txt", "dram_bytes_per_cell")
     launches_sweep = None
     roof = {"bound": "hbm", "achieved": bytes_sw / (ms_sw * 1e-3) / 1e9, "peak": hbm,
             "unit": "GB/s", "frac": bytes_sw / (ms_sw * 1e-3) / 1e9 / hbm, "peak_kind": pk_kind,
