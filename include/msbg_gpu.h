@@ -189,6 +189,9 @@ typedef struct {
                        residual.  16-bit storage always refines (0 = 30). */
   int useGraph;     /* capture one PCG iteration in a CUDA graph */
   float coarseScale; /* coarse-grid correction factor (default 1.8; 1 = plain) */
+  int learned;      /* 0: none; 1: the network attached by
+                       msbg_gpu_pressure_set_cnn predicts the initial guess
+                       (forces the FP64 refinement, maxRefine 0 = 30) */
 } msbg_gpu_solve_params;
 
 typedef struct {
@@ -202,6 +205,8 @@ typedef struct {
   int64_t fineCells;     /* cells of MG level 0 (liquid) */
   int nMgLevels;
   int64_t kernelLaunches; /* kernels launched inside the timed solve */
+  double initialRelResidual; /* |b - A x0| / |b| of the starting iterate
+                                (1 without a learned guess) */
 } msbg_gpu_solve_info;
 
 void msbg_gpu_solve_params_default(msbg_gpu_solve_params* p);

@@ -26,6 +26,7 @@
 #include "pressure.h"
 #include "pressure_kernels.cuh"
 #include "vec_types.cuh"
+#include "cnn.cuh"
 
 namespace msbg {
 namespace ps {
@@ -33,6 +34,7 @@ namespace ps {
 #include "tile_kernels.cuh"
 #include "smooth_pipe.cuh"
 #include "refine.cuh"
+#include "cnn_features.cuh"
 
 // ---------------------------------------------------------------------------
 // solver state
@@ -52,6 +54,15 @@ struct Solver {
   Scalars* hScal = nullptr;  // pinned
   int bsx0 = 0, nbx = 0, nby = 0, nbz = 0;
   std::vector<int> blockLevel;
+  // learned network (not owned) and its level-0 16^3 tiles
+  msbg_cnn* net = nullptr;
+  int nCnnTiles = 0;
+  float levelNorm = 0.f;
+  DeviceBuffer cnnTiles, cnnLevel;          // [nCnnTiles] tile id, resolution level
+  DeviceBuffer cFeat, cScale, cOff, cS1, cS2, guess, cIdx;
+  std::vector<int> cnnTilesHost, cnnLevelHost;
+  int cnnChunk = 0;
+  bool haveX64 = false;  // x64 holds the solution of the last refined solve
 };
 
 // Dynamic shared-memory limits of the kernels a level-0 vector type needs
@@ -246,6 +257,7 @@ extern "C" void msbg_gpu_solve_params_default(msbg_gpu_solve_params* p) {
   // smooth errors; scaling the coarse correction by 1.8 restores
   // size-independent convergence (10-13 PCG iterations from 256^3 to 1024^3).
   p->coarseScale = 1.8f;
+  p->learned = 0;
 }
 
 extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
@@ -298,6 +310,7 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
     MSBG_CUDA_TRY(ctx, upload(D->passTiles, L.passTiles, st));
     MSBG_CUDA_TRY(ctx, upload(D->groupTiles, L.groupTiles, st));
     MSBG_CUDA_TRY(ctx, upload(D->diag, L.diag, st));
+    if (m == 0) MSBG_CUDA_TRY(ctx, upload(D->ctype, L.ctype, st));
     {
       std::vector<float> inv(L.diag.size());
       for (size_t c = 0; c < inv.size(); c++)
@@ -335,6 +348,25 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
     v.cz = D->cz.as<float>();
     v.ifc = D->ifc.as<float>();
     S.views.push_back(v);
+    if (m == 0) {
+      // tiles the learned network runs on: the 16^3 tiles of level 0
+      std::vector<int> ids, lv;
+      int maxLv = 0;
+      for (size_t i = 0; i < L.tiles.size(); i++) {
+        maxLv = std::max(maxLv, L.tiles[i].level);
+        if (L.tiles[i].ts == cnn::TS) {
+          ids.push_back((int)i);
+          lv.push_back(L.tiles[i].level);
+        }
+      }
+      S.nCnnTiles = (int)ids.size();
+      S.cnnTilesHost = ids;
+      S.cnnLevelHost = lv;
+      S.levelNorm = 1.0f / (float)std::max(1, topo->nLevels - 1);
+      MSBG_CUDA_TRY(ctx, upload(S.cnnTiles, ids, st));
+      MSBG_CUDA_TRY(ctx, upload(S.cnnLevel, lv, st));
+      MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));  // host vectors are temporaries
+    }
     S.dev.push_back(std::move(D));
   }
   const Level& L0 = S.H.levels[0];
@@ -498,6 +530,7 @@ int absmax(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const V* v, int64_t n, d
 struct SolveOut {
   int iters = 0, status = 1, refinements = 0;
   double relres = 0;
+  double initialRelres = 1;  // |b - A x0| / |b| of the starting iterate
 };
 
 // Plain MGPCG on the FP32 right-hand side, stopping on the recursive
@@ -533,6 +566,40 @@ int solve_plain(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gpu_s
   return MSBG_OK;
 }
 
+// Learned prediction from a level-0 FP32 vector `val` (right-hand side or
+// residual) into out (all level-0 cells; cells of tiles the network does not
+// cover stay 0), in chunks of up to 4096 tiles.
+int learned_predict(msbg_gpu_ctx* ctx, Solver& S, cudaStream_t st, const float* val, float* out,
+                    int64_t& launches) {
+  const int64_t n = S.H.levels[0].nCells;
+  MSBG_CUDA_TRY(ctx, cudaMemsetAsync(out, 0, sizeof(float) * n, st));
+  if (!S.nCnnTiles) return MSBG_OK;
+  const int CH = std::min(4096, S.nCnnTiles);
+  if (S.cnnChunk < CH) {
+    MSBG_CUDA_TRY(ctx, S.cFeat.ensure(sizeof(float) * CH * cnn::NFEAT * cnn::NPAD));
+    MSBG_CUDA_TRY(ctx, S.cScale.ensure(sizeof(float) * CH));
+    MSBG_CUDA_TRY(ctx, S.cOff.ensure(sizeof(int64_t) * CH));
+    MSBG_CUDA_TRY(ctx, S.cS1.ensure(sizeof(__nv_bfloat16) * (size_t)CH * cnn::NCELL * cnn::NC));
+    MSBG_CUDA_TRY(ctx, S.cS2.ensure(sizeof(__nv_bfloat16) * (size_t)CH * cnn::NCELL * cnn::NC));
+    S.cnnChunk = CH;
+  }
+  for (int c0 = 0; c0 < S.nCnnTiles; c0 += CH) {
+    const int cnt = std::min(CH, S.nCnnTiles - c0);
+    k_cnn_features<<<cnt, FEAT_THREADS, 0, st>>>(
+        S.views[0], S.dev[0]->ctype.as<uint8_t>(), S.cnnTiles.as<int>() + c0,
+        S.cnnLevel.as<int>() + c0, S.levelNorm, val, nullptr, S.cFeat.as<float>(),
+        S.cScale.as<float>(), S.cOff.as<int64_t>(), nullptr, nullptr);
+    if (cnn::forward(S.net, S.cFeat.as<float>(), out, S.cOff.as<int64_t>(), S.cScale.as<float>(),
+                     cnt, st, S.cS1.as<__nv_bfloat16>(), S.cS2.as<__nv_bfloat16>()))
+      return set_error(ctx, MSBG_ERROR, "learned network launch failed");
+    launches += 5;
+  }
+  MSBG_CUDA_TRY(ctx, cudaGetLastError());
+  const int e = cnn::take_error(S.net, st);
+  if (e) return set_error(ctx, e, "learned network: a tensor-core wait gave up");
+  return MSBG_OK;
+}
+
 // Inner relative tolerance floor per storage type: a few unit roundoffs of
 // the stored vectors (FP32 2^-24, FP16 2^-11, BF16 2^-8).
 template <typename VT> constexpr double inner_floor() { return 1e-5; }
@@ -562,13 +629,35 @@ int solve_refined(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const msbg_gpu_so
   VT* rinV = WIDE ? reinterpret_cast<VT*>(rin) : S.rinv.as<VT>();
   VT* e = S.dev[0]->x.as<VT>();
   const float* b = S.rhs0.as<float>();
-  cudaMemsetAsync(x64, 0, sizeof(double) * n, st);
-  double bb = 0, rr = 0, gain = 0;
   int rc = MSBG_OK;
+  if (p->learned >= 1) {
+    // initial guess predicted by the network from the right-hand side
+    rc = learned_predict(ctx, S, st, b, S.guess.as<float>(), R.launches);
+    if (rc) return rc;
+    k_set64_masked<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, S.guess.as<float>(), S.views[0].diag, n);
+    R.launches++;
+  } else {
+    cudaMemsetAsync(x64, 0, sizeof(double) * n, st);
+  }
+  double bb = 0, rr = 0, gain = 0;
   for (int outer = 0;; outer++) {
     rc = residual64(ctx, S, R, b, rin, &rr);
     if (rc) return rc;
-    if (outer == 0) bb = rr;
+    if (outer == 0) {
+      // |b|^2 (the guess, when there is one, is not part of the reference norm)
+      bb = rr;
+      if (p->learned >= 1) {
+        double* part = S.partial.as<double>();
+        Scalars* sc = S.scal.as<Scalars>();
+        k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(b, b, n, part);
+        k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_BB);
+        cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+        R.launches += 2;
+        MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+        bb = S.hScal->bb;
+        o.initialRelres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+      }
+    }
     o.relres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
     if (!(bb > 1e-300) || o.relres <= p->tol) {
       o.status = 0;
@@ -642,12 +731,14 @@ int solve_typed(msbg_gpu_ctx* ctx, Solver& S, const msbg_gpu_solve_params* p, cu
   R.numSMs = S.numSMs;
   const int64_t n = S.H.levels[0].nCells;
   constexpr bool WIDE = std::is_same<VT, float>::value;
-  // 16-bit vectors always run under the FP64 refinement
-  const int maxRefine = p->maxRefine > 0 ? p->maxRefine : (WIDE ? 0 : 30);
+  // 16-bit vectors and the learned guess always run under the FP64 refinement
+  const int maxRefine = p->maxRefine > 0 ? p->maxRefine : (WIDE && !p->learned ? 0 : 30);
+  S.haveX64 = false;
   if (maxRefine > 0) {
     MSBG_CUDA_TRY(ctx, S.x64.ensure(sizeof(double) * n));
     MSBG_CUDA_TRY(ctx, S.rin.ensure(sizeof(float) * n));
     if (!WIDE) MSBG_CUDA_TRY(ctx, S.rinv.ensure(sizeof(VT) * n));
+    if (p->learned) MSBG_CUDA_TRY(ctx, S.guess.ensure(sizeof(float) * n));
   }
   cudaGraphExec_t exec = nullptr;
   int64_t perIter = 0;
@@ -659,6 +750,7 @@ int solve_typed(msbg_gpu_ctx* ctx, Solver& S, const msbg_gpu_solve_params* p, cu
   if (maxRefine > 0) {
     rc = solve_refined(ctx, S, R, p, maxRefine, exec, perIter, o);
     cudaEventRecord(e1, st);
+    S.haveX64 = rc == MSBG_OK;
   }
   if (exec) cudaGraphExecDestroy(exec);
   *launches = R.launches;
@@ -677,8 +769,13 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
     return set_error(ctx, MSBG_EINVARG, "invalid solve parameters");
   if (p->storage != MSBG_F32 && p->storage != MSBG_F16 && p->storage != MSBG_BF16)
     return set_error(ctx, MSBG_ENOTIMPL, "storage type %d not available", p->storage);
+  if (p->learned < 0 || p->learned > 1)
+    return set_error(ctx, MSBG_EINVARG, "learned = %d (0 none, 1 initial guess)", p->learned);
+  if (p->learned && !ctx->cnn)
+    return set_error(ctx, MSBG_EINVARG, "learned solve without a network (msbg_gpu_pressure_set_cnn)");
   cudaSetDevice(ctx->device);
   Solver& S = *sp;
+  S.net = ctx->cnn;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -707,7 +804,46 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
     info->fineCells = L0.nFluid;
     info->nMgLevels = (int)S.H.levels.size();
     info->kernelLaunches = launches;
+    info->initialRelResidual = o.initialRelres;
   }
+  return MSBG_OK;
+}
+
+extern "C" int msbg_gpu_pressure_set_cnn(msbg_gpu_ctx* ctx, msbg_cnn* net) {
+  if (!ctx) return MSBG_EINVARG;
+  ctx->cnn = net;
+  return MSBG_OK;
+}
+
+extern "C" int msbg_gpu_pressure_training_pairs(msbg_gpu_ctx* ctx, float* feat, float* target,
+                                                float* mask, int maxPairs, int* nPairs) {
+  if (!ctx || !feat || !target || !mask || maxPairs <= 0 || !nPairs) return MSBG_EINVARG;
+  auto& sp = solver_of(ctx);
+  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
+  Solver& S = *sp;
+  if (!S.haveX64)
+    return set_error(ctx, MSBG_EINVARG, "training pairs need a refined solve (maxRefine > 0) first");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const int np = std::min(maxPairs, S.nCnnTiles);
+  *nPairs = np;
+  if (np == 0) return MSBG_OK;
+  std::vector<int> sel(2 * (size_t)np);
+  for (int i = 0; i < np; i++) {
+    const int k = (int)((int64_t)i * S.nCnnTiles / np);
+    sel[i] = S.cnnTilesHost[k];
+    sel[np + i] = S.cnnLevelHost[k];
+  }
+  DeviceBuffer scale, off;
+  MSBG_CUDA_TRY(ctx, upload(S.cIdx, sel, st));
+  MSBG_CUDA_TRY(ctx, scale.ensure(sizeof(float) * np));
+  MSBG_CUDA_TRY(ctx, off.ensure(sizeof(int64_t) * np));
+  k_cnn_features<<<np, FEAT_THREADS, 0, st>>>(
+      S.views[0], S.dev[0]->ctype.as<uint8_t>(), S.cIdx.as<int>(), S.cIdx.as<int>() + np,
+      S.levelNorm, S.rhs0.as<float>(), S.x64.as<double>(), feat, scale.as<float>(),
+      off.as<int64_t>(), target, mask);
+  MSBG_CUDA_TRY(ctx, cudaGetLastError());
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   return MSBG_OK;
 }
 

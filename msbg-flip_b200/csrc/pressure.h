@@ -35,6 +35,9 @@ enum { F_KIND = 0, F_T0 = 1, F_OA = 5, F_OB = 6, F_COV = 7, F_NTS = 8 };
 // face plane: dir 0 -> (y,z), dir 1 -> (x,z), dir 2 -> (x,y); plane index
 // a + ts*b.
 
+// Cell types kept for the learned network's mask channels (MG level 0).
+enum : uint8_t { CT_AIR = 0, CT_LIQUID = 1, CT_SOLID = 2 };
+
 struct Tile {
   int level;       // resolution level: cell edge = 2^level fine voxels
   int ts;          // cells per edge
@@ -51,6 +54,7 @@ struct Level {
   // operator: a_ii, lower-face couplings to same-level neighbours, interface
   // couplings (stored on the finer side, one per fine boundary cell)
   std::vector<float> diag, cx, cy, cz, ifc, rhs;
+  std::vector<uint8_t> ctype;      // MG level 0 only: CT_* per cell
   // tile maps per resolution level: dense raster of tile ids (-1 = none)
   std::vector<std::vector<int>> tmap = std::vector<std::vector<int>>(32);
   std::vector<int> tmapN = std::vector<int>(32, 0);  // tiles per edge (0 = level absent)
@@ -79,6 +83,7 @@ struct LevelDev {
   DeviceBuffer diag, invdiag, cx, cy, cz, ifc;
   DeviceBuffer tileRec;            // 256-byte per-tile records (smooth_pipe.cuh)
   DeviceBuffer x, b, r;            // FP32 work vectors of this level
+  DeviceBuffer ctype;              // level 0: CT_* per cell
 };
 
 struct Hierarchy {

@@ -31,6 +31,7 @@ namespace ps {
 namespace {
 
 constexpr uint16_t CELL_NONFLUID = 0x1 | 0x2 | 0x1000;  // SOLID | FIXED | VOID
+constexpr uint16_t CELL_SOLID_BIT = 0x1;
 
 int pow2_divisor(int v, int cap) {
   int p = 1;
@@ -566,6 +567,7 @@ int build_hierarchy(Hierarchy& H, int sx, int sy, int sz, int bsx0, int nLevels,
     register_tiles(L, tiles);
     build_faces(C, L);
     fluid.assign(L.nCells, 0);
+    L.ctype.assign(L.nCells, CT_AIR);
 #pragma omp parallel for schedule(dynamic, 4)
     for (int64_t ti = 0; ti < (int64_t)L.tiles.size(); ti++) {
       const Tile& t = L.tiles[ti];
@@ -574,7 +576,9 @@ int build_hierarchy(Hierarchy& H, int sx, int sy, int sz, int bsx0, int nLevels,
           for (int i = 0; i < t.ts; i++) {
             uint16_t ct = cb->sampleCellType(cb->user, (t.ox + i) << t.level,
                                              (t.oy + j) << t.level, (t.oz + k) << t.level);
-            fluid[t.off + i + (int64_t)t.ts * (j + (int64_t)t.ts * k)] = !(ct & CELL_NONFLUID);
+            const int64_t c = t.off + i + (int64_t)t.ts * (j + (int64_t)t.ts * k);
+            fluid[c] = !(ct & CELL_NONFLUID);
+            L.ctype[c] = fluid[c] ? CT_LIQUID : (ct & CELL_SOLID_BIT) ? CT_SOLID : CT_AIR;
           }
     }
     sample_level0(C, L, fluid);

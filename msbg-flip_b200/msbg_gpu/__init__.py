@@ -114,6 +114,7 @@ class Context:
             raise MsbgError(rc, "msbg_gpu_init")
         self._h = h
         self._L = L
+        self.device = device
 
     def _check(self, rc, what):
         if rc != MSBG_OK:
@@ -206,14 +207,14 @@ class SolveParams(C.Structure):
     _fields_ = [("nPre", C.c_int), ("nPost", C.c_int), ("nCoarse", C.c_int),
                 ("maxIter", C.c_int), ("tol", C.c_float), ("innerIter", C.c_int),
                 ("storage", C.c_int), ("maxRefine", C.c_int), ("useGraph", C.c_int),
-                ("coarseScale", C.c_float)]
+                ("coarseScale", C.c_float), ("learned", C.c_int)]
 
 
 class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("status", C.c_int),
                 ("relResidual", C.c_double), ("solveSeconds", C.c_double),
                 ("fineCells", C.c_int64), ("nMgLevels", C.c_int),
-                ("kernelLaunches", C.c_int64)]
+                ("kernelLaunches", C.c_int64), ("initialRelResidual", C.c_double)]
 
 
 class PressureStats(C.Structure):
@@ -362,3 +363,6 @@ Context.pressure_solve = _ctx_pressure_solve
 Context.pressure_download = _ctx_pressure_download
 Context.pressure_profile = _ctx_pressure_profile
 Context.last_solve_launches = lambda self: getattr(self, "_last_launches", None)
+
+
+from .learned import Cnn, collect_training_pairs, train_cnn  # noqa: E402,F401
