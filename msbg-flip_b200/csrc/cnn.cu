@@ -64,108 +64,124 @@ __global__ void k_pack(const float* __restrict__ w, __nv_bfloat16* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// convolution (tcgen05)
+// layout conversion
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t pack_bf2(float a, float b) {
   __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
   return *reinterpret_cast<uint32_t*>(&h);
 }
 
-template <int IN, int EPI>
+// feat [n][4][NPAD] FP32 planes -> padded bf16 layout (half 0: the 4
+// features and 4 zero channels; half 1: zeros).  One thread per padded cell.
+__global__ void k_feat_pack(int n, const float* __restrict__ feat, uint4* __restrict__ x) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n * NPAD) return;
+  const int64_t t = i / NPAD;
+  const int c = (int)(i % NPAD);
+  const float* f = feat + t * NFEAT * NPAD;
+  uint4 v;
+  v.x = pack_bf2(f[c], f[NPAD + c]);
+  v.y = pack_bf2(f[2 * NPAD + c], f[3 * NPAD + c]);
+  v.z = 0u;
+  v.w = 0u;
+  x[(t * 2) * NPAD + c] = v;
+  x[(t * 2 + 1) * NPAD + c] = make_uint4(0, 0, 0, 0);
+}
+
+// ---------------------------------------------------------------------------
+// convolution (tcgen05)
+// ---------------------------------------------------------------------------
+// One CTA of 256 threads per SM walks its tiles.  A tile's input (padded
+// layout) arrives by two bulk copies of one channel half each.  Thread 0
+// issues the 54 MMAs of plane z+1 (into the other TMEM column set) before
+// everyone drains plane z: warp w reads TMEM lanes 32*(w%4).. of column half
+// w/4 (the x half of the plane), applies the epilogue and writes the cells.
+// The next tile's copies are issued as soon as the last plane's MMAs are
+// done, so they overlap the last epilogue.  A tcgen05.mma of N = 16 costs
+// about 45 cycles whatever its operands (measured), so 864 MMAs bound a tile
+// to ~20 us per layer.  Every wait is bounded.
+template <int EPI>
 __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3_tc(ConvArgs a) {
   extern __shared__ __align__(1024) uint8_t sm[];
   uint8_t* act = sm;
   uint8_t* wts = sm + 2 * HALF_BYTES;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * HALF_BYTES + WIMG * 2);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * HALF_BYTES + WIMG * 2);  // [0,1] MMA, [2] input
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 3);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int G = gridDim.x;
   if ((int)blockIdx.x >= a.n) return;
 
   for (int i = tid; i < WIMG * 2 / 16; i += CONV_THREADS)
     reinterpret_cast<uint4*>(wts)[i] = reinterpret_cast<const uint4*>(a.wimg)[i];
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int b = 0; b < 3; b++) mbar_init(&bar[b], 1);
     fence_mbar_init();
   }
   if (warp == 0) {
     tmem_alloc(tslot, 64);
     tmem_relinquish();
   }
+  fence_proxy_async();  // the weight image (generic writes) -> tensor core
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *tslot;
   const uint32_t idesc = idesc_bf16_f32(128, 16);
-  const uint32_t actA = smem_addr(act), wA = smem_addr(wts);
-  // one plane = 2 M blocks (x halves) x 27 taps, into columns (z&1)*32 + 16*xh
+  const uint64_t a0 = smem_desc(smem_addr(act), HALF_BYTES, PD * 16);
+  const uint64_t b0 = smem_desc(smem_addr(wts), 256, 128);
+  auto load_tile = [&](int t) {
+    mbar_expect_tx(&bar[2], 2 * HALF_BYTES);
+    bulk_g2s(act, a.in + (size_t)t * 2 * NPAD, HALF_BYTES, &bar[2]);
+    bulk_g2s(act + HALF_BYTES, a.in + ((size_t)t * 2 + 1) * NPAD, HALF_BYTES, &bar[2]);
+  };
+  // Descriptors are built once; the start address field (address / 16) is the
+  // low bits: one cell = 16 bytes = +1, and no start reaches 2^14 * 16 bytes.
   auto issue = [&](int z) {
     tc_fence_after();
     const uint32_t cb = tbase + (uint32_t)((z & 1) * 32);
-#pragma unroll 1
-    for (int xh = 0; xh < 2; xh++)
-#pragma unroll 1
-      for (int tap = 0; tap < 27; tap++) {
+    const uint64_t az = a0 + (uint64_t)(z * PLANE);
+#pragma unroll
+    for (int tap = 0; tap < 27; tap++)
+#pragma unroll
+      for (int xh = 0; xh < 2; xh++) {
         const int kz = tap / 9, ky = (tap / 3) % 3, kx = tap % 3;
-        const uint32_t aa = actA + (uint32_t)((((z + kz) * PD + ky) * PD + 8 * xh + kx) * 16);
-        mma_bf16(cb + 16 * xh, smem_desc(aa, HALF_BYTES, PD * 16),
-                 smem_desc(wA + tap * 512, 256, 128), idesc, tap > 0 ? 1u : 0u);
+        mma_bf16(cb + 16 * xh, az + (uint64_t)((kz * PD + ky) * PD + 8 * xh + kx),
+                 b0 + (uint64_t)(tap * 32), idesc, tap > 0 ? 1u : 0u);
       }
     mma_commit(&bar[z & 1]);
   };
+  if (tid == 0) load_tile(blockIdx.x);
+  const int xh = warp >> 2, quarter = warp & 3;
+  const int r = 32 * quarter + lane;
+  const int x = 8 * xh + (r & 7), y = r >> 3;
   bool ok = true;
-  for (int t = blockIdx.x; t < a.n && ok; t += gridDim.x) {
-    // ---- the tile's input -> shared memory (bf16, two channel halves) ----
-    if (IN == IN_FEAT) {
-      const float* f = a.feat + (size_t)t * NFEAT * NPAD;
-      for (int c = tid; c < NPAD; c += CONV_THREADS) {
-        uint4 v;
-        v.x = pack_bf2(f[c], f[NPAD + c]);
-        v.y = pack_bf2(f[2 * NPAD + c], f[3 * NPAD + c]);
-        v.z = 0u;
-        v.w = 0u;
-        *reinterpret_cast<uint4*>(act + (size_t)c * 16) = v;
-        *reinterpret_cast<uint4*>(act + HALF_BYTES + (size_t)c * 16) = make_uint4(0, 0, 0, 0);
-      }
-    } else {
-      const uint4* src = reinterpret_cast<const uint4*>(a.in + (size_t)t * NCELL * NC);
-      for (int c = tid; c < NPAD; c += CONV_THREADS) {
-        const int px = c % PD, py = (c / PD) % PD, pz = c / (PD * PD);
-        uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
-        if (px >= 1 && px <= TS && py >= 1 && py <= TS && pz >= 1 && pz <= TS) {
-          const int cell = (px - 1) + TS * ((py - 1) + TS * (pz - 1));
-          lo = src[2 * cell];
-          hi = src[2 * cell + 1];
-        }
-        *reinterpret_cast<uint4*>(act + (size_t)c * 16) = lo;
-        *reinterpret_cast<uint4*>(act + HALF_BYTES + (size_t)c * 16) = hi;
-      }
+  for (int j = 0, t = blockIdx.x; t < a.n && ok; j++, t += G) {
+    if (!__syncthreads_and(mbar_wait(&bar[2], (uint32_t)(j & 1)))) {
+      ok = false;
+      break;
     }
-    fence_proxy_async();
-    tc_fence_before();
-    __syncthreads();
     if (tid == 0) issue(0);
+    const float s = (EPI == EPI_OUT0 && a.outScale) ? a.outScale[t] : 1.f;
+    const int64_t base = (EPI == EPI_OUT0) ? (a.outOff ? a.outOff[t] : (int64_t)t * NCELL) : 0;
     for (int z = 0; z < TS; z++) {
       if (tid == 0 && z + 1 < TS) issue(z + 1);
       if (!__syncthreads_and(mbar_wait(&bar[z & 1], (uint32_t)((z >> 1) & 1)))) {
         ok = false;
         break;
       }
+      // the tile's MMAs are all done: its input buffer takes the next tile
+      if (z == TS - 1 && tid == 0 && t + G < a.n) load_tile(t + G);
       tc_fence_after();
       float v[16];
-      const int xh = warp >> 2, quarter = warp & 3;
       tmem_ld16(tbase + ((uint32_t)(32 * quarter) << 16) + (uint32_t)((z & 1) * 32 + 16 * xh), v);
-      const int r = 32 * quarter + lane;
-      const int x = 8 * xh + (r & 7), y = r >> 3;
       const int cell = x + TS * (y + TS * z);
       if (EPI == EPI_OUT0) {
-        const float s = a.outScale ? a.outScale[t] : 1.f;
-        const int64_t base = a.outOff ? a.outOff[t] : (int64_t)t * NCELL;
         a.out0[base + cell] = v[0] * s;
       } else {
+        const size_t pc = (size_t)pad_index(cell);
+        const size_t o0 = ((size_t)t * 2) * NPAD + pc, o1 = o0 + NPAD;
         if (EPI == EPI_MASK) {
-          const uint4* mp = reinterpret_cast<const uint4*>(a.mask + ((size_t)t * NCELL + cell) * NC);
-          uint4 m2[2] = {mp[0], mp[1]};
+          uint4 m2[2] = {a.mask[o0], a.mask[o1]};
           const __nv_bfloat16* mb = reinterpret_cast<const __nv_bfloat16*>(m2);
 #pragma unroll
           for (int c = 0; c < 16; c++)
@@ -174,30 +190,28 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3_tc(ConvArgs a) {
 #pragma unroll
           for (int c = 0; c < 16; c++) v[c] = fmaxf(v[c], 0.f);
         }
-        uint4 o0, o1;
-        o0.x = pack_bf2(v[0], v[1]);
-        o0.y = pack_bf2(v[2], v[3]);
-        o0.z = pack_bf2(v[4], v[5]);
-        o0.w = pack_bf2(v[6], v[7]);
-        o1.x = pack_bf2(v[8], v[9]);
-        o1.y = pack_bf2(v[10], v[11]);
-        o1.z = pack_bf2(v[12], v[13]);
-        o1.w = pack_bf2(v[14], v[15]);
-        uint4* op = reinterpret_cast<uint4*>(a.out + ((size_t)t * NCELL + cell) * NC);
-        op[0] = o0;
-        op[1] = o1;
+        uint4 q0, q1;
+        q0.x = pack_bf2(v[0], v[1]);
+        q0.y = pack_bf2(v[2], v[3]);
+        q0.z = pack_bf2(v[4], v[5]);
+        q0.w = pack_bf2(v[6], v[7]);
+        q1.x = pack_bf2(v[8], v[9]);
+        q1.y = pack_bf2(v[10], v[11]);
+        q1.z = pack_bf2(v[12], v[13]);
+        q1.w = pack_bf2(v[14], v[15]);
+        a.out[o0] = q0;
+        a.out[o1] = q1;
       }
       tc_fence_before();
       __syncthreads();
     }
   }
-  if (!ok) {
-    // a wait gave up: flag it, give the MMAs in flight one more bounded wait
-    if (tid == 0) {
-      atomicExch(a.err, 1);
-      mbar_wait(&bar[0], 0);
-      mbar_wait(&bar[1], 0);
-    }
+  if (!ok && tid == 0) {
+    // a wait gave up: flag it, give the work in flight one more bounded wait
+    atomicExch(a.err, 1);
+    mbar_wait(&bar[0], 0);
+    mbar_wait(&bar[1], 0);
+    mbar_wait(&bar[2], 0);
   }
   tc_fence_before();
   __syncthreads();
@@ -209,61 +223,48 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3_tc(ConvArgs a) {
 // weight gradient (FP32 CUDA cores)
 // ---------------------------------------------------------------------------
 // partial[blockIdx][co][ci][tap] = sum over this CTA's tiles and their cells o
-// of dz[o][co] * X[o + tap][ci], X the layer input on the padded box (bf16,
-// as the forward pass reads it).  Thread (co, ci) = (tid >> 4, tid & 15).
+// of dz[o][co] * X[o + tap][ci], X the layer input on the padded box and dz
+// the output gradient (both in the padded bf16 layout, as the forward pass
+// reads them).  Thread (co, ci) = (tid >> 4, tid & 15).
 constexpr int WG_SLAB = 4;  // output planes per shared-memory slab
-constexpr size_t WG_SMEM = (size_t)(WG_SLAB + 2) * PD * PD * NC * 2 + (size_t)WG_SLAB * TS * TS * NC * 2;
+constexpr size_t WG_SMEM = (size_t)(WG_SLAB + 2) * PLANE * 32 + (size_t)WG_SLAB * TS * TS * 32;
 
-template <int IN>
-__global__ void __launch_bounds__(256) k_wgrad(int n, const float* __restrict__ feat,
-                                               const __nv_bfloat16* __restrict__ in,
-                                               const __nv_bfloat16* __restrict__ dz,
+__global__ void __launch_bounds__(256) k_wgrad(int n, const uint4* __restrict__ X,
+                                               const uint4* __restrict__ dz,
                                                float* __restrict__ partial) {
   extern __shared__ __align__(16) uint8_t smw[];
-  __nv_bfloat16* X = reinterpret_cast<__nv_bfloat16*>(smw);  // [(WG_SLAB+2)*PD*PD][16]
-  __nv_bfloat16* D =
-      reinterpret_cast<__nv_bfloat16*>(smw + (size_t)(WG_SLAB + 2) * PD * PD * NC * 2);  // [WG_SLAB*256][16]
+  __nv_bfloat16* Xs = reinterpret_cast<__nv_bfloat16*>(smw);  // [(WG_SLAB+2)*PLANE][16]
+  __nv_bfloat16* Ds = reinterpret_cast<__nv_bfloat16*>(smw + (size_t)(WG_SLAB + 2) * PLANE * 32);
   const int tid = threadIdx.x, co = tid >> 4, ci = tid & 15;
   float acc[27];
 #pragma unroll
   for (int k = 0; k < 27; k++) acc[k] = 0.f;
   for (int t = blockIdx.x; t < n; t += gridDim.x) {
+    const uint4* Xt = X + (size_t)t * 2 * NPAD;
+    const uint4* Dt = dz + (size_t)t * 2 * NPAD;
     for (int z0 = 0; z0 < TS; z0 += WG_SLAB) {
       __syncthreads();
-      // padded planes z0 .. z0+WG_SLAB+1
-      for (int c = tid; c < (WG_SLAB + 2) * PD * PD; c += 256) {
-        const int px = c % PD, py = (c / PD) % PD, pz = z0 + c / (PD * PD);
-        uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
-        if (IN == IN_FEAT) {
-          const float* f = feat + (size_t)t * NFEAT * NPAD;
-          const int pc = px + PD * (py + PD * pz);
-          lo.x = pack_bf2(f[pc], f[NPAD + pc]);
-          lo.y = pack_bf2(f[2 * NPAD + pc], f[3 * NPAD + pc]);
-        } else if (px >= 1 && px <= TS && py >= 1 && py <= TS && pz >= 1 && pz <= TS) {
-          const uint4* s = reinterpret_cast<const uint4*>(in + ((size_t)t * NCELL +
-                                                               (px - 1) + TS * ((py - 1) + TS * (pz - 1))) * NC);
-          lo = s[0];
-          hi = s[1];
-        }
-        reinterpret_cast<uint4*>(X)[2 * c] = lo;
-        reinterpret_cast<uint4*>(X)[2 * c + 1] = hi;
+      for (int c = tid; c < (WG_SLAB + 2) * PLANE; c += 256) {
+        const int pc = z0 * PLANE + c;
+        reinterpret_cast<uint4*>(Xs)[2 * c] = Xt[pc];
+        reinterpret_cast<uint4*>(Xs)[2 * c + 1] = Xt[NPAD + pc];
       }
       for (int c = tid; c < WG_SLAB * TS * TS; c += 256) {
-        const uint4* s = reinterpret_cast<const uint4*>(dz + ((size_t)t * NCELL + (size_t)z0 * TS * TS + c) * NC);
-        reinterpret_cast<uint4*>(D)[2 * c] = s[0];
-        reinterpret_cast<uint4*>(D)[2 * c + 1] = s[1];
+        const int pc = pad_index(z0 * TS * TS + c);
+        reinterpret_cast<uint4*>(Ds)[2 * c] = Dt[pc];
+        reinterpret_cast<uint4*>(Ds)[2 * c + 1] = Dt[NPAD + pc];
       }
       __syncthreads();
 #pragma unroll 1
       for (int o = 0; o < WG_SLAB * TS * TS; o++) {
-        const float d = __bfloat162float(D[o * NC + co]);
+        const float d = __bfloat162float(Ds[o * NC + co]);
         if (d == 0.f) continue;
         const int ox = o % TS, oy = (o / TS) % TS, oz = o / (TS * TS);
         const int base = ox + PD * (oy + PD * oz);
 #pragma unroll
         for (int k = 0; k < 27; k++) {
           const int kz = k / 9, ky = (k / 3) % 3, kx = k % 3;
-          acc[k] = fmaf(d, __bfloat162float(X[(base + kx + PD * (ky + PD * kz)) * NC + ci]), acc[k]);
+          acc[k] = fmaf(d, __bfloat162float(Xs[(base + kx + PD * (ky + PD * kz)) * NC + ci]), acc[k]);
         }
       }
     }
@@ -288,20 +289,25 @@ __global__ void k_wgrad_reduce(const float* __restrict__ partial, int nPart, int
 // loss, Adam
 // ---------------------------------------------------------------------------
 // loss = sum m (y - t)^2 / count; dy = 2 m (y - t) / count into channel 0 of
-// a [n][NCELL][16] bf16 gradient (channels 1..15 stay 0).  Per-CTA partial.
+// a padded-layout bf16 gradient (all other values stay 0).  Per-CTA partial.
 constexpr int LOSS_GRID = 148 * 2;
 __global__ void __launch_bounds__(512) k_loss(int64_t nc, const float* __restrict__ y,
                                               const float* __restrict__ tgt,
                                               const float* __restrict__ m, float invCount,
                                               __nv_bfloat16* __restrict__ dy,
                                               double* __restrict__ partial) {
+  // dy: padded layout, channel 0 of half 0 at the interior cells
   __shared__ double ws[16];
   double acc = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nc;
        i += (int64_t)gridDim.x * blockDim.x) {
     const float d = m[i] > 0.f ? y[i] - tgt[i] : 0.f;
     acc += (double)d * d;
-    if (dy) dy[i * NC] = __float2bfloat16_rn(2.f * d * invCount);
+    if (dy) {
+      const int64_t t = i / NCELL;
+      dy[((size_t)t * 2 * NPAD + pad_index((int)(i % NCELL))) * 8] =
+          __float2bfloat16_rn(2.f * d * invCount);
+    }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
@@ -349,7 +355,7 @@ struct msbg_cnn {
   int numSMs = 148;
   // training scratch for `cap` tiles
   int cap = 0;
-  DeviceBuffer a1, a2, a3, y, dy, dz3, dz2, dz1, part, lossPart;
+  DeviceBuffer x0, a1, a2, a3, y, dy, dz3, dz2, dz1, part, lossPart;  // padded layout
 };
 
 namespace {
@@ -375,22 +381,19 @@ int cnn_error(msbg_cnn* n, int code, const char* fmt, ...) {
 void set_attrs() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(k_conv3_tc<IN_FEAT, EPI_RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
-  cudaFuncSetAttribute(k_conv3_tc<IN_ACT, EPI_RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
-  cudaFuncSetAttribute(k_conv3_tc<IN_ACT, EPI_MASK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
-  cudaFuncSetAttribute(k_conv3_tc<IN_ACT, EPI_OUT0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
-  cudaFuncSetAttribute(k_wgrad<IN_FEAT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WG_SMEM);
-  cudaFuncSetAttribute(k_wgrad<IN_ACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WG_SMEM);
+  cudaFuncSetAttribute(k_conv3_tc<EPI_RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
+  cudaFuncSetAttribute(k_conv3_tc<EPI_MASK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
+  cudaFuncSetAttribute(k_conv3_tc<EPI_OUT0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CONV_SMEM);
+  cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WG_SMEM);
   done = true;
 }
 
-template <int IN, int EPI>
-void conv(msbg_cnn* net, int layer, bool backward, int n, const float* feat,
-          const __nv_bfloat16* in, __nv_bfloat16* out, const __nv_bfloat16* mask, float* out0,
-          const int64_t* outOff, const float* outScale, cudaStream_t st) {
+template <int EPI>
+void conv(msbg_cnn* net, int layer, bool backward, int n, const uint4* in, uint4* out,
+          const uint4* mask, float* out0, const int64_t* outOff, const float* outScale,
+          cudaStream_t st) {
   ConvArgs a;
   a.n = n;
-  a.feat = feat;
   a.in = in;
   a.wimg = (backward ? net->imgB : net->imgF).as<__nv_bfloat16>() + (size_t)layer * WIMG;
   a.out = out;
@@ -400,20 +403,23 @@ void conv(msbg_cnn* net, int layer, bool backward, int n, const float* feat,
   a.outScale = outScale;
   a.err = net->err.as<int>();
   const int grid = std::min(n, net->numSMs);
-  k_conv3_tc<IN, EPI><<<grid, CONV_THREADS, CONV_SMEM, st>>>(a);
+  k_conv3_tc<EPI><<<grid, CONV_THREADS, CONV_SMEM, st>>>(a);
+}
+
+void feat_pack(int n, const float* feat, uint4* x0, cudaStream_t st) {
+  const int64_t cnt = (int64_t)n * NPAD;
+  k_feat_pack<<<(unsigned)((cnt + 255) / 256), 256, 0, st>>>(n, feat, x0);
 }
 
 int ensure_cap(msbg_cnn* net, int n) {
   if (n <= net->cap) return MSBG_OK;
-  const size_t act = (size_t)n * NCELL * NC * sizeof(__nv_bfloat16);
-  CNN_TRY(net, net->a1.ensure(act));
-  CNN_TRY(net, net->a2.ensure(act));
-  CNN_TRY(net, net->a3.ensure(act));
-  CNN_TRY(net, net->dz3.ensure(act));
-  CNN_TRY(net, net->dz2.ensure(act));
-  CNN_TRY(net, net->dz1.ensure(act));
-  CNN_TRY(net, net->dy.ensure(act));
-  CNN_TRY(net, cudaMemsetAsync(net->dy.p, 0, act, net->stream));
+  const size_t act = (size_t)n * ACT_BYTES;
+  DeviceBuffer* bufs[] = {&net->x0, &net->a1, &net->a2, &net->a3,
+                          &net->dz3, &net->dz2, &net->dz1, &net->dy};
+  for (DeviceBuffer* b : bufs) {
+    CNN_TRY(net, b->ensure(act));
+    CNN_TRY(net, cudaMemsetAsync(b->p, 0, act, net->stream));  // zero halos
+  }
   CNN_TRY(net, net->y.ensure((size_t)n * NCELL * sizeof(float)));
   CNN_TRY(net, net->part.ensure((size_t)net->numSMs * NC * NC * 27 * sizeof(float)));
   CNN_TRY(net, net->lossPart.ensure(LOSS_GRID * sizeof(double)));
@@ -445,12 +451,13 @@ namespace msbg {
 namespace cnn {
 // Forward pass into out0 (see msbg_cnn_forward); used by the pressure solver.
 int forward(msbg_cnn* net, const float* feat, float* out0, const int64_t* outOff,
-            const float* outScale, int n, cudaStream_t st, __nv_bfloat16* s1, __nv_bfloat16* s2) {
+            const float* outScale, int n, cudaStream_t st, uint4* x0, uint4* s1, uint4* s2) {
   if (n <= 0) return MSBG_OK;
-  conv<IN_FEAT, EPI_RELU>(net, 0, false, n, feat, nullptr, s1, nullptr, nullptr, nullptr, nullptr, st);
-  conv<IN_ACT, EPI_RELU>(net, 1, false, n, nullptr, s1, s2, nullptr, nullptr, nullptr, nullptr, st);
-  conv<IN_ACT, EPI_RELU>(net, 2, false, n, nullptr, s2, s1, nullptr, nullptr, nullptr, nullptr, st);
-  conv<IN_ACT, EPI_OUT0>(net, 3, false, n, nullptr, s1, nullptr, nullptr, out0, outOff, outScale, st);
+  feat_pack(n, feat, x0, st);
+  conv<EPI_RELU>(net, 0, false, n, x0, s1, nullptr, nullptr, nullptr, nullptr, st);
+  conv<EPI_RELU>(net, 1, false, n, s1, s2, nullptr, nullptr, nullptr, nullptr, st);
+  conv<EPI_RELU>(net, 2, false, n, s2, s1, nullptr, nullptr, nullptr, nullptr, st);
+  conv<EPI_OUT0>(net, 3, false, n, s1, nullptr, nullptr, out0, outOff, outScale, st);
   return cudaGetLastError() == cudaSuccess ? MSBG_OK : MSBG_ERROR;
 }
 
@@ -550,8 +557,8 @@ extern "C" int msbg_cnn_forward(msbg_cnn* net, const float* feat, float* out, in
   cudaSetDevice(net->device);
   int rc = ensure_cap(net, n);
   if (rc) return rc;
-  rc = forward(net, feat, out, nullptr, nullptr, n, net->stream, net->a1.as<__nv_bfloat16>(),
-               net->a2.as<__nv_bfloat16>());
+  rc = forward(net, feat, out, nullptr, nullptr, n, net->stream, net->x0.as<uint4>(),
+               net->a1.as<uint4>(), net->a2.as<uint4>());
   if (rc) return cnn_error(net, rc, "forward launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   return check_err(net);
 }
@@ -567,37 +574,36 @@ extern "C" int msbg_cnn_loss_grad(msbg_cnn* net, const float* feat, const float*
   int rc = ensure_cap(net, n);
   if (rc) return rc;
   cudaStream_t st = net->stream;
-  auto* a1 = net->a1.as<__nv_bfloat16>();
-  auto* a2 = net->a2.as<__nv_bfloat16>();
-  auto* a3 = net->a3.as<__nv_bfloat16>();
-  auto* dy = net->dy.as<__nv_bfloat16>();
-  auto* dz3 = net->dz3.as<__nv_bfloat16>();
-  auto* dz2 = net->dz2.as<__nv_bfloat16>();
-  auto* dz1 = net->dz1.as<__nv_bfloat16>();
+  uint4* x0 = net->x0.as<uint4>();
+  uint4* a1 = net->a1.as<uint4>();
+  uint4* a2 = net->a2.as<uint4>();
+  uint4* a3 = net->a3.as<uint4>();
+  uint4* dy = net->dy.as<uint4>();
+  uint4* dz3 = net->dz3.as<uint4>();
+  uint4* dz2 = net->dz2.as<uint4>();
+  uint4* dz1 = net->dz1.as<uint4>();
   float* y = net->y.as<float>();
   // forward, keeping the activations
-  conv<IN_FEAT, EPI_RELU>(net, 0, false, n, feat, nullptr, a1, nullptr, nullptr, nullptr, nullptr, st);
-  conv<IN_ACT, EPI_RELU>(net, 1, false, n, nullptr, a1, a2, nullptr, nullptr, nullptr, nullptr, st);
-  conv<IN_ACT, EPI_RELU>(net, 2, false, n, nullptr, a2, a3, nullptr, nullptr, nullptr, nullptr, st);
-  conv<IN_ACT, EPI_OUT0>(net, 3, false, n, nullptr, a3, nullptr, nullptr, y, nullptr, nullptr, st);
+  feat_pack(n, feat, x0, st);
+  conv<EPI_RELU>(net, 0, false, n, x0, a1, nullptr, nullptr, nullptr, nullptr, st);
+  conv<EPI_RELU>(net, 1, false, n, a1, a2, nullptr, nullptr, nullptr, nullptr, st);
+  conv<EPI_RELU>(net, 2, false, n, a2, a3, nullptr, nullptr, nullptr, nullptr, st);
+  conv<EPI_OUT0>(net, 3, false, n, a3, nullptr, nullptr, y, nullptr, nullptr, st);
   // loss and dL/dy
-  k_loss<<<LOSS_GRID, 512, 0, st>>>((int64_t)n * NCELL, y, target, mask, (float)(1.0 / count), dy,
-                                    net->lossPart.as<double>());
+  k_loss<<<LOSS_GRID, 512, 0, st>>>((int64_t)n * NCELL, y, target, mask, (float)(1.0 / count),
+                                    reinterpret_cast<__nv_bfloat16*>(dy), net->lossPart.as<double>());
   // backward-data through layers 4, 3, 2 (ReLU masks of their inputs)
-  conv<IN_ACT, EPI_MASK>(net, 3, true, n, nullptr, dy, dz3, a3, nullptr, nullptr, nullptr, st);
-  conv<IN_ACT, EPI_MASK>(net, 2, true, n, nullptr, dz3, dz2, a2, nullptr, nullptr, nullptr, st);
-  conv<IN_ACT, EPI_MASK>(net, 1, true, n, nullptr, dz2, dz1, a1, nullptr, nullptr, nullptr, st);
+  conv<EPI_MASK>(net, 3, true, n, dy, dz3, a3, nullptr, nullptr, nullptr, st);
+  conv<EPI_MASK>(net, 2, true, n, dz3, dz2, a2, nullptr, nullptr, nullptr, st);
+  conv<EPI_MASK>(net, 1, true, n, dz2, dz1, a1, nullptr, nullptr, nullptr, st);
   // weight gradients
   const int grid = std::min(n, net->numSMs);
   float* part = net->part.as<float>();
   float* g = net->g.as<float>();
-  const __nv_bfloat16* dzs[NLAYER] = {dz1, dz2, dz3, dy};
-  const __nv_bfloat16* ins[NLAYER] = {nullptr, a1, a2, a3};
+  const uint4* dzs[NLAYER] = {dz1, dz2, dz3, dy};
+  const uint4* ins[NLAYER] = {x0, a1, a2, a3};
   for (int l = 0; l < NLAYER; l++) {
-    if (l == 0)
-      k_wgrad<IN_FEAT><<<grid, 256, WG_SMEM, st>>>(n, feat, nullptr, dzs[l], part);
-    else
-      k_wgrad<IN_ACT><<<grid, 256, WG_SMEM, st>>>(n, nullptr, ins[l], dzs[l], part);
+    k_wgrad<<<grid, 256, WG_SMEM, st>>>(n, ins[l], dzs[l], part);
     const int cnt = layer_cout(l) * layer_cin(l) * 27;
     k_wgrad_reduce<<<(cnt + 255) / 256, 256, 0, st>>>(part, grid, layer_cin(l), layer_cout(l),
                                                       g + layer_off(l));

@@ -40,30 +40,40 @@ __host__ __device__ constexpr int layer_off(int l) {
 }
 constexpr int NPARAM = 27 * NFEAT * NC + 2 * 27 * NC * NC + 27 * NC;  // 15984
 
-enum { IN_FEAT = 0, IN_ACT = 1 };
+// Activation tensors in global memory use the shared-memory layout of the
+// convolution: per tile two channel halves, each NPAD padded cells x 16 bytes
+// (8 bf16 channels), z slowest; halo cells are zero except in the first
+// layer's input.  One padded z plane of one half is PLANE_BYTES contiguous.
+constexpr int PLANE = PD * PD;
+constexpr uint32_t PLANE_BYTES = PLANE * 16;        // 5184
+constexpr size_t ACT_BYTES = 2 * (size_t)HALF_BYTES;  // per tile
+__host__ __device__ constexpr int pad_index(int cell) {
+  return (cell % TS + 1) + PD * ((cell / TS) % TS + 1 + PD * (cell / (TS * TS) + 1));
+}
+
 enum { EPI_RELU = 0, EPI_MASK = 1, EPI_OUT0 = 2 };
 
 struct ConvArgs {
   int n;                              // tiles
-  const float* feat;                  // IN_FEAT: [n][4][NPAD] (channel planes, padded box)
-  const __nv_bfloat16* in;            // IN_ACT: [n][NCELL][16] (halo = 0)
+  const uint4* in;                    // [n][2][NPAD] 16-byte cells (padded layout)
   const __nv_bfloat16* wimg;          // [27][2][16][8] bf16 image of the layer
-  __nv_bfloat16* out;                 // EPI_RELU / EPI_MASK: [n][NCELL][16]
-  const __nv_bfloat16* mask;          // EPI_MASK: [n][NCELL][16]; out = acc where mask > 0
+  uint4* out;                         // EPI_RELU / EPI_MASK: padded layout, interior written
+  const uint4* mask;                  // EPI_MASK: padded layout; out = acc where mask > 0
   float* out0;                        // EPI_OUT0: channel 0
   const int64_t* outOff;              // EPI_OUT0: per-tile first cell in out0 (null: t*NCELL)
   const float* outScale;              // EPI_OUT0: per-tile factor (null: 1)
   int* err;                           // set when a bounded wait gives up
 };
 
+// 8 warps: warp w drains TMEM lanes 32*(w%4) of column half w/4.
 constexpr int CONV_THREADS = 256;
-constexpr size_t CONV_SMEM = 2 * (size_t)HALF_BYTES + WIMG * 2 + 64;
+constexpr size_t CONV_SMEM = 2 * (size_t)HALF_BYTES + WIMG * 2 + 256;
 
 // Inference of n tiles on stream st: out0[outOff[t] + cell] = outScale[t] *
-// net(feat[t]) (cnn.cu).  s1, s2: bf16 scratch of n * NCELL * 16 values each.
+// net(feat[t]) (cnn.cu).  x0, s1, s2: scratch of n * ACT_BYTES each; s1 and
+// s2 must have zero halos (zeroed once when allocated).
 int forward(msbg_cnn* net, const float* feat, float* out0, const int64_t* outOff,
-            const float* outScale, int n, cudaStream_t st, __nv_bfloat16* s1,
-            __nv_bfloat16* s2);
+            const float* outScale, int n, cudaStream_t st, uint4* x0, uint4* s1, uint4* s2);
 // Status of the network's bounded waits since the last call (0 = none gave up); clears it.
 int take_error(msbg_cnn* net, cudaStream_t st);
 

@@ -59,7 +59,7 @@ struct Solver {
   int nCnnTiles = 0;
   float levelNorm = 0.f;
   DeviceBuffer cnnTiles, cnnLevel;          // [nCnnTiles] tile id, resolution level
-  DeviceBuffer cFeat, cScale, cOff, cS1, cS2, guess, cIdx;
+  DeviceBuffer cFeat, cScale, cOff, cX0, cS1, cS2, guess, cIdx;
   std::vector<int> cnnTilesHost, cnnLevelHost;
   int cnnChunk = 0;
   bool haveX64 = false;  // x64 holds the solution of the last refined solve
@@ -579,8 +579,10 @@ int learned_predict(msbg_gpu_ctx* ctx, Solver& S, cudaStream_t st, const float* 
     MSBG_CUDA_TRY(ctx, S.cFeat.ensure(sizeof(float) * CH * cnn::NFEAT * cnn::NPAD));
     MSBG_CUDA_TRY(ctx, S.cScale.ensure(sizeof(float) * CH));
     MSBG_CUDA_TRY(ctx, S.cOff.ensure(sizeof(int64_t) * CH));
-    MSBG_CUDA_TRY(ctx, S.cS1.ensure(sizeof(__nv_bfloat16) * (size_t)CH * cnn::NCELL * cnn::NC));
-    MSBG_CUDA_TRY(ctx, S.cS2.ensure(sizeof(__nv_bfloat16) * (size_t)CH * cnn::NCELL * cnn::NC));
+    for (DeviceBuffer* b : {&S.cX0, &S.cS1, &S.cS2}) {
+      MSBG_CUDA_TRY(ctx, b->ensure(cnn::ACT_BYTES * CH));
+      MSBG_CUDA_TRY(ctx, cudaMemsetAsync(b->p, 0, cnn::ACT_BYTES * CH, st));  // zero halos
+    }
     S.cnnChunk = CH;
   }
   for (int c0 = 0; c0 < S.nCnnTiles; c0 += CH) {
@@ -590,9 +592,9 @@ int learned_predict(msbg_gpu_ctx* ctx, Solver& S, cudaStream_t st, const float* 
         S.cnnLevel.as<int>() + c0, S.levelNorm, val, nullptr, S.cFeat.as<float>(),
         S.cScale.as<float>(), S.cOff.as<int64_t>(), nullptr, nullptr);
     if (cnn::forward(S.net, S.cFeat.as<float>(), out, S.cOff.as<int64_t>(), S.cScale.as<float>(),
-                     cnt, st, S.cS1.as<__nv_bfloat16>(), S.cS2.as<__nv_bfloat16>()))
+                     cnt, st, S.cX0.as<uint4>(), S.cS1.as<uint4>(), S.cS2.as<uint4>()))
       return set_error(ctx, MSBG_ERROR, "learned network launch failed");
-    launches += 5;
+    launches += 6;
   }
   MSBG_CUDA_TRY(ctx, cudaGetLastError());
   const int e = cnn::take_error(S.net, st);
