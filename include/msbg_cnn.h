@@ -68,6 +68,11 @@ int msbg_cnn_adam_step(msbg_cnn* net, float lr, float beta1, float beta2, float 
  * get no prediction). */
 int msbg_gpu_pressure_set_cnn(msbg_gpu_ctx* ctx, msbg_cnn* net);
 
+/* The network's prediction of the pressure of the prepared problem (the
+ * initial guess of a learned solve; 0 off the liquid and on tiles the network
+ * does not cover), in the layout of msbg_gpu_pressure_download. */
+int msbg_gpu_pressure_learned_guess(msbg_gpu_ctx* ctx, float* packed, int64_t n);
+
 /* Training pairs from the last refined solve of ctx (maxRefine > 0): for up
  * to maxPairs level-0 16^3 tiles spread evenly over the grid, the features of
  * the right-hand side, the normalised FP64 solution as target and the liquid

@@ -1017,6 +1017,29 @@ extern "C" int msbg_gpu_pressure_download(msbg_gpu_ctx* ctx, float* packed, int6
   return to_packed(ctx, *sp, sp->dev[0]->x.as<float>(), packed, n);
 }
 
+extern "C" int msbg_gpu_pressure_learned_guess(msbg_gpu_ctx* ctx, float* packed, int64_t n) {
+  if (!ctx || !packed) return MSBG_EINVARG;
+  auto& sp = solver_of(ctx);
+  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
+  if (!ctx->cnn) return set_error(ctx, MSBG_EINVARG, "no network (msbg_gpu_pressure_set_cnn)");
+  cudaSetDevice(ctx->device);
+  Solver& S = *sp;
+  S.net = ctx->cnn;
+  cudaStream_t st = ctx->stream;
+  const int64_t nc = S.H.levels[0].nCells;
+  MSBG_CUDA_TRY(ctx, S.guess.ensure(sizeof(float) * nc));
+  int64_t launches = 0;
+  int rc = learned_predict(ctx, S, st, S.rhs0.as<float>(), S.guess.as<float>(), launches);
+  if (rc) return rc;
+  DeviceBuffer tmp;
+  MSBG_CUDA_TRY(ctx, tmp.ensure(sizeof(double) * nc));
+  k_set64_masked<<<VEC_GRID, VEC_BLOCK, 0, st>>>(tmp.as<double>(), S.guess.as<float>(),
+                                                 S.views[0].diag, nc);
+  k_narrow<<<VEC_GRID, VEC_BLOCK, 0, st>>>(S.guess.as<float>(), tmp.as<double>(), nc);
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return to_packed(ctx, S, S.guess.as<float>(), packed, n);
+}
+
 extern "C" int msbg_gpu_pressure_download64(msbg_gpu_ctx* ctx, double* packed, int64_t n) {
   if (!ctx || !packed) return MSBG_EINVARG;
   auto& sp = solver_of(ctx);

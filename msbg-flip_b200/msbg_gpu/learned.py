@@ -30,6 +30,7 @@ def _sigs(L):
         "msbg_cnn_adam_step": (i32, [vp, C.c_float, C.c_float, C.c_float, C.c_float]),
         "msbg_gpu_pressure_set_cnn": (i32, [vp, vp]),
         "msbg_gpu_pressure_training_pairs": (i32, [vp, vp, vp, vp, i32, C.POINTER(C.c_int)]),
+        "msbg_gpu_pressure_learned_guess": (i32, [vp, C.POINTER(C.c_float), C.c_int64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -153,9 +154,22 @@ def _ctx_set_cnn(self, net):
     self._cnn = net  # keep it alive while attached
 
 
+def _ctx_learned_guess(self):
+    """The attached network's pressure prediction (packed layout, FP32)."""
+    L = lib()
+    _sigs(L)
+    n = C.c_int64()
+    self._check(L.msbg_gpu_pressure_packed_size(self._h, C.byref(n)), "packed_size")
+    out = np.zeros(n.value, np.float32)
+    self._check(L.msbg_gpu_pressure_learned_guess(self._h, out.ctypes.data_as(C.POINTER(C.c_float)),
+                                                  n.value), "learned_guess")
+    return out
+
+
 def _install():
     from . import Context
     Context.pressure_set_cnn = _ctx_set_cnn
+    Context.pressure_learned_guess = _ctx_learned_guess
 
 
 _install()
