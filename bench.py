@@ -223,6 +223,57 @@ def bench_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# training set of the learned guess: (RHS, solution) tile pairs of the refined
+# solver on seeded sphere-union instances at 512^3 (64 spheres, radii 20-60
+# voxels, 32^3 base blocks, 2 levels), 500 spread-out 16^3 tiles each
+LEARN_CFG = dict(res=512, seeds=(100, 101, 102, 103), pairs_per_instance=500, epochs=60,
+                 batch=64, lr=2e-3)
+
+
+def learned_variants(ctx, c, scene):
+    """Train the network on the GPU, then time the learned solves of the bench
+    problem (FP32 and FP16 level-0 vectors, FP64 refinement to 1e-6)."""
+    import torch
+    import msbg_gpu
+    L = LEARN_CFG
+    t0 = time.perf_counter()
+    F, T, M = [], [], []
+    for sd in L["seeds"]:
+        ctx.pressure_prepare(msbg_gpu.PressureScene(L["res"], 32, 2, 0.0, 64, 20 / 512, 60 / 512, 8,
+                                                    16, 8, 32.0 * L["res"] / 512, sd))
+        ctx.pressure_solve(tol=1e-6, maxRefine=4)
+        f, t, m = msbg_gpu.collect_training_pairs(ctx, L["pairs_per_instance"])
+        F.append(f)
+        T.append(t)
+        M.append(m)
+    F, T, M = torch.cat(F), torch.cat(T), torch.cat(M)
+    data_s = time.perf_counter() - t0
+    net = msbg_gpu.Cnn(ctx.device)
+    t0 = time.perf_counter()
+    losses = msbg_gpu.train_cnn(net, F, T, M, epochs=L["epochs"], batch=L["batch"], lr=L["lr"], seed=1)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    rms = float((T * T * M).sum() / M.sum())
+    ctx.pressure_prepare(scene)
+    ctx.pressure_set_cnn(net)
+    out = {"pairs": int(F.shape[0]), "epochs": L["epochs"], "data_seconds": data_s,
+           "train_seconds": train_s, "final_rel_loss": (losses[-1] / rms) ** 0.5,
+           "network": "4 x conv3^3 16ch ReLU, BF16 tcgen05 implicit GEMM, FP32 accumulate"}
+    for name, storage in (("f32", msbg_gpu.F32), ("f16", msbg_gpu.F16)):
+        vp = msbg_gpu.solve_params(nPre=c["n_pre"], nPost=c["n_post"], tol=c["tol"],
+                                   innerIter=c["inner"], useGraph=1, storage=storage,
+                                   maxRefine=30, learned=1)
+        ctx.pressure_solve(vp)
+        vi = ctx.pressure_solve(vp)
+        out[name + "_vectors_learned_guess"] = {
+            "ms": vi.solveSeconds * 1e3, "pcg_iterations": vi.iterations,
+            "refinements": vi.refinements, "status": vi.status,
+            "true_rel_residual_fp64": vi.relResidual}
+    ctx.pressure_set_cnn(None)
+    net.close()
+    return out
+
+
 def bench_part(args):
     """One solver part (a level-0 smoothing sweep, the level-0 matvec or a
     V-cycle) of the pressure workload, timed through msbg_gpu_pressure_profile:
@@ -313,6 +364,9 @@ def bench_mgpcg(args):
             "ms": vi.solveSeconds * 1e3, "pcg_iterations": vi.iterations,
             "refinements": vi.refinements, "status": vi.status,
             "true_rel_residual_fp64": vi.relResidual}
+    learned = None
+    if not args.no_learned:
+        learned = learned_variants(ctx, c, scene)
     # end to end through the C ABI: prepare from the host callbacks (host
     # sampling + hierarchy + upload), solve, download the pressure
     n_e2e = max(1, min(args.steps, 2))
@@ -340,6 +394,7 @@ def bench_mgpcg(args):
                            "time_to_1e-6_ms": ms_step, "pcg_iterations": iters,
                            "true_rel_residual": infos[-1].relResidual,
                            "refined_variants": variants,
+                           "learned": learned,
                            "liquid_cells": fluid, "stored_cells_level0": cells0,
                            "mg_levels": int(st.nMgLevels),
                            "prepare_s": st.prepareSeconds, "host_build_s": st.buildSeconds,
@@ -538,6 +593,7 @@ def main():
     ap.add_argument("--workload", default="mgpcg", choices=["mgpcg", "mcf"])
     ap.add_argument("--res", type=int, default=0, help="override the pressure resolution")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned guess")
     ap.add_argument("--profile", action="store_true",
                     help="only the resident-data steps (for ncu captures); prints nothing")
     ap.add_argument("--part", default="", choices=["", "smooth", "matvec", "vcycle"],
