@@ -76,11 +76,11 @@ void set_kernel_attrs() {
                        (int)smooth_smem<16>());
   cudaFuncSetAttribute(k_smooth<8, VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)smooth_smem<8>());
-  cudaFuncSetAttribute(k_smooth_pipe16<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       pipeSmem);
-  cudaFuncSetAttribute(k_apply_pipe16<APPLY_MATVEC, VT, VT>,
+  cudaFuncSetAttribute(k_smooth_pipe16<VT, pipe::NT_SMOOTH>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, pipeSmem);
-  cudaFuncSetAttribute(k_apply_pipe16<APPLY_RESIDUAL, VT, float>,
+  cudaFuncSetAttribute(k_apply_pipe16<APPLY_MATVEC, VT, VT, pipe::NT_APPLY>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, pipeSmem);
+  cudaFuncSetAttribute(k_apply_pipe16<APPLY_RESIDUAL, VT, float, pipe::NT_APPLY>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, pipeSmem);
   done = true;
 }
@@ -125,8 +125,8 @@ struct Runner {
       if (P.ts == 16 && usePipe) {
         const int grid = std::min(P.count, numSMs);
         // passes are contiguous tile-id ranges (register_tiles sorts by pass)
-        k_smooth_pipe16<V><<<grid, pipe::NT, pipe::SMEM, st>>>(S.views[m], P.start, P.count, x,
-                                                               b, inner, post ? 1 : 0, err);
+        k_smooth_pipe16<V, pipe::NT_SMOOTH><<<grid, pipe::NT_SMOOTH, pipe::SMEM, st>>>(
+            S.views[m], P.start, P.count, x, b, inner, post ? 1 : 0, err);
       } else {
         TS_DISPATCH(P.ts, (k_smooth<T, V><<<P.count, T * T, smooth_smem<T>(), st>>>(
                                S.views[m], lst, x, b, inner, post ? 1 : 0)));
@@ -171,7 +171,7 @@ struct Runner {
       if (!P.count) continue;
       if (P.ts == 16 && usePipe) {
         const int grid = std::min(P.count, numSMs);
-        k_apply_pipe16<APPLY_MATVEC, VT, VT><<<grid, pipe::NT, pipe::SMEM, st>>>(
+        k_apply_pipe16<APPLY_MATVEC, VT, VT, pipe::NT_APPLY><<<grid, pipe::NT_APPLY, pipe::SMEM, st>>>(
             S.views[0], P.start, P.count, d, nullptr, q, nullptr, nullptr, partial + off, err);
         off += grid;
       } else {
@@ -196,7 +196,7 @@ struct Runner {
       if (!P.count) continue;
       if (P.ts == 16 && usePipe) {
         const int grid = std::min(P.count, numSMs);
-        k_apply_pipe16<APPLY_RESIDUAL, V, float><<<grid, pipe::NT, pipe::SMEM, st>>>(
+        k_apply_pipe16<APPLY_RESIDUAL, V, float, pipe::NT_APPLY><<<grid, pipe::NT_APPLY, pipe::SMEM, st>>>(
             S.views[m], P.start, P.count, x, b, nullptr, bc, coff, nullptr, err);
       } else {
         const int* lst = passList(m) + P.start;

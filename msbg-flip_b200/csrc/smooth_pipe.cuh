@@ -78,6 +78,8 @@ __device__ __forceinline__ void bulk_wait_all() {
 }
 
 constexpr int TS = 16, N = TS * TS * TS, NT = 512;
+constexpr int NT_SMOOTH = 1024;  // threads of the smoother CTA
+constexpr int NT_APPLY = 1024;   // threads of the operator-application CTA
 
 // Per-face data of a tile needed to gather its halo.
 struct FaceRes {
@@ -129,20 +131,25 @@ __device__ __forceinline__ VT* raw_b(float* st) {
   return reinterpret_cast<VT*>(st + N) + (std::is_same<VT, float>::value ? 0 : N);
 }
 // Widen a 16-bit x tile into the FP32 working slot (no-op for FP32).
-template <typename VT>
+template <typename VT, int NTH = NT>
 __device__ __forceinline__ void widen_x(float* st, int tid) {
   if (std::is_same<VT, float>::value) return;
   const VT* xr = raw_x<VT>(st);
-  for (int e = tid; e < N; e += NT) st[e] = to_f(xr[e]);
+  for (int e = tid; e < N; e += NTH) st[e] = to_f(xr[e]);
 }
 
 }  // namespace pipe
 
-template <typename VT>
-__global__ void __launch_bounds__(pipe::NT, 1)
+// NTH threads: each owns KK cells of each colour (NTH = 512: 4, 1024: 2).
+template <typename VT, int NTH>
+__global__ void __launch_bounds__(NTH, 1)
     k_smooth_pipe16(LevelView L, int tileBase, int count, VT* __restrict__ x,
                     const VT* __restrict__ b, int inner, int reverse, int* __restrict__ err) {
   using namespace pipe;
+  constexpr int KK = N / (2 * NTH);           // cells per colour per thread
+  constexpr int KSTRIDE = TS / KK;             // z distance of a thread's cells
+  constexpr int NHALO = 6 * TS * TS;           // halo cells of a tile
+  constexpr int HQ = (NHALO + NTH - 1) / NTH;  // halo cells per thread
   extern __shared__ __align__(128) float sm[];
   float* stages[2] = {sm + GUARD, sm + GUARD + 6 * N};
   float(*gsb)[6][TS * TS] = reinterpret_cast<float(*)[6][TS * TS]>(sm + GUARD + 12 * N);
@@ -154,7 +161,7 @@ __global__ void __launch_bounds__(pipe::NT, 1)
   int t = blockIdx.x;
   if (t >= count) return;
   // every float of shared memory holds 0 or a value of our (finite) arrays
-  for (int q = tid; q < ZERO_FLOATS / 4; q += NT)
+  for (int q = tid; q < ZERO_FLOATS / 4; q += NTH)
     reinterpret_cast<float4*>(sm)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -176,20 +183,22 @@ __global__ void __launch_bounds__(pipe::NT, 1)
     bulk_g2s(st + 5 * N, L.cz + off, N * sizeof(float), br);
     if (rec) bulk_g2s(&recs[slot], grec + tRec, sizeof(TileRec), br);
   };
-  float hx[3], hc[3];
+  float hx[HQ], hc[HQ];
   auto halo_issue = [&](const TileRec& r) {
 #pragma unroll
-    for (int q = 0; q < 3; q++) {
-      const int g = tid + NT * q, f = g >> 8, c = g & 255;
-      halo_load(L, x, r.f[f], f >> 1, f & 1, c & 15, c >> 4, hx[q], hc[q]);
+    for (int q = 0; q < HQ; q++) {
+      const int g = tid + NTH * q, f = g >> 8, c = g & 255;
+      if (NHALO % NTH == 0 || g < NHALO)
+        halo_load(L, x, r.f[f], f >> 1, f & 1, c & 15, c >> 4, hx[q], hc[q]);
     }
   };
   auto halo_combine = [&](const TileRec& r, int ti, int u) {
-    widen_x<VT>(stages[u], tid);
+    widen_x<VT, NTH>(stages[u], tid);
     const float* st = stages[u];
 #pragma unroll
-    for (int q = 0; q < 3; q++) {
-      const int g = tid + NT * q, f = g >> 8, c = g & 255;
+    for (int q = 0; q < HQ; q++) {
+      const int g = tid + NTH * q, f = g >> 8, c = g & 255;
+      if (NHALO % NTH != 0 && g >= NHALO) continue;
       const int dir = f >> 1, side = f & 1, a = c & 15, bb = c >> 4;
       const int kind = r.f[f].kind;
       float v = 0.f;
@@ -249,12 +258,12 @@ __global__ void __launch_bounds__(pipe::NT, 1)
     const float* CY = X + 4 * N;
     const float* CZ = X + 5 * N;
     const float(*gs)[TS * TS] = gsb[s];
-    float R[2][4], I[2][4], Cm[2][4][3], Cp[2][4][3];
+    float R[2][KK], I[2][KK], Cm[2][KK][3], Cp[2][KK][3];
 #pragma unroll
     for (int c = 0; c < 2; c++)
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) {
-        const int k = kb + 4 * kk, ii = 2 * ip + ((jj + k + c) & 1);
+      for (int kk = 0; kk < KK; kk++) {
+        const int k = kb + KSTRIDE * kk, ii = 2 * ip + ((jj + k + c) & 1);
         const int e = tidx(TS, ii, jj, k);
         const float iv = IV[e];
         const bool fl = iv > 0.f;
@@ -278,8 +287,8 @@ __global__ void __launch_bounds__(pipe::NT, 1)
     auto half = [&](auto cc) {
       constexpr int c = decltype(cc)::value;
 #pragma unroll
-      for (int kk = 0; kk < 4; kk++) {
-        const int k = kb + 4 * kk, ii = 2 * ip + ((jj + k + c) & 1);
+      for (int kk = 0; kk < KK; kk++) {
+        const int k = kb + KSTRIDE * kk, ii = 2 * ip + ((jj + k + c) & 1);
         const int e = tidx(TS, ii, jj, k);
         // out-of-tile neighbours have zero coupling; their reads stay inside
         // shared memory (guard band / adjacent arrays, all finite)
@@ -307,7 +316,7 @@ __global__ void __launch_bounds__(pipe::NT, 1)
     // the vectors are 16-bit; slot 1's b is no longer read)
     if (!std::is_same<VT, float>::value) {
       VT* xr = raw_x<VT>(X);
-      for (int e = tid; e < N; e += NT) xr[e] = from_f<VT>(X[e]);
+      for (int e = tid; e < N; e += NTH) xr[e] = from_f<VT>(X[e]);
       __syncthreads();
     }
     if (tid == 0) {
@@ -364,13 +373,16 @@ inline std::vector<pipe::TileRec> build_tile_records(const Level& L) {
 // ---------------------------------------------------------------------------
 enum { APPLY_MATVEC = 0, APPLY_RESIDUAL = 1 };
 
-template <int MODE, typename VT, typename VC>
-__global__ void __launch_bounds__(pipe::NT, 1)
+template <int MODE, typename VT, typename VC, int NTH>
+__global__ void __launch_bounds__(NTH, 1)
     k_apply_pipe16(LevelView L, int tileBase, int count, const VT* __restrict__ x,
                    const VT* __restrict__ b, VT* __restrict__ y,
                    VC* __restrict__ bc, const int64_t* __restrict__ coarseOff,
                    double* __restrict__ partial, int* __restrict__ err) {
   using namespace pipe;
+  constexpr int ZC = TS / (NTH / (TS * TS));  // cells of a thread's z column
+  constexpr int NHALO = 6 * TS * TS;
+  constexpr int HQ = (NHALO + NTH - 1) / NTH;
   constexpr int NVEC = MODE == APPLY_RESIDUAL ? 2 : 1;  // x, [b]
   extern __shared__ __align__(128) float sm[];
   float* stages[2] = {sm + GUARD, sm + GUARD + 6 * N};
@@ -406,21 +418,23 @@ __global__ void __launch_bounds__(pipe::NT, 1)
       bulk_g2s(st + 5 * N, L.cz + off, N * sizeof(float), br);
       if (rec) bulk_g2s(&recs[slot], grec + tRec, sizeof(TileRec), br);
     };
-    float hx[3], hc[3];
+    float hx[HQ], hc[HQ];
     auto halo_issue = [&](const TileRec& r, int ti, int u) {
 #pragma unroll
-      for (int q = 0; q < 3; q++) {
-        const int g = tid + NT * q, f = g >> 8, c = g & 255;
-        halo_load(L, x, r.f[f], f >> 1, f & 1, c & 15, c >> 4, hx[q], hc[q]);
+      for (int q = 0; q < HQ; q++) {
+        const int g = tid + NTH * q, f = g >> 8, c = g & 255;
+        if (NHALO % NTH == 0 || g < NHALO)
+          halo_load(L, x, r.f[f], f >> 1, f & 1, c & 15, c >> 4, hx[q], hc[q]);
       }
       if (MODE == APPLY_RESIDUAL && tid < 6) cmap[u][tid] = L.toCoarse[(size_t)ti * 6 + tid];
     };
     auto halo_combine = [&](const TileRec& r, int ti, int u) {
-      widen_x<VT>(stages[u], tid);
+      widen_x<VT, NTH>(stages[u], tid);
       const float* st = stages[u];
 #pragma unroll
-      for (int q = 0; q < 3; q++) {
-        const int g = tid + NT * q, f = g >> 8, c = g & 255;
+      for (int q = 0; q < HQ; q++) {
+        const int g = tid + NTH * q, f = g >> 8, c = g & 255;
+        if (NHALO % NTH != 0 && g >= NHALO) continue;
         const int dir = f >> 1, side = f & 1, a = c & 15, bb = c >> 4;
         const int kind = r.f[f].kind;
         float v = 0.f;
@@ -476,12 +490,12 @@ __global__ void __launch_bounds__(pipe::NT, 1)
       const float(*gs)[TS * TS] = gsb[s];
       float* Y = X + 2 * N;  // results overwrite the a_ii array in place (each
                              // thread reads its own a_ii before writing it)
-      const int k0 = 8 * kh;
+      const int k0 = ZC * kh;
       float xm = k0 > 0 ? X[tidx(TS, i, j, k0 - 1)] : 0.f;
       float xc = X[tidx(TS, i, j, k0)];
-      float yv[8];
+      float yv[ZC];
 #pragma unroll
-      for (int kk = 0; kk < 8; kk++) {
+      for (int kk = 0; kk < ZC; kk++) {
         const int k = k0 + kk, e = tidx(TS, i, j, k);
         const float xp = k < TS - 1 ? X[e + TS * TS] : 0.f;
         const float dg = D[e];
@@ -508,10 +522,10 @@ __global__ void __launch_bounds__(pipe::NT, 1)
       if (MODE == APPLY_MATVEC) {
         VT* Yv = reinterpret_cast<VT*>(Y);
 #pragma unroll
-        for (int kk = 0; kk < 8; kk++) Yv[tidx(TS, i, j, k0 + kk)] = from_f<VT>(yv[kk]);
+        for (int kk = 0; kk < ZC; kk++) Yv[tidx(TS, i, j, k0 + kk)] = from_f<VT>(yv[kk]);
       } else {
 #pragma unroll
-        for (int kk = 0; kk < 8; kk++) Y[tidx(TS, i, j, k0 + kk)] = yv[kk];
+        for (int kk = 0; kk < ZC; kk++) Y[tidx(TS, i, j, k0 + kk)] = yv[kk];
       }
       __syncthreads();
       if (MODE == APPLY_MATVEC) {
@@ -527,15 +541,16 @@ __global__ void __launch_bounds__(pipe::NT, 1)
           const int ox = tc[1], oy = tc[2], oz = tc[3], cts = tc[5];
           if (tc[4]) {
             constexpr int H = TS / 2;
-            const int c = tid;  // 512 coarse cells, one per thread
+            for (int c = tid; c < H * H * H; c += NTH) {  // 512 coarse cells
             const int ci = c % H, cj = (c / H) % H, ck = c / (H * H);
             const int e = tidx(TS, 2 * ci, 2 * cj, 2 * ck);
             const float sum = Y[e] + Y[e + 1] + Y[e + TS] + Y[e + TS + 1] + Y[e + TS * TS] +
                               Y[e + TS * TS + 1] + Y[e + TS * TS + TS] +
                               Y[e + TS * TS + TS + 1];
             dst[tidx(cts, ox + ci, oy + cj, oz + ck)] = from_f<VC>(sum);
+            }
           } else {
-            for (int e = tid; e < N; e += NT) {
+            for (int e = tid; e < N; e += NTH) {
               const int ii = e % TS, jj = (e / TS) % TS, kk = e / (TS * TS);
               dst[tidx(cts, ox + ii, oy + jj, oz + kk)] = from_f<VC>(Y[e]);
             }
