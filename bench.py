@@ -41,7 +41,7 @@ METRIC = "MGPCG time-to-1e-6 & Gvoxel/s/iter: learned+mixed vs plain FP32, one B
 
 PS_CFG = dict(res=1024, bsx0=32, n_levels=2, z_liquid=0.4, n_spheres=32, r_min=0.03, r_max=0.1,
               n_cuboids=8, n_modes=16, k_max=8, band=64.0, seed=2024, tol=1e-6, n_pre=2,
-              n_post=2, inner=2)
+              n_post=2, inner=3)
 # bounded analogue of the pressure workload the reference CPU solver can run:
 # it aborts for 32^3 base blocks (src/msbg3.cpp:1692-1749), so 16^3 blocks,
 # a quarter of the resolution and the band scaled alike.

@@ -178,15 +178,20 @@ typedef struct {
 typedef struct {
   int nPre, nPost, nCoarse, maxIter;
   float tol;        /* stop when |r| <= tol*|b| */
-  int innerIter;    /* red-black sweeps inside a tile per smoother visit */
+  int innerIter;    /* red-black sweeps inside a tile per smoother visit
+                       (default 3: fastest at V(2,2) on the 1024^3 workload) */
   int storage;      /* MSBG_F32, MSBG_F16 or MSBG_BF16: storage of the MG
                        level-0 vectors (coarser levels, the operator and all
                        arithmetic stay FP32; dots FP64) */
   int maxRefine;    /* 0: plain MGPCG stopping on the recursive residual (as the
-                       reference); >0: up to maxRefine outer steps of FP64
-                       iterative refinement (FP64 solution and residual, inner
-                       MGPCG in the storage type) stopping on the true FP64
-                       residual.  16-bit storage always refines (0 = 30). */
+                       reference); >0: stop on the true FP64 residual, with the
+                       solution kept in FP64.  FP32 vectors: one MGPCG whose x
+                       is accumulated in FP64, the true residual replacing the
+                       recursive one whenever that dropped 10x and when it
+                       converges (at most maxRefine checks at convergence); 16-bit
+                       vectors: up to maxRefine outer steps of
+                       FP64 iterative refinement around the 16-bit MGPCG
+                       (always on for them; 0 = 30). */
   int useGraph;     /* capture one PCG iteration in a CUDA graph */
   float coarseScale; /* coarse-grid correction factor (default 1.8; 1 = plain) */
   int learned;      /* 0: none; 1: the network attached by
@@ -196,7 +201,8 @@ typedef struct {
 
 typedef struct {
   int iterations;        /* PCG iterations (summed over refinement steps) */
-  int refinements;       /* outer refinement steps taken */
+  int refinements;       /* FP64 true-residual replacements (FP32 vectors) or
+                            outer refinement steps (16-bit vectors) */
   int status;            /* 0 converged, 1 maxIter, 2 breakdown, 3 non-finite */
   double relResidual;    /* true |b - A x| / |b| of the delivered iterate: FP32
                             operator and iterate for maxRefine = 0, FP64 for

@@ -249,7 +249,7 @@ extern "C" void msbg_gpu_solve_params_default(msbg_gpu_solve_params* p) {
   p->nCoarse = 24;
   p->maxIter = 500;
   p->tol = 1e-6f;
-  p->innerIter = 2;
+  p->innerIter = 3;
   p->storage = MSBG_F32;
   p->maxRefine = 0;  // plain MGPCG on the recursive residual, as the reference
   p->useGraph = 1;
@@ -723,6 +723,162 @@ int solve_refined(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const msbg_gpu_so
   return MSBG_OK;
 }
 
+// FP32 vectors with the solution accumulated in FP64 and reliable residual
+// replacement: one MGPCG run (no restarts) whose x is kept in FP64
+// (x64 += alpha d) while r, d, q, z stay FP32.  Whenever the recursive
+// residual has dropped by 10x since the last replacement, and when it reaches
+// tol, the true residual b - A x64 is recomputed in FP64 and replaces r; the
+// iteration continues with its search directions (Sleijpen & van der Vorst,
+// "Reliable updated residuals in hybrid Bi-CG methods", Computing 56, 1996).
+// Replacing often keeps the swapped-in residual close to the recursive one
+// (an FP32 product A d on smooth directions loses accuracy in proportion to
+// the condition number, so the two drift apart).  Convergence is judged on
+// the true residual only.  An iteration is two CUDA graphs around
+// the host's convergence check: [q = A d, alpha, x/r update, |r|^2] and
+// [z = V r, rho, beta, d update].
+int solve_reliable(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gpu_solve_params* p,
+                   int maxChecks, SolveOut& o) {
+  cudaStream_t st = R.st;
+  const int64_t n = S.H.levels[0].nCells;
+  double* x64 = S.x64.as<double>();
+  float* r = S.r0.as<float>();
+  float* d = S.d0.as<float>();
+  float* q = S.q0.as<float>();
+  float* z = S.z0.as<float>();
+  double* part = S.partial.as<double>();
+  Scalars* sc = S.scal.as<Scalars>();
+  const float* b = S.rhs0.as<float>();
+  int rc = MSBG_OK;
+  if (p->learned >= 1) {
+    rc = learned_predict(ctx, S, st, b, S.guess.as<float>(), R.launches);
+    if (rc) return rc;
+    k_set64_masked<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, S.guess.as<float>(), S.views[0].diag, n);
+    R.launches++;
+  } else {
+    cudaMemsetAsync(x64, 0, sizeof(double) * n, st);
+  }
+  // r = b - A x64, |b|^2
+  double rr = 0;
+  rc = residual64(ctx, S, R, b, r, &rr);
+  if (rc) return rc;
+  cudaMemsetAsync(sc, 0, sizeof(Scalars), st);
+  k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(b, b, n, part);
+  k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_BB);
+  // z = V r, rho = r.z, d = z
+  R.vcycle(0, z, (const float*)r);
+  k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
+  k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHO);
+  cudaMemcpyAsync(d, z, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  R.launches += 4;
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  const double bb = S.hScal->bb;
+  o.initialRelres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+  o.relres = o.initialRelres;
+  if (!(bb > 1e-300) || o.relres <= p->tol) {
+    o.status = 0;
+    return MSBG_OK;
+  }
+  if (!std::isfinite(rr) || !std::isfinite(S.hScal->rho)) {
+    o.status = 3;
+    return MSBG_OK;
+  }
+  auto part1 = [&]() {
+    R.launches += 3;
+    const int nt = R.matvec_dot(d, q, part);
+    k_finalize<<<1, 1024, 0, st>>>(part, nt, sc, FIN_DQ_ALPHA);
+    k_axpy64_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, r, d, q, n, sc, part);
+    k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
+    cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  };
+  auto part2 = [&]() {
+    R.launches += 3;
+    R.vcycle(0, z, (const float*)r);
+    k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
+    k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHONEW_BETA);
+    k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, n, sc);
+  };
+  cudaGraphExec_t g1 = nullptr, g2 = nullptr;
+  int64_t per1 = 0, per2 = 0;
+  auto capture = [&](auto&& body, cudaGraphExec_t& ex, int64_t& per) -> int {
+    const int64_t before = R.launches;
+    cudaGraph_t g;
+    MSBG_CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    body();
+    MSBG_CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
+    per = R.launches - before;
+    R.launches = before;
+    const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    MSBG_CUDA_TRY(ctx, e);
+    return MSBG_OK;
+  };
+  if (p->useGraph) {
+    rc = capture(part1, g1, per1);
+    if (!rc) rc = capture(part2, g2, per2);
+  }
+  auto run = [&](cudaGraphExec_t ex, int64_t per, auto&& body) -> int {
+    if (ex) {
+      MSBG_CUDA_TRY(ctx, cudaGraphLaunch(ex, st));
+      R.launches += per;
+    } else {
+      body();
+    }
+    return MSBG_OK;
+  };
+  const double tol2 = (double)p->tol * p->tol;
+  constexpr double DELTA2 = 1e-2;  // replace when |r| dropped by 10x
+  double rrRef = rr;               // true |r|^2 at the last replacement
+  int checks = 0;                  // true-residual checks at recursive convergence
+  o.status = 1;
+  for (int it = 0; !rc && it < p->maxIter; it++) {
+    rc = run(g1, per1, part1);
+    if (rc) break;
+    rc = [&]() -> int {
+      MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+      return MSBG_OK;
+    }();
+    if (rc) break;
+    o.iters = it + 1;
+    const Scalars hs = *S.hScal;
+    if (hs.status) {
+      o.status = hs.status;
+      break;
+    }
+    if (hs.rr <= tol2 * bb || hs.rr <= DELTA2 * rrRef) {
+      // replace the recursive residual by the true FP64 one (and judge it)
+      if (hs.rr <= tol2 * bb) checks++;
+      rc = residual64(ctx, S, R, b, r, &rr);
+      if (rc) break;
+      o.refinements++;
+      o.relres = std::sqrt(rr / bb);
+      if (!std::isfinite(rr)) {
+        o.status = 3;
+        break;
+      }
+      if (rr <= tol2 * bb) {
+        o.status = 0;
+        break;
+      }
+      if (checks >= maxChecks) break;  // status 1
+      rrRef = rr;
+      // r now holds the true residual; continue with the directions
+    }
+    rc = run(g2, per2, part2);
+  }
+  if (!rc && o.status == 1 && o.iters > 0) {
+    // the true residual of the delivered iterate
+    rc = residual64(ctx, S, R, b, r, &rr);
+    if (!rc) o.relres = std::sqrt(rr / bb);
+  }
+  if (g1) cudaGraphExecDestroy(g1);
+  if (g2) cudaGraphExecDestroy(g2);
+  if (rc) return rc;
+  k_narrow<<<VEC_GRID, VEC_BLOCK, 0, st>>>(S.dev[0]->x.as<float>(), x64, n);
+  R.launches++;
+  return MSBG_OK;
+}
+
 template <typename VT>
 int solve_typed(msbg_gpu_ctx* ctx, Solver& S, const msbg_gpu_solve_params* p, cudaEvent_t e0,
                 cudaEvent_t e1, SolveOut& o, int64_t* launches) {
@@ -750,7 +906,10 @@ int solve_typed(msbg_gpu_ctx* ctx, Solver& S, const msbg_gpu_solve_params* p, cu
     if (maxRefine == 0) rc = solve_plain(ctx, S, R, p, exec, perIter, e1, o);
   }
   if (maxRefine > 0) {
-    rc = solve_refined(ctx, S, R, p, maxRefine, exec, perIter, o);
+    if constexpr (WIDE)
+      rc = solve_reliable(ctx, S, R, p, maxRefine, o);  // FP32: FP64 x, reliable updates
+    else
+      rc = solve_refined(ctx, S, R, p, maxRefine, exec, perIter, o);
     cudaEventRecord(e1, st);
     S.haveX64 = rc == MSBG_OK;
   }

@@ -96,3 +96,36 @@ __global__ void __launch_bounds__(32) k_finalize_max(const double* __restrict__ 
   for (int i = 0; i < n; i++) m = (partial[i] != partial[i] || m != m) ? NAN : fmax(m, partial[i]);
   s->amax = m;
 }
+
+// x64 += alpha d (FP64 accumulation of the FP32 direction); r -= alpha q;
+// partial |r|^2.  Skipped (norm only) after a breakdown.
+__global__ void __launch_bounds__(VEC_BLOCK) k_axpy64_norm(double* __restrict__ x,
+                                                           float* __restrict__ r,
+                                                           const float* __restrict__ d,
+                                                           const float* __restrict__ q, int64_t n,
+                                                           const Scalars* __restrict__ s,
+                                                           double* __restrict__ partial) {
+  const bool ok = s->status == 0;
+  const double alpha = s->alpha;
+  const float af = (float)alpha;
+  double acc = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n >> 2);
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float4 rv = reinterpret_cast<const float4*>(r)[i];
+    if (ok) {
+      const float4 dv = reinterpret_cast<const float4*>(d)[i];
+      const float4 qv = reinterpret_cast<const float4*>(q)[i];
+      double2* xp = reinterpret_cast<double2*>(x) + 2 * i;
+      double2 x0 = xp[0], x1 = xp[1];
+      x0.x += alpha * dv.x; x0.y += alpha * dv.y; x1.x += alpha * dv.z; x1.y += alpha * dv.w;
+      xp[0] = x0;
+      xp[1] = x1;
+      rv.x = fmaf(-af, qv.x, rv.x); rv.y = fmaf(-af, qv.y, rv.y);
+      rv.z = fmaf(-af, qv.z, rv.z); rv.w = fmaf(-af, qv.w, rv.w);
+      reinterpret_cast<float4*>(r)[i] = rv;
+    }
+    acc += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
