@@ -252,6 +252,20 @@ void sample_level0(const Ctx& C, Level& L, std::vector<uint8_t>& fluid) {
     const int l = t.level, ts = t.ts;
     const double h = (double)(1 << l);
     float* cdir[3] = {&L.cx[t.off], &L.cy[t.off], &L.cz[t.off]};
+    // Across a tile face the neighbour region (and whether it is inside the
+    // domain) is the same for every cell: a tile face lies within one block
+    // face.  Resolve it once per face; interior neighbours are this level.
+    int faceLevel[3][2];
+    bool faceInside[3][2];
+    for (int dir = 0; dir < 3; dir++)
+      for (int side = 0; side < 2; side++) {
+        int fv[3] = {t.ox << l, t.oy << l, t.oz << l};
+        const int pd = side ? (dir == 0 ? t.ox : dir == 1 ? t.oy : t.oz) + ts - 1
+                            : (dir == 0 ? t.ox : dir == 1 ? t.oy : t.oz);
+        fv[dir] = side ? (pd + 1) << l : (pd << l) - 1;
+        faceInside[dir][side] = C.inside(fv[0], fv[1], fv[2]);
+        faceLevel[dir][side] = faceInside[dir][side] ? C.level_at(L.m, fv[0], fv[1], fv[2]) : -1;
+      }
     for (int k = 0; k < ts; k++)
       for (int j = 0; j < ts; j++)
         for (int i = 0; i < ts; i++) {
@@ -263,16 +277,15 @@ void sample_level0(const Ctx& C, Level& L, std::vector<uint8_t>& fluid) {
           for (int dir = 0; dir < 3; dir++)
             for (int side = 0; side < 2; side++) {
               // neighbour region level
-              int fv[3] = {p[0] << l, p[1] << l, p[2] << l};
-              fv[dir] = side ? (p[dir] + 1) << l : (p[dir] << l) - 1;
+              const bool onTileFace = side ? loc[dir] == ts - 1 : loc[dir] == 0;
               int q[3] = {p[0], p[1], p[2]};
               if (side) q[dir] += 1;
               double c;
-              if (!C.inside(fv[0], fv[1], fv[2])) {
+              if (onTileFace && !faceInside[dir][side]) {
                 c = h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
                 if (side == 0) cdir[dir][ci] = (float)c;
               } else {
-                const int l2 = C.level_at(L.m, fv[0], fv[1], fv[2]);
+                const int l2 = onTileFace ? faceLevel[dir][side] : l;
                 if (l2 == l) {
                   c = h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
                   if (side == 0) cdir[dir][ci] = (float)c;

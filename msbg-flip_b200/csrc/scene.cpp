@@ -175,6 +175,17 @@ struct msbg_pressure_scene {
   struct Mode { int k[3]; double a[3], phi; double coef; };  // div = coef*cos(theta)
   std::vector<Mode> modes;
   std::vector<int> levels;
+  // Per mode and axis, exp(i w k_d (x + 0.5)) for every cell index x, and
+  // coef * exp(i phi): cos(theta) of a cell is the real part of a product of
+  // table entries (the callbacks are sampled once per cell, so this replaces
+  // 16 cosines by 16 complex products).
+  std::vector<double> etab;  // [mode][axis][res][2]
+  std::vector<double> ephi;  // [mode][2]
+  // Boxes that can contain a cell centre of each 8^3 region (bit b = box b;
+  // built when there are at most 64 boxes, else every box is tested).
+  static constexpr int RG = 8;
+  int nrg = 0;
+  std::vector<uint64_t> boxMask;
 
   double liquid_sdf(double x, double y, double z) const {
     double d = z - zLiquid * res;
@@ -184,20 +195,41 @@ struct msbg_pressure_scene {
     }
     return d;
   }
+  bool in_box(const Box& b, const double* p) const {
+    return p[0] >= b.lo[0] && p[0] < b.hi[0] && p[1] >= b.lo[1] && p[1] < b.hi[1] &&
+           p[2] >= b.lo[2] && p[2] < b.hi[2];
+  }
   bool solid(int x, int y, int z) const {
     const double p[3] = {x + 0.5, y + 0.5, z + 0.5};
+    if (!boxMask.empty()) {
+      uint64_t m = boxMask[(x / RG) + (size_t)nrg * ((y / RG) + (size_t)nrg * (z / RG))];
+      while (m) {
+        const int b = __builtin_ctzll(m);
+        m &= m - 1;
+        if (in_box(boxes[b], p)) return true;
+      }
+      return false;
+    }
     for (const auto& b : boxes)
-      if (p[0] >= b.lo[0] && p[0] < b.hi[0] && p[1] >= b.lo[1] && p[1] < b.hi[1] &&
-          p[2] >= b.lo[2] && p[2] < b.hi[2])
-        return true;
+      if (in_box(b, p)) return true;
     return false;
   }
   bool inside(int x, int y, int z) const {
     return x >= 0 && y >= 0 && z >= 0 && x < res && y < res && z < res;
   }
+  // liquid: below the plane or inside a sphere (the sign of liquid_sdf,
+  // tested on squared distances)
+  bool liquid(double x, double y, double z) const {
+    if (z - zLiquid * res < 0) return true;
+    for (const auto& s : spheres) {
+      double dx = x - s.cx, dy = y - s.cy, dz = z - s.cz;
+      if (dx * dx + dy * dy + dz * dz < s.r * s.r) return true;
+    }
+    return false;
+  }
   uint16_t cell_type(int x, int y, int z) const {
     if (!inside(x, y, z) || solid(x, y, z)) return 1;  // CELL_SOLID
-    return liquid_sdf(x + 0.5, y + 0.5, z + 0.5) < 0 ? 0 : 0x1000;  // CELL_VOID
+    return liquid(x + 0.5, y + 0.5, z + 0.5) ? 0 : 0x1000;  // CELL_VOID
   }
   float face(int dir, int x, int y, int z) const {
     int xm = x - (dir == 0), ym = y - (dir == 1), zm = z - (dir == 2);
@@ -207,10 +239,16 @@ struct msbg_pressure_scene {
   }
   float rhs(int x, int y, int z) const {
     if (cell_type(x, y, z) != 0) return 0.f;
-    const double w = 2.0 * M_PI / res;
     double s = 0;
-    for (const auto& m : modes)
-      s += m.coef * std::cos(w * (m.k[0] * (x + 0.5) + m.k[1] * (y + 0.5) + m.k[2] * (z + 0.5)) + m.phi);
+    const int nm = (int)modes.size();
+    for (int m = 0; m < nm; m++) {
+      const double* ex = &etab[((size_t)(m * 3 + 0) * res + x) * 2];
+      const double* ey = &etab[((size_t)(m * 3 + 1) * res + y) * 2];
+      const double* ez = &etab[((size_t)(m * 3 + 2) * res + z) * 2];
+      const double pr = ex[0] * ey[0] - ex[1] * ey[1], pi = ex[0] * ey[1] + ex[1] * ey[0];
+      const double qr = pr * ez[0] - pi * ez[1], qi = pr * ez[1] + pi * ez[0];
+      s += qr * ephi[2 * m] - qi * ephi[2 * m + 1];  // Re(coef e^{i phi} q)
+    }
     return (float)s;
   }
 };
@@ -246,6 +284,23 @@ extern "C" msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, in
     }
     s->boxes.push_back(b);
   }
+  if (res % msbg_pressure_scene::RG == 0 && s->boxes.size() <= 64) {
+    const int RG = msbg_pressure_scene::RG;
+    s->nrg = res / RG;
+    s->boxMask.assign((size_t)s->nrg * s->nrg * s->nrg, 0);
+    for (size_t bi = 0; bi < s->boxes.size(); bi++) {
+      const auto& b = s->boxes[bi];
+      int r0[3], r1[3];  // regions whose cell centres can fall inside the box
+      for (int k = 0; k < 3; k++) {
+        r0[k] = std::max(0, (int)std::floor(b.lo[k] - 0.5) / RG);
+        r1[k] = std::min(s->nrg - 1, (int)std::floor(std::max(b.hi[k] - 0.5, 0.0)) / RG);
+      }
+      for (int z = r0[2]; z <= r1[2]; z++)
+        for (int y = r0[1]; y <= r1[1]; y++)
+          for (int x = r0[0]; x <= r1[0]; x++)
+            s->boxMask[x + (size_t)s->nrg * (y + (size_t)s->nrg * z)] |= 1ull << bi;
+    }
+  }
   // Box-Muller normals for the amplitudes.
   auto normal = [&]() {
     double u1 = std::max(rng.uniform(), 1e-300), u2 = rng.uniform();
@@ -265,6 +320,20 @@ extern "C" msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, in
     for (int k = 0; k < 3; k++) c += m.a[k] * std::sin(M_PI * m.k[k] / res);
     m.coef = 2 * c;
     s->modes.push_back(m);
+  }
+  const double w = 2.0 * M_PI / res;
+  s->etab.resize((size_t)nModes * 3 * res * 2);
+  s->ephi.resize((size_t)nModes * 2);
+  for (int i = 0; i < nModes; i++) {
+    const auto& m = s->modes[i];
+    s->ephi[2 * i] = m.coef * std::cos(m.phi);
+    s->ephi[2 * i + 1] = m.coef * std::sin(m.phi);
+    for (int d = 0; d < 3; d++)
+      for (int x = 0; x < res; x++) {
+        const double a = w * m.k[d] * (x + 0.5);
+        s->etab[((size_t)(i * 3 + d) * res + x) * 2] = std::cos(a);
+        s->etab[((size_t)(i * 3 + d) * res + x) * 2 + 1] = std::sin(a);
+      }
   }
   // Refinement map.
   const int nb1 = res / bsx0;
