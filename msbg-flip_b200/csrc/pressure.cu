@@ -63,6 +63,7 @@ struct Solver {
   std::vector<int> cnnTilesHost, cnnLevelHost;
   int cnnChunk = 0;
   bool haveX64 = false;  // x64 holds the solution of the last refined solve
+  DeviceBuffer packTiles, packBuf;  // device-side packing into the block layout
 };
 
 // Dynamic shared-memory limits of the kernels a level-0 vector type needs
@@ -223,12 +224,120 @@ std::map<msbg_gpu_ctx*, std::unique_ptr<Solver>>& solvers() {
 
 std::unique_ptr<Solver>& solver_of(msbg_gpu_ctx* ctx) { return solvers()[ctx]; }
 
+// Host -> device copies of the prepared arrays.  Large arrays go through two
+// pinned 64 MB staging buffers of the calling thread: a parallel memcpy fills
+// one while the DMA of the other runs (a pageable copy is staged by the
+// driver on one thread at a few GB/s).
+struct PinnedStaging {
+  static constexpr size_t CH = 64u << 20;
+  void* buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  int device = -1;
+  bool used[2] = {false, false};
+  ~PinnedStaging() {
+    for (int i = 0; i < 2; i++) {
+      if (ev[i]) cudaEventDestroy(ev[i]);
+      if (buf[i]) cudaFreeHost(buf[i]);
+    }
+  }
+  bool ready(int dev) {
+    if (device == dev) return true;
+    if (device >= 0) return false;  // one device per host thread
+    for (int i = 0; i < 2; i++)
+      if (cudaMallocHost(&buf[i], CH) != cudaSuccess ||
+          cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess)
+        return false;
+    device = dev;
+    return true;
+  }
+};
+
+PinnedStaging& staging() {
+  thread_local PinnedStaging stg;
+  return stg;
+}
+
+cudaError_t copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  PinnedStaging& stg = staging();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (bytes < (8u << 20) || !stg.ready(dev))
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+  for (size_t o = 0, c = 0; o < bytes; o += PinnedStaging::CH, c++) {
+    const int k = (int)(c & 1);
+    const size_t len = std::min(PinnedStaging::CH, bytes - o);
+    if (stg.used[k]) {
+      cudaError_t e = cudaEventSynchronize(stg.ev[k]);
+      if (e != cudaSuccess) return e;
+    }
+    const char* s = static_cast<const char*>(src) + o;
+    char* d = static_cast<char*>(stg.buf[k]);
+    const int64_t parts = 16;
+#pragma omp parallel for schedule(static)
+    for (int64_t q = 0; q < parts; q++) {
+      const size_t a = len * q / parts, b = len * (q + 1) / parts;
+      std::memcpy(d + a, s + a, b - a);
+    }
+    cudaError_t e = cudaMemcpyAsync(static_cast<char*>(dst) + o, d, len, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    e = cudaEventRecord(stg.ev[k], st);
+    if (e != cudaSuccess) return e;
+    stg.used[k] = true;
+  }
+  return cudaSuccess;
+}
+
+// Device -> host into pageable memory, through the same staging buffers: the
+// DMA of chunk c+1 runs while chunk c is copied out in parallel.  Returns
+// after the last byte has landed.
+cudaError_t copy_d2h(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  PinnedStaging& stg = staging();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (bytes < (8u << 20) || !stg.ready(dev)) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+    return e != cudaSuccess ? e : cudaStreamSynchronize(st);
+  }
+  const size_t CH = PinnedStaging::CH;
+  const size_t nch = (bytes + CH - 1) / CH;
+  auto issue = [&](size_t c) {
+    const int k = (int)(c & 1);
+    const size_t o = c * CH, len = std::min(CH, bytes - o);
+    cudaError_t e = cudaMemcpyAsync(stg.buf[k], static_cast<const char*>(src) + o, len,
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(stg.ev[k], st);
+    stg.used[k] = true;
+    return e;
+  };
+  cudaError_t e = issue(0);
+  for (size_t c = 0; c < nch && e == cudaSuccess; c++) {
+    const int k = (int)(c & 1);
+    const size_t o = c * CH, len = std::min(CH, bytes - o);
+    e = cudaEventSynchronize(stg.ev[k]);
+    if (e != cudaSuccess) break;
+    if (c + 1 < nch) {
+      // the other buffer was copied out in the previous round
+      e = issue(c + 1);
+      if (e != cudaSuccess) break;
+    }
+    const char* s = static_cast<const char*>(stg.buf[k]);
+    char* d = static_cast<char*>(dst) + o;
+    const int64_t parts = 16;
+#pragma omp parallel for schedule(static)
+    for (int64_t q = 0; q < parts; q++) {
+      const size_t a = len * q / parts, b = len * (q + 1) / parts;
+      std::memcpy(d + a, s + a, b - a);
+    }
+  }
+  return e;
+}
+
 template <typename T>
 cudaError_t upload(DeviceBuffer& buf, const std::vector<T>& v, cudaStream_t st) {
   cudaError_t e = buf.ensure(sizeof(T) * std::max<size_t>(v.size(), 1));
   if (e != cudaSuccess) return e;
   if (v.empty()) return cudaSuccess;
-  return cudaMemcpyAsync(buf.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st);
+  return copy_h2d(buf.p, v.data(), sizeof(T) * v.size(), st);
 }
 
 }  // namespace
@@ -1123,32 +1232,72 @@ extern "C" int msbg_gpu_pressure_profile(msbg_gpu_ctx* ctx, int what, int reps, 
 namespace {
 
 // Copy a level-0 vector (tile layout) into the reference's packed block layout.
-int to_packed(msbg_gpu_ctx* ctx, Solver& S, const float* dvec, float* packed, int64_t n) {
+// The reference's block layout (packed): per block in bid order,
+// (bsx0 >> level)^3 values, vid = x + y*bs + z*bs*bs.  A tile lies inside one
+// block, so its cell (i, j, k) lands at base + i + bs*(j + bs*k).
+struct PackTile {
+  int64_t base;  // packed index of the tile's first cell
+  int bs, ts;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_to_packed(const T* __restrict__ v,
+                                                   const int64_t* __restrict__ tileOff,
+                                                   const PackTile* __restrict__ pt,
+                                                   T* __restrict__ out) {
+  const PackTile P = pt[blockIdx.x];
+  const int64_t off = tileOff[blockIdx.x];
+  const int n = P.ts * P.ts * P.ts;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int i = e % P.ts, j = (e / P.ts) % P.ts, k = e / (P.ts * P.ts);
+    out[P.base + i + (int64_t)P.bs * (j + (int64_t)P.bs * k)] = v[off + e];
+  }
+}
+
+int64_t packed_count(const Solver& S) {
+  int64_t s = 0;
+  for (int l : S.blockLevel) {
+    const int bs = S.bsx0 >> l;
+    s += (int64_t)bs * bs * bs;
+  }
+  return s;
+}
+
+// Packs level-0 vector dvec on the device and copies it into `packed`.
+template <typename T>
+int to_packed(msbg_gpu_ctx* ctx, Solver& S, const T* dvec, T* packed, int64_t n) {
   const Level& L = S.H.levels[0];
-  std::vector<float> h(L.nCells);
-  MSBG_CUDA_TRY(ctx, cudaMemcpy(h.data(), dvec, sizeof(float) * L.nCells, cudaMemcpyDeviceToHost));
-  // block offsets in the packed layout
-  const int64_t nb = (int64_t)S.nbx * S.nby * S.nbz;
-  std::vector<int64_t> boff(nb + 1, 0);
-  for (int64_t b = 0; b < nb; b++) {
-    const int bs = S.bsx0 >> S.blockLevel[b];
-    boff[b + 1] = boff[b] + (int64_t)bs * bs * bs;
+  const int64_t need = packed_count(S);
+  if (n < need)
+    return set_error(ctx, MSBG_EINVARG, "packed buffer too small (%lld < %lld)", (long long)n,
+                     (long long)need);
+  cudaStream_t st = ctx->stream;
+  if (!S.packTiles.p) {
+    const int64_t nb = (int64_t)S.nbx * S.nby * S.nbz;
+    std::vector<int64_t> boff(nb + 1, 0);
+    for (int64_t bb = 0; bb < nb; bb++) {
+      const int bs = S.bsx0 >> S.blockLevel[bb];
+      boff[bb + 1] = boff[bb] + (int64_t)bs * bs * bs;
+    }
+    std::vector<PackTile> pt(L.tiles.size());
+    for (size_t ti = 0; ti < L.tiles.size(); ti++) {
+      const Tile& t = L.tiles[ti];
+      const int bs = S.bsx0 >> t.level;
+      const int64_t blk = (t.ox / bs) + (int64_t)S.nbx * ((t.oy / bs) + (int64_t)S.nby * (t.oz / bs));
+      pt[ti].base = boff[blk] + (t.ox % bs) + (int64_t)bs * ((t.oy % bs) + (int64_t)bs * (t.oz % bs));
+      pt[ti].bs = bs;
+      pt[ti].ts = t.ts;
+    }
+    MSBG_CUDA_TRY(ctx, upload(S.packTiles, pt, st));
+    MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   }
-  if (n < boff[nb]) return set_error(ctx, MSBG_EINVARG, "packed buffer too small (%lld < %lld)",
-                                     (long long)n, (long long)boff[nb]);
-  std::memset(packed, 0, sizeof(float) * boff[nb]);
-  for (const Tile& t : L.tiles) {
-    for (int k = 0; k < t.ts; k++)
-      for (int j = 0; j < t.ts; j++)
-        for (int i = 0; i < t.ts; i++) {
-          const int X = t.ox + i, Y = t.oy + j, Z = t.oz + k;
-          const int bs = S.bsx0 >> t.level;
-          const int64_t b = (X / bs) + (int64_t)S.nbx * ((Y / bs) + (int64_t)S.nby * (Z / bs));
-          const int vx = X % bs, vy = Y % bs, vz = Z % bs;
-          packed[boff[b] + vx + (int64_t)bs * (vy + (int64_t)bs * vz)] =
-              h[t.off + i + (int64_t)t.ts * (j + (int64_t)t.ts * k)];
-        }
-  }
+  MSBG_CUDA_TRY(ctx, S.packBuf.ensure(sizeof(T) * need));
+  MSBG_CUDA_TRY(ctx, cudaMemsetAsync(S.packBuf.p, 0, sizeof(T) * need, st));
+  if (!L.tiles.empty())
+    k_to_packed<T><<<(unsigned)L.tiles.size(), 256, 0, st>>>(
+        dvec, S.dev[0]->tileOff.as<int64_t>(), S.packTiles.as<PackTile>(), S.packBuf.as<T>());
+  MSBG_CUDA_TRY(ctx, cudaGetLastError());
+  MSBG_CUDA_TRY(ctx, copy_d2h(packed, S.packBuf.p, sizeof(T) * need, st));
   return MSBG_OK;
 }
 
@@ -1158,12 +1307,7 @@ extern "C" int msbg_gpu_pressure_packed_size(msbg_gpu_ctx* ctx, int64_t* n) {
   if (!ctx || !n) return MSBG_EINVARG;
   auto& sp = solver_of(ctx);
   if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
-  int64_t s = 0;
-  for (int l : sp->blockLevel) {
-    const int bs = sp->bsx0 >> l;
-    s += (int64_t)bs * bs * bs;
-  }
-  *n = s;
+  *n = packed_count(*sp);
   return MSBG_OK;
 }
 
@@ -1207,29 +1351,7 @@ extern "C" int msbg_gpu_pressure_download64(msbg_gpu_ctx* ctx, double* packed, i
   if (!S.x64.p) return set_error(ctx, MSBG_EINVARG, "no FP64 solution (solve with maxRefine > 0)");
   cudaSetDevice(ctx->device);
   MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  const Level& L = S.H.levels[0];
-  std::vector<double> h(L.nCells);
-  MSBG_CUDA_TRY(ctx, cudaMemcpy(h.data(), S.x64.p, sizeof(double) * L.nCells,
-                                cudaMemcpyDeviceToHost));
-  const int64_t nb = (int64_t)S.nbx * S.nby * S.nbz;
-  std::vector<int64_t> boff(nb + 1, 0);
-  for (int64_t b = 0; b < nb; b++) {
-    const int bs = S.bsx0 >> S.blockLevel[b];
-    boff[b + 1] = boff[b] + (int64_t)bs * bs * bs;
-  }
-  if (n < boff[nb]) return set_error(ctx, MSBG_EINVARG, "packed buffer too small");
-  std::memset(packed, 0, sizeof(double) * boff[nb]);
-  for (const Tile& t : L.tiles)
-    for (int k = 0; k < t.ts; k++)
-      for (int j = 0; j < t.ts; j++)
-        for (int i = 0; i < t.ts; i++) {
-          const int X = t.ox + i, Y = t.oy + j, Z = t.oz + k;
-          const int bs = S.bsx0 >> t.level;
-          const int64_t b = (X / bs) + (int64_t)S.nbx * ((Y / bs) + (int64_t)S.nby * (Z / bs));
-          packed[boff[b] + (X % bs) + (int64_t)bs * ((Y % bs) + (int64_t)bs * (Z % bs))] =
-              h[t.off + i + (int64_t)t.ts * (j + (int64_t)t.ts * k)];
-        }
-  return MSBG_OK;
+  return to_packed(ctx, S, S.x64.as<double>(), packed, n);
 }
 
 extern "C" int msbg_gpu_pressure_download_rhs(msbg_gpu_ctx* ctx, float* packed, int64_t n) {
