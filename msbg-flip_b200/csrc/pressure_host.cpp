@@ -266,56 +266,72 @@ void sample_level0(const Ctx& C, Level& L, std::vector<uint8_t>& fluid) {
         faceInside[dir][side] = C.inside(fv[0], fv[1], fv[2]);
         faceLevel[dir][side] = faceInside[dir][side] ? C.level_at(L.m, fv[0], fv[1], fv[2]) : -1;
       }
+    // coupling of cell (i,j,k) across face (dir, side); records the interface
+    // couplings and, for lower faces to the same level, the face array
+    auto face_c = [&](int i, int j, int k, int dir, int side) -> double {
+      const int64_t ci = i + (int64_t)ts * (j + (int64_t)ts * k);
+      const int X = t.ox + i, Y = t.oy + j, Z = t.oz + k;
+      const int p[3] = {X, Y, Z}, loc[3] = {i, j, k};
+      const bool onTileFace = side ? loc[dir] == ts - 1 : loc[dir] == 0;
+      int q[3] = {p[0], p[1], p[2]};
+      if (side) q[dir] += 1;
+      double c;
+      if (onTileFace && !faceInside[dir][side]) {
+        c = h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
+        if (side == 0) cdir[dir][ci] = (float)c;
+        return c;
+      }
+      const int l2 = onTileFace ? faceLevel[dir][side] : l;
+      if (l2 == l) {
+        c = h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
+        if (side == 0) cdir[dir][ci] = (float)c;
+      } else if (l2 == l + 1) {
+        c = interface_coupling(cb, l, dir, side, X, Y, Z);
+        int64_t io = L.ifOff[(size_t)ti * 6 + dir * 2 + side];
+        int ax, bx;
+        face_axes(dir, ax, bx);
+        if (io >= 0) L.ifc[io + loc[ax] + (int64_t)ts * loc[bx]] = (float)c;
+      } else {
+        // finer neighbours: 4 fine cells share this face
+        int ax, bx;
+        face_axes(dir, ax, bx);
+        c = 0;
+        for (int u = 0; u < 2; u++)
+          for (int v = 0; v < 2; v++) {
+            int f[3];
+            f[dir] = side ? (p[dir] + 1) * 2 : p[dir] * 2 - 1;
+            f[ax] = p[ax] * 2 + u;
+            f[bx] = p[bx] * 2 + v;
+            c += interface_coupling(cb, l - 1, dir, 1 - side, f[0], f[1], f[2]);
+          }
+      }
+      return c;
+    };
+    // pass 1: lower faces (each interior face once); pass 2: upper faces,
+    // which inside the tile are the next cell's lower faces
+    const size_t n3 = (size_t)ts * ts * ts;
+    thread_local std::vector<double> low;  // reused across this thread's tiles
+    if (low.size() < 3 * n3) low.resize(3 * n3);
     for (int k = 0; k < ts; k++)
       for (int j = 0; j < ts; j++)
         for (int i = 0; i < ts; i++) {
           const int64_t ci = i + (int64_t)ts * (j + (int64_t)ts * k);
-          const int X = t.ox + i, Y = t.oy + j, Z = t.oz + k;
-          const int p[3] = {X, Y, Z}, loc[3] = {i, j, k};
+          for (int dir = 0; dir < 3; dir++) low[dir * n3 + ci] = face_c(i, j, k, dir, 0);
+        }
+    const int64_t stride[3] = {1, ts, (int64_t)ts * ts};
+    for (int k = 0; k < ts; k++)
+      for (int j = 0; j < ts; j++)
+        for (int i = 0; i < ts; i++) {
+          const int64_t ci = i + (int64_t)ts * (j + (int64_t)ts * k);
+          const int loc[3] = {i, j, k};
           const bool isFluid = !fluid.empty() ? fluid[t.off + ci] : false;
           double diag = 0;
-          for (int dir = 0; dir < 3; dir++)
-            for (int side = 0; side < 2; side++) {
-              // neighbour region level
-              const bool onTileFace = side ? loc[dir] == ts - 1 : loc[dir] == 0;
-              int q[3] = {p[0], p[1], p[2]};
-              if (side) q[dir] += 1;
-              double c;
-              if (onTileFace && !faceInside[dir][side]) {
-                c = h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
-                if (side == 0) cdir[dir][ci] = (float)c;
-              } else {
-                const int l2 = onTileFace ? faceLevel[dir][side] : l;
-                if (l2 == l) {
-                  c = h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
-                  if (side == 0) cdir[dir][ci] = (float)c;
-                } else if (l2 == l + 1) {
-                  c = interface_coupling(cb, l, dir, side, X, Y, Z);
-                  const bool onFace = side ? loc[dir] == ts - 1 : loc[dir] == 0;
-                  if (onFace) {
-                    int64_t io = L.ifOff[(size_t)ti * 6 + dir * 2 + side];
-                    int ax, bx;
-                    face_axes(dir, ax, bx);
-                    if (io >= 0) L.ifc[io + loc[ax] + (int64_t)ts * loc[bx]] = (float)c;
-                  }
-                } else {
-                  // finer neighbours: 4 fine cells share this face
-                  int ax, bx;
-                  face_axes(dir, ax, bx);
-                  c = 0;
-                  for (int u = 0; u < 2; u++)
-                    for (int v = 0; v < 2; v++) {
-                      int f[3];
-                      f[dir] = side ? (p[dir] + 1) * 2 : p[dir] * 2 - 1;
-                      f[ax] = p[ax] * 2 + u;
-                      f[bx] = p[bx] * 2 + v;
-                      c += interface_coupling(cb, l - 1, dir, 1 - side, f[0], f[1], f[2]);
-                    }
-                }
-              }
-              diag += c;
-            }
+          for (int dir = 0; dir < 3; dir++) {
+            diag += low[dir * n3 + ci];
+            diag += loc[dir] < ts - 1 ? low[dir * n3 + ci + stride[dir]] : face_c(i, j, k, dir, 1);
+          }
           if (isFluid) {
+            const int X = t.ox + i, Y = t.oy + j, Z = t.oz + k;
             L.diag[t.off + ci] = (float)diag;
             L.rhs[t.off + ci] =
                 (float)(cb->sampleRhs(cb->user, X << l, Y << l, Z << l) * h * h * h);
@@ -419,6 +435,29 @@ void galerkin(const Ctx& C, const Level& F, const std::vector<uint8_t>& fineFlui
     const Tile& t = G.tiles[ti];
     const int lc = t.level, ts = t.ts;
     float* cdir[3] = {&G.cx[t.off], &G.cy[t.off], &G.cz[t.off]};
+    // Fast path of an aggregated tile (the tile lies in one block, so all its
+    // cells aggregate or none do): its children fill a fine region of
+    // (2 ts)^3 cells at level lc-1 covered by whole fine tiles, resolved once.
+    const int P0[3] = {t.ox, t.oy, t.oz};
+    const bool aggT = aggregated(lc, P0);
+    const int tsf = aggT ? F.tsOf[lc - 1] : 0;
+    const int nsub = aggT && tsf > 0 ? (2 * ts) / tsf : 0;
+    int64_t subOff[64];
+    bool fast = aggT && tsf > 0 && nsub * tsf == 2 * ts && nsub * nsub * nsub <= 64;
+    for (int sz = 0; fast && sz < nsub; sz++)
+      for (int sy = 0; sy < nsub; sy++)
+        for (int sx = 0; sx < nsub; sx++) {
+          const int ft = tile_at(F, lc - 1, 2 * t.ox + sx * tsf, 2 * t.oy + sy * tsf,
+                                 2 * t.oz + sz * tsf);
+          subOff[sx + nsub * (sy + nsub * sz)] = ft >= 0 ? F.tiles[ft].off : -1;
+        }
+    // fine cell of region coords (x, y, z) in [0, 2 ts), or -1
+    auto fidx = [&](int x, int y, int z) -> int64_t {
+      const int64_t o = subOff[(x / tsf) + nsub * ((y / tsf) + nsub * (z / tsf))];
+      if (o < 0) return -1;
+      return o + (x % tsf) + (int64_t)tsf * ((y % tsf) + (int64_t)tsf * (z % tsf));
+    };
+    const float* fcd[3] = {F.cx.data(), F.cy.data(), F.cz.data()};
     for (int k = 0; k < ts; k++)
       for (int j = 0; j < ts; j++)
         for (int i = 0; i < ts; i++) {
@@ -426,6 +465,57 @@ void galerkin(const Ctx& C, const Level& F, const std::vector<uint8_t>& fineFlui
           const int P[3] = {t.ox + i, t.oy + j, t.oz + k};
           const int loc[3] = {i, j, k};
           if (!coarseFluid[t.off + ci]) continue;
+          if (fast) {
+            // children, their diagonal and internal pairs
+            int64_t ch[8];
+            for (int c = 0; c < 8; c++) {
+              const int64_t fc = fidx(2 * i + (c & 1), 2 * j + ((c >> 1) & 1), 2 * k + (c >> 2));
+              ch[c] = fine_fluid(fc) ? fc : -1;
+            }
+            double d = 0;
+            for (int c = 0; c < 8; c++) {
+              if (ch[c] < 0) continue;
+              d += F.diag[ch[c]];
+              for (int dir = 0; dir < 3; dir++)
+                if ((c >> dir) & 1)
+                  if (ch[c ^ (1 << dir)] >= 0) d -= 2.0 * fcd[dir][ch[c]];
+            }
+            G.diag[t.off + ci] = (float)d;
+            // lower faces inside the tile: 4 fine pairs each
+            for (int dir = 0; dir < 3; dir++) {
+              if (loc[dir] == 0) continue;  // tile face: generic path below
+              double cs = 0;
+              for (int c = 0; c < 8; c++) {
+                if ((c >> dir) & 1 || ch[c] < 0) continue;  // lower children of P
+                int f[3] = {2 * i + (c & 1), 2 * j + ((c >> 1) & 1), 2 * k + (c >> 2)};
+                f[dir] -= 1;
+                if (fine_fluid(fidx(f[0], f[1], f[2]))) cs += fcd[dir][ch[c]];
+              }
+              cdir[dir][ci] = (float)cs;
+            }
+            // tile faces (same level, lower side) and level interfaces
+            for (int dir = 0; dir < 3; dir++)
+              for (int side = 0; side < 2; side++) {
+                const bool onFace = side ? loc[dir] == ts - 1 : loc[dir] == 0;
+                if (!onFace) continue;
+                int fv[3] = {P[0] << lc, P[1] << lc, P[2] << lc};
+                fv[dir] = side ? (P[dir] + 1) << lc : (P[dir] << lc) - 1;
+                if (!C.inside(fv[0], fv[1], fv[2])) continue;
+                const int l2 = C.level_at(G.m, fv[0], fv[1], fv[2]);
+                if (l2 == lc && side == 0) {
+                  cdir[dir][ci] = (float)coarse_face(lc, P, dir, side);
+                } else if (l2 == lc + 1) {
+                  int64_t io = G.ifOff[(size_t)ti * 6 + dir * 2 + side];
+                  if (io >= 0) {
+                    int ax, bx;
+                    face_axes(dir, ax, bx);
+                    G.ifc[io + loc[ax] + (int64_t)ts * loc[bx]] =
+                        (float)coarse_face(lc, P, dir, side);
+                  }
+                }
+              }
+            continue;
+          }
           // diagonal
           double d = 0;
           if (aggregated(lc, P)) {
