@@ -129,13 +129,14 @@ def dist_env():
     return ws, rank, local
 
 
-def init_dist(ws):
+def init_dist(ws, backend="nccl"):
+    """Process group of the replicas (one per GPU; gloo for CPU tests)."""
     if ws <= 1:
         return None
     import datetime
 
     import torch.distributed as dist
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return dist
 
 
