@@ -259,30 +259,53 @@ __global__ void __launch_bounds__(NTH, 1)
     const float* CZ = X + 5 * N;
     const float(*gs)[TS * TS] = gsb[s];
     float R[2][KK], I[2][KK], Cm[2][KK][3], Cp[2][KK][3];
+    // A thread's two cells at (jj, k) are x-neighbours 2ip, 2ip+1 (one per
+    // colour): their coefficients come as float2 pairs.  The even cell has
+    // colour (jj + k) & 1; runtime selects keep the arrays compile-time indexed.
 #pragma unroll
-    for (int c = 0; c < 2; c++)
+    for (int kk = 0; kk < KK; kk++) {
+      const int k = kb + KSTRIDE * kk;
+      const int e0 = tidx(TS, 2 * ip, jj, k);
+      const float2 iv2 = *reinterpret_cast<const float2*>(IV + e0);
+      const float2 cx2 = *reinterpret_cast<const float2*>(CX + e0);
+      const float cxn = CX[e0 + 2];  // past the row end only when unused (ii = 15)
+      const float2 cy2 = *reinterpret_cast<const float2*>(CY + e0);
+      const float2 cyn = *reinterpret_cast<const float2*>(CY + e0 + TS);
+      const float2 cz2 = *reinterpret_cast<const float2*>(CZ + e0);
+      const float2 czn = *reinterpret_cast<const float2*>(CZ + e0 + TS * TS);
+      const float ivv[2] = {iv2.x, iv2.y};
+      float rr[2] = {to_f(B[e0]), to_f(B[e0 + 1])};
+      float cm[2][3], cp[2][3];
 #pragma unroll
-      for (int kk = 0; kk < KK; kk++) {
-        const int k = kb + KSTRIDE * kk, ii = 2 * ip + ((jj + k + c) & 1);
-        const int e = tidx(TS, ii, jj, k);
-        const float iv = IV[e];
-        const bool fl = iv > 0.f;
-        I[c][kk] = iv;
-        float r = to_f(B[e]);
-        if (ii == 0) r += gs[0][jj + TS * k];
-        if (ii == TS - 1) r += gs[1][jj + TS * k];
-        if (jj == 0) r += gs[2][ii + TS * k];
-        if (jj == TS - 1) r += gs[3][ii + TS * k];
-        if (k == 0) r += gs[4][ii + TS * jj];
-        if (k == TS - 1) r += gs[5][ii + TS * jj];
-        R[c][kk] = r;
-        Cm[c][kk][0] = (fl && ii > 0) ? CX[e] : 0.f;
-        Cp[c][kk][0] = (fl && ii < TS - 1) ? CX[e + 1] : 0.f;
-        Cm[c][kk][1] = (fl && jj > 0) ? CY[e] : 0.f;
-        Cp[c][kk][1] = (fl && jj < TS - 1) ? CY[e + TS] : 0.f;
-        Cm[c][kk][2] = (fl && k > 0) ? CZ[e] : 0.f;
-        Cp[c][kk][2] = (fl && k < TS - 1) ? CZ[e + TS * TS] : 0.f;
+      for (int h = 0; h < 2; h++) {
+        const int ii = 2 * ip + h;
+        const bool fl = ivv[h] > 0.f;
+        if (ii == 0) rr[h] += gs[0][jj + TS * k];
+        if (ii == TS - 1) rr[h] += gs[1][jj + TS * k];
+        if (jj == 0) rr[h] += gs[2][ii + TS * k];
+        if (jj == TS - 1) rr[h] += gs[3][ii + TS * k];
+        if (k == 0) rr[h] += gs[4][ii + TS * jj];
+        if (k == TS - 1) rr[h] += gs[5][ii + TS * jj];
+        cm[h][0] = (fl && ii > 0) ? (h ? cx2.y : cx2.x) : 0.f;
+        cp[h][0] = (fl && ii < TS - 1) ? (h ? cxn : cx2.y) : 0.f;
+        cm[h][1] = (fl && jj > 0) ? (h ? cy2.y : cy2.x) : 0.f;
+        cp[h][1] = (fl && jj < TS - 1) ? (h ? cyn.y : cyn.x) : 0.f;
+        cm[h][2] = (fl && k > 0) ? (h ? cz2.y : cz2.x) : 0.f;
+        cp[h][2] = (fl && k < TS - 1) ? (h ? czn.y : czn.x) : 0.f;
       }
+      const bool evenIs0 = ((jj + k) & 1) == 0;  // colour 0 is the even cell
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const bool ev = (c == 0) == evenIs0;
+        I[c][kk] = ev ? ivv[0] : ivv[1];
+        R[c][kk] = ev ? rr[0] : rr[1];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          Cm[c][kk][d] = ev ? cm[0][d] : cm[1][d];
+          Cp[c][kk][d] = ev ? cp[0][d] : cp[1][d];
+        }
+      }
+    }
     // 3: red-black sweeps (colour compile-time so the arrays stay in registers)
     auto half = [&](auto cc) {
       constexpr int c = decltype(cc)::value;
