@@ -224,54 +224,68 @@ def bench_reference(args):
     print(json.dumps(line), flush=True)
 
 
-# training set of the learned guess: (RHS, solution) tile pairs of the refined
-# solver on seeded sphere-union instances at 512^3 (64 spheres, radii 20-60
-# voxels, 32^3 base blocks, 2 levels), 500 spread-out 16^3 tiles each
+# training sets, from the refined solver on seeded sphere-union instances at
+# 512^3 (64 spheres, radii 20-60 voxels, 32^3 base blocks, 2 levels): the
+# guess network's (RHS, solution) pairs on 500 spread-out 16^3 tiles each; the
+# correction network's (residual, error) pairs after a V-cycle at PCG
+# iterations 0, 1 and 2, 166 tiles each
 LEARN_CFG = dict(res=512, seeds=(100, 101, 102, 103), pairs_per_instance=500, epochs=60,
                  batch=64, lr=2e-3)
 
 
 def learned_variants(ctx, c, scene):
-    """Train the network on the GPU, then time the learned solves of the bench
-    problem (FP32 and FP16 level-0 vectors, FP64 refinement to 1e-6)."""
+    """Train the guess and correction networks on the GPU, then time the
+    learned solves of the bench problem (FP64 refinement to 1e-6)."""
     import torch
     import msbg_gpu
     L = LEARN_CFG
+    vc = dict(nPre=c["n_pre"], nPost=c["n_post"], innerIter=c["inner"])
     t0 = time.perf_counter()
-    F, T, M = [], [], []
+    G, K = [], []
     for sd in L["seeds"]:
         ctx.pressure_prepare(msbg_gpu.PressureScene(L["res"], 32, 2, 0.0, 64, 20 / 512, 60 / 512, 8,
                                                     16, 8, 32.0 * L["res"] / 512, sd))
         ctx.pressure_solve(tol=1e-6, maxRefine=4)
-        f, t, m = msbg_gpu.collect_training_pairs(ctx, L["pairs_per_instance"])
-        F.append(f)
-        T.append(t)
-        M.append(m)
-    F, T, M = torch.cat(F), torch.cat(T), torch.cat(M)
+        G.append(msbg_gpu.collect_training_pairs(ctx, L["pairs_per_instance"]))
+        for k in (0, 1, 2):
+            K.append(msbg_gpu.collect_correction_pairs(ctx, L["pairs_per_instance"] // 3, k, **vc))
+    cat = lambda P: [torch.cat([q[j] for q in P]) for j in range(3)]
+    G, K = cat(G), cat(K)
     data_s = time.perf_counter() - t0
-    net = msbg_gpu.Cnn(ctx.device)
+    net, corr = msbg_gpu.Cnn(ctx.device), msbg_gpu.Cnn(ctx.device)
     t0 = time.perf_counter()
-    losses = msbg_gpu.train_cnn(net, F, T, M, epochs=L["epochs"], batch=L["batch"], lr=L["lr"], seed=1)
+    losses = msbg_gpu.train_cnn(net, *G, epochs=L["epochs"], batch=L["batch"], lr=L["lr"], seed=1)
+    closs = msbg_gpu.train_cnn(corr, *K, epochs=L["epochs"], batch=L["batch"], lr=L["lr"], seed=2)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
-    rms = float((T * T * M).sum() / M.sum())
+    rel = lambda ls, T, M: (ls[-1] / float((T * T * M).sum() / M.sum())) ** 0.5
     ctx.pressure_prepare(scene)
     ctx.pressure_set_cnn(net)
-    out = {"pairs": int(F.shape[0]), "epochs": L["epochs"], "data_seconds": data_s,
-           "train_seconds": train_s, "final_rel_loss": (losses[-1] / rms) ** 0.5,
+    ctx.pressure_set_correction_cnn(corr)
+    out = {"pairs": int(G[0].shape[0]), "correction_pairs": int(K[0].shape[0]),
+           "epochs": L["epochs"], "data_seconds": data_s, "train_seconds": train_s,
+           "final_rel_loss": rel(losses, G[1], G[2]),
+           "correction_final_rel_loss": rel(closs, K[1], K[2]),
            "network": "4 x conv3^3 16ch ReLU, BF16 tcgen05 implicit GEMM, FP32 accumulate"}
-    for name, storage in (("f32", msbg_gpu.F32), ("f16", msbg_gpu.F16)):
+    for name, storage, mode in (("f32_vectors_learned_guess", msbg_gpu.F32, 1),
+                                ("f16_vectors_learned_guess", msbg_gpu.F16, 1),
+                                ("f32_vectors_learned_correction", msbg_gpu.F32, 2),
+                                ("f32_vectors_learned_guess_and_correction", msbg_gpu.F32, 3)):
         vp = msbg_gpu.solve_params(nPre=c["n_pre"], nPost=c["n_post"], tol=c["tol"],
                                    innerIter=c["inner"], useGraph=1, storage=storage,
-                                   maxRefine=30, learned=1)
+                                   maxRefine=30, learned=mode)
         ctx.pressure_solve(vp)
         vi = ctx.pressure_solve(vp)
-        out[name + "_vectors_learned_guess"] = {
+        out[name] = {
             "ms": vi.solveSeconds * 1e3, "pcg_iterations": vi.iterations,
             "refinements": vi.refinements, "status": vi.status,
+            "fallback_to_plain": vi.learnedFallback,
+            "initial_rel_residual": vi.initialRelResidual,
             "true_rel_residual_fp64": vi.relResidual}
     ctx.pressure_set_cnn(None)
+    ctx.pressure_set_correction_cnn(None)
     net.close()
+    corr.close()
     return out
 
 

@@ -81,6 +81,22 @@ int msbg_gpu_pressure_learned_guess(msbg_gpu_ctx* ctx, float* packed, int64_t n)
 int msbg_gpu_pressure_training_pairs(msbg_gpu_ctx* ctx, float* feat, float* target,
                                      float* mask, int maxPairs, int* nPairs);
 
+/* Attaches (or with NULL detaches) the network used as the per-V-cycle
+ * correction of solves with (msbg_gpu_solve_params.learned & 2): from the
+ * residual r' the V-cycle leaves it estimates the remaining error c, and the
+ * preconditioner returns V r + omega c with the energy-optimal
+ * omega = (c.r')/(c.Ac). */
+int msbg_gpu_pressure_set_correction_cnn(msbg_gpu_ctx* ctx, msbg_cnn* net);
+
+/* Training pairs of the correction network, from the last refined solve of
+ * ctx: after pcgIters iterations of plain MGPCG from zero (V-cycle of p),
+ * y = x_k + V(b - A x_k); features of r' = b - A y, target the normalised
+ * error x* - y (x* = the refined solution, kept), liquid mask.  Same layouts
+ * and tile choice as msbg_gpu_pressure_training_pairs. */
+int msbg_gpu_pressure_correction_pairs(msbg_gpu_ctx* ctx, const msbg_gpu_solve_params* p,
+                                       int pcgIters, float* feat, float* target, float* mask,
+                                       int maxPairs, int* nPairs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -194,9 +194,13 @@ typedef struct {
                        (always on for them; 0 = 30). */
   int useGraph;     /* capture one PCG iteration in a CUDA graph */
   float coarseScale; /* coarse-grid correction factor (default 1.8; 1 = plain) */
-  int learned;      /* 0: none; 1: the network attached by
-                       msbg_gpu_pressure_set_cnn predicts the initial guess
-                       (forces the FP64 refinement, maxRefine 0 = 30) */
+  int learned;      /* bit 0: the network attached by msbg_gpu_pressure_set_cnn
+                       predicts the initial guess (scaled by the
+                       energy-optimal factor); bit 1: the network attached
+                       by msbg_gpu_pressure_set_correction_cnn corrects every
+                       V-cycle, under flexible CG (FP32 vectors only).  Any
+                       bit forces the FP64 path (maxRefine 0 = 30); a learned
+                       solve that ends unconverged is redone by plain MGPCG. */
 } msbg_gpu_solve_params;
 
 typedef struct {
@@ -213,6 +217,9 @@ typedef struct {
   int64_t kernelLaunches; /* kernels launched inside the timed solve */
   double initialRelResidual; /* |b - A x0| / |b| of the starting iterate
                                 (1 without a learned guess) */
+  int learnedFallback;       /* 1: the learned solve stopped unconverged and
+                                plain MGPCG solved again from zero (iterations,
+                                refinements, time and launches count both) */
 } msbg_gpu_solve_info;
 
 void msbg_gpu_solve_params_default(msbg_gpu_solve_params* p);

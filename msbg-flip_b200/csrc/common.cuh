@@ -63,7 +63,8 @@ struct msbg_cnn;
 
 struct msbg_gpu_ctx {
   int device = 0;
-  msbg_cnn* cnn = nullptr;  // learned network for the pressure solves (not owned)
+  msbg_cnn* cnn = nullptr;      // learned initial guess of the pressure solves (not owned)
+  msbg_cnn* cnnCorr = nullptr;  // learned per-V-cycle correction (not owned)
   cudaStream_t stream = nullptr;
   int sx = 0, sy = 0, sz = 0, bsx0 = 0, nLevels = 1;
   int nbx = 0, nby = 0, nbz = 0;

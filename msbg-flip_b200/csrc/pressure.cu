@@ -50,12 +50,15 @@ struct Solver {
   DeviceBuffer rhs0, d0, q0, z0, r0, partial, scal;
   DeviceBuffer x64, rin;  // FP64 solution and inner right-hand side of the refinement
   DeviceBuffer rinv;      // the inner right-hand side scaled and stored in 16 bits
+  DeviceBuffer tq;        // A z of the learned two-stage preconditioner
   int maxPartial = 0;
   Scalars* hScal = nullptr;  // pinned
   int bsx0 = 0, nbx = 0, nby = 0, nbz = 0;
   std::vector<int> blockLevel;
-  // learned network (not owned) and its level-0 16^3 tiles
+  // learned networks (not owned: initial guess, per-V-cycle correction) and
+  // the level-0 16^3 tiles they run on
   msbg_cnn* net = nullptr;
+  msbg_cnn* netCorr = nullptr;
   int nCnnTiles = 0;
   float levelNorm = 0.f;
   DeviceBuffer cnnTiles, cnnLevel;          // [nCnnTiles] tile id, resolution level
@@ -678,8 +681,8 @@ int solve_plain(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gpu_s
 // Learned prediction from a level-0 FP32 vector `val` (right-hand side or
 // residual) into out (all level-0 cells; cells of tiles the network does not
 // cover stay 0), in chunks of up to 4096 tiles.
-int learned_predict(msbg_gpu_ctx* ctx, Solver& S, cudaStream_t st, const float* val, float* out,
-                    int64_t& launches) {
+int learned_predict(msbg_gpu_ctx* ctx, Solver& S, msbg_cnn* net, cudaStream_t st, const float* val,
+                    float* out, int64_t& launches, bool inGraph = false) {
   const int64_t n = S.H.levels[0].nCells;
   MSBG_CUDA_TRY(ctx, cudaMemsetAsync(out, 0, sizeof(float) * n, st));
   if (!S.nCnnTiles) return MSBG_OK;
@@ -700,14 +703,41 @@ int learned_predict(msbg_gpu_ctx* ctx, Solver& S, cudaStream_t st, const float* 
         S.views[0], S.dev[0]->ctype.as<uint8_t>(), S.cnnTiles.as<int>() + c0,
         S.cnnLevel.as<int>() + c0, S.levelNorm, val, nullptr, S.cFeat.as<float>(),
         S.cScale.as<float>(), S.cOff.as<int64_t>(), nullptr, nullptr);
-    if (cnn::forward(S.net, S.cFeat.as<float>(), out, S.cOff.as<int64_t>(), S.cScale.as<float>(),
+    if (cnn::forward(net, S.cFeat.as<float>(), out, S.cOff.as<int64_t>(), S.cScale.as<float>(),
                      cnt, st, S.cX0.as<uint4>(), S.cS1.as<uint4>(), S.cS2.as<uint4>()))
       return set_error(ctx, MSBG_ERROR, "learned network launch failed");
     launches += 6;
   }
+  if (inGraph) return MSBG_OK;  // no host sync inside a capture; checked after the solve
   MSBG_CUDA_TRY(ctx, cudaGetLastError());
-  const int e = cnn::take_error(S.net, st);
+  const int e = cnn::take_error(net, st);
   if (e) return set_error(ctx, e, "learned network: a tensor-core wait gave up");
+  return MSBG_OK;
+}
+
+// x64 = omega g: the guess g the network predicts from b, scaled by the
+// energy-optimal omega = (g.b)/(g.Ag), so that |x* - x64|_A <= |x*|_A
+// whatever the network returns.  Leaves r32 = b - A g.
+template <typename VT>
+int learned_start(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const float* b, float* r32) {
+  cudaStream_t st = R.st;
+  const int64_t n = S.H.levels[0].nCells;
+  float* g = S.guess.as<float>();
+  double* part = S.partial.as<double>();
+  Scalars* sc = S.scal.as<Scalars>();
+  int rc = learned_predict(ctx, S, S.net, st, b, g, R.launches);
+  if (rc) return rc;
+  k_mask<<<VEC_GRID, VEC_BLOCK, 0, st>>>(g, S.views[0].diag, n);
+  k_set64_masked<<<VEC_GRID, VEC_BLOCK, 0, st>>>(S.x64.as<double>(), g, S.views[0].diag, n);
+  double rr = 0;
+  rc = residual64(ctx, S, R, b, r32, &rr);
+  if (rc) return rc;
+  k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(g, b, n, part);
+  k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_CR);
+  k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(g, (const float*)r32, n, part);
+  k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_OMEGA_GUESS);
+  k_scale64<<<VEC_GRID, VEC_BLOCK, 0, st>>>(S.x64.as<double>(), sc, n);
+  R.launches += 7;
   return MSBG_OK;
 }
 
@@ -741,12 +771,10 @@ int solve_refined(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const msbg_gpu_so
   VT* e = S.dev[0]->x.as<VT>();
   const float* b = S.rhs0.as<float>();
   int rc = MSBG_OK;
-  if (p->learned >= 1) {
+  if (p->learned & 1) {
     // initial guess predicted by the network from the right-hand side
-    rc = learned_predict(ctx, S, st, b, S.guess.as<float>(), R.launches);
+    rc = learned_start(ctx, S, R, b, rin);
     if (rc) return rc;
-    k_set64_masked<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, S.guess.as<float>(), S.views[0].diag, n);
-    R.launches++;
   } else {
     cudaMemsetAsync(x64, 0, sizeof(double) * n, st);
   }
@@ -757,7 +785,7 @@ int solve_refined(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const msbg_gpu_so
     if (outer == 0) {
       // |b|^2 (the guess, when there is one, is not part of the reference norm)
       bb = rr;
-      if (p->learned >= 1) {
+      if (p->learned & 1) {
         double* part = S.partial.as<double>();
         Scalars* sc = S.scal.as<Scalars>();
         k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(b, b, n, part);
@@ -858,11 +886,9 @@ int solve_reliable(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gp
   Scalars* sc = S.scal.as<Scalars>();
   const float* b = S.rhs0.as<float>();
   int rc = MSBG_OK;
-  if (p->learned >= 1) {
-    rc = learned_predict(ctx, S, st, b, S.guess.as<float>(), R.launches);
+  if (p->learned & 1) {
+    rc = learned_start(ctx, S, R, b, r);
     if (rc) return rc;
-    k_set64_masked<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, S.guess.as<float>(), S.views[0].diag, n);
-    R.launches++;
   } else {
     cudaMemsetAsync(x64, 0, sizeof(double) * n, st);
   }
@@ -873,8 +899,35 @@ int solve_reliable(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gp
   cudaMemsetAsync(sc, 0, sizeof(Scalars), st);
   k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(b, b, n, part);
   k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_BB);
-  // z = V r, rho = r.z, d = z
-  R.vcycle(0, z, (const float*)r);
+  // learned & 2: the preconditioner is the V-cycle followed by the
+  // correction network's estimate c of the error the V-cycle leaves,
+  // z = V r + omega c, c = N(r'), r' = r - A V r, omega = (c.r')/(c.Ac) (the
+  // energy-optimal multiple, 0 for a useless c).  It is not linear, so the
+  // iteration is flexible CG (Notay 2000, FCG(1)): alpha = (d.r)/(d.q),
+  // beta = -(z.q)/(d.q).
+  const bool corr = (p->learned & 2) != 0;
+  float* tq = corr ? S.tq.as<float>() : nullptr;
+  float* rt = corr ? S.rin.as<float>() : nullptr;
+  float* ec = corr ? S.guess.as<float>() : nullptr;
+  auto precond = [&](bool inGraph) -> int {
+    R.vcycle(0, z, (const float*)r);
+    if (!corr) return MSBG_OK;
+    R.matvec_dot(z, tq, part);
+    k_sub<<<VEC_GRID, VEC_BLOCK, 0, st>>>(rt, r, tq, n);
+    int e = learned_predict(ctx, S, S.netCorr, st, rt, ec, R.launches, inGraph);
+    if (e) return e;
+    k_mask<<<VEC_GRID, VEC_BLOCK, 0, st>>>(ec, S.views[0].diag, n);
+    const int nt = R.matvec_dot((const float*)ec, tq, part);
+    k_finalize<<<1, 1024, 0, st>>>(part, nt, sc, FIN_CC);
+    k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>((const float*)ec, (const float*)rt, n, part);
+    k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_OMEGA_CORR);
+    k_add_omega<<<VEC_GRID, VEC_BLOCK, 0, st>>>(z, ec, sc, n);
+    R.launches += 6;
+    return MSBG_OK;
+  };
+  // z = B r, rho = r.z, d = z
+  rc = precond(false);
+  if (rc) return rc;
   k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
   k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHO);
   cudaMemcpyAsync(d, z, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
@@ -895,17 +948,29 @@ int solve_reliable(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gp
   auto part1 = [&]() {
     R.launches += 3;
     const int nt = R.matvec_dot(d, q, part);
-    k_finalize<<<1, 1024, 0, st>>>(part, nt, sc, FIN_DQ_ALPHA);
+    k_finalize<<<1, 1024, 0, st>>>(part, nt, sc, corr ? FIN_FCG_DQ_ALPHA : FIN_DQ_ALPHA);
     k_axpy64_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, r, d, q, n, sc, part);
     k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
     cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
   };
+  int precondRc = MSBG_OK;
   auto part2 = [&]() {
     R.launches += 3;
-    R.vcycle(0, z, (const float*)r);
-    k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
-    k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHONEW_BETA);
-    k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, n, sc);
+    const int e = precond(true);
+    if (e) precondRc = e;
+    if (!corr) {
+      k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
+      k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHONEW_BETA);
+      k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, n, sc);
+    } else {
+      // beta = -(z.q)/(d.q); d = z + beta d; rho = d.r for the next alpha
+      k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(z, q, n, part);
+      k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_FCG_BETA);
+      k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, n, sc);
+      k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, r, n, part);
+      k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHO);
+      R.launches += 3;
+    }
   };
   cudaGraphExec_t g1 = nullptr, g2 = nullptr;
   int64_t per1 = 0, per2 = 0;
@@ -982,6 +1047,11 @@ int solve_reliable(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gp
   }
   if (g1) cudaGraphExecDestroy(g1);
   if (g2) cudaGraphExecDestroy(g2);
+  if (!rc && precondRc) rc = precondRc;
+  if (!rc && corr) {
+    const int e = cnn::take_error(S.netCorr, st);
+    if (e) rc = set_error(ctx, e, "learned network: a tensor-core wait gave up");
+  }
   if (rc) return rc;
   k_narrow<<<VEC_GRID, VEC_BLOCK, 0, st>>>(S.dev[0]->x.as<float>(), x64, n);
   R.launches++;
@@ -1006,6 +1076,7 @@ int solve_typed(msbg_gpu_ctx* ctx, Solver& S, const msbg_gpu_solve_params* p, cu
     MSBG_CUDA_TRY(ctx, S.rin.ensure(sizeof(float) * n));
     if (!WIDE) MSBG_CUDA_TRY(ctx, S.rinv.ensure(sizeof(VT) * n));
     if (p->learned) MSBG_CUDA_TRY(ctx, S.guess.ensure(sizeof(float) * n));
+    if (p->learned & 2) MSBG_CUDA_TRY(ctx, S.tq.ensure(sizeof(float) * n));
   }
   cudaGraphExec_t exec = nullptr;
   int64_t perIter = 0;
@@ -1039,31 +1110,62 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
     return set_error(ctx, MSBG_EINVARG, "invalid solve parameters");
   if (p->storage != MSBG_F32 && p->storage != MSBG_F16 && p->storage != MSBG_BF16)
     return set_error(ctx, MSBG_ENOTIMPL, "storage type %d not available", p->storage);
-  if (p->learned < 0 || p->learned > 1)
-    return set_error(ctx, MSBG_EINVARG, "learned = %d (0 none, 1 initial guess)", p->learned);
-  if (p->learned && !ctx->cnn)
-    return set_error(ctx, MSBG_EINVARG, "learned solve without a network (msbg_gpu_pressure_set_cnn)");
+  if (p->learned < 0 || p->learned > 3)
+    return set_error(ctx, MSBG_EINVARG, "learned = %d (bit 0 guess, bit 1 correction)", p->learned);
+  if ((p->learned & 2) && p->storage != MSBG_F32)
+    return set_error(ctx, MSBG_ENOTIMPL, "the learned correction runs with FP32 vectors");
+  if ((p->learned & 1) && !ctx->cnn)
+    return set_error(ctx, MSBG_EINVARG, "learned guess without a network (msbg_gpu_pressure_set_cnn)");
+  if ((p->learned & 2) && !ctx->cnnCorr)
+    return set_error(ctx, MSBG_EINVARG,
+                     "learned correction without a network (msbg_gpu_pressure_set_correction_cnn)");
   cudaSetDevice(ctx->device);
   Solver& S = *sp;
   S.net = ctx->cnn;
+  S.netCorr = ctx->cnnCorr;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  auto run = [&](const msbg_gpu_solve_params* q, SolveOut& o, int64_t* launches, float* ms) -> int {
+    int rc;
+    switch (q->storage) {
+      case MSBG_F16: rc = solve_typed<__half>(ctx, S, q, e0, e1, o, launches); break;
+      case MSBG_BF16: rc = solve_typed<__nv_bfloat16>(ctx, S, q, e0, e1, o, launches); break;
+      default: rc = solve_typed<float>(ctx, S, q, e0, e1, o, launches); break;
+    }
+    const cudaError_t se = cudaStreamSynchronize(ctx->stream);
+    *ms = 0;
+    if (rc == MSBG_OK && se == cudaSuccess) cudaEventElapsedTime(ms, e0, e1);
+    if (rc) return rc;
+    MSBG_CUDA_TRY(ctx, se);
+    return MSBG_OK;
+  };
   SolveOut o;
   int64_t launches = 0;
-  int rc;
-  switch (p->storage) {
-    case MSBG_F16: rc = solve_typed<__half>(ctx, S, p, e0, e1, o, &launches); break;
-    case MSBG_BF16: rc = solve_typed<__nv_bfloat16>(ctx, S, p, e0, e1, o, &launches); break;
-    default: rc = solve_typed<float>(ctx, S, p, e0, e1, o, &launches); break;
-  }
-  const cudaError_t se = cudaStreamSynchronize(ctx->stream);
   float ms = 0;
-  if (rc == MSBG_OK && se == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+  int rc = run(p, o, &launches, &ms);
+  int fellBack = 0;
+  if (rc == MSBG_OK && p->learned && o.status != 0) {
+    // plain MGPCG is the fallback of the learned solve: the same storage and
+    // FP64 refinement from a zero guess; the time and work of both count
+    msbg_gpu_solve_params q = *p;
+    q.learned = 0;
+    if (q.storage == MSBG_F32 && q.maxRefine == 0) q.maxRefine = 30;
+    SolveOut o2;
+    int64_t l2 = 0;
+    float ms2 = 0;
+    rc = run(&q, o2, &l2, &ms2);
+    o2.iters += o.iters;
+    o2.refinements += o.refinements;
+    o2.initialRelres = o.initialRelres;
+    o = o2;
+    launches += l2;
+    ms += ms2;
+    fellBack = 1;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
-  MSBG_CUDA_TRY(ctx, se);
   if (info) {
     const Level& L0 = S.H.levels[0];
     info->iterations = o.iters;
@@ -1075,6 +1177,7 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
     info->nMgLevels = (int)S.H.levels.size();
     info->kernelLaunches = launches;
     info->initialRelResidual = o.initialRelres;
+    info->learnedFallback = fellBack;
   }
   return MSBG_OK;
 }
@@ -1084,6 +1187,27 @@ extern "C" int msbg_gpu_pressure_set_cnn(msbg_gpu_ctx* ctx, msbg_cnn* net) {
   ctx->cnn = net;
   return MSBG_OK;
 }
+
+extern "C" int msbg_gpu_pressure_set_correction_cnn(msbg_gpu_ctx* ctx, msbg_cnn* net) {
+  if (!ctx) return MSBG_EINVARG;
+  ctx->cnnCorr = net;
+  return MSBG_OK;
+}
+
+namespace {
+// np training tiles spread evenly over the network's tile list, uploaded to
+// S.cIdx as [tile ids | levels].
+int select_pair_tiles(msbg_gpu_ctx* ctx, Solver& S, int np, cudaStream_t st) {
+  std::vector<int> sel(2 * (size_t)np);
+  for (int i = 0; i < np; i++) {
+    const int k = (int)((int64_t)i * S.nCnnTiles / np);
+    sel[i] = S.cnnTilesHost[k];
+    sel[np + i] = S.cnnLevelHost[k];
+  }
+  MSBG_CUDA_TRY(ctx, upload(S.cIdx, sel, st));
+  return MSBG_OK;
+}
+}  // namespace
 
 extern "C" int msbg_gpu_pressure_training_pairs(msbg_gpu_ctx* ctx, float* feat, float* target,
                                                 float* mask, int maxPairs, int* nPairs) {
@@ -1098,14 +1222,9 @@ extern "C" int msbg_gpu_pressure_training_pairs(msbg_gpu_ctx* ctx, float* feat, 
   const int np = std::min(maxPairs, S.nCnnTiles);
   *nPairs = np;
   if (np == 0) return MSBG_OK;
-  std::vector<int> sel(2 * (size_t)np);
-  for (int i = 0; i < np; i++) {
-    const int k = (int)((int64_t)i * S.nCnnTiles / np);
-    sel[i] = S.cnnTilesHost[k];
-    sel[np + i] = S.cnnLevelHost[k];
-  }
+  int rc = select_pair_tiles(ctx, S, np, st);
+  if (rc) return rc;
   DeviceBuffer scale, off;
-  MSBG_CUDA_TRY(ctx, upload(S.cIdx, sel, st));
   MSBG_CUDA_TRY(ctx, scale.ensure(sizeof(float) * np));
   MSBG_CUDA_TRY(ctx, off.ensure(sizeof(int64_t) * np));
   k_cnn_features<<<np, FEAT_THREADS, 0, st>>>(
@@ -1114,6 +1233,87 @@ extern "C" int msbg_gpu_pressure_training_pairs(msbg_gpu_ctx* ctx, float* feat, 
       off.as<int64_t>(), target, mask);
   MSBG_CUDA_TRY(ctx, cudaGetLastError());
   MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return MSBG_OK;
+}
+
+// Training pairs of the correction network: the state a PCG iteration hands
+// to the correction stage.  After pcgIters iterations of plain MGPCG (FP32
+// vectors, FP64 iterate x_k) from zero, y = x_k + V(b - A x_k); the input is
+// the residual r' = b - A y and the target the error x* - y, x* being the
+// refined solution of the last solve (which is restored afterwards).
+extern "C" int msbg_gpu_pressure_correction_pairs(msbg_gpu_ctx* ctx,
+                                                  const msbg_gpu_solve_params* p, int pcgIters,
+                                                  float* feat, float* target, float* mask,
+                                                  int maxPairs, int* nPairs) {
+  if (!ctx || !p || !feat || !target || !mask || maxPairs <= 0 || !nPairs || pcgIters < 0)
+    return MSBG_EINVARG;
+  auto& sp = solver_of(ctx);
+  if (!sp) return set_error(ctx, MSBG_EINVARG, "msbg_gpu_pressure_prepare not called");
+  Solver& S = *sp;
+  if (!S.haveX64)
+    return set_error(ctx, MSBG_EINVARG, "training pairs need a refined solve (maxRefine > 0) first");
+  if (p->nPre < 0 || p->nPost < 0 || p->innerIter < 1)
+    return set_error(ctx, MSBG_EINVARG, "invalid V-cycle parameters");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const int np = std::min(maxPairs, S.nCnnTiles);
+  *nPairs = np;
+  if (np == 0) return MSBG_OK;
+  const int64_t n = S.H.levels[0].nCells;
+  double* x64 = S.x64.as<double>();
+  DeviceBuffer xs, err, scale, off;
+  MSBG_CUDA_TRY(ctx, xs.ensure(sizeof(double) * n));
+  MSBG_CUDA_TRY(ctx, err.ensure(sizeof(double) * n));
+  MSBG_CUDA_TRY(ctx, scale.ensure(sizeof(float) * np));
+  MSBG_CUDA_TRY(ctx, off.ensure(sizeof(int64_t) * np));
+  MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(xs.p, x64, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  int rc = MSBG_OK;
+  if (pcgIters > 0) {
+    msbg_gpu_solve_params q = *p;
+    q.storage = MSBG_F32;
+    q.learned = 0;
+    q.tol = 0;
+    q.maxIter = pcgIters;
+    q.maxRefine = 1 << 20;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    SolveOut o;
+    int64_t launches = 0;
+    rc = solve_typed<float>(ctx, S, &q, e0, e1, o, &launches);
+    cudaStreamSynchronize(st);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+  } else {
+    MSBG_CUDA_TRY(ctx, cudaMemsetAsync(x64, 0, sizeof(double) * n, st));
+  }
+  Runner<float> R{S, st, p->nPre, p->nPost, p->innerIter};
+  R.coarseScale = p->coarseScale > 0 ? p->coarseScale : 1.0f;
+  R.err = ctx->errBuf.as<int>();
+  R.numSMs = S.numSMs;
+  const float* b = S.rhs0.as<float>();
+  float* r = S.r0.as<float>();
+  float* z = S.z0.as<float>();
+  double rr = 0;
+  rc = residual64(ctx, S, R, b, r, &rr);
+  if (rc) return rc;
+  R.vcycle(0, z, (const float*)r);
+  k_add64<float><<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, z, n, 1.0);
+  rc = residual64(ctx, S, R, b, r, &rr);
+  if (rc) return rc;
+  k_sub64<<<VEC_GRID, VEC_BLOCK, 0, st>>>(err.as<double>(), xs.as<double>(), x64, n);
+  rc = select_pair_tiles(ctx, S, np, st);
+  if (rc) return rc;
+  k_cnn_features<<<np, FEAT_THREADS, 0, st>>>(
+      S.views[0], S.dev[0]->ctype.as<uint8_t>(), S.cIdx.as<int>(), S.cIdx.as<int>() + np,
+      S.levelNorm, r, err.as<double>(), feat, scale.as<float>(), off.as<int64_t>(), target, mask);
+  MSBG_CUDA_TRY(ctx, cudaGetLastError());
+  // restore the refined solution
+  MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(x64, xs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  k_narrow<<<VEC_GRID, VEC_BLOCK, 0, st>>>(S.dev[0]->x.as<float>(), x64, n);
+  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  S.haveX64 = true;
   return MSBG_OK;
 }
 
@@ -1332,7 +1532,7 @@ extern "C" int msbg_gpu_pressure_learned_guess(msbg_gpu_ctx* ctx, float* packed,
   const int64_t nc = S.H.levels[0].nCells;
   MSBG_CUDA_TRY(ctx, S.guess.ensure(sizeof(float) * nc));
   int64_t launches = 0;
-  int rc = learned_predict(ctx, S, st, S.rhs0.as<float>(), S.guess.as<float>(), launches);
+  int rc = learned_predict(ctx, S, S.net, st, S.rhs0.as<float>(), S.guess.as<float>(), launches);
   if (rc) return rc;
   DeviceBuffer tmp;
   MSBG_CUDA_TRY(ctx, tmp.ensure(sizeof(double) * nc));

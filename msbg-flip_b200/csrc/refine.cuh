@@ -129,3 +129,49 @@ __global__ void __launch_bounds__(VEC_BLOCK) k_axpy64_norm(double* __restrict__ 
   acc = block_sum(acc);
   if (threadIdx.x == 0) partial[blockIdx.x] = acc;
 }
+
+// y = a - b (all cells)
+__global__ void __launch_bounds__(VEC_BLOCK) k_sub(float* __restrict__ y, const float* __restrict__ a,
+                                                   const float* __restrict__ b, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n >> 2);
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float4 u = reinterpret_cast<const float4*>(a)[i], v = reinterpret_cast<const float4*>(b)[i];
+    reinterpret_cast<float4*>(y)[i] = make_float4(u.x - v.x, u.y - v.y, u.z - v.z, u.w - v.w);
+  }
+}
+
+// v = 0 outside the liquid cells
+__global__ void __launch_bounds__(VEC_BLOCK) k_mask(float* __restrict__ v,
+                                                    const float* __restrict__ diag, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (!(diag[i] > 0.f)) v[i] = 0.f;
+}
+
+// z += omega c
+__global__ void __launch_bounds__(VEC_BLOCK) k_add_omega(float* __restrict__ z,
+                                                         const float* __restrict__ c,
+                                                         const Scalars* __restrict__ s, int64_t n) {
+  const float w = (float)s->omega;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    z[i] = fmaf(w, c[i], z[i]);
+}
+
+// x *= omega (FP64)
+__global__ void __launch_bounds__(VEC_BLOCK) k_scale64(double* __restrict__ x,
+                                                       const Scalars* __restrict__ s, int64_t n) {
+  const double w = s->omega;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] *= w;
+}
+
+// e = a - b (FP64)
+__global__ void __launch_bounds__(VEC_BLOCK) k_sub64(double* __restrict__ e,
+                                                     const double* __restrict__ a,
+                                                     const double* __restrict__ b, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    e[i] = a[i] - b[i];
+}

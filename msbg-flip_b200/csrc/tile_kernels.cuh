@@ -28,11 +28,24 @@ __device__ __forceinline__ double block_sum(double v) {
 
 struct Scalars {
   double bb, rho, rhoNew, dq, rr, alpha, beta, amax;
+  double cc, cr, omega;  // energy-optimal scaling of a learned vector c
   int status;  // 0 ok, 2 breakdown, 3 non-finite
   int pad;
 };
 
-enum { FIN_BB = 0, FIN_DQ_ALPHA = 1, FIN_RR = 2, FIN_RHO = 3, FIN_RHONEW_BETA = 4 };
+enum {
+  FIN_BB = 0,
+  FIN_DQ_ALPHA = 1,
+  FIN_RR = 2,
+  FIN_RHO = 3,
+  FIN_RHONEW_BETA = 4,
+  FIN_FCG_BETA = 5,      // flexible CG: beta = -(z.q)/(d.q)
+  FIN_FCG_DQ_ALPHA = 6,  // flexible CG: alpha = (d.r)/(d.q), d.r of either sign
+  FIN_CC = 7,            // c.Ac
+  FIN_CR = 8,            // c.r
+  FIN_OMEGA_CORR = 9,    // omega = (c.r)/(c.Ac): v = c.r
+  FIN_OMEGA_GUESS = 10,  // omega = (g.b)/(g.b - g.r), r = b - A g: v = g.r
+};
 
 // Deterministic second stage: fixed-order sum of the CTA partials, then the
 // scalar step of PCG that depends on it.
@@ -63,6 +76,31 @@ __global__ void __launch_bounds__(1024) k_finalize(const double* __restrict__ pa
         s->beta = v / s->rho;
         s->rho = v;
       }
+      break;
+    case FIN_FCG_BETA:  // q = A d of the last step
+      if (!isfinite(v)) s->status = 3;
+      else s->beta = -v / s->dq;
+      break;
+    case FIN_CC: s->cc = v; break;
+    case FIN_CR: s->cr = v; break;
+    // The scaled vector omega*c minimises |e - omega c|_A for A e = r: it
+    // never leaves a larger energy error than c = 0 does.  A degenerate c
+    // gets omega = 0.
+    case FIN_OMEGA_CORR:
+      s->omega = (isfinite(v) && isfinite(s->cc) && s->cc > 1e-300) ? v / s->cc : 0.0;
+      break;
+    case FIN_OMEGA_GUESS: {
+      const double gag = s->cr - v;  // g.Ag = g.b - g.(b - Ag)
+      s->omega = (isfinite(v) && isfinite(s->cr) && gag > 1e-300) ? s->cr / gag : 0.0;
+      break;
+    }
+    case FIN_FCG_DQ_ALPHA:
+      // a non-linear preconditioner need not make d.r positive; the step
+      // along d still minimises the energy norm as long as d.q > 0
+      s->dq = v;
+      if (!isfinite(v) || !isfinite(s->rho)) s->status = 3;
+      else if (!(v > 1e-300)) s->status = 2;
+      else s->alpha = s->rho / v;
       break;
   }
 }

@@ -214,7 +214,8 @@ class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("status", C.c_int),
                 ("relResidual", C.c_double), ("solveSeconds", C.c_double),
                 ("fineCells", C.c_int64), ("nMgLevels", C.c_int),
-                ("kernelLaunches", C.c_int64), ("initialRelResidual", C.c_double)]
+                ("kernelLaunches", C.c_int64), ("initialRelResidual", C.c_double),
+                ("learnedFallback", C.c_int)]
 
 
 class PressureStats(C.Structure):
@@ -365,4 +366,4 @@ Context.pressure_profile = _ctx_pressure_profile
 Context.last_solve_launches = lambda self: getattr(self, "_last_launches", None)
 
 
-from .learned import Cnn, collect_training_pairs, train_cnn  # noqa: E402,F401
+from .learned import Cnn, collect_correction_pairs, collect_training_pairs, train_cnn  # noqa: E402,F401

@@ -31,6 +31,9 @@ def _sigs(L):
         "msbg_gpu_pressure_set_cnn": (i32, [vp, vp]),
         "msbg_gpu_pressure_training_pairs": (i32, [vp, vp, vp, vp, i32, C.POINTER(C.c_int)]),
         "msbg_gpu_pressure_learned_guess": (i32, [vp, C.POINTER(C.c_float), C.c_int64]),
+        "msbg_gpu_pressure_set_correction_cnn": (i32, [vp, vp]),
+        "msbg_gpu_pressure_correction_pairs": (i32, [vp, vp, i32, vp, vp, vp, i32,
+                                                     C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -119,6 +122,27 @@ def collect_training_pairs(ctx, max_pairs):
     return feat[:n].contiguous(), target[:n].contiguous(), mask[:n].contiguous()
 
 
+def collect_correction_pairs(ctx, max_pairs, pcg_iters, params=None, **kw):
+    """Pairs of the correction network (see msbg_gpu_pressure_correction_pairs):
+    the residual the V-cycle leaves after `pcg_iters` PCG iterations and the
+    error it leaves, from the last refined solve of ctx."""
+    import torch
+    from . import solve_params
+    L = lib()
+    _sigs(L)
+    p = params or solve_params(**kw)
+    dev = torch.device("cuda", ctx.device)
+    feat = torch.zeros((max_pairs, NFEAT * NPAD), dtype=torch.float32, device=dev)
+    target = torch.zeros((max_pairs, NCELL), dtype=torch.float32, device=dev)
+    mask = torch.zeros((max_pairs, NCELL), dtype=torch.float32, device=dev)
+    n = C.c_int()
+    ctx._check(L.msbg_gpu_pressure_correction_pairs(ctx._h, C.byref(p), pcg_iters, _ptr(feat),
+                                                    _ptr(target), _ptr(mask), max_pairs,
+                                                    C.byref(n)), "correction_pairs")
+    n = n.value
+    return feat[:n].contiguous(), target[:n].contiguous(), mask[:n].contiguous()
+
+
 def train_cnn(net, feat, target, mask, epochs=40, batch=128, lr=2e-3, seed=0, log=None):
     """Adam on mini-batches of tiles (fixed seed); returns the loss per epoch.
 
@@ -154,6 +178,14 @@ def _ctx_set_cnn(self, net):
     self._cnn = net  # keep it alive while attached
 
 
+def _ctx_set_correction_cnn(self, net):
+    L = lib()
+    _sigs(L)
+    self._check(L.msbg_gpu_pressure_set_correction_cnn(self._h, net._h if net is not None else None),
+                "set_correction_cnn")
+    self._cnn_corr = net
+
+
 def _ctx_learned_guess(self):
     """The attached network's pressure prediction (packed layout, FP32)."""
     L = lib()
@@ -169,6 +201,7 @@ def _ctx_learned_guess(self):
 def _install():
     from . import Context
     Context.pressure_set_cnn = _ctx_set_cnn
+    Context.pressure_set_correction_cnn = _ctx_set_correction_cnn
     Context.pressure_learned_guess = _ctx_learned_guess
 
 
