@@ -81,7 +81,7 @@ void set_kernel_attrs() {
   cudaFuncSetAttribute(k_smooth<8, VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)smooth_smem<8>());
   cudaFuncSetAttribute(k_smooth_pipe16<VT, pipe::NT_SMOOTH>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, pipeSmem);
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe::SMEM_SMOOTH);
   cudaFuncSetAttribute(k_apply_pipe16<APPLY_MATVEC, VT, VT, pipe::NT_APPLY>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, pipeSmem);
   cudaFuncSetAttribute(k_apply_pipe16<APPLY_RESIDUAL, VT, float, pipe::NT_APPLY>,
@@ -129,7 +129,7 @@ struct Runner {
       if (P.ts == 16 && usePipe) {
         const int grid = std::min(P.count, numSMs);
         // passes are contiguous tile-id ranges (register_tiles sorts by pass)
-        k_smooth_pipe16<V, pipe::NT_SMOOTH><<<grid, pipe::NT_SMOOTH, pipe::SMEM, st>>>(
+        k_smooth_pipe16<V, pipe::NT_SMOOTH><<<grid, pipe::NT_SMOOTH, pipe::SMEM_SMOOTH, st>>>(
             S.views[m], P.start, P.count, x, b, inner, post ? 1 : 0, err);
       } else {
         TS_DISPATCH(P.ts, (k_smooth<T, V><<<P.count, T * T, smooth_smem<T>(), st>>>(

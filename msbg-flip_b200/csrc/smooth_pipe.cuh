@@ -6,21 +6,22 @@
 // colour) with a stride of gridDim.x.  Per tile:
 //   * the six contiguous 16 KB arrays (x, b, 1/a_ii, cx, cy, cz) arrive by bulk
 //     asynchronous copies (cp.async.bulk, completion on an mbarrier) into one
-//     of two shared-memory stages, issued one tile ahead;
+//     of two shared-memory stages, issued one tile ahead (x plane by plane
+//     into a padded slot);
 //   * the tile's 256-byte record (its offset and the resolved data of its six
 //     faces) arrives the same way two tiles ahead, so no dependent global load
 //     sits on the critical path;
 //   * the halo values of the next tile are loaded into registers before the
 //     current tile is smoothed and summed afterwards;
-//   * the smoothed x leaves by one bulk store.
-// 512 threads; per colour each thread owns 4 cells whose couplings, 1/a_ii
-// and right-hand side (with the constant halo sums folded in) sit in
-// registers, laid out so a warp's shared-memory accesses hit 32 banks.
+//   * the smoothed x leaves by bulk stores.
+// 1024 threads, each owning a 2 x 2 block of cells (x pair, z pair) whose
+// couplings, 1/a_ii, right-hand side (with the constant halo sums folded in)
+// and x values sit in registers.
 //
 // Vectors may be stored in 16 bits (VT = __half / __nv_bfloat16): x and b
-// then arrive together in stage slot 1 and x is widened into the FP32
-// working slot 0; the smoothed tile is narrowed back into slot 1 for the
-// bulk store.  The operator arrays are always FP32.
+// then arrive together in the b slot and x is widened into the FP32 working
+// slot; the smoothed tile is narrowed back into the b slot for the bulk store.
+// The operator arrays are always FP32.
 
 namespace pipe {
 
@@ -119,8 +120,9 @@ __device__ __forceinline__ void halo_load(const LevelView& L, const VT* __restri
   }
 }
 
-// Where the x and b vectors of a tile land in a stage: FP32 x straight into
-// the working slot 0 and b into slot 1; 16-bit x and b both into slot 1.
+// Where the x and b vectors of a tile land in a stage of the operator
+// kernels: FP32 x straight into the working slot 0 and b into slot 1; 16-bit
+// x and b both into slot 1.
 template <typename VT>
 __device__ __forceinline__ VT* raw_x(float* st) {
   return std::is_same<VT, float>::value ? reinterpret_cast<VT*>(st)
@@ -138,30 +140,63 @@ __device__ __forceinline__ void widen_x(float* st, int tid) {
   for (int e = tid; e < N; e += NTH) st[e] = to_f(xr[e]);
 }
 
+// Shared-memory layout of the smoother: two stages of [x | b | 1/a_ii | cx |
+// cy | cz], x with its z planes XP = 264 floats apart (the 8-float pad per
+// plane makes the z-pair thread map below bank-conflict free), behind a
+// zeroed guard of one padded plane, then the halo sums of both stages.
+constexpr int XP = TS * TS + 8;
+constexpr int XS = TS * XP;
+constexpr int SGUARD = XP;
+constexpr int SSTAGE = XS + 5 * N;
+constexpr int SOFF_B = XS, SOFF_IV = XS + N, SOFF_C = XS + 2 * N;  // cx, cy, cz follow
+constexpr int SZERO_FLOATS = SGUARD + 2 * SSTAGE + 2 * 6 * TS * TS;
+constexpr size_t SMEM_SMOOTH =
+    sizeof(float) * SZERO_FLOATS + 3 * sizeof(TileRec) + 3 * sizeof(uint64_t);
+static_assert((SGUARD * 4) % 16 == 0 && (SSTAGE * 4) % 16 == 0 && (XP * 4) % 16 == 0,
+              "bulk copy destinations stay 16-byte aligned");
+static_assert(SMEM_SMOOTH <= 227 * 1024, "smoother stages fit one SM");
+__host__ __device__ __forceinline__ int xpad(int e) { return e + 8 * (e >> 8); }
+
+// 16-bit x and b of a tile arrive together in the b slot; FP32 b alone.
+template <typename VT>
+__device__ __forceinline__ VT* sraw_x(float* st) {
+  return reinterpret_cast<VT*>(st + SOFF_B);
+}
+template <typename VT>
+__device__ __forceinline__ VT* sraw_b(float* st) {
+  return reinterpret_cast<VT*>(st + SOFF_B) + (std::is_same<VT, float>::value ? 0 : N);
+}
+
 }  // namespace pipe
 
-// NTH threads: each owns KK cells of each colour (NTH = 512: 4, 1024: 2).
+// 1024 threads.  Thread (ip, jj, kp) owns the 2 x 2 cells x = 2ip + {0,1},
+// z = 2kp + {0,1} of row jj: per colour one cell of each z plane, and for
+// each of them the x- and the z-neighbour of the other colour are the
+// thread's own cells, held in registers; 4 of the 6 neighbour values come
+// from shared memory.  The arithmetic per update is that of the reference's
+// order (x-, x+, y-, y+, z-, z+).
 template <typename VT, int NTH>
 __global__ void __launch_bounds__(NTH, 1)
     k_smooth_pipe16(LevelView L, int tileBase, int count, VT* __restrict__ x,
                     const VT* __restrict__ b, int inner, int reverse, int* __restrict__ err) {
   using namespace pipe;
-  constexpr int KK = N / (2 * NTH);           // cells per colour per thread
-  constexpr int KSTRIDE = TS / KK;             // z distance of a thread's cells
+  static_assert(NTH == 1024, "the z-pair thread map covers a 16^3 tile with 1024 threads");
   constexpr int NHALO = 6 * TS * TS;           // halo cells of a tile
   constexpr int HQ = (NHALO + NTH - 1) / NTH;  // halo cells per thread
+  constexpr bool WIDE = std::is_same<VT, float>::value;
   extern __shared__ __align__(128) float sm[];
-  float* stages[2] = {sm + GUARD, sm + GUARD + 6 * N};
-  float(*gsb)[6][TS * TS] = reinterpret_cast<float(*)[6][TS * TS]>(sm + GUARD + 12 * N);
-  TileRec* recs = reinterpret_cast<TileRec*>(sm + ZERO_FLOATS);
+  auto stage = [&](int i) { return sm + SGUARD + i * SSTAGE; };
+  float(*gsb)[6][TS * TS] = reinterpret_cast<float(*)[6][TS * TS]>(sm + SGUARD + 2 * SSTAGE);
+  TileRec* recs = reinterpret_cast<TileRec*>(sm + SZERO_FLOATS);
   uint64_t* bar = reinterpret_cast<uint64_t*>(recs + 3);  // [0],[1] stages, [2] prologue
   const TileRec* grec = reinterpret_cast<const TileRec*>(L.tileRec) + tileBase;
   const int tid = threadIdx.x;
   const int G = gridDim.x;
   int t = blockIdx.x;
   if (t >= count) return;
-  // every float of shared memory holds 0 or a value of our (finite) arrays
-  for (int q = tid; q < ZERO_FLOATS / 4; q += NTH)
+  // every float of shared memory holds 0, a value of our (finite) arrays or
+  // two finite 16-bit values (never a float NaN/Inf pattern)
+  for (int q = tid; q < SZERO_FLOATS / 4; q += NTH)
     reinterpret_cast<float4*>(sm)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -175,12 +210,19 @@ __global__ void __launch_bounds__(NTH, 1)
     const bool rec = tRec < count;
     mbar_expect_tx(br, 2 * N * sizeof(VT) + 4 * N * sizeof(float) + (rec ? sizeof(TileRec) : 0));
     const int64_t off = r.off;
-    bulk_g2s(raw_x<VT>(st), x + off, N * sizeof(VT), br);
-    bulk_g2s(raw_b<VT>(st), b + off, N * sizeof(VT), br);
-    bulk_g2s(st + 2 * N, L.invdiag + off, N * sizeof(float), br);
-    bulk_g2s(st + 3 * N, L.cx + off, N * sizeof(float), br);
-    bulk_g2s(st + 4 * N, L.cy + off, N * sizeof(float), br);
-    bulk_g2s(st + 5 * N, L.cz + off, N * sizeof(float), br);
+    if (WIDE) {
+      // x plane by plane into the padded working slot
+#pragma unroll 1
+      for (int k = 0; k < TS; k++)
+        bulk_g2s(st + k * XP, x + off + k * TS * TS, TS * TS * sizeof(VT), br);
+    } else {
+      bulk_g2s(sraw_x<VT>(st), x + off, N * sizeof(VT), br);
+    }
+    bulk_g2s(sraw_b<VT>(st), b + off, N * sizeof(VT), br);
+    bulk_g2s(st + SOFF_IV, L.invdiag + off, N * sizeof(float), br);
+    bulk_g2s(st + SOFF_C, L.cx + off, N * sizeof(float), br);
+    bulk_g2s(st + SOFF_C + N, L.cy + off, N * sizeof(float), br);
+    bulk_g2s(st + SOFF_C + 2 * N, L.cz + off, N * sizeof(float), br);
     if (rec) bulk_g2s(&recs[slot], grec + tRec, sizeof(TileRec), br);
   };
   float hx[HQ], hc[HQ];
@@ -193,8 +235,11 @@ __global__ void __launch_bounds__(NTH, 1)
     }
   };
   auto halo_combine = [&](const TileRec& r, int ti, int u) {
-    widen_x<VT, NTH>(stages[u], tid);
-    const float* st = stages[u];
+    float* st = stage(u);
+    if (!WIDE) {
+      const VT* xr = sraw_x<VT>(st);
+      for (int e = tid; e < N; e += NTH) st[xpad(e)] = to_f(xr[e]);
+    }
 #pragma unroll
     for (int q = 0; q < HQ; q++) {
       const int g = tid + NTH * q, f = g >> 8, c = g & 255;
@@ -203,7 +248,7 @@ __global__ void __launch_bounds__(NTH, 1)
       const int kind = r.f[f].kind;
       float v = 0.f;
       if (kind == FACE_SAME) {
-        const float cown = st[(3 + dir) * N + plane_idx(TS, dir, 0, a, bb)];
+        const float cown = st[SOFF_C + dir * N + plane_idx(TS, dir, 0, a, bb)];
         v = (side ? hc[q] : cown) * hx[q];
       } else if (kind == FACE_COARSER) {
         v = hc[q] * hx[q];
@@ -223,7 +268,7 @@ __global__ void __launch_bounds__(NTH, 1)
     if (tid == 0) atomicExch(err, 1);
     return;
   }
-  if (tid == 0) issue_arrays(recs[0], stages[0], &bar[0], t + G, 1);
+  if (tid == 0) issue_arrays(recs[0], stage(0), &bar[0], t + G, 1);
   halo_issue(recs[0]);
   if (!__syncthreads_and(mbar_wait(&bar[0], 0))) {
     if (tid == 0) {
@@ -234,8 +279,13 @@ __global__ void __launch_bounds__(NTH, 1)
   }
   halo_combine(recs[0], tileBase + t, 0);
   __syncthreads();
-  const int ip = tid & 7, jj = 2 * ((tid >> 5) & 7) + ((tid >> 3) & 1);
-  const int kb = ((tid >> 4) & 1) + 2 * (tid >> 8);
+  const int ip = tid & 7;
+  const int jj = ((tid >> 3) & 1) + 2 * ((tid >> 5) & 7);
+  const int kp = ((tid >> 4) & 1) + 2 * (tid >> 8);
+  const int q = jj & 1;
+  // colour c, z slot s: the cell x = 2ip + dx(c, s), z = 2kp + s
+  auto dxof = [&](int c, int s) { return (c + q + s) & 1; };
+  const int eb = 2 * ip + TS * jj + XP * 2 * kp;  // padded index of (2ip, jj, 2kp)
   for (int n = 0; t < count; n++, t += G) {
     const int s = n & 1, u = s ^ 1;
     const int tn = t + G;
@@ -246,63 +296,78 @@ __global__ void __launch_bounds__(NTH, 1)
     if (hasNext) {
       if (tid == 0) {
         bulk_wait_read();  // the store from stage u (tile n-1) has read it
-        issue_arrays(rn, stages[u], &bar[u], tn + G, (n + 2) % 3);
+        issue_arrays(rn, stage(u), &bar[u], tn + G, (n + 2) % 3);
       }
       halo_issue(rn);
     }
-    // 2: registers: couplings, 1/a_ii, b with the halo sums folded in
-    float* X = stages[s];
-    const VT* B = raw_b<VT>(X);
-    const float* IV = X + 2 * N;
-    const float* CX = X + 3 * N;
-    const float* CY = X + 4 * N;
-    const float* CZ = X + 5 * N;
+    // 2: registers: couplings, 1/a_ii, b with the halo sums folded in, and
+    // the thread's own four x values
+    float* X = stage(s);
+    const VT* B = sraw_b<VT>(X);
+    const float* IV = X + SOFF_IV;
+    const float* CX = X + SOFF_C;
+    const float* CY = CX + N;
+    const float* CZ = CY + N;
     const float(*gs)[TS * TS] = gsb[s];
-    float R[2][KK], I[2][KK], Cm[2][KK][3], Cp[2][KK][3];
-    // A thread's two cells at (jj, k) are x-neighbours 2ip, 2ip+1 (one per
-    // colour): their coefficients come as float2 pairs.  The even cell has
-    // colour (jj + k) & 1; runtime selects keep the arrays compile-time indexed.
+    // Per colour c and z slot sl: 1/a_ii, b + halo sums, x, and the
+    // couplings to the x- and z-neighbours read from shared memory (Cxo,
+    // Czo) and to y-1, y+1.  The coupling inside the x pair (cx of cell
+    // 2ip+1) and inside the z pair (cz of plane 2kp+1) is shared by the two
+    // cells it joins.  Couplings across the tile boundary are zero; the
+    // reference's extra zeroing for non-liquid cells is implied by their
+    // 1/a_ii = 0.
+    float R[2][2], I[2][2], xv[2][2], Cxo[2][2], Cym[2][2], Cyp[2][2], Czo[2][2];
+    float Cxp[2], Czp[2];  // pair couplings: x per z slot, z per x cell (h)
+    const int u0 = 2 * ip + TS * jj + TS * TS * 2 * kp;
+    {
+      // cz of the planes 2kp, 2kp+1, 2kp+2 (the last read past plane 15
+      // only when kp = 7, where it is unused)
+      const float2 cz0 = *reinterpret_cast<const float2*>(CZ + u0);
+      const float2 cz1 = *reinterpret_cast<const float2*>(CZ + u0 + TS * TS);
+      const float2 cz2 = *reinterpret_cast<const float2*>(CZ + u0 + 2 * TS * TS);
+      Czp[0] = cz1.x;
+      Czp[1] = cz1.y;
 #pragma unroll
-    for (int kk = 0; kk < KK; kk++) {
-      const int k = kb + KSTRIDE * kk;
-      const int e0 = tidx(TS, 2 * ip, jj, k);
-      const float2 iv2 = *reinterpret_cast<const float2*>(IV + e0);
-      const float2 cx2 = *reinterpret_cast<const float2*>(CX + e0);
-      const float cxn = CX[e0 + 2];  // past the row end only when unused (ii = 15)
-      const float2 cy2 = *reinterpret_cast<const float2*>(CY + e0);
-      const float2 cyn = *reinterpret_cast<const float2*>(CY + e0 + TS);
-      const float2 cz2 = *reinterpret_cast<const float2*>(CZ + e0);
-      const float2 czn = *reinterpret_cast<const float2*>(CZ + e0 + TS * TS);
-      const float ivv[2] = {iv2.x, iv2.y};
-      float rr[2] = {to_f(B[e0]), to_f(B[e0 + 1])};
-      float cm[2][3], cp[2][3];
+      for (int sl = 0; sl < 2; sl++) {
+        const int k = 2 * kp + sl;
+        const int e0 = u0 + TS * TS * sl;
+        const float2 iv2 = *reinterpret_cast<const float2*>(IV + e0);
+        const float2 cx2 = *reinterpret_cast<const float2*>(CX + e0);
+        const float cxn = CX[e0 + 2];  // past the row end only when unused (ip = 7)
+        const float2 cy2 = *reinterpret_cast<const float2*>(CY + e0);
+        const float2 cyn = *reinterpret_cast<const float2*>(CY + e0 + TS);
+        const float2 x2 = *reinterpret_cast<const float2*>(X + eb + XP * sl);
+        Cxp[sl] = cx2.y;
+        const float ivv[2] = {iv2.x, iv2.y};
+        const float xx[2] = {x2.x, x2.y};
+        // the x coupling away from the pair: x-1 of cell 0, x+1 of cell 1
+        const float cxo[2] = {ip > 0 ? cx2.x : 0.f, ip < 7 ? cxn : 0.f};
+        const float cym[2] = {jj > 0 ? cy2.x : 0.f, jj > 0 ? cy2.y : 0.f};
+        const float cyp[2] = {jj < TS - 1 ? cyn.x : 0.f, jj < TS - 1 ? cyn.y : 0.f};
+        // the z coupling away from the pair: z-1 of plane 2kp, z+1 of 2kp+1
+        const float czo[2] = {sl ? (kp < 7 ? cz2.x : 0.f) : (kp > 0 ? cz0.x : 0.f),
+                              sl ? (kp < 7 ? cz2.y : 0.f) : (kp > 0 ? cz0.y : 0.f)};
+        float rr[2] = {to_f(B[e0]), to_f(B[e0 + 1])};
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int ii = 2 * ip + h;
-        const bool fl = ivv[h] > 0.f;
-        if (ii == 0) rr[h] += gs[0][jj + TS * k];
-        if (ii == TS - 1) rr[h] += gs[1][jj + TS * k];
-        if (jj == 0) rr[h] += gs[2][ii + TS * k];
-        if (jj == TS - 1) rr[h] += gs[3][ii + TS * k];
-        if (k == 0) rr[h] += gs[4][ii + TS * jj];
-        if (k == TS - 1) rr[h] += gs[5][ii + TS * jj];
-        cm[h][0] = (fl && ii > 0) ? (h ? cx2.y : cx2.x) : 0.f;
-        cp[h][0] = (fl && ii < TS - 1) ? (h ? cxn : cx2.y) : 0.f;
-        cm[h][1] = (fl && jj > 0) ? (h ? cy2.y : cy2.x) : 0.f;
-        cp[h][1] = (fl && jj < TS - 1) ? (h ? cyn.y : cyn.x) : 0.f;
-        cm[h][2] = (fl && k > 0) ? (h ? cz2.y : cz2.x) : 0.f;
-        cp[h][2] = (fl && k < TS - 1) ? (h ? czn.y : czn.x) : 0.f;
-      }
-      const bool evenIs0 = ((jj + k) & 1) == 0;  // colour 0 is the even cell
+        for (int h = 0; h < 2; h++) {
+          const int ii = 2 * ip + h;
+          if (ii == 0) rr[h] += gs[0][jj + TS * k];
+          if (ii == TS - 1) rr[h] += gs[1][jj + TS * k];
+          if (jj == 0) rr[h] += gs[2][ii + TS * k];
+          if (jj == TS - 1) rr[h] += gs[3][ii + TS * k];
+          if (k == 0) rr[h] += gs[4][ii + TS * jj];
+          if (k == TS - 1) rr[h] += gs[5][ii + TS * jj];
+        }
 #pragma unroll
-      for (int c = 0; c < 2; c++) {
-        const bool ev = (c == 0) == evenIs0;
-        I[c][kk] = ev ? ivv[0] : ivv[1];
-        R[c][kk] = ev ? rr[0] : rr[1];
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-          Cm[c][kk][d] = ev ? cm[0][d] : cm[1][d];
-          Cp[c][kk][d] = ev ? cp[0][d] : cp[1][d];
+        for (int c = 0; c < 2; c++) {
+          const bool h1 = dxof(c, sl) == 1;
+          I[c][sl] = h1 ? ivv[1] : ivv[0];
+          R[c][sl] = h1 ? rr[1] : rr[0];
+          xv[c][sl] = h1 ? xx[1] : xx[0];
+          Cxo[c][sl] = h1 ? cxo[1] : cxo[0];
+          Cym[c][sl] = h1 ? cym[1] : cym[0];
+          Cyp[c][sl] = h1 ? cyp[1] : cyp[0];
+          Czo[c][sl] = h1 ? czo[1] : czo[0];
         }
       }
     }
@@ -310,19 +375,31 @@ __global__ void __launch_bounds__(NTH, 1)
     auto half = [&](auto cc) {
       constexpr int c = decltype(cc)::value;
 #pragma unroll
-      for (int kk = 0; kk < KK; kk++) {
-        const int k = kb + KSTRIDE * kk, ii = 2 * ip + ((jj + k + c) & 1);
-        const int e = tidx(TS, ii, jj, k);
-        // out-of-tile neighbours have zero coupling; their reads stay inside
-        // shared memory (guard band / adjacent arrays, all finite)
-        float S = R[c][kk];
-        S = fmaf(Cm[c][kk][0], X[e - 1], S);
-        S = fmaf(Cp[c][kk][0], X[e + 1], S);
-        S = fmaf(Cm[c][kk][1], X[e - TS], S);
-        S = fmaf(Cp[c][kk][1], X[e + TS], S);
-        S = fmaf(Cm[c][kk][2], X[e - TS * TS], S);
-        S = fmaf(Cp[c][kk][2], X[e + TS * TS], S);
-        X[e] = S * I[c][kk];
+      for (int sl = 0; sl < 2; sl++) {
+        const int dx = dxof(c, sl);
+        const int e = eb + dx + XP * sl;
+        // the x-neighbour of the other colour inside the pair is ours; the
+        // one beyond is read (out-of-tile reads have zero coupling and stay
+        // inside shared memory: guard band, pads, adjacent arrays)
+        const float xo = X[dx ? e + 1 : e - 1], xs = xv[1 - c][sl];
+        // z: plane 2kp reads z-1 and owns z+1; plane 2kp+1 the reverse
+        const float zo = X[sl ? e + XP : e - XP], zs = xv[1 - c][1 - sl];
+        const float czs = dx ? Czp[1] : Czp[0];
+        // terms in the order x-, x+, y-, y+, z-, z+
+        float S = R[c][sl];
+        S = fmaf(dx ? Cxp[sl] : Cxo[c][sl], dx ? xs : xo, S);
+        S = fmaf(dx ? Cxo[c][sl] : Cxp[sl], dx ? xo : xs, S);
+        S = fmaf(Cym[c][sl], X[e - TS], S);
+        S = fmaf(Cyp[c][sl], X[e + TS], S);
+        if (sl) {
+          S = fmaf(czs, zs, S);
+          S = fmaf(Czo[c][sl], zo, S);
+        } else {
+          S = fmaf(Czo[c][sl], zo, S);
+          S = fmaf(czs, zs, S);
+        }
+        xv[c][sl] = S * I[c][sl];
+        X[e] = xv[c][sl];
       }
       __syncthreads();
     };
@@ -335,16 +412,26 @@ __global__ void __launch_bounds__(NTH, 1)
         half(std::integral_constant<int, 1>());
       }
     }
-    // 4: the tile leaves by one bulk store (narrowed into slot 1 first when
-    // the vectors are 16-bit; slot 1's b is no longer read)
-    if (!std::is_same<VT, float>::value) {
-      VT* xr = raw_x<VT>(X);
-      for (int e = tid; e < N; e += NTH) xr[e] = from_f<VT>(X[e]);
+    // 4: the tile leaves by bulk stores: FP32 plane by plane from the padded
+    // slot; 16-bit narrowed first into the b slot (b is no longer read)
+    if (!WIDE) {
+      VT* xr = sraw_x<VT>(X);
+      for (int e = tid; e < N; e += NTH) xr[e] = from_f<VT>(X[xpad(e)]);
       __syncthreads();
     }
     if (tid == 0) {
       fence_proxy_async();
-      bulk_s2g(x + rc.off, raw_x<VT>(X), N * sizeof(VT));
+      if (WIDE) {
+#pragma unroll 1
+        for (int k = 0; k < TS; k++)
+          asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(
+                           x + rc.off + k * TS * TS),
+                       "r"(smem_u32(X + k * XP)), "r"((int)(TS * TS * sizeof(VT)))
+                       : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+      } else {
+        bulk_s2g(x + rc.off, sraw_x<VT>(X), N * sizeof(VT));
+      }
     }
     // 5: next tile's arrays landed -> its halo sums
     if (hasNext) {
