@@ -101,23 +101,27 @@ constexpr int GUARD = TS * TS;
 constexpr int ZERO_FLOATS = GUARD + 12 * N + 2 * 6 * TS * TS;
 constexpr size_t SMEM = sizeof(float) * ZERO_FLOATS + 3 * sizeof(TileRec) + 3 * sizeof(uint64_t);
 
-// Issue the global loads of one halo cell of a SAME/COARSER face; the own
-// lower-face coupling of a SAME face is taken later from shared memory.
+// Issue the global loads of one halo cell of a SAME/COARSER face (the own
+// lower-face coupling of a SAME face is taken later from shared memory).
+// The branches only choose the addresses: each value is one load straight
+// into its register, raw, so nothing waits for it before it is used (faces
+// without these values load a harmless word and ignore it).
 template <typename VT>
 __device__ __forceinline__ void halo_load(const LevelView& L, const VT* __restrict__ x,
                                           const FaceRes& r, int dir, int side, int a, int b,
-                                          float& xv, float& cv) {
+                                          VT& xv, float& cv) {
   const float* cd = dir == 0 ? L.cx : dir == 1 ? L.cy : L.cz;
-  xv = 0.f;
-  cv = 0.f;
+  const VT* px = x;
+  const float* pc = cd;
   if (r.kind == FACE_SAME) {
-    xv = to_f(__ldg(x + r.nOff + plane_idx(TS, dir, side ? 0 : TS - 1, a, b)));
-    if (side) cv = __ldg(cd + r.nOff + plane_idx(TS, dir, 0, a, b));
+    px = x + r.nOff + plane_idx(TS, dir, side ? 0 : TS - 1, a, b);
+    if (side) pc = cd + r.nOff + plane_idx(TS, dir, 0, a, b);
   } else if (r.kind == FACE_COARSER) {
-    xv = to_f(__ldg(x + r.nOff + plane_idx(r.nts, dir, side ? 0 : r.nts - 1, r.oa + (a >> 1),
-                                           r.ob + (b >> 1))));
-    cv = __ldg(L.ifc + r.ifOwn + a + TS * b);
+    px = x + r.nOff + plane_idx(r.nts, dir, side ? 0 : r.nts - 1, r.oa + (a >> 1), r.ob + (b >> 1));
+    pc = L.ifc + r.ifOwn + a + TS * b;
   }
+  xv = __ldg(px);
+  cv = __ldg(pc);
 }
 
 // Where the x and b vectors of a tile land in a stage of the operator
@@ -198,34 +202,57 @@ __global__ void __launch_bounds__(NTH, 1)
   // two finite 16-bit values (never a float NaN/Inf pattern)
   for (int q = tid; q < SZERO_FLOATS / 4; q += NTH)
     reinterpret_cast<float4*>(sm)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+  // The copies of a stage are issued in parallel, each by lane 0 of its own
+  // warp (a bulk copy holds its issuing thread for ~100 cycles): FP32 x
+  // plane by plane (warps 0-15) or 16-bit x whole (warp 0), then b, 1/a_ii,
+  // cx, cy, cz, then the record; the stage barrier counts one arrival each.
+  constexpr int NXC = WIDE ? TS : 1;
+  constexpr int NISS = NXC + 6;
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    mbar_init(&bar[0], NISS);
+    mbar_init(&bar[1], NISS);
     mbar_init(&bar[2], 1);
     fence_mbar_init();
   }
   __syncthreads();
   auto issue_arrays = [&](const TileRec& r, float* st, uint64_t* br, int tRec, int slot) {
+    const int w = tid >> 5;
+    if ((tid & 31) != 0 || w >= NISS) return;
     fence_proxy_async();
-    const bool rec = tRec < count;
-    mbar_expect_tx(br, 2 * N * sizeof(VT) + 4 * N * sizeof(float) + (rec ? sizeof(TileRec) : 0));
     const int64_t off = r.off;
-    if (WIDE) {
-      // x plane by plane into the padded working slot
-#pragma unroll 1
-      for (int k = 0; k < TS; k++)
-        bulk_g2s(st + k * XP, x + off + k * TS * TS, TS * TS * sizeof(VT), br);
-    } else {
-      bulk_g2s(sraw_x<VT>(st), x + off, N * sizeof(VT), br);
+    if (w == NISS - 1) {  // the record two tiles ahead, if there is one
+      const bool rec = tRec < count;
+      mbar_expect_tx(br, rec ? sizeof(TileRec) : 0);
+      if (rec) bulk_g2s(&recs[slot], grec + tRec, sizeof(TileRec), br);
+      return;
     }
-    bulk_g2s(sraw_b<VT>(st), b + off, N * sizeof(VT), br);
-    bulk_g2s(st + SOFF_IV, L.invdiag + off, N * sizeof(float), br);
-    bulk_g2s(st + SOFF_C, L.cx + off, N * sizeof(float), br);
-    bulk_g2s(st + SOFF_C + N, L.cy + off, N * sizeof(float), br);
-    bulk_g2s(st + SOFF_C + 2 * N, L.cz + off, N * sizeof(float), br);
-    if (rec) bulk_g2s(&recs[slot], grec + tRec, sizeof(TileRec), br);
+    const void* src;
+    void* dst;
+    uint32_t bytes = N * sizeof(float);
+    if (w < NXC) {
+      if (WIDE) {
+        src = x + off + w * TS * TS;
+        dst = st + w * XP;
+        bytes = TS * TS * sizeof(VT);
+      } else {
+        src = x + off;
+        dst = sraw_x<VT>(st);
+        bytes = N * sizeof(VT);
+      }
+    } else {
+      switch (w - NXC) {
+        case 0: src = b + off; dst = sraw_b<VT>(st); bytes = N * sizeof(VT); break;
+        case 1: src = L.invdiag + off; dst = st + SOFF_IV; break;
+        case 2: src = L.cx + off; dst = st + SOFF_C; break;
+        case 3: src = L.cy + off; dst = st + SOFF_C + N; break;
+        default: src = L.cz + off; dst = st + SOFF_C + 2 * N; break;
+      }
+    }
+    mbar_expect_tx(br, bytes);
+    bulk_g2s(dst, src, bytes, br);
   };
-  float hx[HQ], hc[HQ];
+  VT hx[HQ];
+  float hc[HQ];
   auto halo_issue = [&](const TileRec& r) {
 #pragma unroll
     for (int q = 0; q < HQ; q++) {
@@ -249,9 +276,9 @@ __global__ void __launch_bounds__(NTH, 1)
       float v = 0.f;
       if (kind == FACE_SAME) {
         const float cown = st[SOFF_C + dir * N + plane_idx(TS, dir, 0, a, bb)];
-        v = (side ? hc[q] : cown) * hx[q];
+        v = (side ? hc[q] : cown) * to_f(hx[q]);
       } else if (kind == FACE_COARSER) {
-        v = hc[q] * hx[q];
+        v = hc[q] * to_f(hx[q]);
       } else if (kind == FACE_FINER) {
         v = ghost_sum(L, x, ti, TS, dir, side, a, bb);
       }
@@ -268,13 +295,11 @@ __global__ void __launch_bounds__(NTH, 1)
     if (tid == 0) atomicExch(err, 1);
     return;
   }
-  if (tid == 0) issue_arrays(recs[0], stage(0), &bar[0], t + G, 1);
+  issue_arrays(recs[0], stage(0), &bar[0], t + G, 1);
   halo_issue(recs[0]);
   if (!__syncthreads_and(mbar_wait(&bar[0], 0))) {
-    if (tid == 0) {
-      atomicExch(err, 1);
-      mbar_wait(&bar[0], 0);  // one more bounded wait for the copies in flight
-    }
+    if (tid == 0) atomicExch(err, 1);
+    mbar_wait(&bar[0], 0);  // one more bounded wait for the copies in flight
     return;
   }
   halo_combine(recs[0], tileBase + t, 0);
@@ -294,10 +319,7 @@ __global__ void __launch_bounds__(NTH, 1)
     const TileRec& rn = recs[(n + 1) % 3];
     // 1: prefetch the next tile (arrays + the record two ahead), halo loads
     if (hasNext) {
-      if (tid == 0) {
-        bulk_wait_read();  // the store from stage u (tile n-1) has read it
-        issue_arrays(rn, stage(u), &bar[u], tn + G, (n + 2) % 3);
-      }
+      issue_arrays(rn, stage(u), &bar[u], tn + G, (n + 2) % 3);
       halo_issue(rn);
     }
     // 2: registers: couplings, 1/a_ii, b with the halo sums folded in, and
@@ -412,41 +434,28 @@ __global__ void __launch_bounds__(NTH, 1)
         half(std::integral_constant<int, 1>());
       }
     }
-    // 4: the tile leaves by bulk stores: FP32 plane by plane from the padded
-    // slot; 16-bit narrowed first into the b slot (b is no longer read)
-    if (!WIDE) {
-      VT* xr = sraw_x<VT>(X);
-      for (int e = tid; e < N; e += NTH) xr[e] = from_f<VT>(X[xpad(e)]);
-      __syncthreads();
-    }
-    if (tid == 0) {
-      fence_proxy_async();
-      if (WIDE) {
-#pragma unroll 1
-        for (int k = 0; k < TS; k++)
-          asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(
-                           x + rc.off + k * TS * TS),
-                       "r"(smem_u32(X + k * XP)), "r"((int)(TS * TS * sizeof(VT)))
-                       : "memory");
-        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-      } else {
-        bulk_s2g(x + rc.off, sraw_x<VT>(X), N * sizeof(VT));
+    // 4: the tile leaves from the registers: each thread stores its two
+    // x pairs (a warp writes four full 64-byte rows)
+    {
+      VT* xg = x + rc.off + 2 * ip + TS * jj + TS * TS * 2 * kp;
+#pragma unroll
+      for (int sl = 0; sl < 2; sl++) {
+        const bool c1lo = dxof(1, sl) == 0;  // colour 1 holds the even cell
+        const float lo = c1lo ? xv[1][sl] : xv[0][sl], hi = c1lo ? xv[0][sl] : xv[1][sl];
+        store2(xg + TS * TS * sl, lo, hi);
       }
     }
     // 5: next tile's arrays landed -> its halo sums
     if (hasNext) {
       if (!__syncthreads_and(mbar_wait(&bar[u], ((n + 1) >> 1) & 1))) {
-        if (tid == 0) {
-          atomicExch(err, 1);
-          bulk_wait_all();
-        }
+        if (tid == 0) atomicExch(err, 1);
+        mbar_wait(&bar[u], ((n + 1) >> 1) & 1);  // bounded: copies in flight
         return;
       }
       halo_combine(rn, tileBase + tn, u);
     }
     __syncthreads();  // stage s, gsb[s] and record slot n%3 are free again
   }
-  if (tid == 0) bulk_wait_all();
 }
 
 // Host side: the 256-byte tile records of one level (offset + resolved faces).
@@ -495,7 +504,7 @@ __global__ void __launch_bounds__(NTH, 1)
   constexpr int HQ = (NHALO + NTH - 1) / NTH;
   constexpr int NVEC = MODE == APPLY_RESIDUAL ? 2 : 1;  // x, [b]
   extern __shared__ __align__(128) float sm[];
-  float* stages[2] = {sm + GUARD, sm + GUARD + 6 * N};
+  auto stage = [&](int i) { return sm + GUARD + i * 6 * N; };
   float(*gsb)[6][TS * TS] = reinterpret_cast<float(*)[6][TS * TS]>(sm + GUARD + 12 * N);
   TileRec* recs = reinterpret_cast<TileRec*>(sm + ZERO_FLOATS);
   uint64_t* bar = reinterpret_cast<uint64_t*>(recs + 3);
@@ -505,30 +514,46 @@ __global__ void __launch_bounds__(NTH, 1)
   const int G = gridDim.x;
   int t = blockIdx.x;
   double acc = 0;
+  // one issuing thread (lane 0 of its own warp) per copy: x, [b], a_ii,
+  // cx, cy, cz, record; the stage barrier counts one arrival each
+  constexpr int NISS = NVEC + 5;
   if (t < count) {
     if (tid == 0) {
-      mbar_init(&bar[0], 1);
-      mbar_init(&bar[1], 1);
+      mbar_init(&bar[0], NISS);
+      mbar_init(&bar[1], NISS);
       mbar_init(&bar[2], 1);
       fence_mbar_init();
     }
     __syncthreads();
     // stage arrays: 0 x, 1 b (residual), 2 a_ii, 3..5 couplings
     auto issue_arrays = [&](const TileRec& r, float* st, uint64_t* br, int tRec, int slot) {
+      const int w = tid >> 5;
+      if ((tid & 31) != 0 || w >= NISS) return;
       fence_proxy_async();
-      const bool rec = tRec < count;
-      mbar_expect_tx(br, NVEC * N * sizeof(VT) + 4 * N * sizeof(float) +
-                             (rec ? sizeof(TileRec) : 0));
       const int64_t off = r.off;
-      bulk_g2s(raw_x<VT>(st), x + off, N * sizeof(VT), br);
-      if (MODE == APPLY_RESIDUAL) bulk_g2s(raw_b<VT>(st), b + off, N * sizeof(VT), br);
-      bulk_g2s(st + 2 * N, L.diag + off, N * sizeof(float), br);
-      bulk_g2s(st + 3 * N, L.cx + off, N * sizeof(float), br);
-      bulk_g2s(st + 4 * N, L.cy + off, N * sizeof(float), br);
-      bulk_g2s(st + 5 * N, L.cz + off, N * sizeof(float), br);
-      if (rec) bulk_g2s(&recs[slot], grec + tRec, sizeof(TileRec), br);
+      if (w == NISS - 1) {
+        const bool rec = tRec < count;
+        mbar_expect_tx(br, rec ? sizeof(TileRec) : 0);
+        if (rec) bulk_g2s(&recs[slot], grec + tRec, sizeof(TileRec), br);
+        return;
+      }
+      const int a = w < NVEC ? w : w - NVEC + 2;  // array index 0..5
+      const void* src;
+      void* dst;
+      uint32_t bytes = N * sizeof(float);
+      switch (a) {
+        case 0: src = x + off; dst = raw_x<VT>(st); bytes = N * sizeof(VT); break;
+        case 1: src = b + off; dst = raw_b<VT>(st); bytes = N * sizeof(VT); break;
+        case 2: src = L.diag + off; dst = st + 2 * N; break;
+        case 3: src = L.cx + off; dst = st + 3 * N; break;
+        case 4: src = L.cy + off; dst = st + 4 * N; break;
+        default: src = L.cz + off; dst = st + 5 * N; break;
+      }
+      mbar_expect_tx(br, bytes);
+      bulk_g2s(dst, src, bytes, br);
     };
-    float hx[HQ], hc[HQ];
+    VT hx[HQ];
+    float hc[HQ];
     auto halo_issue = [&](const TileRec& r, int ti, int u) {
 #pragma unroll
       for (int q = 0; q < HQ; q++) {
@@ -539,8 +564,8 @@ __global__ void __launch_bounds__(NTH, 1)
       if (MODE == APPLY_RESIDUAL && tid < 6) cmap[u][tid] = L.toCoarse[(size_t)ti * 6 + tid];
     };
     auto halo_combine = [&](const TileRec& r, int ti, int u) {
-      widen_x<VT, NTH>(stages[u], tid);
-      const float* st = stages[u];
+      widen_x<VT, NTH>(stage(u), tid);
+      const float* st = stage(u);
 #pragma unroll
       for (int q = 0; q < HQ; q++) {
         const int g = tid + NTH * q, f = g >> 8, c = g & 255;
@@ -550,9 +575,9 @@ __global__ void __launch_bounds__(NTH, 1)
         float v = 0.f;
         if (kind == FACE_SAME) {
           const float cown = st[(3 + dir) * N + plane_idx(TS, dir, 0, a, bb)];
-          v = (side ? hc[q] : cown) * hx[q];
+          v = (side ? hc[q] : cown) * to_f(hx[q]);
         } else if (kind == FACE_COARSER) {
-          v = hc[q] * hx[q];
+          v = hc[q] * to_f(hx[q]);
         } else if (kind == FACE_FINER) {
           v = ghost_sum(L, x, ti, TS, dir, side, a, bb);
         }
@@ -565,10 +590,10 @@ __global__ void __launch_bounds__(NTH, 1)
     }
     bool ok = __syncthreads_and(mbar_wait(&bar[2], 0));
     if (ok) {
-      if (tid == 0) issue_arrays(recs[0], stages[0], &bar[0], t + G, 1);
+      issue_arrays(recs[0], stage(0), &bar[0], t + G, 1);
       halo_issue(recs[0], tileBase + t, 0);
       ok = __syncthreads_and(mbar_wait(&bar[0], 0));
-      if (!ok && tid == 0) mbar_wait(&bar[0], 0);
+      if (!ok) mbar_wait(&bar[0], 0);
     }
     if (!ok) {
       if (tid == 0) atomicExch(err, 1);
@@ -585,13 +610,10 @@ __global__ void __launch_bounds__(NTH, 1)
       const TileRec& rc = recs[n % 3];
       const TileRec& rn = recs[(n + 1) % 3];
       if (hasNext) {
-        if (tid == 0) {
-          bulk_wait_read();
-          issue_arrays(rn, stages[u], &bar[u], tn + G, (n + 2) % 3);
-        }
+        issue_arrays(rn, stage(u), &bar[u], tn + G, (n + 2) % 3);
         halo_issue(rn, tileBase + tn, u);
       }
-      float* X = stages[s];
+      float* X = stage(s);
       const VT* B = raw_b<VT>(X);
       const float* D = X + 2 * N;
       const float* CX = X + 3 * N;
@@ -628,22 +650,15 @@ __global__ void __launch_bounds__(NTH, 1)
         xm = xc;
         xc = xp;
       }
-      __syncthreads();  // every thread has read its D / neighbours before Y is written
       if (MODE == APPLY_MATVEC) {
-        VT* Yv = reinterpret_cast<VT*>(Y);
+        // q leaves from the registers (a warp writes two full 64-byte rows)
 #pragma unroll
-        for (int kk = 0; kk < ZC; kk++) Yv[tidx(TS, i, j, k0 + kk)] = from_f<VT>(yv[kk]);
+        for (int kk = 0; kk < ZC; kk++) y[rc.off + tidx(TS, i, j, k0 + kk)] = from_f<VT>(yv[kk]);
       } else {
+        __syncthreads();  // every thread has read its D / neighbours before Y is written
 #pragma unroll
         for (int kk = 0; kk < ZC; kk++) Y[tidx(TS, i, j, k0 + kk)] = yv[kk];
-      }
-      __syncthreads();
-      if (MODE == APPLY_MATVEC) {
-        if (tid == 0) {
-          fence_proxy_async();
-          bulk_s2g(y + rc.off, Y, N * sizeof(VT));
-        }
-      } else {
+        __syncthreads();
         const int* tc = cmap[s];
         const int ct = tc[0];
         if (ct >= 0) {
@@ -669,17 +684,14 @@ __global__ void __launch_bounds__(NTH, 1)
       }
       if (hasNext) {
         if (!__syncthreads_and(mbar_wait(&bar[u], ((n + 1) >> 1) & 1))) {
-          if (tid == 0) {
-            atomicExch(err, 1);
-            bulk_wait_all();
-          }
+          if (tid == 0) atomicExch(err, 1);
+          mbar_wait(&bar[u], ((n + 1) >> 1) & 1);  // bounded: copies in flight
           break;
         }
         halo_combine(rn, tileBase + tn, u);
       }
       __syncthreads();
     }
-    if (tid == 0) bulk_wait_all();
   }
   if (MODE == APPLY_MATVEC && partial) {
     acc = block_sum(acc);

@@ -75,5 +75,21 @@ __device__ __forceinline__ void store4<__nv_bfloat16>(__nv_bfloat16* p, F4 v) {
   *reinterpret_cast<uint2*>(p) = u;
 }
 
+// Two consecutive elements (8-byte aligned for FP32, 4-byte for 16-bit).
+template <typename VT>
+__device__ __forceinline__ void store2(VT* p, float a, float b);
+template <>
+__device__ __forceinline__ void store2<float>(float* p, float a, float b) {
+  *reinterpret_cast<float2*>(p) = make_float2(a, b);
+}
+template <>
+__device__ __forceinline__ void store2<__half>(__half* p, float a, float b) {
+  *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a, b);
+}
+template <>
+__device__ __forceinline__ void store2<__nv_bfloat16>(__nv_bfloat16* p, float a, float b) {
+  *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(a, b);
+}
+
 }  // namespace ps
 }  // namespace msbg

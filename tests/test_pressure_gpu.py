@@ -149,3 +149,19 @@ def test_uncovered_coarse_cells_read_as_zero():
         assert info.status == 0, (storage, info.status)
         assert info.relResidual <= 1e-6
     ctx.close()
+
+
+@pytest.mark.parametrize("bsx0,nl,band", [(16, 2, 8.0), (32, 2, 8.0), (16, 3, 4.0)])
+def test_pipelined_smoother_matches_per_tile_kernel(gpu_ctx, bsx0, nl, band):
+    """Two level-0 smoothing sweeps (3 inner red-black iterations per tile)
+    from x = 0: the persistent pipelined 16^3 kernel against the plain
+    one-CTA-per-tile kernel, up to FP32 rounding of the sums."""
+    s = msbg_gpu.PressureScene(128, bsx0, nl, band=band, seed=21)
+    xs = []
+    for what in (3, 0):  # 3: per-tile kernel, 0: pipelined kernel
+        gpu_ctx.pressure_prepare(s)
+        gpu_ctx.pressure_profile(what, 1, 3)
+        xs.append(gpu_ctx.pressure_download())
+    a, b = xs
+    assert np.abs(a).max() > 0
+    assert np.abs(a - b).max() <= 1e-5 * np.abs(a).max(), np.abs(a - b).max()
