@@ -549,6 +549,7 @@ def bench_mcf(args):
             "frac": achieved / hbm, "peak_kind": pk_kind,
             "traffic": dpc * nvox / 8.0 if dpc else None,
             "alg_bytes_per_launch": 8.0 * nvox / 8.0, "kernel": "mcf_colour_kernel<16>"}
+    ctx.set_topology(c["res"], c["res"], c["res"], c["bsx"])  # the C-ABI path needs the raster
     host_in = torch.from_numpy(vals).pin_memory()
     host_out = torch.empty_like(host_in).pin_memory()
     kind_c = np.ascontiguousarray(kind)

@@ -68,6 +68,16 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
+// 4-byte asynchronous global -> shared copy (no register round trip); the
+// thread's copies complete at cp_async_wait_all.
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 template <int BSX>
 struct McfTile {
   static constexpr int H = BSX + 2;
@@ -145,7 +155,9 @@ __global__ void __launch_bounds__(BSX* BSX)
     bulk_g2s(dense, own, NV * sizeof(float), bar);
   }
 
-  // Gather the 26 neighbour pieces straight into the padded tile.
+  // Gather the 26 neighbour pieces straight into the padded tile: voxels of
+  // stored blocks by asynchronous copies (all of a thread's copies in flight
+  // at once), constant blocks by plain stores.
   for (int i = tid; i < T::NHALO; i += NT) {
     int hx, hy, hz;
     shell_coord<H>(i, hx, hy, hz);
@@ -154,19 +166,19 @@ __global__ void __launch_bounds__(BSX* BSX)
     int dy = y < 0 ? -1 : (y >= BSX ? 1 : 0);
     int dz = z < 0 ? -1 : (z >= BSX ? 1 : 0);
     int s = nbSlot[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
-    float v;
+    float* d = tile + hx + H * hy + H2 * hz;
     if (s >= 0) {
-      v = __ldg(pool + (size_t)s * NV + ((x & (BSX - 1)) + BSX * ((y & (BSX - 1)) + BSX * (z & (BSX - 1)))));
+      cp_async4(d, pool + (size_t)s * NV + ((x & (BSX - 1)) + BSX * ((y & (BSX - 1)) + BSX * (z & (BSX - 1)))));
     } else if (s == SLOT_EMPTY) {
-      v = emptyVal;
+      *d = emptyVal;
     } else if (s == SLOT_FULL) {
-      v = fullVal;
+      *d = fullVal;
     } else {  // NULL block or outside the domain: Neumann, own value clamped
       int cx = min(max(x, 0), BSX - 1), cy = min(max(y, 0), BSX - 1), cz = min(max(z, 0), BSX - 1);
-      v = __ldg(own + (cx + BSX * (cy + BSX * cz)));
+      cp_async4(d, own + (cx + BSX * (cy + BSX * cz)));
     }
-    tile[hx + H * hy + H2 * hz] = v;
   }
+  cp_async_wait_all();
 
   // Interior: wait for the bulk copy (or load directly), spread into the
   // padded tile.
