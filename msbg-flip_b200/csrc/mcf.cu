@@ -12,10 +12,11 @@
 //
 // CTA layout: one block per CTA, BSX*BSX threads, thread (x,y) owns a z
 // column and keeps a 3-plane register window of the 5-point cross, so each
-// voxel costs 9 shared-memory reads instead of 19.  The block interior
-// arrives by one bulk async copy (TMA engine, cp.async.bulk) into a dense
-// staging tile while the threads gather the 26 neighbour pieces, then is
-// spread into the padded (BSX+2)^3 tile.
+// voxel costs 9 shared-memory reads instead of 19.  The block and its
+// 26-neighbour shell arrive in the padded (BSX+2)^3 tile by asynchronous
+// 4-byte copies (cp.async), every thread's copies in flight at once; with no
+// staging buffer a 16^3 block needs 23 KB and 8 CTAs fill an SM.  The
+// kernel has no waits that could time out, so it never sets errFlag.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -27,45 +28,6 @@ namespace {
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void fence_mbar_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-// Bounded wait on phase 0 of the mbarrier: returns false if the copy did not
-// land within the spin limit (the caller then skips the block and flags it).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
-  uint32_t done = 0;
-  for (int i = 0; i < (1 << 22); i++) {
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(phase)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
-                                         uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
 }
 
 // 4-byte asynchronous global -> shared copy (no register round trip); the
@@ -84,12 +46,9 @@ struct McfTile {
   static constexpr int NV = BSX * BSX * BSX;
   static constexpr int NT = BSX * BSX;
   static constexpr int NHALO = 2 * H * H + 2 * H * (H - 2) + 2 * (H - 2) * (H - 2);
-  // The interior goes through a dense bulk-copy staging tile when it fits
-  // next to the padded tile (BSX <= 16); 32^3 blocks load it directly.
-  static constexpr bool kBulk = sizeof(float) * (NV + H * H * H) + 16 <= 200 * 1024;
-  static constexpr int NDENSE = kBulk ? NV : 0;
-  // dynamic smem: [dense NDENSE floats][padded H^3 floats][mbarrier]
-  static constexpr size_t SMEM = sizeof(float) * (NDENSE + H * H * H) + 16;
+  // dynamic smem: the padded H^3 tile (23 KB for 16^3 blocks, so 8 CTAs of
+  // 256 threads fit an SM)
+  static constexpr size_t SMEM = sizeof(float) * H * H * H;
 };
 
 // Decode the i-th voxel of the 1-voxel shell around the block into padded
@@ -126,9 +85,7 @@ __global__ void __launch_bounds__(BSX* BSX)
   using T = McfTile<BSX>;
   constexpr int H = T::H, H2 = H * H, NV = T::NV, NT = T::NT;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  float* dense = reinterpret_cast<float*>(smem_raw);
-  float* tile = dense + T::NDENSE;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tile + H * H * H);
+  float* tile = reinterpret_cast<float*>(smem_raw);
   __shared__ int nbSlot[27];
 
   const int tid = threadIdx.x;
@@ -137,10 +94,6 @@ __global__ void __launch_bounds__(BSX* BSX)
   const int slot0 = slotOf[bid];
   const float* own = pool + (size_t)slot0 * NV;
 
-  if (T::kBulk && tid == 0) {
-    mbar_init(bar, 1);
-    fence_mbar_init();
-  }
   if (tid < 27) {
     int dx = tid % 3 - 1, dy = (tid / 3) % 3 - 1, dz = tid / 9 - 1;
     int x = bx + dx, y = by + dy, z = bz + dz;
@@ -150,9 +103,11 @@ __global__ void __launch_bounds__(BSX* BSX)
     nbSlot[tid] = s;
   }
   __syncthreads();
-  if (T::kBulk && tid == 0) {
-    mbar_expect_tx(bar, NV * sizeof(float));
-    bulk_g2s(dense, own, NV * sizeof(float), bar);
+  // The interior: one asynchronous 4-byte copy per voxel straight into the
+  // padded tile (consecutive threads, consecutive voxels).
+  for (int e = tid; e < NV; e += NT) {
+    const int x = e % BSX, y = (e / BSX) % BSX, z = e / (BSX * BSX);
+    cp_async4(tile + (x + 1) + H * (y + 1) + H2 * (z + 1), own + e);
   }
 
   // Gather the 26 neighbour pieces straight into the padded tile: voxels of
@@ -180,34 +135,7 @@ __global__ void __launch_bounds__(BSX* BSX)
   }
   cp_async_wait_all();
 
-  // Interior: wait for the bulk copy (or load directly), spread into the
-  // padded tile.
-  if constexpr (T::kBulk) {
-    const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0));
-    if (!ok) {
-      // The copy never completed: leave the block unchanged, flag the error
-      // (the host reports MSBG_ETIMEOUT) and give the copy one more bounded
-      // wait so no transfer is left targeting this CTA's shared memory.
-      if (tid == 0) {
-        atomicExch(errFlag, 1);
-        mbar_wait_bounded(bar, 0);
-      }
-      return;
-    }
-  }
-  const float4* src4 = T::kBulk ? reinterpret_cast<const float4*>(dense)
-                                : reinterpret_cast<const float4*>(own);
-  for (int i = tid; i < NV / 4; i += NT) {
-    float4 v = src4[i];
-    int e = i * 4;
-    int x = e % BSX, y = (e / BSX) % BSX, z = e / (BSX * BSX);
-    float* d = tile + (x + 1) + H * (y + 1) + H2 * (z + 1);
-    d[0] = v.x;
-    d[1] = v.y;
-    d[2] = v.z;
-    d[3] = v.w;
-  }
-  __syncthreads();
+  __syncthreads();  // every thread's copies have landed (waited above)
 
   // Column sweep with a 3-plane register window of the 5-point cross.
   const int x = tid % BSX, y = tid / BSX;
