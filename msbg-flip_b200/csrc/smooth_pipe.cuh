@@ -6,22 +6,23 @@
 // colour) with a stride of gridDim.x.  Per tile:
 //   * the six contiguous 16 KB arrays (x, b, 1/a_ii, cx, cy, cz) arrive by bulk
 //     asynchronous copies (cp.async.bulk, completion on an mbarrier) into one
-//     of two shared-memory stages, issued one tile ahead (x plane by plane
-//     into a padded slot);
+//     of two shared-memory stages, issued one tile ahead, each copy by lane 0
+//     of its own warp (FP32 x plane by plane into a padded slot);
 //   * the tile's 256-byte record (its offset and the resolved data of its six
 //     faces) arrives the same way two tiles ahead, so no dependent global load
 //     sits on the critical path;
 //   * the halo values of the next tile are loaded into registers before the
 //     current tile is smoothed and summed afterwards;
-//   * the smoothed x leaves by bulk stores.
+//   * the smoothed x leaves from the registers (each thread stores its own
+//     cells), so no store has to drain before a stage is refilled.
 // 1024 threads, each owning a 2 x 2 block of cells (x pair, z pair) whose
 // couplings, 1/a_ii, right-hand side (with the constant halo sums folded in)
 // and x values sit in registers.
 //
 // Vectors may be stored in 16 bits (VT = __half / __nv_bfloat16): x and b
 // then arrive together in the b slot and x is widened into the FP32 working
-// slot; the smoothed tile is narrowed back into the b slot for the bulk store.
-// The operator arrays are always FP32.
+// slot; results are narrowed in registers as they are stored.  The operator
+// arrays are always FP32.
 
 namespace pipe {
 
@@ -64,20 +65,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
-               "r"(smem_u32(src)), "r"(bytes)
-               : "memory");
-  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-}
-// Wait until the bulk stores issued so far have finished reading shared memory.
-__device__ __forceinline__ void bulk_wait_read() {
-  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-}
-__device__ __forceinline__ void bulk_wait_all() {
-  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-}
-
 constexpr int TS = 16, N = TS * TS * TS, NT = 512;
 constexpr int NT_SMOOTH = 1024;  // threads of the smoother CTA
 constexpr int NT_APPLY = 1024;   // threads of the operator-application CTA
