@@ -308,11 +308,42 @@ __global__ void __launch_bounds__(TS* TS) k_prolong(LevelView L, const int* __re
   if (ct < 0) return;
   const VC* src = xc + coarseOff[ct];
   const int sh = agg ? 1 : 0;
-  for (int e = threadIdx.x; e < N; e += NT) {
-    if (!(L.diag[off + e] > 0.f)) continue;
-    const int i = e % TS, j = (e / TS) % TS, k = e / (TS * TS);
-    const float c = to_f(src[tidx(cts, ox + (i >> sh), oy + (j >> sh), oz + (k >> sh))]);
-    x[off + e] = from_f<VT>(to_f(x[off + e]) + scale * c);
+  if constexpr (TS >= 4) {
+    // groups of 4 x-consecutive cells: every load of a thread's groups is
+    // issued before any is used (non-liquid cells are written back unchanged)
+    constexpr int PER = (N / 4 + NT - 1) / NT;
+    F4 dv[PER], xv[PER], cv[PER];
+#pragma unroll
+    for (int p = 0; p < PER; p++) {
+      const int e = 4 * (threadIdx.x + NT * p);
+      if (e >= N) continue;
+      const int i = e % TS, j = (e / TS) % TS, k = e / (TS * TS);
+      dv[p] = load4(L.diag + off + e);
+      xv[p] = load4(x + off + e);
+      const VC* row = src + tidx(cts, 0, oy + (j >> sh), oz + (k >> sh));
+      cv[p].x = to_f(row[ox + (i >> sh)]);
+      cv[p].y = to_f(row[ox + ((i + 1) >> sh)]);
+      cv[p].z = to_f(row[ox + ((i + 2) >> sh)]);
+      cv[p].w = to_f(row[ox + ((i + 3) >> sh)]);
+    }
+#pragma unroll
+    for (int p = 0; p < PER; p++) {
+      const int e = 4 * (threadIdx.x + NT * p);
+      if (e >= N) continue;
+      F4 o = xv[p];
+      if (dv[p].x > 0.f) o.x = to_f(from_f<VT>(xv[p].x + scale * cv[p].x));
+      if (dv[p].y > 0.f) o.y = to_f(from_f<VT>(xv[p].y + scale * cv[p].y));
+      if (dv[p].z > 0.f) o.z = to_f(from_f<VT>(xv[p].z + scale * cv[p].z));
+      if (dv[p].w > 0.f) o.w = to_f(from_f<VT>(xv[p].w + scale * cv[p].w));
+      store4(x + off + e, o);
+    }
+  } else {
+    for (int e = threadIdx.x; e < N; e += NT) {
+      if (!(L.diag[off + e] > 0.f)) continue;
+      const int i = e % TS, j = (e / TS) % TS, k = e / (TS * TS);
+      const float c = to_f(src[tidx(cts, ox + (i >> sh), oy + (j >> sh), oz + (k >> sh))]);
+      x[off + e] = from_f<VT>(to_f(x[off + e]) + scale * c);
+    }
   }
 }
 
