@@ -335,8 +335,9 @@ cudaError_t copy_d2h(void* dst, const void* src, size_t bytes, cudaStream_t st) 
   return e;
 }
 
-template <typename T>
-cudaError_t upload(DeviceBuffer& buf, const std::vector<T>& v, cudaStream_t st) {
+template <typename V>
+cudaError_t upload(DeviceBuffer& buf, const V& v, cudaStream_t st) {
+  using T = typename V::value_type;
   cudaError_t e = buf.ensure(sizeof(T) * std::max<size_t>(v.size(), 1));
   if (e != cudaSuccess) return e;
   if (v.empty()) return cudaSuccess;
@@ -424,8 +425,11 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
     MSBG_CUDA_TRY(ctx, upload(D->diag, L.diag, st));
     if (m == 0) MSBG_CUDA_TRY(ctx, upload(D->ctype, L.ctype, st));
     {
-      std::vector<float> inv(L.diag.size());
-      for (size_t c = 0; c < inv.size(); c++)
+      HostArray<float> inv;
+      inv.resize(L.diag.size());
+      const int64_t nInv = (int64_t)inv.size();
+#pragma omp parallel for schedule(static)
+      for (int64_t c = 0; c < nInv; c++)
         inv[c] = L.diag[c] > 0.f ? (float)(1.0 / (double)L.diag[c]) : 0.f;
       MSBG_CUDA_TRY(ctx, upload(D->invdiag, inv, st));
       MSBG_CUDA_TRY(ctx, upload(D->tileRec, build_tile_records(L), st));

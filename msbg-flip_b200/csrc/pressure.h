@@ -7,6 +7,8 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -16,6 +18,32 @@ namespace msbg {
 namespace ps {
 
 constexpr int TS_MAX = 16;  // tile edge in cells (a 32^3 block is 8 tiles)
+
+// Allocator whose resize() leaves new elements uninitialised: the per-cell
+// arrays of the hierarchy (hundreds of MB at 1024^3) are then first touched,
+// zeroed and filled by the threads that own their tiles, instead of by one
+// thread's serial zero-fill.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+  using value_type = T;
+  template <typename U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <typename U>
+  NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <typename T>
+using HostArray = std::vector<T, NoInitAlloc<T>>;
 
 // Face neighbour kinds of a tile face.
 enum : int {
@@ -53,8 +81,8 @@ struct Level {
   int64_t nCells = 0, nIf = 0;
   // operator: a_ii, lower-face couplings to same-level neighbours, interface
   // couplings (stored on the finer side, one per fine boundary cell)
-  std::vector<float> diag, cx, cy, cz, ifc, rhs;
-  std::vector<uint8_t> ctype;      // MG level 0 only: CT_* per cell
+  HostArray<float> diag, cx, cy, cz, ifc, rhs;
+  HostArray<uint8_t> ctype;        // MG level 0 only: CT_* per cell
   // tile maps per resolution level: dense raster of tile ids (-1 = none)
   std::vector<std::vector<int>> tmap = std::vector<std::vector<int>>(32);
   std::vector<int> tmapN = std::vector<int>(32, 0);  // tiles per edge (0 = level absent)

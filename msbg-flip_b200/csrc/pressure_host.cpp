@@ -236,21 +236,39 @@ inline double interface_coupling(const msbg_pressure_callbacks* cb, int l, int d
   return (2.0 / 3.0) * h * cb->sampleFaceCoeff(cb->user, dir, c[0] << l, c[1] << l, c[2] << l);
 }
 
+// Zeroes tile ti's cells of diag, cx, cy, cz (and rhs) and its interface
+// planes: the first touch of that memory, by the thread that fills it.
+void zero_tile(Level& L, int ti, bool withRhs) {
+  const Tile& t = L.tiles[ti];
+  const size_t n3 = (size_t)t.ts * t.ts * t.ts;
+  std::fill_n(L.diag.begin() + t.off, n3, 0.f);
+  std::fill_n(L.cx.begin() + t.off, n3, 0.f);
+  std::fill_n(L.cy.begin() + t.off, n3, 0.f);
+  std::fill_n(L.cz.begin() + t.off, n3, 0.f);
+  if (withRhs) std::fill_n(L.rhs.begin() + t.off, n3, 0.f);
+  for (int f = 0; f < 6; f++) {
+    const int64_t io = L.ifOff[(size_t)ti * 6 + f];
+    if (io >= 0) std::fill_n(L.ifc.begin() + io, (size_t)t.ts * t.ts, 0.f);
+  }
+}
+
 // Level 0 operator from the callbacks.
 void sample_level0(const Ctx& C, Level& L, std::vector<uint8_t>& fluid) {
   const msbg_pressure_callbacks* cb = C.cb;
   const int nT = (int)L.tiles.size();
-  L.diag.assign(L.nCells, 0.f);
-  L.cx.assign(L.nCells, 0.f);
-  L.cy.assign(L.nCells, 0.f);
-  L.cz.assign(L.nCells, 0.f);
-  L.rhs.assign(L.nCells, 0.f);
-  L.ifc.assign(L.nIf, 0.f);
+  // allocated untouched; each tile zeroes its own cells and interface planes
+  L.diag.resize(L.nCells);
+  L.cx.resize(L.nCells);
+  L.cy.resize(L.nCells);
+  L.cz.resize(L.nCells);
+  L.rhs.resize(L.nCells);
+  L.ifc.resize(L.nIf);
 #pragma omp parallel for schedule(dynamic, 1)
   for (int ti = 0; ti < nT; ti++) {
     const Tile& t = L.tiles[ti];
     const int l = t.level, ts = t.ts;
     const double h = (double)(1 << l);
+    zero_tile(L, ti, true);
     float* cdir[3] = {&L.cx[t.off], &L.cy[t.off], &L.cz[t.off]};
     // Across a tile face the neighbour region (and whether it is inside the
     // domain) is the same for every cell: a tile face lies within one block
@@ -345,11 +363,12 @@ void sample_level0(const Ctx& C, Level& L, std::vector<uint8_t>& fluid) {
 void galerkin(const Ctx& C, const Level& F, const std::vector<uint8_t>& fineFluid, Level& G,
               const std::vector<uint8_t>& coarseFluid) {
   const int nT = (int)G.tiles.size();
-  G.diag.assign(G.nCells, 0.f);
-  G.cx.assign(G.nCells, 0.f);
-  G.cy.assign(G.nCells, 0.f);
-  G.cz.assign(G.nCells, 0.f);
-  G.ifc.assign(G.nIf, 0.f);
+  // allocated untouched; each tile zeroes its own cells and interface planes
+  G.diag.resize(G.nCells);
+  G.cx.resize(G.nCells);
+  G.cy.resize(G.nCells);
+  G.cz.resize(G.nCells);
+  G.ifc.resize(G.nIf);
   // fine cell lookup: (level, cell coords) -> global fine cell index or -1
   auto fine_cell = [&](int l, int X, int Y, int Z) -> int64_t {
     int t = tile_at(F, l, X, Y, Z);
@@ -434,6 +453,7 @@ void galerkin(const Ctx& C, const Level& F, const std::vector<uint8_t>& fineFlui
   for (int ti = 0; ti < nT; ti++) {
     const Tile& t = G.tiles[ti];
     const int lc = t.level, ts = t.ts;
+    zero_tile(G, ti, false);
     float* cdir[3] = {&G.cx[t.off], &G.cy[t.off], &G.cz[t.off]};
     // Fast path of an aggregated tile (the tile lies in one block, so all its
     // cells aggregate or none do): its children fill a fine region of
@@ -670,7 +690,7 @@ int build_hierarchy(Hierarchy& H, int sx, int sy, int sz, int bsx0, int nLevels,
     register_tiles(L, tiles);
     build_faces(C, L);
     fluid.assign(L.nCells, 0);
-    L.ctype.assign(L.nCells, CT_AIR);
+    L.ctype.resize(L.nCells);  // every cell is written below
 #pragma omp parallel for schedule(dynamic, 4)
     for (int64_t ti = 0; ti < (int64_t)L.tiles.size(); ti++) {
       const Tile& t = L.tiles[ti];

@@ -179,13 +179,16 @@ struct msbg_pressure_scene {
   // coef * exp(i phi): cos(theta) of a cell is the real part of a product of
   // table entries (the callbacks are sampled once per cell, so this replaces
   // 16 cosines by 16 complex products).
-  std::vector<double> etab;  // [mode][axis][res][2]
+  std::vector<double> etab;  // [axis][res][mode][2]: a cell's entries are contiguous
   std::vector<double> ephi;  // [mode][2]
   // Boxes that can contain a cell centre of each 8^3 region (bit b = box b;
   // built when there are at most 64 boxes, else every box is tested).
   static constexpr int RG = 8;
   int nrg = 0;
   std::vector<uint64_t> boxMask;
+  // Spheres that can contain a cell centre of each 8^3 region (at most 64
+  // spheres; else every sphere is tested).
+  std::vector<uint64_t> sphereMask;
 
   double liquid_sdf(double x, double y, double z) const {
     double d = z - zLiquid * res;
@@ -219,17 +222,29 @@ struct msbg_pressure_scene {
   }
   // liquid: below the plane or inside a sphere (the sign of liquid_sdf,
   // tested on squared distances)
-  bool liquid(double x, double y, double z) const {
+  bool in_sphere(const Sphere& s, double x, double y, double z) const {
+    double dx = x - s.cx, dy = y - s.cy, dz = z - s.cz;
+    return dx * dx + dy * dy + dz * dz < s.r * s.r;
+  }
+  bool liquid_cell(int ix, int iy, int iz) const {
+    const double x = ix + 0.5, y = iy + 0.5, z = iz + 0.5;
     if (z - zLiquid * res < 0) return true;
-    for (const auto& s : spheres) {
-      double dx = x - s.cx, dy = y - s.cy, dz = z - s.cz;
-      if (dx * dx + dy * dy + dz * dz < s.r * s.r) return true;
+    if (!sphereMask.empty()) {
+      uint64_t m = sphereMask[(ix / RG) + (size_t)nrg * ((iy / RG) + (size_t)nrg * (iz / RG))];
+      while (m) {
+        const int b = __builtin_ctzll(m);
+        m &= m - 1;
+        if (in_sphere(spheres[b], x, y, z)) return true;
+      }
+      return false;
     }
+    for (const auto& s : spheres)
+      if (in_sphere(s, x, y, z)) return true;
     return false;
   }
   uint16_t cell_type(int x, int y, int z) const {
     if (!inside(x, y, z) || solid(x, y, z)) return 1;  // CELL_SOLID
-    return liquid(x + 0.5, y + 0.5, z + 0.5) ? 0 : 0x1000;  // CELL_VOID
+    return liquid_cell(x, y, z) ? 0 : 0x1000;           // CELL_VOID
   }
   float face(int dir, int x, int y, int z) const {
     int xm = x - (dir == 0), ym = y - (dir == 1), zm = z - (dir == 2);
@@ -242,9 +257,9 @@ struct msbg_pressure_scene {
     double s = 0;
     const int nm = (int)modes.size();
     for (int m = 0; m < nm; m++) {
-      const double* ex = &etab[((size_t)(m * 3 + 0) * res + x) * 2];
-      const double* ey = &etab[((size_t)(m * 3 + 1) * res + y) * 2];
-      const double* ez = &etab[((size_t)(m * 3 + 2) * res + z) * 2];
+      const double* ex = &etab[(((size_t)0 * res + x) * nm + m) * 2];
+      const double* ey = &etab[(((size_t)1 * res + y) * nm + m) * 2];
+      const double* ez = &etab[(((size_t)2 * res + z) * nm + m) * 2];
       const double pr = ex[0] * ey[0] - ex[1] * ey[1], pi = ex[0] * ey[1] + ex[1] * ey[0];
       const double qr = pr * ez[0] - pi * ez[1], qi = pr * ez[1] + pi * ez[0];
       s += qr * ephi[2 * m] - qi * ephi[2 * m + 1];  // Re(coef e^{i phi} q)
@@ -301,6 +316,35 @@ extern "C" msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, in
             s->boxMask[x + (size_t)s->nrg * (y + (size_t)s->nrg * z)] |= 1ull << bi;
     }
   }
+  if (res % msbg_pressure_scene::RG == 0 && s->spheres.size() <= 64) {
+    const int RG = msbg_pressure_scene::RG, nrg = res / RG;
+    s->nrg = nrg;
+    s->sphereMask.assign((size_t)nrg * nrg * nrg, 0);
+    for (size_t si = 0; si < s->spheres.size(); si++) {
+      const Sphere& sp = s->spheres[si];
+      const double c[3] = {sp.cx, sp.cy, sp.cz};
+      int r0[3], r1[3];
+      for (int k = 0; k < 3; k++) {
+        r0[k] = std::max(0, (int)std::floor((c[k] - sp.r - 1) / RG));
+        r1[k] = std::min(nrg - 1, (int)std::floor((c[k] + sp.r + 1) / RG));
+      }
+      for (int z = r0[2]; z <= r1[2]; z++)
+        for (int y = r0[1]; y <= r1[1]; y++)
+          for (int x = r0[0]; x <= r1[0]; x++) {
+            // distance from the centre to the region's cell-centre box; a
+            // unit of slack keeps every sphere a point could be inside
+            const int rr[3] = {x, y, z};
+            double d2 = 0;
+            for (int k = 0; k < 3; k++) {
+              const double lo = rr[k] * RG + 0.5, hi = rr[k] * RG + RG - 0.5;
+              const double q = std::min(std::max(c[k], lo), hi) - c[k];
+              d2 += q * q;
+            }
+            if (d2 < sp.r * sp.r + 1.0)
+              s->sphereMask[x + (size_t)nrg * (y + (size_t)nrg * z)] |= 1ull << si;
+          }
+    }
+  }
   // Box-Muller normals for the amplitudes.
   auto normal = [&]() {
     double u1 = std::max(rng.uniform(), 1e-300), u2 = rng.uniform();
@@ -331,8 +375,8 @@ extern "C" msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, in
     for (int d = 0; d < 3; d++)
       for (int x = 0; x < res; x++) {
         const double a = w * m.k[d] * (x + 0.5);
-        s->etab[((size_t)(i * 3 + d) * res + x) * 2] = std::cos(a);
-        s->etab[((size_t)(i * 3 + d) * res + x) * 2 + 1] = std::sin(a);
+        s->etab[(((size_t)d * res + x) * nModes + i) * 2] = std::cos(a);
+        s->etab[(((size_t)d * res + x) * nModes + i) * 2 + 1] = std::sin(a);
       }
   }
   // Refinement map.
