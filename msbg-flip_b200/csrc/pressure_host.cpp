@@ -740,9 +740,26 @@ int build_hierarchy(Hierarchy& H, int sx, int sy, int sz, int bsx0, int nLevels,
     };
     std::vector<std::vector<uint8_t>> candFluid(cand.size());
     std::vector<uint8_t> keep(cand.size(), 0);
+    // does any fine tile (level t.level-1 or t.level) overlap coarse tile t?
+    // Without one every coarse cell is dry, so the per-cell test is skipped.
+    auto any_fine_tile = [&](const Tile& t) {
+      for (int lv = std::max(0, t.level - 1); lv <= t.level; lv++) {
+        const int fts = F.tsOf[lv];
+        if (!fts || !F.tmapN[lv]) continue;
+        const int sh = t.level - lv;
+        const int o[3] = {t.ox << sh, t.oy << sh, t.oz << sh}, e = t.ts << sh;
+        // start on the fine tile grid so every overlapping fine tile is visited
+        for (int z = o[2] - o[2] % fts; z < o[2] + e; z += fts)
+          for (int y = o[1] - o[1] % fts; y < o[1] + e; y += fts)
+            for (int x = o[0] - o[0] % fts; x < o[0] + e; x += fts)
+              if (tile_at(F, lv, x, y, z) >= 0) return true;
+      }
+      return false;
+    };
 #pragma omp parallel for schedule(dynamic, 4)
     for (int64_t i = 0; i < (int64_t)cand.size(); i++) {
       const Tile& t = cand[i];
+      if (!any_fine_tile(t)) continue;  // keep[i] stays 0
       auto& cf = candFluid[i];
       cf.assign((size_t)t.ts * t.ts * t.ts, 0);
       bool any = false;
