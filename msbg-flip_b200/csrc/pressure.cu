@@ -1271,53 +1271,63 @@ extern "C" int msbg_gpu_pressure_correction_pairs(msbg_gpu_ctx* ctx,
   MSBG_CUDA_TRY(ctx, scale.ensure(sizeof(float) * np));
   MSBG_CUDA_TRY(ctx, off.ensure(sizeof(int64_t) * np));
   MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(xs.p, x64, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  int rc = MSBG_OK;
-  if (pcgIters > 0) {
-    msbg_gpu_solve_params q = *p;
-    q.storage = MSBG_F32;
-    q.learned = 0;
-    q.tol = 0;
-    q.maxIter = pcgIters;
-    q.maxRefine = 1 << 20;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    SolveOut o;
-    int64_t launches = 0;
-    rc = solve_typed<float>(ctx, S, &q, e0, e1, o, &launches);
-    cudaStreamSynchronize(st);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+  auto body = [&]() -> int {
+    int rc = MSBG_OK;
+    if (pcgIters > 0) {
+      msbg_gpu_solve_params q = *p;
+      q.storage = MSBG_F32;
+      q.learned = 0;
+      q.tol = 0;
+      q.maxIter = pcgIters;
+      q.maxRefine = 1 << 20;
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      SolveOut o;
+      int64_t launches = 0;
+      rc = solve_typed<float>(ctx, S, &q, e0, e1, o, &launches);
+      cudaStreamSynchronize(st);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      if (rc) return rc;
+    } else {
+      MSBG_CUDA_TRY(ctx, cudaMemsetAsync(x64, 0, sizeof(double) * n, st));
+    }
+    Runner<float> R{S, st, p->nPre, p->nPost, p->innerIter};
+    R.coarseScale = p->coarseScale > 0 ? p->coarseScale : 1.0f;
+    R.err = ctx->errBuf.as<int>();
+    R.numSMs = S.numSMs;
+    const float* b = S.rhs0.as<float>();
+    float* r = S.r0.as<float>();
+    float* z = S.z0.as<float>();
+    double rr = 0;
+    rc = residual64(ctx, S, R, b, r, &rr);
     if (rc) return rc;
-  } else {
-    MSBG_CUDA_TRY(ctx, cudaMemsetAsync(x64, 0, sizeof(double) * n, st));
+    R.vcycle(0, z, (const float*)r);
+    k_add64<float><<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, z, n, 1.0);
+    rc = residual64(ctx, S, R, b, r, &rr);
+    if (rc) return rc;
+    k_sub64<<<VEC_GRID, VEC_BLOCK, 0, st>>>(err.as<double>(), xs.as<double>(), x64, n);
+    rc = select_pair_tiles(ctx, S, np, st);
+    if (rc) return rc;
+    k_cnn_features<<<np, FEAT_THREADS, 0, st>>>(
+        S.views[0], S.dev[0]->ctype.as<uint8_t>(), S.cIdx.as<int>(), S.cIdx.as<int>() + np,
+        S.levelNorm, r, err.as<double>(), feat, scale.as<float>(), off.as<int64_t>(), target, mask);
+    MSBG_CUDA_TRY(ctx, cudaGetLastError());
+    return MSBG_OK;
+  };
+  const int rc = body();
+  // restore the refined solution (after a failure in between too)
+  cudaError_t e = cudaMemcpyAsync(x64, xs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) {
+    k_narrow<<<VEC_GRID, VEC_BLOCK, 0, st>>>(S.dev[0]->x.as<float>(), x64, n);
+    e = cudaGetLastError();
   }
-  Runner<float> R{S, st, p->nPre, p->nPost, p->innerIter};
-  R.coarseScale = p->coarseScale > 0 ? p->coarseScale : 1.0f;
-  R.err = ctx->errBuf.as<int>();
-  R.numSMs = S.numSMs;
-  const float* b = S.rhs0.as<float>();
-  float* r = S.r0.as<float>();
-  float* z = S.z0.as<float>();
-  double rr = 0;
-  rc = residual64(ctx, S, R, b, r, &rr);
+  const cudaError_t es = cudaStreamSynchronize(st);
+  S.haveX64 = e == cudaSuccess && es == cudaSuccess;
   if (rc) return rc;
-  R.vcycle(0, z, (const float*)r);
-  k_add64<float><<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, z, n, 1.0);
-  rc = residual64(ctx, S, R, b, r, &rr);
-  if (rc) return rc;
-  k_sub64<<<VEC_GRID, VEC_BLOCK, 0, st>>>(err.as<double>(), xs.as<double>(), x64, n);
-  rc = select_pair_tiles(ctx, S, np, st);
-  if (rc) return rc;
-  k_cnn_features<<<np, FEAT_THREADS, 0, st>>>(
-      S.views[0], S.dev[0]->ctype.as<uint8_t>(), S.cIdx.as<int>(), S.cIdx.as<int>() + np,
-      S.levelNorm, r, err.as<double>(), feat, scale.as<float>(), off.as<int64_t>(), target, mask);
-  MSBG_CUDA_TRY(ctx, cudaGetLastError());
-  // restore the refined solution
-  MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(x64, xs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  k_narrow<<<VEC_GRID, VEC_BLOCK, 0, st>>>(S.dev[0]->x.as<float>(), x64, n);
-  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  S.haveX64 = true;
+  MSBG_CUDA_TRY(ctx, e);
+  MSBG_CUDA_TRY(ctx, es);
   return MSBG_OK;
 }
 
