@@ -126,7 +126,9 @@ int msbg_gpu_pde_mcf(msbg_gpu_ctx* ctx, int chan, const int* blockList, int n,
  * (cudaStream_t as void*; NULL = the legacy default stream): pool = value blocks [nSlots][bsx^3] FP32,
  * slotOf[nBlocks] = slot or -1 NULL / -2 empty / -3 full; colourList holds
  * the updated blocks' ids grouped by colour with colourStart[9] offsets
- * (device arrays).  For callers that keep the grid resident on the GPU. */
+ * (device arrays).  For callers that keep the grid resident on the GPU.
+ * A listed block whose slotOf entry is negative is skipped on the device,
+ * and the next msbg_gpu_sync returns MSBG_EINVARG for it. */
 int msbg_gpu_pde_mcf_device(msbg_gpu_ctx* ctx, float* pool, const int* slotOf,
                             const int* colourList, const int* colourStartHost,
                             int nbx, int nby, int nbz, int bsx, float emptyVal,
@@ -143,13 +145,18 @@ int msbg_gpu_pde_mcf_device(msbg_gpu_ctx* ctx, float* pool, const int* slotOf,
  *   blockList, n   host array of the block ids to update (value blocks only)
  *   stream         cudaStream_t as void* (NULL = legacy default stream)
  *   timedOut       NULL: return right after the launches; non-NULL: wait for
- *                  the stream and report whether a bounded wait gave up
+ *                  the stream and report whether a bounded wait gave up; a
+ *                  listed block whose slotOf entry is negative is skipped on
+ *                  the device and then makes the call return MSBG_EINVARG
  * No context, no cudaMalloc/cudaFree: the colour-grouped block list and the
  * error flag live in a fixed device array of 2*MSBG_MCF_NOALLOC_MAX_BLOCKS+16
  * ints (2 MB) that every device using this library keeps until the process
  * exits.  n > MSBG_MCF_NOALLOC_MAX_BLOCKS is rejected with MSBG_EINVARG.
- * The first call on a device looks up that array's device address; make
- * that first call before any stream capture.  All calls on a device share
+ * The first call on a device looks up that array's device address, and with
+ * CUDA's default lazy module loading it is also the call that places the
+ * array and the kernels' code on the device.  Make that first call (n = 0 is
+ * enough) before reserving the device's memory with your own pool and before
+ * any stream capture, or run with CUDA_MODULE_LOADING=EAGER.  All calls on a device share
  * the array (each call resets what must start at zero), so calls whose work
  * overlaps on the GPU race: serialise them on one stream. */
 #define MSBG_MCF_NOALLOC_MAX_BLOCKS 262144
@@ -274,6 +281,97 @@ int msbg_gpu_pressure_stats(msbg_gpu_ctx* ctx, msbg_gpu_pressure_stats_t* out);
  * 2 vector values per matvec; summed over the MG levels for a V-cycle). */
 int msbg_gpu_pressure_profile(msbg_gpu_ctx* ctx, int what, int reps, int innerIter,
                               double* msPerCall, double* algBytesPerCall);
+
+/* ---- bulk-array prepare and solver components ---------------------------- */
+
+/* Bulk-array form of msbg_gpu_pressure_prepare: the per-cell data that
+ * preparePressureSolveFLIPLevel0_ samples through the callbacks
+ * (src/msbg3.cpp:2472-2584) handed over as arrays in the packed block layout
+ * of MG level 0 (blocks in bid order, each (bsx0>>level)^3 cells at its
+ * refinement level, vid = x + y*bs + z*bs*bs):
+ *   flags[]  CELL_* bits per cell (CH_CELL_FLAGS)
+ *   faceX/Y/Z[] coefficient of the cell's LOWER face in x/y/z (CH_FACE_AREA)
+ *   rhs[]    right-hand side per unit volume (CH_DIVERGENCE; may be NULL = 0)
+ * A cell's upper face is its +1 neighbour's lower face; faces on the domain
+ * boundary outside the arrays have coefficient 0 (the reference's
+ * getValueGen_ reads 0 there, src/msbg3.cpp:2700-2708). */
+int msbg_gpu_pressure_prepare_arrays(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
+                                     const uint16_t* flags, const float* faceX,
+                                     const float* faceY, const float* faceZ, const float* rhs);
+
+/* The component entry points below run one piece of the prepared solver on
+ * vectors in the packed block layout of MG level levelMg: every base block b
+ * at level max(map[b], levelMg) (src/msbg.cpp:1650), (bsx0>>level)^3 values,
+ * blocks in bid order.  Levels 0 .. nLevels-1 have this layout.  Inputs are
+ * host arrays of exactly msbg_gpu_pressure_level_size values; values of
+ * blocks that hold no liquid are ignored on input and 0 on output.  Each call
+ * waits for its result.  Vectors must be 0 on cells that are not liquid, as
+ * the solver keeps them (the reference's CHECK_NONFLUID_ZERO invariant,
+ * src/msbgcell.h:89-92). */
+int msbg_gpu_pressure_level_size(msbg_gpu_ctx* ctx, int levelMg, int64_t* n);
+
+/* a_ii per cell (0 off liquid) of MG level levelMg.  The reference's
+ * CH_DIAGONAL holds D = 1/(sum of the 6 face weights) (computeDiagonalFLIP_,
+ * src/msbg3.cpp:2586-2779); away from level interfaces a_ii = h / D. */
+int msbg_gpu_pressure_diagonal(msbg_gpu_ctx* ctx, int levelMg, float* diag, int64_t n);
+
+/* y = A x on MG level levelMg.  Replaces multiplyLaplacianMatrixOpt(0,
+ * levelMg, chX, CH_NULL, 0, chY, ...) (src/msbg3.cpp:1757-1912, cell kernel
+ * 1282-1321: Y = F0/D - sum W F with F = x h), which equals A x wherever the
+ * two operators coincide (same-level faces). */
+int msbg_gpu_matvec(msbg_gpu_ctx* ctx, int levelMg, const float* x, float* y, int64_t n);
+
+/* r = b - A x on MG level levelMg (0 off liquid).  Replaces
+ * multiplyLaplacianMatrixOpt(OPT_CALC_RESIDUAL, levelMg, chX, chB, ...). */
+int msbg_gpu_residual(msbg_gpu_ctx* ctx, int levelMg, const float* x, const float* b, float* r,
+                      int64_t n);
+
+/* coarse = R fine from MG level levelMgCoarse-1 to levelMgCoarse: the sum over
+ * the liquid children of each coarse cell, through the solve's fused
+ * residual-and-restriction kernels (with x = 0).  Replaces
+ * downsampleChannel<float,float>(levelMgCoarse, src, dst,
+ * OPT_SIMPLE_AVERAGE|OPT_ALL_CELLS) (src/msbg4.cpp:1512-1914), whose
+ * coarsened blocks hold the 1/8 average (src/msbg4.cpp:1562-1566): for a
+ * vector that is 0 off liquid the sum is 8x the average.  Blocks that are not
+ * coarsened at that step are copied, as the reference aliases them
+ * (src/msbg4.cpp:1648-1650). */
+int msbg_gpu_restrict(msbg_gpu_ctx* ctx, int levelMgCoarse, const float* fine, int64_t nFine,
+                      float* coarse, int64_t nCoarse);
+
+/* fine += scale * P coarse on the liquid cells of MG level levelMgFine
+ * (constant interpolation from the parent).  Replaces
+ * prolongateChannel<float>(levelMgFine, chSrc, chDst, 0, alpha)
+ * (src/msbg4.cpp:1920-2030, alpha = MG_CONST_PROLONGATION_ALPHA = 1). */
+int msbg_gpu_prolongate(msbg_gpu_ctx* ctx, int levelMgFine, const float* coarse, int64_t nCoarse,
+                        float* fine, int64_t nFine, float scale);
+
+/* nIter smoothing sweeps of A x = b on MG level levelMg, x updated in place.
+ * Replaces relax(0, reverse, levelMg, chX, chB, chTmp, nIter, 0)
+ * (src/msbg3.cpp:2245-2369).
+ *   mode 0: the solve's smoother: tiles red-black by (level, colour), inside
+ *           each tile innerIter red-black Gauss-Seidel sweeps (reverse = the
+ *           adjoint order of the post-smoother);
+ *   mode 1: the reference's smoother: blocks red-black by (bx+by+bz)&1, in
+ *           each block innerIter damped sweeps over 8-cell x groups (Jacobi
+ *           inside a group, Gauss-Seidel across groups, directions
+ *           alternating, last sweep Jacobi; src/msbg3.cpp:1109-1506,
+ *           2171-2240) with damping omega (the reference's _mgSmOmega,
+ *           src/msbg3.cpp:3088-3093; innerIter = _mgSmBlockIter = 5).  It needs
+ *           one tile per block (16^3 base blocks) and follows the reference
+ *           term by term across same-level faces. */
+int msbg_gpu_relax(msbg_gpu_ctx* ctx, int levelMg, float* x, const float* b, int64_t n, int nIter,
+                   int reverse, int innerIter, int mode, float omega);
+
+/* z = V r on MG level 0 from z = 0: the solve's V-cycle (nPre / nPost
+ * smoothing sweeps of innerIter tile sweeps, fused residual and restriction,
+ * Galerkin coarse levels, FP64 direct coarsest solve, coarse correction
+ * scaled by coarseScale).  Replaces vCycle(0, chZ, chR, chTmp, ...)
+ * (src/msbg3.cpp:2412-2465).  The coarse levels differ: the reference's
+ * restrictPressureMetaFLIP_ reads the fine flags at the coarse block level
+ * (src/msbg3.cpp:2891) and leaves its coarse levels without liquid, so its
+ * V-cycle reduces to the pre- and post-smoothing of level 0. */
+int msbg_gpu_vcycle(msbg_gpu_ctx* ctx, const float* r, float* z, int64_t n, int nPre, int nPost,
+                    int innerIter, float coarseScale);
 
 /* Diagnostics without a GPU (no counterpart in the reference): builds the
  * multigrid hierarchy as msbg_gpu_pressure_prepare does, then on the host

@@ -80,6 +80,9 @@ extern "C" int msbg_gpu_sync(msbg_gpu_ctx* ctx) {
     MSBG_CUDA_TRY(ctx, cudaMemcpy(&h, f, sizeof(int), cudaMemcpyDeviceToHost));
     if (h) {
       cudaMemset(f, 0, sizeof(int));
+      if (h & MCF_ERR_NOT_VALUE)
+        return set_error(ctx, MSBG_EINVARG,
+                         "a listed block is not a value block of the pool (skipped)");
       return set_error(ctx, MSBG_ETIMEOUT, "a kernel gave up a bounded wait");
     }
   }

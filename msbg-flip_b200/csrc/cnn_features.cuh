@@ -16,7 +16,7 @@
 
 constexpr int FEAT_THREADS = 256;
 
-__global__ void __launch_bounds__(FEAT_THREADS) k_cnn_features(
+static __global__ void __launch_bounds__(FEAT_THREADS) k_cnn_features(
     LevelView L, const uint8_t* __restrict__ ctype, const int* __restrict__ tiles,
     const int* __restrict__ tileLevel, float levelNorm, const float* __restrict__ val,
     const double* __restrict__ solution, float* __restrict__ feat, float* __restrict__ outScale,
@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(FEAT_THREADS) k_cnn_features(
 }
 
 // x64[i] = guess[i] on liquid cells, 0 elsewhere.
-__global__ void __launch_bounds__(512) k_set64_masked(double* __restrict__ x,
+static __global__ void __launch_bounds__(512) k_set64_masked(double* __restrict__ x,
                                                       const float* __restrict__ g,
                                                       const float* __restrict__ diag, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;

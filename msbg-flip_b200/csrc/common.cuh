@@ -22,6 +22,12 @@ enum : int {
   SLOT_OUT = -4     // outside the domain: BC_NEUMANN clamp to own block
 };
 
+// Bits of the device error flag that kernels set (msbg_gpu_sync reads it).
+enum : int {
+  ERR_WAIT_TIMEOUT = 1,   // a bounded wait gave up
+  MCF_ERR_NOT_VALUE = 2   // a listed block is not a value block; it was skipped
+};
+
 struct DeviceBuffer {
   void* p = nullptr;
   size_t bytes = 0;

@@ -16,9 +16,12 @@
 // 26-neighbour shell arrive in the padded (BSX+2)^3 tile by asynchronous
 // 4-byte copies (cp.async), every thread's copies in flight at once; with no
 // staging buffer a 16^3 block needs 23 KB and 8 CTAs fill an SM.  The
-// kernel has no waits that could time out, so it never sets errFlag.
+// kernel has no waits that could time out.  A listed block whose slot is not
+// a value block (NULL, const, or a caller's slot map that disagrees with the
+// list) is skipped and reported through errFlag (MCF_ERR_NOT_VALUE).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "common.cuh"
@@ -92,6 +95,10 @@ __global__ void __launch_bounds__(BSX* BSX)
   const int bid = list[blockIdx.x];
   const int bx = bid % nbx, by = (bid / nbx) % nby, bz = bid / (nbx * nby);
   const int slot0 = slotOf[bid];
+  if (slot0 < 0) {  // uniform per CTA, before any barrier or copy
+    if (tid == 0) atomicOr(errFlag, MCF_ERR_NOT_VALUE);
+    return;
+  }
   const float* own = pool + (size_t)slot0 * NV;
 
   if (tid < 27) {
@@ -180,13 +187,18 @@ cudaError_t launch_mcf_t(float* pool, const int* slotOf, const int* colourList,
                          float emptyVal, float fullVal, int nIter, float dt,
                          int clamp01, int* errFlag, cudaStream_t stream) {
   using T = McfTile<BSX>;
-  static bool attrSet = false;
-  if (!attrSet) {
-    cudaError_t e = cudaFuncSetAttribute(mcf_colour_kernel<BSX>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)T::SMEM);
+  // The shared-memory limit is an attribute of the kernel on each device:
+  // set it once per device (bit per device; a race only repeats the call).
+  static std::atomic<uint64_t> attrSet{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
+  if (!bit || !(attrSet.load(std::memory_order_acquire) & bit)) {
+    e = cudaFuncSetAttribute(mcf_colour_kernel<BSX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)T::SMEM);
     if (e != cudaSuccess) return e;
-    attrSet = true;
+    attrSet.fetch_or(bit, std::memory_order_acq_rel);
   }
   for (int it = 0; it < nIter; it++)
     for (int c = 0; c < 8; c++) {

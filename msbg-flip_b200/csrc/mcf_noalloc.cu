@@ -106,7 +106,8 @@ extern "C" int msbg_gpu_pde_mcf_noalloc(float* pool, const int* slotOf, const in
     if (cudaStreamSynchronize(st) != cudaSuccess ||
         cudaMemcpy(&h, errFlag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
       return MSBG_ERROR;
-    *timedOut = h;
+    *timedOut = (h & msbg::ERR_WAIT_TIMEOUT) ? 1 : 0;
+    if (h & msbg::MCF_ERR_NOT_VALUE) return MSBG_EINVARG;  // that block was skipped
     if (h) return MSBG_ETIMEOUT;
   }
   return MSBG_OK;

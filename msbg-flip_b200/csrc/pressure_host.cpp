@@ -19,6 +19,7 @@
 // hierarchy level(b, m) = max(map(b), m) of the reference (src/msbg.cpp:1650).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -705,6 +706,45 @@ int build_hierarchy(Hierarchy& H, int sx, int sy, int sz, int bsx0, int nLevels,
           }
     }
     sample_level0(C, L, fluid);
+    // A liquid cell whose faces all have coefficient 0 is coupled to nothing:
+    // its equation 0 * p = b holds only for b = 0.  The reference gives such a
+    // cell D = 0 and skips it (src/msbg3.cpp:2727, 1284-1285), leaving its
+    // equation unmet; here a consistent one (b = 0) is dropped (p = 0) and an
+    // unsatisfiable one is an error.  A non-finite coefficient is an error too.
+    int64_t badCell = -1;
+    bool badIsolated = false;
+    for (int64_t c = 0; c < L.nCells && badCell < 0; c++) {
+      if (!fluid[c]) continue;
+      if (!std::isfinite(L.diag[c])) {
+        badCell = c;
+      } else if (!(L.diag[c] > 0.f)) {
+        if (L.rhs[c] != 0.f) {
+          badCell = c;
+          badIsolated = true;
+        } else {
+          fluid[c] = 0;
+          L.ctype[c] = CT_SOLID;
+        }
+      }
+    }
+    if (badCell >= 0) {
+      size_t ti = 0;
+      while (ti + 1 < L.tiles.size() && L.tiles[ti + 1].off <= badCell) ti++;
+      const Tile& t = L.tiles[ti];
+      const int64_t e = badCell - t.off;
+      const int X = t.ox + (int)(e % t.ts), Y = t.oy + (int)((e / t.ts) % t.ts),
+                Z = t.oz + (int)(e / ((int64_t)t.ts * t.ts));
+      if (err) {
+        char buf[200];
+        snprintf(buf, sizeof(buf),
+                 badIsolated ? "liquid cell (%d,%d,%d) of level %d has no face with a nonzero "
+                               "coefficient but a nonzero right-hand side"
+                             : "non-finite face coefficient at liquid cell (%d,%d,%d) of level %d",
+                 X, Y, Z, t.level);
+        *err = buf;
+      }
+      return MSBG_EMATH;
+    }
     int64_t nf = 0;
     for (auto f : fluid) nf += f;
     L.nFluid = nf;

@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(512) k_add64(double* __restrict__ x, const VT*
 }
 
 // x32 = (float) x64
-__global__ void __launch_bounds__(512) k_narrow(float* __restrict__ y, const double* __restrict__ x,
+static __global__ void __launch_bounds__(512) k_narrow(float* __restrict__ y, const double* __restrict__ x,
                                                 int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(VEC_BLOCK) k_absmax(const VT* __restrict__ v, 
 }
 
 // Max of the partials into s->amax.
-__global__ void __launch_bounds__(32) k_finalize_max(const double* __restrict__ partial, int n,
+static __global__ void __launch_bounds__(32) k_finalize_max(const double* __restrict__ partial, int n,
                                                      Scalars* s) {
   if (threadIdx.x != 0) return;
   double m = 0;
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(32) k_finalize_max(const double* __restrict__ 
 
 // x64 += alpha d (FP64 accumulation of the FP32 direction); r -= alpha q;
 // partial |r|^2.  Skipped (norm only) after a breakdown.
-__global__ void __launch_bounds__(VEC_BLOCK) k_axpy64_norm(double* __restrict__ x,
+static __global__ void __launch_bounds__(VEC_BLOCK) k_axpy64_norm(double* __restrict__ x,
                                                            float* __restrict__ r,
                                                            const float* __restrict__ d,
                                                            const float* __restrict__ q, int64_t n,
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(VEC_BLOCK) k_axpy64_norm(double* __restrict__ 
 }
 
 // y = a - b (all cells)
-__global__ void __launch_bounds__(VEC_BLOCK) k_sub(float* __restrict__ y, const float* __restrict__ a,
+static __global__ void __launch_bounds__(VEC_BLOCK) k_sub(float* __restrict__ y, const float* __restrict__ a,
                                                    const float* __restrict__ b, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n >> 2);
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(VEC_BLOCK) k_sub(float* __restrict__ y, const 
 }
 
 // v = 0 outside the liquid cells
-__global__ void __launch_bounds__(VEC_BLOCK) k_mask(float* __restrict__ v,
+static __global__ void __launch_bounds__(VEC_BLOCK) k_mask(float* __restrict__ v,
                                                     const float* __restrict__ diag, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(VEC_BLOCK) k_mask(float* __restrict__ v,
 }
 
 // z += omega c
-__global__ void __launch_bounds__(VEC_BLOCK) k_add_omega(float* __restrict__ z,
+static __global__ void __launch_bounds__(VEC_BLOCK) k_add_omega(float* __restrict__ z,
                                                          const float* __restrict__ c,
                                                          const Scalars* __restrict__ s, int64_t n) {
   const float w = (float)s->omega;
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(VEC_BLOCK) k_add_omega(float* __restrict__ z,
 }
 
 // x *= omega (FP64)
-__global__ void __launch_bounds__(VEC_BLOCK) k_scale64(double* __restrict__ x,
+static __global__ void __launch_bounds__(VEC_BLOCK) k_scale64(double* __restrict__ x,
                                                        const Scalars* __restrict__ s, int64_t n) {
   const double w = s->omega;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(VEC_BLOCK) k_scale64(double* __restrict__ x,
 }
 
 // e = a - b (FP64)
-__global__ void __launch_bounds__(VEC_BLOCK) k_sub64(double* __restrict__ e,
+static __global__ void __launch_bounds__(VEC_BLOCK) k_sub64(double* __restrict__ e,
                                                      const double* __restrict__ a,
                                                      const double* __restrict__ b, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;

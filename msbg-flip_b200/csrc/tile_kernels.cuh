@@ -49,7 +49,7 @@ enum {
 
 // Deterministic second stage: fixed-order sum of the CTA partials, then the
 // scalar step of PCG that depends on it.
-__global__ void __launch_bounds__(1024) k_finalize(const double* __restrict__ partial, int n,
+static __global__ void __launch_bounds__(1024) k_finalize(const double* __restrict__ partial, int n,
                                                    Scalars* s, int what) {
   double v = 0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) v += partial[i];

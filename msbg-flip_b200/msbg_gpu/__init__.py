@@ -242,6 +242,22 @@ def _pressure_sigs(L):
         "msbg_gpu_pressure_stats": (i32, [vp, C.POINTER(PressureStats)]),
         "msbg_gpu_pressure_profile": (i32, [vp, i32, i32, i32, C.POINTER(C.c_double),
                                             C.POINTER(C.c_double)]),
+        "msbg_gpu_pressure_prepare_arrays": (i32, [vp, C.POINTER(TopoDesc), C.POINTER(C.c_uint16),
+                                                   C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                                   C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "msbg_gpu_pressure_level_size": (i32, [vp, i32, C.POINTER(C.c_int64)]),
+        "msbg_gpu_pressure_diagonal": (i32, [vp, i32, C.POINTER(C.c_float), C.c_int64]),
+        "msbg_gpu_matvec": (i32, [vp, i32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int64]),
+        "msbg_gpu_residual": (i32, [vp, i32, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                    C.POINTER(C.c_float), C.c_int64]),
+        "msbg_gpu_restrict": (i32, [vp, i32, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_float),
+                                    C.c_int64]),
+        "msbg_gpu_prolongate": (i32, [vp, i32, C.POINTER(C.c_float), C.c_int64,
+                                      C.POINTER(C.c_float), C.c_int64, C.c_float]),
+        "msbg_gpu_relax": (i32, [vp, i32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int64,
+                                 i32, i32, i32, i32, C.c_float]),
+        "msbg_gpu_vcycle": (i32, [vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int64, i32,
+                                  i32, i32, C.c_float]),
         "msbg_gpu_pressure_host_check": (i32, [C.POINTER(TopoDesc), C.POINTER(PressureCallbacks),
                                                C.POINTER(C.c_float), C.POINTER(C.c_double),
                                                C.POINTER(C.c_int), C.POINTER(C.c_int64),
@@ -359,6 +375,95 @@ def _ctx_pressure_download(self, rhs=False, fp64=False):
     return out
 
 
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def _ctx_pressure_prepare_arrays(self, res, bsx0, n_levels, block_levels, flags, face, rhs=None):
+    """msbg_gpu_pressure_prepare_arrays: per-cell flags, lower-face coefficients
+    face[3] and rhs in the packed block layout of MG level 0."""
+    _pressure_sigs(self._L)
+    self._bl_p = np.ascontiguousarray(block_levels, np.int32)
+    d = TopoDesc(res, res, res, bsx0, n_levels, _p(self._bl_p, C.c_int))
+    fl = np.ascontiguousarray(flags, np.uint16)
+    fx, fy, fz = (_f32(f) for f in face)
+    rh = None if rhs is None else _f32(rhs)
+    self._check(self._L.msbg_gpu_pressure_prepare_arrays(
+        self._h, C.byref(d), _p(fl, C.c_uint16), _p(fx, C.c_float), _p(fy, C.c_float),
+        _p(fz, C.c_float), _p(rh, C.c_float)), "pressure_prepare_arrays")
+
+
+def _ctx_level_size(self, level_mg):
+    n = C.c_int64()
+    self._check(self._L.msbg_gpu_pressure_level_size(self._h, level_mg, C.byref(n)), "level_size")
+    return n.value
+
+
+def _ctx_diagonal(self, level_mg=0):
+    out = np.zeros(self.level_size(level_mg), np.float32)
+    self._check(self._L.msbg_gpu_pressure_diagonal(self._h, level_mg, _p(out, C.c_float),
+                                                   len(out)), "pressure_diagonal")
+    return out
+
+
+def _ctx_matvec(self, level_mg, x):
+    x = _f32(x)
+    y = np.zeros_like(x)
+    self._check(self._L.msbg_gpu_matvec(self._h, level_mg, _p(x, C.c_float), _p(y, C.c_float),
+                                        len(x)), "matvec")
+    return y
+
+
+def _ctx_residual(self, level_mg, x, b):
+    x, b = _f32(x), _f32(b)
+    r = np.zeros_like(x)
+    self._check(self._L.msbg_gpu_residual(self._h, level_mg, _p(x, C.c_float), _p(b, C.c_float),
+                                          _p(r, C.c_float), len(x)), "residual")
+    return r
+
+
+def _ctx_restrict(self, level_mg_coarse, fine):
+    fine = _f32(fine)
+    coarse = np.zeros(self.level_size(level_mg_coarse), np.float32)
+    self._check(self._L.msbg_gpu_restrict(self._h, level_mg_coarse, _p(fine, C.c_float), len(fine),
+                                          _p(coarse, C.c_float), len(coarse)), "restrict")
+    return coarse
+
+
+def _ctx_prolongate(self, level_mg_fine, coarse, fine, scale=1.0):
+    coarse = _f32(coarse)
+    out = _f32(fine).copy()
+    self._check(self._L.msbg_gpu_prolongate(self._h, level_mg_fine, _p(coarse, C.c_float),
+                                            len(coarse), _p(out, C.c_float), len(out), scale),
+                "prolongate")
+    return out
+
+
+def _ctx_relax(self, level_mg, x, b, n_iter, reverse=0, inner=3, mode=0, omega=1.0):
+    out = _f32(x).copy()
+    b = _f32(b)
+    self._check(self._L.msbg_gpu_relax(self._h, level_mg, _p(out, C.c_float), _p(b, C.c_float),
+                                       len(out), n_iter, reverse, inner, mode, omega), "relax")
+    return out
+
+
+def _ctx_vcycle(self, r, n_pre=2, n_post=2, inner=3, coarse_scale=1.8):
+    r = _f32(r)
+    z = np.zeros_like(r)
+    self._check(self._L.msbg_gpu_vcycle(self._h, _p(r, C.c_float), _p(z, C.c_float), len(r), n_pre,
+                                        n_post, inner, coarse_scale), "vcycle")
+    return z
+
+
+Context.pressure_prepare_arrays = _ctx_pressure_prepare_arrays
+Context.level_size = _ctx_level_size
+Context.diagonal = _ctx_diagonal
+Context.matvec = _ctx_matvec
+Context.residual = _ctx_residual
+Context.restrict = _ctx_restrict
+Context.prolongate = _ctx_prolongate
+Context.relax = _ctx_relax
+Context.vcycle = _ctx_vcycle
 Context.pressure_prepare = _ctx_pressure_prepare
 Context.pressure_solve = _ctx_pressure_solve
 Context.pressure_download = _ctx_pressure_download

@@ -56,6 +56,18 @@ int oracle_pressure_apply(int sx, int sy, int sz, int bsx0, const int* blockLeve
                           oracle_cell_type_fn cellType, oracle_face_fn face, void* user,
                           const double* x, double* y);
 
+/* Callbacks over per-cell arrays in the packed block layout of MG level 0:
+ * flags, lower-face coefficient per direction, rhs (see
+ * msbg_oracle_pressure.c).  The user pointer comes from
+ * oracle_array_scene_create; the arrays must outlive it. */
+void* oracle_array_scene_create(int sx, int sy, int sz, int bsx0, const int* lev,
+                                const unsigned short* flags, const float* fx, const float* fy,
+                                const float* fz, const float* rhs);
+void oracle_array_scene_destroy(void* scene);
+unsigned short oracle_array_cell_type(void* scene, int x, int y, int z);
+float oracle_array_face(void* scene, int dir, int x, int y, int z);
+float oracle_array_rhs(void* scene, int x, int y, int z);
+
 #ifdef __cplusplus
 }
 #endif

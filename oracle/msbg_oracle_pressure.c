@@ -287,3 +287,85 @@ int oracle_pressure_solve(int sx, int sy, int sz, int bsx0, const int* blockLeve
   free(g.boff);
   return 0;
 }
+
+/* ---- array-backed scene ----------------------------------------------------
+ * Callbacks that read per-cell arrays in the packed block layout of MG level 0
+ * (blocks in bid order, (bsx0>>L)^3 cells each at the block's level L): cell
+ * flags, the LOWER face coefficient per direction and the rhs.  A fine voxel
+ * maps to the level-L cell that contains it.  Outside the domain a cell is
+ * solid and a face has coefficient 0 (the reference's getValueGen_ reads 0
+ * there, src/msbg3.cpp:2700-2708).  Used to feed the reference's own prepared
+ * channels (preparePressureSolveFLIPLevel0_, src/msbg3.cpp:2472-2584) to the
+ * oracle, so both assemble from identical inputs. */
+typedef struct {
+  int sx, sy, sz, bsx0, nbx, nby;
+  const int* lev;
+  int64_t* boff;
+  const unsigned short* flags;
+  const float* face[3];
+  const float* rhs;
+} ArrayScene;
+
+static int64_t array_cell(const ArrayScene* a, int x, int y, int z) {
+  if (x < 0 || y < 0 || z < 0 || x >= a->sx || y >= a->sy || z >= a->sz) return -1;
+  const int64_t b = (x / a->bsx0) + (int64_t)a->nbx * ((y / a->bsx0) + (int64_t)a->nby * (z / a->bsx0));
+  const int L = a->lev[b], bs = a->bsx0 >> L;
+  const int vx = (x % a->bsx0) >> L, vy = (y % a->bsx0) >> L, vz = (z % a->bsx0) >> L;
+  return a->boff[b] + vx + (int64_t)bs * (vy + (int64_t)bs * vz);
+}
+
+void* oracle_array_scene_create(int sx, int sy, int sz, int bsx0, const int* lev,
+                                const unsigned short* flags, const float* fx, const float* fy,
+                                const float* fz, const float* rhs) {
+  ArrayScene* a = (ArrayScene*)calloc(1, sizeof(ArrayScene));
+  if (!a) return NULL;
+  a->sx = sx;
+  a->sy = sy;
+  a->sz = sz;
+  a->bsx0 = bsx0;
+  a->nbx = sx / bsx0;
+  a->nby = sy / bsx0;
+  const int64_t nb = (int64_t)a->nbx * a->nby * (sz / bsx0);
+  a->boff = (int64_t*)malloc(sizeof(int64_t) * (nb + 1));
+  if (!a->boff) {
+    free(a);
+    return NULL;
+  }
+  a->boff[0] = 0;
+  for (int64_t b = 0; b < nb; b++) {
+    const int bs = bsx0 >> lev[b];
+    a->boff[b + 1] = a->boff[b] + (int64_t)bs * bs * bs;
+  }
+  a->lev = lev;
+  a->flags = flags;
+  a->face[0] = fx;
+  a->face[1] = fy;
+  a->face[2] = fz;
+  a->rhs = rhs;
+  return a;
+}
+
+void oracle_array_scene_destroy(void* p) {
+  ArrayScene* a = (ArrayScene*)p;
+  if (!a) return;
+  free(a->boff);
+  free(a);
+}
+
+unsigned short oracle_array_cell_type(void* p, int x, int y, int z) {
+  const ArrayScene* a = (const ArrayScene*)p;
+  const int64_t c = array_cell(a, x, y, z);
+  return c < 0 ? (unsigned short)0x1 : a->flags[c];
+}
+
+float oracle_array_face(void* p, int dir, int x, int y, int z) {
+  const ArrayScene* a = (const ArrayScene*)p;
+  const int64_t c = array_cell(a, x, y, z);
+  return c < 0 ? 0.f : a->face[dir][c];
+}
+
+float oracle_array_rhs(void* p, int x, int y, int z) {
+  const ArrayScene* a = (const ArrayScene*)p;
+  const int64_t c = array_cell(a, x, y, z);
+  return c < 0 || !a->rhs ? 0.f : a->rhs[c];
+}

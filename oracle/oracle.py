@@ -154,3 +154,58 @@ def pressure_apply_oracle(scene, x):
     if rc:
         raise RuntimeError(f"oracle_pressure_apply rc={rc}")
     return y
+
+
+class ArrayScene:
+    """Pressure problem given by per-cell arrays in the packed block layout of
+    MG level 0 (flags, lower-face coefficients per direction, rhs), with the
+    interface of msbg_gpu.PressureScene that the oracle functions read.  Its
+    callbacks are C functions of the oracle library
+    (oracle_array_scene_*, oracle/msbg_oracle_pressure.c)."""
+
+    def __init__(self, res, bsx0, n_levels, block_levels, flags, face, rhs):
+        L = oracle()
+        if not hasattr(L, "_arr_sig"):
+            L.oracle_array_scene_create.restype = C.c_void_p
+            L.oracle_array_scene_create.argtypes = [C.c_int] * 4 + [
+                C.POINTER(C.c_int), C.POINTER(C.c_uint16)] + [C.POINTER(C.c_float)] * 4
+            L.oracle_array_scene_destroy.argtypes = [C.c_void_p]
+            L._arr_sig = True
+        self._L = L
+        self.res, self.bsx0, self.n_levels = res, bsx0, n_levels
+        self.block_levels = np.ascontiguousarray(block_levels, np.int32)
+        self.flags = np.ascontiguousarray(flags, np.uint16)
+        self.face = [np.ascontiguousarray(f, np.float32) for f in face]
+        self.rhs = np.ascontiguousarray(rhs, np.float32)
+        self.h = L.oracle_array_scene_create(res, res, res, bsx0, _p(self.block_levels, C.c_int),
+                                             _p(self.flags, C.c_uint16),
+                                             *[_p(f, C.c_float) for f in self.face],
+                                             _p(self.rhs, C.c_float))
+        if not self.h:
+            raise MemoryError("oracle_array_scene_create")
+
+    def callbacks(self):
+        L = self._L
+
+        class _Cb:
+            pass
+        cb = _Cb()
+        cb.sampleCellType = C.cast(L.oracle_array_cell_type, C.c_void_p).value
+        cb.sampleFaceCoeff = C.cast(L.oracle_array_face, C.c_void_p).value
+        cb.sampleRhs = C.cast(L.oracle_array_rhs, C.c_void_p).value
+        cb.user = self.h
+        return cb
+
+    def packed_size(self):
+        return int(sum((self.bsx0 >> int(l)) ** 3 for l in self.block_levels))
+
+    def close(self):
+        if self.h:
+            self._L.oracle_array_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
