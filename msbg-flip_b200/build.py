@@ -1,8 +1,11 @@
-"""In-tree build of the sm_100a solver library (libmsbg_gpu.so).
+"""In-tree build of the sm_100a solver library (libmsbg_gpu.so) and of the
+synthetic-scene library (libmsbg_scene.so).
 
 Compiles every CUDA/C++ source under csrc/ with nvcc for sm_100a and links
-them, with the static CUDA runtime, into ``libmsbg_gpu.so`` next to this file.
-Run ``python msbg-flip_b200/build.py`` or call :func:`build`.
+them, with the static CUDA runtime, into ``libmsbg_gpu.so`` next to this file;
+compiles scene/scene.cpp (host C++/OpenMP, the seeded input generators) into
+``libmsbg_scene.so``.  Run ``python msbg-flip_b200/build.py`` or call
+:func:`build`.
 """
 from __future__ import annotations
 
@@ -17,6 +20,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmsbg_gpu.so")
+SCENE_SRC = os.path.join(HERE, "scene", "scene.cpp")
+SCENE_LIB = os.path.join(HERE, "libmsbg_scene.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp,-O3",
@@ -76,10 +81,20 @@ def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
 
     with ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
         list(ex.map(run, jobs))
-    if jobs or force or not os.path.exists(LIB):
+    # relink when a source was compiled, added or removed
+    stamp = os.path.join(OBJ, "objects.txt")
+    listed = open(stamp).read() if os.path.exists(stamp) else ""
+    if jobs or force or not os.path.exists(LIB) or listed != "\n".join(objs):
         cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + \
             ["-Xcompiler", "-fopenmp", "-lgomp", "-cudart", "static"]
         run(cmd)
+        with open(stamp, "w") as f:
+            f.write("\n".join(objs))
+    hdr_scene = os.path.getmtime(os.path.join(ROOT, "include", "msbg_scene.h"))
+    if force or not os.path.exists(SCENE_LIB) or \
+            os.path.getmtime(SCENE_LIB) < max(os.path.getmtime(SCENE_SRC), hdr_scene):
+        run(["g++", "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-shared",
+             "-I" + os.path.join(ROOT, "include"), SCENE_SRC, "-o", SCENE_LIB])
     return LIB
 
 

@@ -14,6 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 LIB_PATH = os.path.join(PKG, "libmsbg_gpu.so")
+SCENE_LIB_PATH = os.path.join(PKG, "libmsbg_scene.so")
 
 MSBG_OK = 0
 STATUS = {0: "MSBG_OK", 1: "MSBG_ERROR", 2: "MSBG_ENOMEM", 4: "MSBG_ENOTIMPL",
@@ -26,6 +27,7 @@ BLOCK_NULL, BLOCK_VALUE, BLOCK_EMPTY, BLOCK_FULL = 0, 1, 2, 3
 F32, F16, BF16, F64 = 0, 1, 2, 3
 
 _lib = None
+_scene_lib = None
 
 
 class MsbgError(RuntimeError):
@@ -68,8 +70,6 @@ def lib():
         "msbg_gpu_pde_mcf": (i32, [vp, i32, pi32, i32, i32, f32, i32]),
         "msbg_gpu_pde_mcf_device": (i32, [vp, vp, vp, vp, pi32, i32, i32, i32, i32, f32, f32,
                                           i32, f32, i32, vp]),
-        "msbg_scene_sphere_sdf": (i32, [i32, i32, i32, f32, f32, f32, i32, C.c_uint64, pi8, pf32,
-                                        C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -79,13 +79,40 @@ def lib():
     return L
 
 
+def scene_lib():
+    """Load libmsbg_scene.so, the seeded input generators (include/msbg_scene.h).
+    It is separate from the solver library and does not load it."""
+    global _scene_lib
+    if _scene_lib is not None:
+        return _scene_lib
+    if not os.path.exists(SCENE_LIB_PATH):
+        raise ImportError(f"{SCENE_LIB_PATH} missing: run msbg-flip_b200/build.py")
+    L = C.CDLL(SCENE_LIB_PATH)
+    vp, i32, f32 = C.c_void_p, C.c_int, C.c_float
+    sig = {
+        "msbg_scene_sphere_sdf": (i32, [i32, i32, i32, f32, f32, f32, i32, C.c_uint64,
+                                        C.POINTER(C.c_int8), C.POINTER(C.c_float),
+                                        C.POINTER(C.c_int64)]),
+        "msbg_scene_pressure_create": (vp, [i32, i32, i32, f32, i32, f32, f32, i32, i32, i32, f32,
+                                            C.c_uint64]),
+        "msbg_scene_pressure_destroy": (None, [vp]),
+        "msbg_scene_pressure_block_levels": (i32, [vp, C.POINTER(C.c_int)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _scene_lib = L
+    return L
+
+
 def sphere_sdf_scene(res, bsx, n_spheres=64, rmin=20.0, rmax=60.0, band=4.0, dilate=1,
                      seed=1234, with_values=True):
     """Seeded union-of-spheres signed distance field on a single-level grid.
 
     Returns (kind[nb] int8, values[nValue, bsx, bsx, bsx] float32 or None).
     """
-    L = lib()
+    L = scene_lib()
     nb = (res // bsx) ** 3
     kind = np.zeros(nb, np.int8)
     nval = C.c_int64(0)
@@ -228,10 +255,6 @@ class PressureStats(C.Structure):
 def _pressure_sigs(L):
     vp, i32 = C.c_void_p, C.c_int
     sig = {
-        "msbg_scene_pressure_create": (vp, [i32, i32, i32, C.c_float, i32, C.c_float, C.c_float,
-                                            i32, i32, i32, C.c_float, C.c_uint64]),
-        "msbg_scene_pressure_destroy": (None, [vp]),
-        "msbg_scene_pressure_block_levels": (i32, [vp, C.POINTER(C.c_int)]),
         "msbg_gpu_solve_params_default": (None, [C.POINTER(SolveParams)]),
         "msbg_gpu_pressure_prepare": (i32, [vp, C.POINTER(TopoDesc), C.POINTER(PressureCallbacks)]),
         "msbg_gpu_pressure_solve": (i32, [vp, C.POINTER(SolveParams), C.POINTER(SolveInfo)]),
@@ -274,8 +297,7 @@ class PressureScene:
 
     def __init__(self, res, bsx0, n_levels, z_liquid=0.4, n_spheres=32, r_min=0.03, r_max=0.1,
                  n_cuboids=8, n_modes=16, k_max=8, band=64.0, seed=2024):
-        L = lib()
-        _pressure_sigs(L)
+        L = scene_lib()
         self._L = L
         self.res, self.bsx0, self.n_levels = res, bsx0, n_levels
         self.h = L.msbg_scene_pressure_create(res, bsx0, n_levels, z_liquid, n_spheres, r_min,

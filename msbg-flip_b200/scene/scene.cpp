@@ -1,4 +1,9 @@
 // Seeded synthetic workloads (host side).  See include/msbg_scene.h.
+//
+// Built into its own library, libmsbg_scene.so, apart from the solver
+// library: the tests, the benchmark and the reference CPU baseline all load
+// it to produce identical inputs, and the reference's timed path never loads
+// the solver library.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>

@@ -20,6 +20,10 @@ OUT = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(OUT, "libmsbg_oracle.so")
 REF_SO = os.path.join(OUT, "libmsbg_ref.so")
 
+# The reference tree the recipe compiles: $MSBG_REFERENCE, else its usual
+# mount point.  Only the build reads it; the prebuilt libraries need no tree.
+REFERENCE_ROOT = os.environ.get("MSBG_REFERENCE", "/root/reference")
+
 _oracle = None
 _ref = None
 
@@ -32,7 +36,7 @@ def build_oracle():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def build_ref(ref_root="/root/reference"):
+def build_ref(ref_root=REFERENCE_ROOT):
     if not os.path.isdir(os.path.join(ref_root, "src")):
         return False
     subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF_ROOT={ref_root}"], check=True)

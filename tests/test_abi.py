@@ -11,25 +11,43 @@ import msbg_gpu
 from conftest import ROOT
 
 
-def declared_symbols():
+def declared_symbols(header):
     syms = set()
-    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
-        src = open(h).read()
-        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        for m in re.finditer(r"^\s*(?:const\s+)?[\w\s\*]+?\b(msbg_\w+)\s*\(", src, re.M):
-            syms.add(m.group(1))
+    src = open(os.path.join(ROOT, "include", header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    for m in re.finditer(r"^\s*(?:const\s+)?[\w\s\*]+?\b(msbg_\w+)\s*\(", src, re.M):
+        syms.add(m.group(1))
     return syms
 
 
-def test_library_exports_every_declared_symbol():
+def exported(path):
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True,
+                         check=True).stdout
+    return {l.split()[-1] for l in out.splitlines() if l.strip()}
+
+
+# each header and the library that implements it
+LIBS = {"msbg_gpu.h": msbg_gpu.LIB_PATH, "msbg_cnn.h": msbg_gpu.LIB_PATH,
+        "msbg_scene.h": msbg_gpu.SCENE_LIB_PATH}
+
+
+def test_every_header_has_its_library():
+    heads = {os.path.basename(h) for h in glob.glob(os.path.join(ROOT, "include", "*.h"))}
+    assert heads == set(LIBS)
+
+
+@pytest.mark.parametrize("header", sorted(LIBS))
+def test_library_exports_every_declared_symbol(header):
     msbg_gpu.lib()
-    out = subprocess.run(["nm", "-D", "--defined-only", msbg_gpu.LIB_PATH], capture_output=True,
-                         text=True, check=True).stdout
-    exported = {l.split()[-1] for l in out.splitlines() if l.strip()}
-    decl = declared_symbols()
-    assert len(decl) >= 10
-    missing = decl - exported
+    msbg_gpu.scene_lib()
+    decl = declared_symbols(header)
+    assert len(decl) >= 5
+    missing = decl - exported(LIBS[header])
     assert not missing, missing
+
+
+def test_solver_library_holds_no_scene_generator():
+    assert not any(s.startswith("msbg_scene") for s in exported(msbg_gpu.LIB_PATH))
 
 
 def test_library_is_sm100a():
