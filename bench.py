@@ -1,19 +1,34 @@
 #!/usr/bin/env python
 """Benchmark of the B200 sparse block-grid PDE solver.
 
-Default workload ``mgpcg`` — the FLIP pressure solve on a 2-level adaptive
+Default workload ``mgpcg`` - the FLIP pressure solve on a 2-level adaptive
 MSBG at 1024^3 effective resolution: 32^3 base blocks, level 0 within 64
 voxels of the liquid surface and 2x coarser elsewhere, liquid = half-space
 z < 0.4 plus 32 seeded spheres, 8 seeded solid cuboids, Dirichlet p = 0 in
 air, Neumann at walls and solids, RHS = MAC divergence of 16 random Fourier
-modes (|k|_inf 1..8, N(0,1) amplitudes).  One step = one plain FP32 MGPCG
-solve from p = 0 to relative residual 1e-6 (V(2,2) preconditioner) on the
-resident operator.  value = liquid cells x PCG iterations / solve time
-(Gvoxel/s per iteration); the time to 1e-6 is reported beside it.
+modes (|k|_inf 1..8, N(0,1) amplitudes).
 
-Workload ``mcf``: the 8-colour mean-curvature-flow smoother at 512^3
-(16^3 blocks, band +-4 around 64 seeded spheres, 20 iterations, dt 0.1).
+One step = one MGPCG solve from p = 0 to a TRUE relative residual of 1e-6
+(|b - A x| / |b| recomputed in FP64): V(2,2) preconditioner, FP32 level-0
+vectors, the solution accumulated in FP64 with reliable residual
+replacement, FP64 inner products, FP64 coarsest solve.  value = liquid cells
+x PCG iterations / device solve time (Gvoxel/s per iteration); ms_per_step
+is the time to 1e-6.  Beside it, in the same line, each over --steps timed
+calls after one warm-up:
+  - the plain FP32 solve that stops on its recursive residual (the
+    reference's criterion; its true residual stalls near 1e-4);
+  - FP16 and BF16 level-0 storage under FP64 iterative refinement;
+  - the learned variants (networks trained in this run on the GPU);
+  - the error against the FP64 oracle, on the same scene family at 256^3
+    (a CPU FP64 solve at 1024^3 is out of reach; stated as a proxy);
+  - the same solve on the reference's runnable analogue (1024^3 with 16^3
+    base blocks: the reference's smoother aborts for 32^3 blocks,
+    src/msbg3.cpp:1692-1749), next to the reference's own CPU solver on it;
+  - the mean-curvature-flow smoother at 512^3 (16^3 blocks, band +-4 around
+    64 seeded spheres, 20 iterations, dt 0.1) with its roofline and the
+    reference's CPU smoother on the same input.
 
+``--workload mcf`` benches only the smoother.
 ``--impl reference`` times the reference's own CPU implementation (compiled
 from its sources into oracle/_ref/libmsbg_ref.so) with all host threads.
 
@@ -42,10 +57,12 @@ METRIC = "MGPCG time-to-1e-6 & Gvoxel/s/iter: learned+mixed vs plain FP32, one B
 PS_CFG = dict(res=1024, bsx0=32, n_levels=2, z_liquid=0.4, n_spheres=32, r_min=0.03, r_max=0.1,
               n_cuboids=8, n_modes=16, k_max=8, band=64.0, seed=2024, tol=1e-6, n_pre=2,
               n_post=2, inner=3)
-# bounded analogue of the pressure workload the reference CPU solver can run:
-# it aborts for 32^3 base blocks (src/msbg3.cpp:1692-1749), so 16^3 blocks,
-# a quarter of the resolution and the band scaled alike.
-PS_REF_CFG = dict(res=256, bsx0=16, n_levels=2, band=16.0, iters=10)
+# the reference's runnable analogue: same scene with 16^3 base blocks (its
+# smoother aborts for 32^3 blocks, src/msbg3.cpp:1692-1749)
+PS_SAME_CFG = dict(PS_CFG, bsx0=16)
+REF_ITERS = 2        # PCG iterations per timed reference call
+# the scene family at 256^3 where the FP64 oracle solves in seconds
+ERR_RES = 256
 
 MCF_CFG = dict(res=512, bsx=16, n_spheres=64, rmin=20.0, rmax=60.0, band=4.0, dilate=1,
                seed=1234, iters=20, dt=0.1)
@@ -149,6 +166,10 @@ def max_over_ranks(dist, v, dev):
     return float(t.item())
 
 
+def workload_name(c):
+    return f"flip_pressure_mgpcg_{c['res']}_b{c['bsx0']}_{c['n_levels']}lvl"
+
+
 # ---------------------------------------------------------------------------
 # pressure workload
 # ---------------------------------------------------------------------------
@@ -167,41 +188,62 @@ def ps_stats(ctx):
     return st
 
 
-def cpu_reference_ps(max_seconds=60.0):
-    """Reference solvePressureFLIP (all host threads) on the bounded analogue."""
+def solve_params(c, **kw):
+    import msbg_gpu
+    return msbg_gpu.solve_params(nPre=c["n_pre"], nPost=c["n_post"], tol=c["tol"],
+                                 innerIter=c["inner"], useGraph=1, **kw)
+
+
+def timed_solves(ctx, params, warmup, steps):
+    """warmup untimed solves, then `steps` solves; their solve infos."""
+    for _ in range(warmup):
+        ctx.pressure_solve(params)
+    return [ctx.pressure_solve(params) for _ in range(steps)]
+
+
+def summarize(infos, fluid):
+    secs = sum(i.solveSeconds for i in infos)
+    its = sum(i.iterations for i in infos)
+    return {"ms": secs / len(infos) * 1e3, "gvoxel_s_iter": fluid * its / secs / 1e9,
+            "calls": len(infos), "pcg_iterations": [i.iterations for i in infos][:3],
+            "refinements": infos[-1].refinements, "status": max(i.status for i in infos),
+            "true_rel_residual": max(i.relResidual for i in infos)}
+
+
+def ref_pressure_rate(cfg, max_seconds=40.0):
+    """The reference's solvePressureFLIP (all host threads) on a scene:
+    prepare (untimed), one warm-up iteration, then calls of REF_ITERS PCG
+    iterations until max_seconds/2 or 3 calls.  Liquid cells are counted
+    from the reference's own prepared flags."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    c = dict(PS_CFG)
-    c.update(PS_REF_CFG)
     cores = os.cpu_count() or 1
     if not oracle.ref_available():
         return {"value": None, "unit": "Gvoxel/s/iter", "cores": cores, "kind": "reference",
                 "sample": "unavailable: oracle/_ref/libmsbg_ref.so not built"}
     import ref_pressure
     oracle.ref().ref_init(cores)
-    scene = ps_scene(c)
+    scene = ps_scene(cfg)
     r = ref_pressure.RefPressure(scene)
-    # liquid cells of the analogue (from our FP64 oracle's assembly of the same scene)
-    import msbg_gpu
-    nfl = msbg_gpu.count_liquid_cells(scene)
+    nfl = int(r.liquid().sum())
     r.solve(max_iter=1)  # warm-up (allocations inside the first V-cycle)
-    times, iters = [], []
+    times, iters, rr = [], [], None
     t0 = time.perf_counter()
     while True:
-        it, rr, secs = r.solve(max_iter=c["iters"])
+        it, rr, secs = r.solve(max_iter=REF_ITERS)
         times.append(secs)
         iters.append(it)
         if time.perf_counter() - t0 > max_seconds * 0.5 or len(times) >= 3:
             break
+    prep = r.prep_seconds
     r.close()
-    rate = nfl * sum(iters) / sum(times) / 1e9
-    return {"value": rate, "unit": "Gvoxel/s/iter", "cores": cores, "kind": "reference",
-            "sample": (f"reference solvePressureFLIP (V(2,2)-PCG, src/msbg3.cpp:3098) on the "
-                       f"{c['res']}^3, {c['bsx0']}^3-block, 2-level analogue of the workload "
-                       f"(band {c['band']:.0f}), {c['iters']} iterations per call, "
-                       f"{len(times)} calls; {nfl} liquid cells; prepare {r.prep_seconds:.1f}s "
-                       f"not counted; its |r|/|b| after {c['iters']} its: {rr:.2e} "
-                       f"(it does not reach 1e-6)")}
+    return {"value": nfl * sum(iters) / sum(times) / 1e9, "unit": "Gvoxel/s/iter",
+            "cores": cores, "kind": "reference", "liquid_cells": nfl,
+            "sample": (f"reference solvePressureFLIP (V(2,2)-PCG, src/msbg3.cpp:3098) on "
+                       f"{workload_name(cfg)}: {len(times)} calls of {REF_ITERS} PCG "
+                       f"iterations after a 1-iteration warm-up; {nfl} liquid cells (its own "
+                       f"flags); prepare {prep:.1f} s not counted; |r|/|b| after "
+                       f"{REF_ITERS} iterations {rr:.3g} (it does not reach 1e-6)")}
 
 
 def bench_reference(args):
@@ -210,14 +252,20 @@ def bench_reference(args):
         return
     if args.workload == "mcf":
         return bench_reference_mcf(args)
-    cb = cpu_reference_ps(max_seconds=120.0)
+    c = dict(PS_SAME_CFG)
+    cb = ref_pressure_rate(c, max_seconds=60.0)
+    kind, vals, upd = mcf_scene()
+    mcf = cpu_reference_mcf(kind, vals, upd)
     line = {"metric": METRIC, "value": cb["value"], "unit": "Gvoxel/s/iter", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded free-surface pressure problem)", "impl": "reference",
-            "config": {"workload": "flip_pressure_mgpcg_analogue_256_b16_2lvl",
-                       "time_to_1e-6": "not reached (reference MGPCG stalls)",
-                       "parallelism": "cpu"},
+            "config": {"workload": workload_name(c),
+                       "note": ("the reference's runnable analogue of "
+                                f"{workload_name(PS_CFG)}: same scene with 16^3 base blocks "
+                                "(its smoother aborts for 32^3 blocks)"),
+                       "time_to_1e-6": "not reached (the reference MGPCG stalls)",
+                       "mcf_512_b16": mcf, "parallelism": "cpu"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "Gvoxel/s/iter", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -233,9 +281,10 @@ LEARN_CFG = dict(res=512, seeds=(100, 101, 102, 103), pairs_per_instance=500, ep
                  batch=64, lr=2e-3)
 
 
-def learned_variants(ctx, c, scene):
+def learned_variants(ctx, c, scene, fluid, steps):
     """Train the guess and correction networks on the GPU, then time the
-    learned solves of the bench problem (FP64 refinement to 1e-6)."""
+    learned solves of the bench problem (FP64 refinement to 1e-6), one
+    warm-up and `steps` timed calls each."""
     import torch
     import msbg_gpu
     L = LEARN_CFG
@@ -271,17 +320,12 @@ def learned_variants(ctx, c, scene):
                                 ("f16_vectors_learned_guess", msbg_gpu.F16, 1),
                                 ("f32_vectors_learned_correction", msbg_gpu.F32, 2),
                                 ("f32_vectors_learned_guess_and_correction", msbg_gpu.F32, 3)):
-        vp = msbg_gpu.solve_params(nPre=c["n_pre"], nPost=c["n_post"], tol=c["tol"],
-                                   innerIter=c["inner"], useGraph=1, storage=storage,
-                                   maxRefine=30, learned=mode)
-        ctx.pressure_solve(vp)
-        vi = ctx.pressure_solve(vp)
-        out[name] = {
-            "ms": vi.solveSeconds * 1e3, "pcg_iterations": vi.iterations,
-            "refinements": vi.refinements, "status": vi.status,
-            "fallback_to_plain": vi.learnedFallback,
-            "initial_rel_residual": vi.initialRelResidual,
-            "true_rel_residual_fp64": vi.relResidual}
+        vp = solve_params(c, storage=storage, maxRefine=30, learned=mode)
+        infos = timed_solves(ctx, vp, 1, steps)
+        s = summarize(infos, fluid)
+        s["fallback_to_plain"] = max(i.learnedFallback for i in infos)
+        s["initial_rel_residual"] = infos[-1].initialRelResidual
+        out[name] = s
     ctx.pressure_set_cnn(None)
     ctx.pressure_set_correction_cnn(None)
     net.close()
@@ -289,29 +333,30 @@ def learned_variants(ctx, c, scene):
     return out
 
 
-def bench_part(args):
-    """One solver part (a level-0 smoothing sweep, the level-0 matvec or a
-    V-cycle) of the pressure workload, timed through msbg_gpu_pressure_profile:
-    one warm-up call, then --steps calls.  Prints the level-0 cell count so a
-    capture's DRAM bytes can be put per cell."""
-    import torch
+def error_vs_oracle(ctx, c):
+    """Error of the GPU solutions (FP32, FP16, BF16 level-0 vectors, each to a
+    true FP64 residual of 1e-6) against the FP64 oracle (Jacobi-PCG to 1e-11
+    on the same system), on the bench's scene family at ERR_RES^3."""
     import msbg_gpu
-    torch.cuda.set_device(0)
-    c = dict(PS_CFG)
-    if args.res:
-        c["res"] = args.res
-        c["band"] = PS_CFG["band"] * args.res / PS_CFG["res"]
-    ctx = msbg_gpu.Context(0)
-    ctx.pressure_prepare(ps_scene(c))
-    st = ps_stats(ctx)
-    what = {"smooth": 0, "matvec": 1, "vcycle": 2}[args.part]
-    storage = {"f32": msbg_gpu.F32, "f16": msbg_gpu.F16, "bf16": msbg_gpu.BF16}[args.storage]
-    ms, by = ctx.pressure_profile(what | (storage << 4), max(1, args.steps), c["inner"])
-    print(json.dumps({"part": args.part, "storage": args.storage, "res": c["res"],
-                      "cells_level0": int(st.cells[0]), "ms_per_call": ms,
-                      "alg_bytes_per_call": by, "achieved_gbs": by / (ms * 1e-3) / 1e9}),
-          flush=True)
-    ctx.close()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    e = dict(c, res=ERR_RES, band=c["band"] * ERR_RES / c["res"])
+    scene = ps_scene(e)
+    t0 = time.perf_counter()
+    xo, _, its, rr = oracle.pressure_oracle(scene, tol=1e-11)
+    oracle_s = time.perf_counter() - t0
+    ctx.pressure_prepare(scene)
+    nrm = float(np.linalg.norm(xo))
+    mx = float(np.abs(xo).max())
+    out = {"workload": workload_name(e), "oracle": f"FP64 Jacobi-PCG, {its} iterations, "
+           f"true |r|/|b| {rr:.2e}, {oracle_s:.1f} s on {os.cpu_count()} host threads"}
+    for name, storage in (("f32", msbg_gpu.F32), ("f16", msbg_gpu.F16), ("bf16", msbg_gpu.BF16)):
+        info = ctx.pressure_solve(solve_params(c, storage=storage, maxRefine=30))
+        x = ctx.pressure_download(fp64=True)
+        out[name] = {"rel_l2_err": float(np.linalg.norm(x - xo)) / nrm,
+                     "max_abs_err_rel": float(np.abs(x - xo).max()) / mx,
+                     "true_rel_residual": info.relResidual, "status": info.status}
+    return out
 
 
 def bench_mgpcg(args):
@@ -329,8 +374,9 @@ def bench_mgpcg(args):
     scene = ps_scene(c)
     ctx.pressure_prepare(scene)
     st = ps_stats(ctx)
-    params = msbg_gpu.solve_params(nPre=c["n_pre"], nPost=c["n_post"], tol=c["tol"],
-                                   innerIter=c["inner"], useGraph=1)
+    fluid = int(st.fluid[0])
+    # the step: MGPCG to a true FP64 residual of 1e-6, FP32 level-0 vectors
+    params = solve_params(c, storage=msbg_gpu.F32, maxRefine=30)
     for _ in range(args.warmup):
         ctx.pressure_solve(params)
     torch.cuda.synchronize()
@@ -343,48 +389,20 @@ def bench_mgpcg(args):
             infos.append(ctx.pressure_solve(params))
         torch.cuda.synchronize()
     clocks = clk.summary()
-    solve_s = sum(i.solveSeconds for i in infos)
-    solve_s = max_over_ranks(dist, solve_s, dev)
+    solve_s = max_over_ranks(dist, sum(i.solveSeconds for i in infos), dev)
     iters = [i.iterations for i in infos]
-    fluid = int(st.fluid[0])
     ms_step = solve_s / args.steps * 1e3
     rate = fluid * sum(iters) / solve_s / 1e9 * ws
+    launches = sum(i.kernelLaunches for i in infos)
     if args.profile:
         ctx.close()
         return
-    # dominant kernel: the level-0 tile smoother, timed on its own (same stream)
-    hbm, _, pk_kind = peaks()
-    ms_sw, bytes_sw = ctx.pressure_profile(0, 20, c["inner"])
-    ms_vc, bytes_vc = ctx.pressure_profile(2, 5, c["inner"])
-    cells0 = int(st.cells[0])
-    dpc = read_profile_value("k_smooth_pipe16_mgpcg_b32.txt", "dram_bytes_per_cell")
-    launches_sweep = None
-    roof = {"bound": "hbm", "achieved": bytes_sw / (ms_sw * 1e-3) / 1e9, "peak": hbm,
-            "unit": "GB/s", "frac": bytes_sw / (ms_sw * 1e-3) / 1e9 / hbm, "peak_kind": pk_kind,
-            "traffic": dpc * cells0 if dpc else None, "alg_bytes_per_sweep": bytes_sw,
-            "kernel": "k_smooth_pipe16 (one level-0 pre-smoothing sweep, one launch per pass)",
-            "vcycle_achieved_gbs": bytes_vc / (ms_vc * 1e-3) / 1e9,
-            "vcycle_frac": bytes_vc / (ms_vc * 1e-3) / 1e9 / hbm}
-    del launches_sweep
-    # the same solve to a true FP64 residual of 1e-6 with the FP64 outer
-    # refinement, level-0 vectors in FP32, FP16 and BF16 (one warm-up each)
-    variants = {}
-    for name, storage in (("f32", msbg_gpu.F32), ("f16", msbg_gpu.F16), ("bf16", msbg_gpu.BF16)):
-        vp = msbg_gpu.solve_params(nPre=c["n_pre"], nPost=c["n_post"], tol=c["tol"],
-                                   innerIter=c["inner"], useGraph=1, storage=storage,
-                                   maxRefine=30)
-        ctx.pressure_solve(vp)
-        vi = ctx.pressure_solve(vp)
-        variants[name + "_vectors_fp64_refined"] = {
-            "ms": vi.solveSeconds * 1e3, "pcg_iterations": vi.iterations,
-            "refinements": vi.refinements, "status": vi.status,
-            "true_rel_residual_fp64": vi.relResidual}
-    learned = None
-    if not args.no_learned:
-        learned = learned_variants(ctx, c, scene)
     # end to end through the C ABI: prepare from the host callbacks (host
-    # sampling + hierarchy + upload), solve, download the pressure
-    n_e2e = max(1, min(args.steps, 2))
+    # sampling + hierarchy build + upload), the same solve, download of the
+    # pressure; averaged over 3 calls
+    n_e2e = 3
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     e2e_iters = 0
     for _ in range(n_e2e):
@@ -392,44 +410,95 @@ def bench_mgpcg(args):
         inf = ctx.pressure_solve(params)
         e2e_iters += inf.iterations
         out = ctx.pressure_download()
-    e2e_s = (time.perf_counter() - t0) / n_e2e
-    e2e_s = max_over_ranks(dist, e2e_s, dev)
+    e2e_s = max_over_ranks(dist, (time.perf_counter() - t0) / n_e2e, dev)
     e2e_rate = fluid * (e2e_iters / n_e2e) / e2e_s / 1e9 * ws
     st2 = ps_stats(ctx)
+    extras = {}
+    roof = None
     cb = None
-    if rank == 0 and ws == 1 and not args.no_cpu:
-        cb = cpu_reference_ps()
+    if ws == 1 and not args.quick:
+        extras, roof, cb = mgpcg_extras(args, ctx, c, scene, st, fluid)
     if rank == 0:
         line = {"metric": METRIC, "value": rate, "unit": "Gvoxel/s/iter", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded free-surface pressure problem)",
-                "config": {"workload": f"flip_pressure_mgpcg_{c['res']}_b{c['bsx0']}_2lvl",
-                           "mode": "plain FP32 MGPCG (V(2,2), FP64 dots, FP64 coarsest solve)",
-                           "time_to_1e-6_ms": ms_step, "pcg_iterations": iters,
-                           "true_rel_residual": infos[-1].relResidual,
-                           "refined_variants": variants,
-                           "learned": learned,
-                           "liquid_cells": fluid, "stored_cells_level0": cells0,
+                "config": {"workload": workload_name(c),
+                           "mode": ("MGPCG to a true FP64 residual of 1e-6: V(2,2), FP32 level-0 "
+                                    "vectors, FP64 solution with reliable residual replacement, "
+                                    "FP64 dots, FP64 coarsest solve"),
+                           "time_to_1e-6_ms": ms_step, "pcg_iterations": iters[:3],
+                           "true_rel_residual": max(i.relResidual for i in infos),
+                           "status": max(i.status for i in infos),
+                           "refinements": infos[-1].refinements,
+                           "liquid_cells": fluid, "stored_cells_level0": int(st.cells[0]),
                            "mg_levels": int(st.nMgLevels),
                            "prepare_s": st.prepareSeconds, "host_build_s": st.buildSeconds,
                            "l2": "inputs larger than L2 (%.1f GB operator+vectors)" %
                                  (st.deviceBytesUsed / 1e9),
-                           "parallelism": f"replicas{ws}"},
-                "gpu_launches": None,
+                           "parallelism": f"replicas{ws}", **extras},
+                "gpu_launches": launches,
                 "roofline": roof, "clocks": clocks,
                 "e2e": {"value": e2e_rate, "unit": "Gvoxel/s/iter",
                         "h2d_bytes_per_step": int(st2.h2dBytes),
                         "d2h_bytes_per_step": int(out.nbytes),
-                        "seconds_per_step": e2e_s},
+                        "seconds_per_step": e2e_s, "calls": n_e2e,
+                        "host_build_s": st2.buildSeconds},
                 "cpu_baseline": cb}
-        launches = ctx.last_solve_launches()
-        line["gpu_launches"] = launches * args.steps if launches else None
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def mgpcg_extras(args, ctx, c, scene, st, fluid):
+    """Sub-figures of the default line (one GPU): roofline of the dominant
+    kernel, the other solve variants, the learned variants, the reference's
+    analogue, the error against the FP64 oracle and the smoother workload."""
+    import msbg_gpu
+    hbm, _, pk_kind = peaks()
+    K = args.steps
+    # dominant kernel: the level-0 tile smoother, one sweep timed on its own
+    ms_sw, bytes_sw = ctx.pressure_profile(0, 20, c["inner"])
+    ms_vc, bytes_vc = ctx.pressure_profile(2, 5, c["inner"])
+    ms_mv, bytes_mv = ctx.pressure_profile(1, 20, c["inner"])
+    cells0 = int(st.cells[0])
+    dpc = read_profile_value("k_smooth_pipe16_mgpcg_b32.txt", "dram_bytes_per_cell")
+    roof = {"bound": "hbm", "achieved": bytes_sw / (ms_sw * 1e-3) / 1e9, "peak": hbm,
+            "unit": "GB/s", "frac": bytes_sw / (ms_sw * 1e-3) / 1e9 / hbm, "peak_kind": pk_kind,
+            "traffic": dpc * cells0 if dpc else None, "alg_bytes_per_sweep": bytes_sw,
+            "kernel": "k_smooth_pipe16 (one level-0 pre-smoothing sweep, one launch per pass)",
+            "sweep_ms": ms_sw,
+            "matvec_achieved_gbs": bytes_mv / (ms_mv * 1e-3) / 1e9,
+            "vcycle_achieved_gbs": bytes_vc / (ms_vc * 1e-3) / 1e9,
+            "vcycle_frac": bytes_vc / (ms_vc * 1e-3) / 1e9 / hbm}
+    x = {}
+    variants = {}
+    for name, kw in (("f32_plain_recursive_residual", dict(storage=msbg_gpu.F32, maxRefine=0)),
+                     ("f16_vectors_fp64_refined", dict(storage=msbg_gpu.F16, maxRefine=30)),
+                     ("bf16_vectors_fp64_refined", dict(storage=msbg_gpu.BF16, maxRefine=30))):
+        variants[name] = summarize(timed_solves(ctx, solve_params(c, **kw), 1, K), fluid)
+    x["variants"] = variants
+    if not args.no_learned:
+        x["learned"] = learned_variants(ctx, c, scene, fluid, K)
+    # the reference's runnable analogue (16^3 base blocks), GPU and CPU
+    s = dict(PS_SAME_CFG, res=c["res"], band=c["band"])
+    ctx.pressure_prepare(ps_scene(s))
+    st_s = ps_stats(ctx)
+    same = {"workload": workload_name(s),
+            "gpu": summarize(timed_solves(ctx, solve_params(s, maxRefine=30), 1, K),
+                             int(st_s.fluid[0])),
+            "gpu_plain_recursive_residual": summarize(
+                timed_solves(ctx, solve_params(s, maxRefine=0), 1, K), int(st_s.fluid[0]))}
+    cb = None
+    if not args.no_cpu:
+        cb = ref_pressure_rate(s)
+        same["reference_cpu"] = cb
+    x["same_config"] = same
+    x["max_err_vs_fp64_oracle"] = error_vs_oracle(ctx, c)
+    x["mcf_512_b16"] = mcf_line(args, ctx)
+    return x, roof, cb
 
 
 # ---------------------------------------------------------------------------
@@ -449,6 +518,9 @@ def cpu_reference_mcf(kind, vals, upd, max_seconds=20.0):
     import oracle
     c = MCF_CFG
     cores = os.cpu_count() or 1
+    if not oracle.ref_available():
+        return {"value": None, "unit": "Gvoxel/s/iter", "cores": cores, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/libmsbg_ref.so not built"}
     nvox = len(upd) * c["bsx"] ** 3
     oracle.ref().ref_init(cores)
     oracle.mcf_reference((c["res"],) * 3, c["bsx"], kind, vals, upd, 2, c["dt"])
@@ -473,7 +545,7 @@ def bench_reference_mcf(args):
     nvox = len(upd) * c["bsx"] ** 3
     line = {"metric": METRIC, "value": cb["value"], "unit": "Gvoxel/s/iter", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": nvox * c["iters"] / (cb["value"] * 1e9) * 1e3,
+            "ms_per_step": nvox * c["iters"] / (cb["value"] * 1e9) * 1e3 if cb["value"] else None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded sphere-union SDF)", "impl": "reference",
             "config": {"workload": "mcf_512_b16_spheres64_band4_it20", "active_voxels": nvox,
@@ -484,19 +556,18 @@ def bench_reference_mcf(args):
     print(json.dumps(line), flush=True)
 
 
-def bench_mcf(args):
+def mcf_line(args, ctx, dist=None, dev=None, ws=1, local=0):
+    """The MCF smoother at 512^3 on the device (resident pool, --steps calls
+    of 20 iterations after --warmup), end to end through the C ABI, and the
+    reference's CPU smoother on the same input."""
     import torch
     import msbg_gpu
-    ws, rank, local = dist_env()
-    torch.cuda.set_device(local)
-    dist = init_dist(ws)
-    dev = torch.device("cuda", local)
     c = MCF_CFG
     kind, vals, upd = mcf_scene()
     nb1 = c["res"] // c["bsx"]
     nvox = len(upd) * c["bsx"] ** 3
-    ctx = msbg_gpu.Context(local)
     L = msbg_gpu.lib()
+    dev = dev or torch.device("cuda", local)
     slot = np.where(kind == 1, np.cumsum(kind == 1) - 1,
                     np.where(kind == 2, -2, np.where(kind == 3, -3, -1))).astype(np.int32)
     bx, by, bz = upd % nb1, (upd // nb1) % nb1, upd // (nb1 * nb1)
@@ -519,7 +590,7 @@ def bench_mcf(args):
             raise RuntimeError(f"mcf rc={rc}")
 
     launches_per_step = c["iters"] * int((np.diff(cstart) > 0).sum())
-    for _ in range(args.warmup):
+    for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()
     if dist:
@@ -534,9 +605,6 @@ def bench_mcf(args):
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     ctx.sync()
-    if args.profile:
-        ctx.close()
-        return
     ms = max_over_ranks(dist, ms, dev)
     clocks = clk.summary()
     ms_step = ms / args.steps
@@ -576,28 +644,70 @@ def bench_mcf(args):
         e2e_step()
     e2e_s = max_over_ranks(dist, (time.perf_counter() - t0) / args.steps, dev)
     cb = None
-    if rank == 0 and ws == 1 and not args.no_cpu:
+    if not args.no_cpu and ws == 1:
         cb = cpu_reference_mcf(kind, vals, upd)
-    if rank == 0:
-        line = {"metric": METRIC, "value": rate, "unit": "Gvoxel/s/iter", "n_gpus": ws,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+    return {"workload": "mcf_512_b16_spheres64_band4_it20", "value": rate,
+            "unit": "Gvoxel/s/iter", "ms_per_step": ms_step, "active_voxels": nvox,
+            "value_blocks": int(len(upd)), "iters_per_step": c["iters"],
+            "gpu_launches": launches_per_step * args.steps, "roofline": roof, "clocks": clocks,
+            "e2e": {"value": nvox * c["iters"] / e2e_s / 1e9 * ws, "unit": "Gvoxel/s/iter",
+                    "h2d_bytes_per_step": int(vals.nbytes + kind.nbytes * 4 + upd.nbytes),
+                    "d2h_bytes_per_step": int(vals.nbytes)},
+            "cpu_baseline": cb}
+
+
+def bench_mcf(args):
+    import torch
+    import msbg_gpu
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = init_dist(ws)
+    dev = torch.device("cuda", local)
+    ctx = msbg_gpu.Context(local)
+    m = mcf_line(args, ctx, dist, dev, ws, local)
+    if rank == 0 and not args.profile:
+        line = {"metric": METRIC, "value": m["value"], "unit": "Gvoxel/s/iter", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded sphere-union SDF, 64 spheres)",
-                "config": {"workload": "mcf_512_b16_spheres64_band4_it20", "active_voxels": nvox,
-                           "value_blocks": int(len(upd)), "iters_per_step": c["iters"],
-                           "l2": "inputs larger than L2 (%.0f MB)" % (vals.nbytes / 1e6),
-                           "parallelism": f"replicas{ws}"},
-                "gpu_launches": launches_per_step * args.steps, "roofline": roof,
-                "clocks": clocks,
-                "e2e": {"value": nvox * c["iters"] / e2e_s / 1e9 * ws, "unit": "Gvoxel/s/iter",
-                        "h2d_bytes_per_step": int(vals.nbytes + kind.nbytes * 4 + upd.nbytes),
-                        "d2h_bytes_per_step": int(vals.nbytes)},
-                "cpu_baseline": cb}
+                "config": {"workload": m["workload"], "active_voxels": m["active_voxels"],
+                           "value_blocks": m["value_blocks"], "iters_per_step": m["iters_per_step"],
+                           "l2": "inputs larger than L2", "parallelism": f"replicas{ws}"},
+                "gpu_launches": m["gpu_launches"], "roofline": m["roofline"],
+                "clocks": m["clocks"], "e2e": m["e2e"], "cpu_baseline": m["cpu_baseline"]}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# part timings for profiles
+# ---------------------------------------------------------------------------
+def bench_part(args):
+    """One solver part (a level-0 smoothing sweep, the level-0 matvec or a
+    V-cycle) of the pressure workload, timed through msbg_gpu_pressure_profile:
+    one warm-up call, then --steps calls.  Prints the level-0 cell count so a
+    capture's DRAM bytes can be put per cell."""
+    import torch
+    import msbg_gpu
+    torch.cuda.set_device(0)
+    c = dict(PS_CFG)
+    if args.res:
+        c["res"] = args.res
+        c["band"] = PS_CFG["band"] * args.res / PS_CFG["res"]
+    ctx = msbg_gpu.Context(0)
+    ctx.pressure_prepare(ps_scene(c))
+    st = ps_stats(ctx)
+    what = {"smooth": 0, "matvec": 1, "vcycle": 2}[args.part]
+    storage = {"f32": msbg_gpu.F32, "f16": msbg_gpu.F16, "bf16": msbg_gpu.BF16}[args.storage]
+    ms, by = ctx.pressure_profile(what | (storage << 4), max(1, args.steps), c["inner"])
+    print(json.dumps({"part": args.part, "storage": args.storage, "res": c["res"],
+                      "cells_level0": int(st.cells[0]), "ms_per_call": ms,
+                      "alg_bytes_per_call": by, "achieved_gbs": by / (ms * 1e-3) / 1e9}),
+          flush=True)
+    ctx.close()
 
 
 def main():
@@ -608,8 +718,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mgpcg", choices=["mgpcg", "mcf"])
     ap.add_argument("--res", type=int, default=0, help="override the pressure resolution")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline legs")
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned guess")
+    ap.add_argument("--quick", action="store_true",
+                    help="only the headline solve and its end-to-end figure")
     ap.add_argument("--profile", action="store_true",
                     help="only the resident-data steps (for ncu captures); prints nothing")
     ap.add_argument("--part", default="", choices=["", "smooth", "matvec", "vcycle"],
