@@ -28,7 +28,9 @@ calls after one warm-up:
     64 seeded spheres, 20 iterations, dt 0.1) with its roofline and the
     reference's CPU smoother on the same input.
 
-``--workload mcf`` benches only the smoother.
+``--workload mcf`` benches only the smoother; ``--workload c3`` / ``c5`` the
+2048^3 mixed-precision and 4096^3 three-level configurations (one JSON line
+of figures each, see bench_large).
 ``--impl reference`` times the reference's own CPU implementation (compiled
 from its sources into oracle/_ref/libmsbg_ref.so) with all host threads.
 
@@ -66,6 +68,16 @@ ERR_RES = 256
 
 MCF_CFG = dict(res=512, bsx=16, n_spheres=64, rmin=20.0, rmax=60.0, band=4.0, dilate=1,
                seed=1234, iters=20, dt=0.1)
+
+# 2048^3: the 1024^3 scene family at twice the resolution (~4e8 active cells),
+# level-0 vectors in FP16 and in BF16 under FP64 refinement
+C3_CFG = dict(PS_CFG, res=2048)
+# 4096^3, 3 levels, fine band of 48 voxels around a wavy free surface
+# z = (0.3 + 0.05 sum of 8 seeded sinusoids) * res plus 256 seeded spheres of
+# radius 20-60 voxels, no obstacles; FP16 storage with FP64 refinement and
+# the learned guess and correction, against plain FP32 on the same GPU
+C5_CFG = dict(PS_CFG, res=4096, n_levels=3, band=48.0, z_liquid=0.3, n_spheres=256,
+              r_min=20 / 4096, r_max=60 / 4096, n_cuboids=0, wave_amp=0.05, n_waves=8, seed=4096)
 
 
 def peaks():
@@ -177,7 +189,8 @@ def ps_scene(cfg):
     import msbg_gpu
     return msbg_gpu.PressureScene(cfg["res"], cfg["bsx0"], cfg["n_levels"], cfg["z_liquid"],
                                   cfg["n_spheres"], cfg["r_min"], cfg["r_max"], cfg["n_cuboids"],
-                                  cfg["n_modes"], cfg["k_max"], cfg["band"], cfg["seed"])
+                                  cfg["n_modes"], cfg["k_max"], cfg["band"], cfg["seed"],
+                                  cfg.get("wave_amp", 0.0), cfg.get("n_waves", 0))
 
 
 def ps_stats(ctx):
@@ -501,6 +514,50 @@ def mgpcg_extras(args, ctx, c, scene, st, fluid):
     return x, roof, cb
 
 
+def bench_large(args):
+    """The 2048^3 (c3) and 4096^3 (c5) configurations on one GPU: the host
+    build of the hierarchy, the smoother's level-0 sweep rate (Gvoxel/s per
+    smoother iteration) and the time to a true FP64 residual of 1e-6 of each
+    variant, one warm-up and --steps timed calls each."""
+    import torch
+    import msbg_gpu
+    torch.cuda.set_device(0)
+    c = dict(C3_CFG if args.workload == "c3" else C5_CFG)
+    if args.res:
+        c["band"] = c["band"] * args.res / c["res"]
+        c["res"] = args.res
+    ctx = msbg_gpu.Context(0)
+    scene = ps_scene(c)
+    t0 = time.perf_counter()
+    ctx.pressure_prepare(scene)
+    prep_s = time.perf_counter() - t0
+    st = ps_stats(ctx)
+    fluid = int(st.fluid[0])
+    free, total = torch.cuda.mem_get_info(0)
+    out = {"workload": workload_name(c) + ("_wavy" if c.get("n_waves") else ""),
+           "liquid_cells_level0": fluid,
+           "active_cells_all_levels": int(sum(st.fluid[m] for m in range(st.nMgLevels))),
+           "stored_cells_level0": int(st.cells[0]), "mg_levels": int(st.nMgLevels),
+           "prepare_s": prep_s, "host_build_s": st.buildSeconds,
+           "device_bytes_used": int(st.deviceBytesUsed), "device_free_after_prepare": int(free)}
+    hbm, _, _ = peaks()
+    for name, storage in (("f32", msbg_gpu.F32), ("f16", msbg_gpu.F16), ("bf16", msbg_gpu.BF16)):
+        ms, by = ctx.pressure_profile(0 | (storage << 4), 5, c["inner"])
+        out[f"sweep_{name}"] = {"ms": ms, "gvoxel_s_per_smoother_iteration":
+                                int(st.cells[0]) / (ms * 1e-3) / 1e9,
+                                "hbm_frac": by / (ms * 1e-3) / 1e9 / hbm}
+    variants = [("f32_plain_recursive_residual", dict(storage=msbg_gpu.F32, maxRefine=0)),
+                ("f32_vectors_fp64_refined", dict(storage=msbg_gpu.F32, maxRefine=30)),
+                ("f16_vectors_fp64_refined", dict(storage=msbg_gpu.F16, maxRefine=30)),
+                ("bf16_vectors_fp64_refined", dict(storage=msbg_gpu.BF16, maxRefine=30))]
+    for name, kw in variants:
+        out[name] = summarize(timed_solves(ctx, solve_params(c, **kw), 1, args.steps), fluid)
+    if args.workload == "c5" and not args.no_learned:
+        out["learned"] = learned_variants(ctx, c, scene, fluid, args.steps)
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 # ---------------------------------------------------------------------------
 # mean-curvature-flow workload
 # ---------------------------------------------------------------------------
@@ -716,7 +773,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mgpcg", choices=["mgpcg", "mcf"])
+    ap.add_argument("--workload", default="mgpcg", choices=["mgpcg", "mcf", "c3", "c5"])
     ap.add_argument("--res", type=int, default=0, help="override the pressure resolution")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline legs")
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned guess")
@@ -736,6 +793,8 @@ def main():
         bench_reference(args)
     elif args.workload == "mcf":
         bench_mcf(args)
+    elif args.workload in ("c3", "c5"):
+        bench_large(args)
     else:
         bench_mgpcg(args)
 

@@ -50,6 +50,15 @@ msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, int nLevels, 
                                                 int nSpheres, float rMin, float rMax,
                                                 int nCuboids, int nModes, int kMax, float band,
                                                 uint64_t seed);
+/* Same problem with a wavy free surface: liquid below
+ *   z = res * (zLiquid + waveAmp * sum_i a_i sin(2 pi (kx_i x + ky_i y)/res + phi_i))
+ * with nWaves seeded sinusoids (|kx|, ky in 1..3, a_i > 0 summing to 1), plus
+ * the spheres (up to 4096).  nWaves = 0 gives msbg_scene_pressure_create. */
+msbg_pressure_scene* msbg_scene_pressure_create_wavy(int res, int bsx0, int nLevels,
+                                                     float zLiquid, float waveAmp, int nWaves,
+                                                     int nSpheres, float rMin, float rMax,
+                                                     int nCuboids, int nModes, int kMax,
+                                                     float band, uint64_t seed);
 void msbg_scene_pressure_destroy(msbg_pressure_scene* s);
 /* Refinement map (levels per base block, bid order). */
 int msbg_scene_pressure_block_levels(const msbg_pressure_scene* s, int* levels);

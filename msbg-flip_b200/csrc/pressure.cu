@@ -622,12 +622,14 @@ int solve_refined(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const msbg_gpu_so
       }
     }
     o.relres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
-    if (!(bb > 1e-300) || o.relres <= p->tol) {
-      o.status = 0;
+    // a non-finite right-hand side or residual is reported before any
+    // convergence test (NaN compares false with every tolerance)
+    if (!std::isfinite(rr) || !std::isfinite(bb)) {
+      o.status = 3;
       break;
     }
-    if (!std::isfinite(rr)) {
-      o.status = 3;
+    if (!(bb > 1e-300) || o.relres <= p->tol) {
+      o.status = 0;
       break;
     }
     if (outer >= maxRefine || o.iters >= p->maxIter) {
@@ -761,12 +763,12 @@ int solve_reliable(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gp
   const double bb = S.hScal->bb;
   o.initialRelres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
   o.relres = o.initialRelres;
-  if (!(bb > 1e-300) || o.relres <= p->tol) {
-    o.status = 0;
+  if (!std::isfinite(rr) || !std::isfinite(bb) || !std::isfinite(S.hScal->rho)) {
+    o.status = 3;  // before the convergence test: NaN compares false with any tolerance
     return MSBG_OK;
   }
-  if (!std::isfinite(rr) || !std::isfinite(S.hScal->rho)) {
-    o.status = 3;
+  if (!(bb > 1e-300) || o.relres <= p->tol) {
+    o.status = 0;
     return MSBG_OK;
   }
   auto part1 = [&]() {

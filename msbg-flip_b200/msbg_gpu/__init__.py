@@ -95,6 +95,8 @@ def scene_lib():
                                         C.POINTER(C.c_int64)]),
         "msbg_scene_pressure_create": (vp, [i32, i32, i32, f32, i32, f32, f32, i32, i32, i32, f32,
                                             C.c_uint64]),
+        "msbg_scene_pressure_create_wavy": (vp, [i32, i32, i32, f32, f32, i32, i32, f32, f32, i32,
+                                                 i32, i32, f32, C.c_uint64]),
         "msbg_scene_pressure_destroy": (None, [vp]),
         "msbg_scene_pressure_block_levels": (i32, [vp, C.POINTER(C.c_int)]),
     }
@@ -296,12 +298,14 @@ class PressureScene:
     """Seeded free-surface pressure problem (include/msbg_scene.h)."""
 
     def __init__(self, res, bsx0, n_levels, z_liquid=0.4, n_spheres=32, r_min=0.03, r_max=0.1,
-                 n_cuboids=8, n_modes=16, k_max=8, band=64.0, seed=2024):
+                 n_cuboids=8, n_modes=16, k_max=8, band=64.0, seed=2024, wave_amp=0.0,
+                 n_waves=0):
         L = scene_lib()
         self._L = L
         self.res, self.bsx0, self.n_levels = res, bsx0, n_levels
-        self.h = L.msbg_scene_pressure_create(res, bsx0, n_levels, z_liquid, n_spheres, r_min,
-                                              r_max, n_cuboids, n_modes, k_max, band, seed)
+        self.h = L.msbg_scene_pressure_create_wavy(res, bsx0, n_levels, z_liquid, wave_amp,
+                                                   n_waves, n_spheres, r_min, r_max, n_cuboids,
+                                                   n_modes, k_max, band, seed)
         if not self.h:
             raise MsbgError(5, "scene")
         nb = (res // bsx0) ** 3

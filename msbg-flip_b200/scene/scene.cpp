@@ -174,6 +174,9 @@ extern "C" int msbg_scene_sphere_sdf(int res, int bsx, int nSpheres, float rmin,
 struct msbg_pressure_scene {
   int res, bsx0, nLevels;
   float zLiquid, band;
+  // free-surface height per (x, y) column at the cell centre, in voxels
+  // (a plane z = zLiquid * res, or that plane plus the waves)
+  std::vector<double> surf;
   std::vector<Sphere> spheres;
   struct Box { double lo[3], hi[3]; };
   std::vector<Box> boxes;
@@ -186,17 +189,25 @@ struct msbg_pressure_scene {
   // 16 cosines by 16 complex products).
   std::vector<double> etab;  // [axis][res][mode][2]: a cell's entries are contiguous
   std::vector<double> ephi;  // [mode][2]
-  // Boxes that can contain a cell centre of each 8^3 region (bit b = box b;
+  // Boxes that can contain a cell centre of each RG^3 region (bit b = box b;
   // built when there are at most 64 boxes, else every box is tested).
-  static constexpr int RG = 8;
+  // RG = 8, or res/128 for larger grids (the masks then stay small).
+  int RG = 8;
   int nrg = 0;
   std::vector<uint64_t> boxMask;
-  // Spheres that can contain a cell centre of each 8^3 region (at most 64
-  // spheres; else every sphere is tested).
+  // Spheres that can contain a cell centre of each RG^3 region: sphereWords
+  // 64-bit words per region (bit s = sphere s).
+  int sphereWords = 0;
   std::vector<uint64_t> sphereMask;
 
+  double surface(double x, double y) const {
+    const int ix = std::min(std::max((int)std::floor(x), 0), res - 1);
+    const int iy = std::min(std::max((int)std::floor(y), 0), res - 1);
+    return surf[ix + (size_t)res * iy];
+  }
+  // signed distance to the liquid (vertical distance to the free surface)
   double liquid_sdf(double x, double y, double z) const {
-    double d = z - zLiquid * res;
+    double d = z - surface(x, y);
     for (const auto& s : spheres) {
       double dx = x - s.cx, dy = y - s.cy, dz = z - s.cz;
       d = std::min(d, std::sqrt(dx * dx + dy * dy + dz * dz) - s.r);
@@ -233,13 +244,18 @@ struct msbg_pressure_scene {
   }
   bool liquid_cell(int ix, int iy, int iz) const {
     const double x = ix + 0.5, y = iy + 0.5, z = iz + 0.5;
-    if (z - zLiquid * res < 0) return true;
+    if (z < surf[ix + (size_t)res * iy]) return true;
     if (!sphereMask.empty()) {
-      uint64_t m = sphereMask[(ix / RG) + (size_t)nrg * ((iy / RG) + (size_t)nrg * (iz / RG))];
-      while (m) {
-        const int b = __builtin_ctzll(m);
-        m &= m - 1;
-        if (in_sphere(spheres[b], x, y, z)) return true;
+      const uint64_t* m0 =
+          &sphereMask[((ix / RG) + (size_t)nrg * ((iy / RG) + (size_t)nrg * (iz / RG))) *
+                      sphereWords];
+      for (int w = 0; w < sphereWords; w++) {
+        uint64_t m = m0[w];
+        while (m) {
+          const int b = __builtin_ctzll(m);
+          m &= m - 1;
+          if (in_sphere(spheres[64 * w + b], x, y, z)) return true;
+        }
       }
       return false;
     }
@@ -278,8 +294,18 @@ extern "C" msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, in
                                                            float rMin, float rMax, int nCuboids,
                                                            int nModes, int kMax, float band,
                                                            uint64_t seed) {
-  if (res <= 0 || bsx0 <= 0 || res % bsx0 || nLevels < 1 || nLevels > 4) return nullptr;
+  return msbg_scene_pressure_create_wavy(res, bsx0, nLevels, zLiquid, 0.f, 0, nSpheres, rMin,
+                                         rMax, nCuboids, nModes, kMax, band, seed);
+}
+
+extern "C" msbg_pressure_scene* msbg_scene_pressure_create_wavy(
+    int res, int bsx0, int nLevels, float zLiquid, float waveAmp, int nWaves, int nSpheres,
+    float rMin, float rMax, int nCuboids, int nModes, int kMax, float band, uint64_t seed) {
+  if (res <= 0 || bsx0 <= 0 || res % bsx0 || nLevels < 1 || nLevels > 4 || nWaves < 0 ||
+      nSpheres < 0 || nSpheres > 4096)
+    return nullptr;
   auto* s = new msbg_pressure_scene();
+  s->RG = std::max(8, res / 128);
   s->res = res;
   s->bsx0 = bsx0;
   s->nLevels = nLevels;
@@ -304,8 +330,8 @@ extern "C" msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, in
     }
     s->boxes.push_back(b);
   }
-  if (res % msbg_pressure_scene::RG == 0 && s->boxes.size() <= 64) {
-    const int RG = msbg_pressure_scene::RG;
+  if (res % s->RG == 0 && s->boxes.size() <= 64) {
+    const int RG = s->RG;
     s->nrg = res / RG;
     s->boxMask.assign((size_t)s->nrg * s->nrg * s->nrg, 0);
     for (size_t bi = 0; bi < s->boxes.size(); bi++) {
@@ -321,10 +347,12 @@ extern "C" msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, in
             s->boxMask[x + (size_t)s->nrg * (y + (size_t)s->nrg * z)] |= 1ull << bi;
     }
   }
-  if (res % msbg_pressure_scene::RG == 0 && s->spheres.size() <= 64) {
-    const int RG = msbg_pressure_scene::RG, nrg = res / RG;
+  if (res % s->RG == 0 && !s->spheres.empty()) {
+    const int RG = s->RG, nrg = res / RG;
     s->nrg = nrg;
-    s->sphereMask.assign((size_t)nrg * nrg * nrg, 0);
+    const int W = (int)(s->spheres.size() + 63) / 64;
+    s->sphereWords = W;
+    s->sphereMask.assign((size_t)nrg * nrg * nrg * W, 0);
     for (size_t si = 0; si < s->spheres.size(); si++) {
       const Sphere& sp = s->spheres[si];
       const double c[3] = {sp.cx, sp.cy, sp.cz};
@@ -346,7 +374,8 @@ extern "C" msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, in
               d2 += q * q;
             }
             if (d2 < sp.r * sp.r + 1.0)
-              s->sphereMask[x + (size_t)nrg * (y + (size_t)nrg * z)] |= 1ull << si;
+              s->sphereMask[(x + (size_t)nrg * (y + (size_t)nrg * z)) * W + si / 64] |=
+                  1ull << (si % 64);
           }
     }
   }
@@ -383,6 +412,35 @@ extern "C" msbg_pressure_scene* msbg_scene_pressure_create(int res, int bsx0, in
         s->etab[(((size_t)d * res + x) * nModes + i) * 2] = std::cos(a);
         s->etab[(((size_t)d * res + x) * nModes + i) * 2 + 1] = std::sin(a);
       }
+  }
+  // Free surface: the plane z = zLiquid*res plus nWaves sinusoids in x and y
+  // (wave numbers 1..3 per axis, random phases) whose amplitudes sum to
+  // waveAmp*res.  The waves are drawn last, so scenes without waves keep
+  // their sequence of random numbers.
+  {
+    std::vector<double> wa(nWaves), wp(nWaves);
+    std::vector<int> wk(2 * nWaves);
+    double asum = 0;
+    for (int i = 0; i < nWaves; i++) {
+      wk[2 * i] = 1 + (int)(rng.uniform() * 3);
+      wk[2 * i + 1] = 1 + (int)(rng.uniform() * 3);
+      if (rng.uniform() < 0.5) wk[2 * i] = -wk[2 * i];
+      wa[i] = 0.2 + rng.uniform();
+      wp[i] = rng.uniform() * 2 * M_PI;
+      asum += wa[i];
+    }
+    s->surf.assign((size_t)res * res, zLiquid * (double)res);
+    if (nWaves > 0) {
+      const double scale = waveAmp * res / asum;
+#pragma omp parallel for schedule(static)
+      for (int y = 0; y < res; y++)
+        for (int x = 0; x < res; x++) {
+          double h = 0;
+          for (int i = 0; i < nWaves; i++)
+            h += wa[i] * std::sin(w * (wk[2 * i] * (x + 0.5) + wk[2 * i + 1] * (y + 0.5)) + wp[i]);
+          s->surf[x + (size_t)res * y] += scale * h;
+        }
+    }
   }
   // Refinement map.
   const int nb1 = res / bsx0;
