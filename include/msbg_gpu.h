@@ -51,8 +51,11 @@ enum {
   MSBG_BLOCK_FULL = 3
 };
 
-/* Storage type of a channel's values. */
-enum { MSBG_F32 = 0, MSBG_F16 = 1, MSBG_BF16 = 2, MSBG_F64 = 3 };
+/* Storage type of a channel's values.  MSBG_U16 is the reference's 16-bit
+ * render density (RenderDensity = uint16_t under RSURF_16_BIT,
+ * src/msbgcell.h:67-68, src/msbg.h:369-376): q in [0, 65535] stands for
+ * q / 65535 (src/sbg.h:225-232). */
+enum { MSBG_F32 = 0, MSBG_F16 = 1, MSBG_BF16 = 2, MSBG_F64 = 3, MSBG_U16 = 4 };
 
 typedef struct msbg_gpu_ctx msbg_gpu_ctx;
 
@@ -65,7 +68,16 @@ typedef struct {
   int bsx0;              /* base block size: 8, 16 or 32 */
   int nLevels;           /* resolution levels (1..4) */
   const int* blockLevel; /* [nbx*nby*nbz] level per block, or NULL */
+  /* Pressure boundary of the six domain faces (-x, +x, -y, +y, -z, +z), as
+   * setDomainBoundarySpec_ gives them (src/msbg.cpp:2462, flip_sim.cpp:1621):
+   * MSBG_DBC_OPEN (air outside: p = 0 with the face coefficient the callback
+   * returns for that face) or MSBG_DBC_SOLID (a wall: coefficient 0, the
+   * callback is not asked).  NULL: every domain face is OPEN, i.e. the
+   * callbacks alone decide. */
+  const int* domainBc;
 } msbg_topo_desc;
+
+enum { MSBG_DBC_OPEN = 0, MSBG_DBC_SOLID = 1 }; /* DBC_OPEN, DBC_SOLID (src/msbg.h:191-192) */
 
 /* ---- context ------------------------------------------------------------ */
 
@@ -102,6 +114,15 @@ int msbg_gpu_upload_channel(msbg_gpu_ctx* ctx, int chan, int level,
 int msbg_gpu_download_channel(msbg_gpu_ctx* ctx, int chan, float* const* blockPtrs,
                               float* packed);
 
+/* The same for a 16-bit render-density channel (SparseGrid<uint16_t> of
+ * getUint16Channel, src/msbg.h:3085): raw values, const blocks hold the raw
+ * emptyVal / fullVal.  msbg_gpu_pde_mcf runs on either kind of channel. */
+int msbg_gpu_upload_channel_u16(msbg_gpu_ctx* ctx, int chan, int level, const int8_t* kind,
+                                const uint16_t* const* blockPtrs, const uint16_t* packed,
+                                uint16_t emptyVal, uint16_t fullVal);
+int msbg_gpu_download_channel_u16(msbg_gpu_ctx* ctx, int chan, uint16_t* const* blockPtrs,
+                                  uint16_t* packed);
+
 /* Number of value blocks of a channel (size of the packed layout / bsx^3). */
 int msbg_gpu_channel_num_value_blocks(msbg_gpu_ctx* ctx, int chan, int64_t* out);
 
@@ -114,6 +135,9 @@ int msbg_gpu_channel_device_ptr(msbg_gpu_ctx* ctx, int chan, void** out);
 /* Replaces MultiresSparseGrid::applyChannelPdeFast<float>(chan, CH_NULL, CH_NULL,
  * &blockList, -(PDE_MEAN_CURVATURE+OPT_8_COLOR_SCHEME), clamp01, 0,0,0,
  * numIter, 1.0f, dt)                        src/msbg4.cpp:59-957, msbg.h:2176
+ * and, on a 16-bit channel, applyChannelPdeFast<uint16_t> (the demo's call,
+ * src/msbg_demo.cpp:716-727): values widened on load, the result stored as
+ * round(phi * 65535) (src/msbg4.cpp:829-839).
  * In-place 8-colour block Gauss-Seidel (Jacobi inside a block) of the
  * 19-point mean-curvature stencil, halo BC_NEUMANN.  numIter is rounded up
  * to an even count as the reference does (src/msbg4.cpp:150-152).  Only
@@ -127,6 +151,7 @@ int msbg_gpu_pde_mcf(msbg_gpu_ctx* ctx, int chan, const int* blockList, int n,
  * slotOf[nBlocks] = slot or -1 NULL / -2 empty / -3 full; colourList holds
  * the updated blocks' ids grouped by colour with colourStart[9] offsets
  * (device arrays).  For callers that keep the grid resident on the GPU.
+ * pool must be 8-byte aligned (MSBG_EINVARG otherwise).
  * A listed block whose slotOf entry is negative is skipped on the device,
  * and the next msbg_gpu_sync returns MSBG_EINVARG for it. */
 int msbg_gpu_pde_mcf_device(msbg_gpu_ctx* ctx, float* pool, const int* slotOf,

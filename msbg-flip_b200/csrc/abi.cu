@@ -121,9 +121,14 @@ extern "C" int msbg_gpu_sync_topology(msbg_gpu_ctx* ctx, const msbg_topo_desc* d
   return MSBG_OK;
 }
 
-extern "C" int msbg_gpu_upload_channel(msbg_gpu_ctx* ctx, int chan, int level,
-                                       const int8_t* kind, const float* const* blockPtrs,
-                                       const float* packed, float emptyVal, float fullVal) {
+namespace {
+
+// Upload of one channel of element type T (float, or uint16_t for the 16-bit
+// render density): block kinds -> slot map, value blocks -> device pool.
+template <typename T>
+int upload_channel_t(msbg_gpu_ctx* ctx, int chan, int level, const int8_t* kind,
+                     const T* const* blockPtrs, const T* packed, int dtype, float emptyVal,
+                     float fullVal, uint16_t emptyQ, uint16_t fullQ) {
   if (!ctx || !kind || (!blockPtrs && !packed)) return MSBG_EINVARG;
   if (ctx->nbx <= 0) return set_error(ctx, MSBG_EINVARG, "no topology");
   if (level < 0 || level >= ctx->nLevels)
@@ -133,8 +138,11 @@ extern "C" int msbg_gpu_upload_channel(msbg_gpu_ctx* ctx, int chan, int level,
   auto ch = std::make_unique<Channel>();
   ch->level = level;
   ch->bsx = ctx->bsx0 >> level;
+  ch->dtype = dtype;
   ch->emptyVal = emptyVal;
   ch->fullVal = fullVal;
+  ch->emptyQ = emptyQ;
+  ch->fullQ = fullQ;
   ch->kindHost.assign(kind, kind + nb);
   ch->slotHost.resize(nb);
   int64_t s = 0;
@@ -149,17 +157,17 @@ extern "C" int msbg_gpu_upload_channel(msbg_gpu_ctx* ctx, int chan, int level,
   }
   ch->nValue = s;
   const size_t nv = (size_t)ch->bsx * ch->bsx * ch->bsx;
-  MSBG_CUDA_TRY(ctx, ch->pool.ensure(sizeof(float) * nv * (size_t)s));
+  const size_t bytes = sizeof(T) * nv * (size_t)s;
+  MSBG_CUDA_TRY(ctx, ch->pool.ensure(bytes));
   MSBG_CUDA_TRY(ctx, ch->slot.ensure(sizeof(int) * nb));
   MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(ch->slot.p, ch->slotHost.data(), sizeof(int) * nb,
                                      cudaMemcpyHostToDevice, ctx->stream));
   if (packed) {
-    MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(ch->pool.p, packed, sizeof(float) * nv * (size_t)s,
-                                       cudaMemcpyHostToDevice, ctx->stream));
+    MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(ch->pool.p, packed, bytes, cudaMemcpyHostToDevice,
+                                       ctx->stream));
   } else {
     // Gather the scattered host blocks into one pinned staging buffer, then
     // one transfer (MSBG blocks live in separate pool allocations).
-    const size_t bytes = sizeof(float) * nv * (size_t)s;
     if (ctx->pinnedBytes < bytes) {
       MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
       if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -170,12 +178,12 @@ extern "C" int msbg_gpu_upload_channel(msbg_gpu_ctx* ctx, int chan, int level,
     } else {
       MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     }
-    float* stage = static_cast<float*>(ctx->pinned);
+    T* stage = static_cast<T*>(ctx->pinned);
     for (int64_t b = 0; b < nb; b++) {
       if (kind[b] != MSBG_BLOCK_VALUE) continue;
       if (!blockPtrs[b])
         return set_error(ctx, MSBG_EINVARG, "value block %lld has no pointer", (long long)b);
-      std::memcpy(stage + (size_t)ch->slotHost[b] * nv, blockPtrs[b], sizeof(float) * nv);
+      std::memcpy(stage + (size_t)ch->slotHost[b] * nv, blockPtrs[b], sizeof(T) * nv);
     }
     MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(ch->pool.p, stage, bytes, cudaMemcpyHostToDevice,
                                        ctx->stream));
@@ -184,15 +192,17 @@ extern "C" int msbg_gpu_upload_channel(msbg_gpu_ctx* ctx, int chan, int level,
   return MSBG_OK;
 }
 
-extern "C" int msbg_gpu_download_channel(msbg_gpu_ctx* ctx, int chan, float* const* blockPtrs,
-                                         float* packed) {
+template <typename T>
+int download_channel_t(msbg_gpu_ctx* ctx, int chan, int dtype, T* const* blockPtrs, T* packed) {
   if (!ctx || (!blockPtrs && !packed)) return MSBG_EINVARG;
   auto it = ctx->channels.find(chan);
   if (it == ctx->channels.end()) return set_error(ctx, MSBG_EINVARG, "channel %d not uploaded", chan);
-  cudaSetDevice(ctx->device);
   Channel& ch = *it->second;
+  if (ch.dtype != dtype)
+    return set_error(ctx, MSBG_EINVARG, "channel %d holds another value type", chan);
+  cudaSetDevice(ctx->device);
   const size_t nv = (size_t)ch.bsx * ch.bsx * ch.bsx;
-  const size_t bytes = sizeof(float) * nv * (size_t)ch.nValue;
+  const size_t bytes = sizeof(T) * nv * (size_t)ch.nValue;
   if (packed) {
     MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(packed, ch.pool.p, bytes, cudaMemcpyDeviceToHost,
                                        ctx->stream));
@@ -210,12 +220,39 @@ extern "C" int msbg_gpu_download_channel(msbg_gpu_ctx* ctx, int chan, float* con
   MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->pinned, ch.pool.p, bytes, cudaMemcpyDeviceToHost,
                                      ctx->stream));
   MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  const float* stage = static_cast<const float*>(ctx->pinned);
+  const T* stage = static_cast<const T*>(ctx->pinned);
   for (size_t b = 0; b < ch.slotHost.size(); b++) {
     if (ch.slotHost[b] < 0 || !blockPtrs[b]) continue;
-    std::memcpy(blockPtrs[b], stage + (size_t)ch.slotHost[b] * nv, sizeof(float) * nv);
+    std::memcpy(blockPtrs[b], stage + (size_t)ch.slotHost[b] * nv, sizeof(T) * nv);
   }
   return MSBG_OK;
+}
+
+}  // namespace
+
+extern "C" int msbg_gpu_upload_channel(msbg_gpu_ctx* ctx, int chan, int level,
+                                       const int8_t* kind, const float* const* blockPtrs,
+                                       const float* packed, float emptyVal, float fullVal) {
+  return upload_channel_t<float>(ctx, chan, level, kind, blockPtrs, packed, MSBG_F32, emptyVal,
+                                 fullVal, 0, 0);
+}
+
+extern "C" int msbg_gpu_upload_channel_u16(msbg_gpu_ctx* ctx, int chan, int level,
+                                           const int8_t* kind, const uint16_t* const* blockPtrs,
+                                           const uint16_t* packed, uint16_t emptyVal,
+                                           uint16_t fullVal) {
+  return upload_channel_t<uint16_t>(ctx, chan, level, kind, blockPtrs, packed, MSBG_U16, 0.f, 0.f,
+                                    emptyVal, fullVal);
+}
+
+extern "C" int msbg_gpu_download_channel(msbg_gpu_ctx* ctx, int chan, float* const* blockPtrs,
+                                         float* packed) {
+  return download_channel_t<float>(ctx, chan, MSBG_F32, blockPtrs, packed);
+}
+
+extern "C" int msbg_gpu_download_channel_u16(msbg_gpu_ctx* ctx, int chan,
+                                             uint16_t* const* blockPtrs, uint16_t* packed) {
+  return download_channel_t<uint16_t>(ctx, chan, MSBG_U16, blockPtrs, packed);
 }
 
 extern "C" int msbg_gpu_channel_num_value_blocks(msbg_gpu_ctx* ctx, int chan, int64_t* out) {
@@ -273,9 +310,15 @@ extern "C" int msbg_gpu_pde_mcf(msbg_gpu_ctx* ctx, int chan, const int* blockLis
   const int nIter = numIter + (numIter & 1);  // src/msbg4.cpp:150-152
   int* ef = err_flag(ctx);
   if (!ef) return set_error(ctx, MSBG_ENOMEM, "error flag allocation failed");
-  MSBG_CUDA_TRY(ctx, launch_mcf(ch.pool.as<float>(), ch.slot.as<int>(), ctx->listBuf.as<int>(),
-                                start, ctx->nbx, ctx->nby, ctx->nbz, ch.bsx, ch.emptyVal,
-                                ch.fullVal, nIter, dt, clamp01, ef, ctx->stream));
+  if (ch.dtype == MSBG_U16)
+    MSBG_CUDA_TRY(ctx, launch_mcf_u16(ch.pool.as<uint16_t>(), ch.slot.as<int>(),
+                                      ctx->listBuf.as<int>(), start, ctx->nbx, ctx->nby, ctx->nbz,
+                                      ch.bsx, ch.emptyQ, ch.fullQ, nIter, dt, clamp01, ef,
+                                      ctx->stream));
+  else
+    MSBG_CUDA_TRY(ctx, launch_mcf(ch.pool.as<float>(), ch.slot.as<int>(), ctx->listBuf.as<int>(),
+                                  start, ctx->nbx, ctx->nby, ctx->nbz, ch.bsx, ch.emptyVal,
+                                  ch.fullVal, nIter, dt, clamp01, ef, ctx->stream));
   return MSBG_OK;
 }
 
@@ -288,6 +331,8 @@ extern "C" int msbg_gpu_pde_mcf_device(msbg_gpu_ctx* ctx, float* pool, const int
     return MSBG_EINVARG;
   if (!(bsx == 8 || bsx == 16 || bsx == 32)) return set_error(ctx, MSBG_EINVARG, "bsx=%d", bsx);
   if (!pow2(bsx)) return MSBG_EINVARG;
+  if (reinterpret_cast<uintptr_t>(pool) % 8)
+    return set_error(ctx, MSBG_EINVARG, "pool must be 8-byte aligned (voxel pairs are copied whole)");
   const int nIter = numIter + (numIter & 1);
   int* ef = err_flag(ctx);
   if (!ef) return set_error(ctx, MSBG_ENOMEM, "error flag allocation failed");

@@ -51,15 +51,18 @@ struct DeviceBuffer {
   T* as() const { return reinterpret_cast<T*>(p); }
 };
 
-// One uploaded FP32 channel at one resolution level.
+// One uploaded channel at one resolution level: FP32 or 16-bit render
+// density (dtype MSBG_F32 / MSBG_U16).
 struct Channel {
   int level = 0;
   int bsx = 0;
+  int dtype = MSBG_F32;
+  uint16_t emptyQ = 0, fullQ = 0;  // const values of a 16-bit channel (raw)
   int64_t nValue = 0;
   float emptyVal = 0.f, fullVal = 0.f;
   std::vector<int> slotHost;   // [nb] slot or SLOT_* code
   std::vector<int8_t> kindHost;
-  DeviceBuffer pool;           // [nValue][bsx^3] float
+  DeviceBuffer pool;           // [nValue][bsx^3] float or uint16_t
   DeviceBuffer slot;           // [nb] int
 };
 
@@ -108,5 +111,10 @@ cudaError_t launch_mcf(float* pool, const int* slotOf, const int* colourList,
                        const int* colourStart, int nbx, int nby, int nbz, int bsx,
                        float emptyVal, float fullVal, int nIter, float dt, int clamp01,
                        int* errFlag, cudaStream_t stream);
+// The same passes on a 16-bit render-density pool (const values raw).
+cudaError_t launch_mcf_u16(uint16_t* pool, const int* slotOf, const int* colourList,
+                           const int* colourStart, int nbx, int nby, int nbz, int bsx,
+                           uint16_t emptyVal, uint16_t fullVal, int nIter, float dt, int clamp01,
+                           int* errFlag, cudaStream_t stream);
 
 }  // namespace msbg

@@ -3,26 +3,45 @@
 // Restates the GPU way what MultiresSparseGrid::applyChannelPdeFast<float>
 // does for laplTyp PDE_MEAN_CURVATURE with OPT_8_COLOR_SCHEME
 // (src/msbg4.cpp:348-851): per iteration, 8 colour passes; in a pass every
-// block of that colour copies itself plus a 1-voxel halo (26 neighbours,
-// src/halo.cpp:266-479, BC_NEUMANN src/halo.h:280-287) into on-chip memory,
-// applies the 19-point curvature stencil (src/msbg4.cpp:559-637) and writes
-// the result in place.  Same-colour blocks are never 26-neighbours, so one
-// CTA per block and one launch per colour reproduces the reference's
-// parallel pass exactly.
+// block of that colour copies itself plus a 1-voxel halo (src/halo.cpp:266-479,
+// BC_NEUMANN src/halo.h:280-287) into on-chip memory, applies the 19-point
+// curvature stencil (src/msbg4.cpp:559-637) and writes the result in place.
+// Same-colour blocks are never 26-neighbours, so one CTA per block and one
+// launch per colour reproduces the reference's parallel pass exactly.
 //
-// CTA layout: one block per CTA, BSX*BSX threads, thread (x,y) owns a z
-// column and keeps a 3-plane register window of the 5-point cross, so each
-// voxel costs 9 shared-memory reads instead of 19.  The block and its
-// 26-neighbour shell arrive in the padded (BSX+2)^3 tile by asynchronous
-// 4-byte copies (cp.async), every thread's copies in flight at once; with no
-// staging buffer a 16^3 block needs 23 KB and 8 CTAs fill an SM.  The
-// kernel has no waits that could time out.  A listed block whose slot is not
-// a value block (NULL, const, or a caller's slot map that disagrees with the
-// list) is skipped and reported through errFlag (MCF_ERR_NOT_VALUE).
+// The stencil is issue-bound (about 60 FP32 operations and 9 shared-memory
+// reads per voxel against 8 bytes of HBM traffic), so the kernel works on
+// pairs of x-adjacent voxels with the packed FP32 instructions of sm_100
+// (add/sub/mul/fma.rn.f32x2): one instruction updates both voxels of a pair,
+// and a pair arrives from shared memory in one 8-byte load.
+//   * CTA layout: one block per CTA, BSX*BSX/2 threads; thread (i, y) owns
+//     the x pair (2i, 2i+1) of row y and marches up z with a three-plane
+//     register window of the 5-point cross.
+//   * The padded tile holds x in [-2, BSX+1] (row pitch BSX+4, so every pair
+//     starts on an 8-byte boundary) and y, z in [-1, BSX].  The x-1 and x+1
+//     pairs are rebuilt in registers from three aligned pairs.
+//   * The block and its 1-voxel shell (faces and edges; the 19-point stencil
+//     reads no corner) arrive by asynchronous copies straight into the tile:
+//     8-byte copies for x pairs, 4-byte copies for the x faces.
+//   * The curvature is evaluated with the central differences left unscaled:
+//     with d = f(+1) - f(-1) (= 2 f_x) and s = the mixed second difference
+//     (= 4 f_xy) the reference's H = [...] / |grad f|^2 becomes
+//     (N1 - N2/2) / G, G = |d|^2, with the threshold |grad f|^2 > 1e-7 read as
+//     G > 4e-7: every rescaling is by a power of two and so exact.
+// Channels are FP32 or the reference's 16-bit render density (RSURF_16_BIT,
+// src/msbgcell.h:67-68): q in [0, 65535] read as q * (1/65535) and stored as
+// round(phi * 65535) (src/sbg.h:225-232, 360-368; src/msbg4.cpp:829-839).
+// 16-bit blocks arrive through ordinary loads and are widened into the
+// FP32 tile.
+// A listed block whose slot is not a value block (NULL, const, or a caller's
+// slot map that disagrees with the list) is skipped and reported through
+// errFlag (MCF_ERR_NOT_VALUE).  The kernel has no waits that could time out.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -33,160 +52,341 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// 4-byte asynchronous global -> shared copy (no register round trip); the
-// thread's copies complete at cp_async_wait_all.
+// Asynchronous global -> shared copies (no register round trip); a thread's
+// copies complete at cp_async_wait_all.
 __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src)
                : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_all;" ::: "memory");
+__device__ __forceinline__ void cp_async8(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// A pair of FP32 values in one 64-bit register and the packed arithmetic.
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 pk(float lo, float hi) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void upk(f2 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+  f2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+  f2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+  f2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+  f2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ f2 ld2(const float* p) {
+  return *reinterpret_cast<const f2*>(p);
+}
+// (hi of a, lo of b): the pair shifted by one voxel
+__device__ __forceinline__ f2 mid2(f2 a, f2 b) {
+  float a0, a1, b0, b1;
+  upk(a, a0, a1);
+  upk(b, b0, b1);
+  return pk(a1, b0);
 }
 
 template <int BSX>
 struct McfTile {
-  static constexpr int H = BSX + 2;
+  static constexpr int RP = BSX + 4;         // row pitch: x + 2 in [0, BSX + 4)
+  static constexpr int PP = RP * (BSX + 2);  // plane pitch: y + 1 in [0, BSX + 2)
   static constexpr int NV = BSX * BSX * BSX;
-  static constexpr int NT = BSX * BSX;
-  static constexpr int NHALO = 2 * H * H + 2 * H * (H - 2) + 2 * (H - 2) * (H - 2);
-  // dynamic smem: the padded H^3 tile (23 KB for 16^3 blocks, so 8 CTAs of
-  // 256 threads fit an SM)
-  static constexpr size_t SMEM = sizeof(float) * H * H * H;
+  static constexpr int NT = BSX * BSX / 2;   // one thread per x pair of a row
+  static constexpr int HP = BSX / 2;         // pairs per row
+  static constexpr size_t SMEM = sizeof(float) * PP * (BSX + 2);
+  __device__ static int at(int x, int y, int z) { return (x + 2) + RP * (y + 1) + PP * (z + 1); }
 };
 
-// Decode the i-th voxel of the 1-voxel shell around the block into padded
-// tile coordinates (hx,hy,hz) in [0,H).
-template <int H>
-__device__ __forceinline__ void shell_coord(int i, int& hx, int& hy, int& hz) {
-  constexpr int A = H * H, B = H * (H - 2), C = (H - 2) * (H - 2);
-  if (i < 2 * A) {
-    hz = (i >= A) ? H - 1 : 0;
-    int r = i - ((i >= A) ? A : 0);
-    hy = r / H;
-    hx = r - hy * H;
-  } else if (i < 2 * A + 2 * B) {
-    int j = i - 2 * A;
-    hy = (j >= B) ? H - 1 : 0;
-    int r = j - ((j >= B) ? B : 0);
-    hz = 1 + r / H;
-    hx = r - (hz - 1) * H;
-  } else {
-    int k = i - 2 * A - 2 * B;
-    hx = (k >= C) ? H - 1 : 0;
-    int r = k - ((k >= C) ? C : 0);
-    hz = 1 + r / (H - 2);
-    hy = 1 + (r - (hz - 1) * (H - 2));
+// Where halo voxel (x, y, z) (block coordinates, some outside [0, BSX)) comes
+// from: a neighbour value block, a const block, or the own block clamped to
+// its boundary (BC_NEUMANN for NULL neighbours and the domain boundary).
+template <int BSX, typename T>
+__device__ __forceinline__ const T* halo_src(const T* pool, const int* nbSlot, const T* own,
+                                             int x, int y, int z, int& constKind) {
+  constexpr int M = BSX - 1;
+  const int dx = x < 0 ? -1 : (x > M ? 1 : 0);
+  const int dy = y < 0 ? -1 : (y > M ? 1 : 0);
+  const int dz = z < 0 ? -1 : (z > M ? 1 : 0);
+  const int s = nbSlot[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
+  constKind = 0;
+  if (s >= 0)
+    return pool + (size_t)s * (BSX * BSX * BSX) + ((x & M) + BSX * ((y & M) + BSX * (z & M)));
+  if (s == SLOT_EMPTY || s == SLOT_FULL) {
+    constKind = s == SLOT_EMPTY ? 1 : 2;
+    return nullptr;
   }
+  const int cx = min(max(x, 0), M), cy = min(max(y, 0), M), cz = min(max(z, 0), M);
+  return own + (cx + BSX * (cy + BSX * cz));
 }
 
-template <int BSX>
-__global__ void __launch_bounds__(BSX* BSX)
-    mcf_colour_kernel(float* __restrict__ pool, const int* __restrict__ slotOf,
-                      const int* __restrict__ list, int nbx, int nby, int nbz,
-                      float emptyVal, float fullVal, float dt, int clamp01,
-                      int* __restrict__ errFlag) {
-  using T = McfTile<BSX>;
-  constexpr int H = T::H, H2 = H * H, NV = T::NV, NT = T::NT;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  float* tile = reinterpret_cast<float*>(smem_raw);
-  __shared__ int nbSlot[27];
+constexpr float U16_SCALE = 1.0f / 65535.0f;  // RENDER_DENS_TO_FLOAT_UI16
 
-  const int tid = threadIdx.x;
-  const int bid = list[blockIdx.x];
-  const int bx = bid % nbx, by = (bid / nbx) % nby, bz = bid / (nbx * nby);
-  const int slot0 = slotOf[bid];
-  if (slot0 < 0) {  // uniform per CTA, before any barrier or copy
-    if (tid == 0) atomicOr(errFlag, MCF_ERR_NOT_VALUE);
-    return;
-  }
-  const float* own = pool + (size_t)slot0 * NV;
-
-  if (tid < 27) {
-    int dx = tid % 3 - 1, dy = (tid / 3) % 3 - 1, dz = tid / 9 - 1;
-    int x = bx + dx, y = by + dy, z = bz + dz;
-    int s = SLOT_OUT;
-    if (x >= 0 && y >= 0 && z >= 0 && x < nbx && y < nby && z < nbz)
-      s = slotOf[x + nbx * (y + nby * z)];
-    nbSlot[tid] = s;
-  }
-  __syncthreads();
-  // The interior: one asynchronous 4-byte copy per voxel straight into the
-  // padded tile (consecutive threads, consecutive voxels).
-  for (int e = tid; e < NV; e += NT) {
+// Issue the copies of one block and its shell into a tile (FP32: asynchronous
+// copies, completed by the caller's cp.async wait; 16-bit: loads widened into
+// the tile on the spot).  nbSlot: the slots of the 27 blocks around it.
+template <int BSX, typename T>
+__device__ __forceinline__ void mcf_fill(float* tile, const T* __restrict__ pool,
+                                         const int* nbSlot, float emptyVal, float fullVal,
+                                         int tid) {
+  using Tl = McfTile<BSX>;
+  constexpr int NV = Tl::NV, NT = Tl::NT, HP = Tl::HP;
+  constexpr bool F32 = std::is_same<T, float>::value;
+  const T* own = pool + (size_t)nbSlot[13] * NV;
+  // interior: one x pair per copy (8-byte asynchronous copies for FP32; for
+  // 16-bit values one 4-byte load, widened into the tile)
+#pragma unroll 8
+  for (int p = tid; p < NV / 2; p += NT) {
+    const int e = 2 * p;
     const int x = e % BSX, y = (e / BSX) % BSX, z = e / (BSX * BSX);
-    cp_async4(tile + (x + 1) + H * (y + 1) + H2 * (z + 1), own + e);
-  }
-
-  // Gather the 26 neighbour pieces straight into the padded tile: voxels of
-  // stored blocks by asynchronous copies (all of a thread's copies in flight
-  // at once), constant blocks by plain stores.
-  for (int i = tid; i < T::NHALO; i += NT) {
-    int hx, hy, hz;
-    shell_coord<H>(i, hx, hy, hz);
-    int x = hx - 1, y = hy - 1, z = hz - 1;
-    int dx = x < 0 ? -1 : (x >= BSX ? 1 : 0);
-    int dy = y < 0 ? -1 : (y >= BSX ? 1 : 0);
-    int dz = z < 0 ? -1 : (z >= BSX ? 1 : 0);
-    int s = nbSlot[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
-    float* d = tile + hx + H * hy + H2 * hz;
-    if (s >= 0) {
-      cp_async4(d, pool + (size_t)s * NV + ((x & (BSX - 1)) + BSX * ((y & (BSX - 1)) + BSX * (z & (BSX - 1)))));
-    } else if (s == SLOT_EMPTY) {
-      *d = emptyVal;
-    } else if (s == SLOT_FULL) {
-      *d = fullVal;
-    } else {  // NULL block or outside the domain: Neumann, own value clamped
-      int cx = min(max(x, 0), BSX - 1), cy = min(max(y, 0), BSX - 1), cz = min(max(z, 0), BSX - 1);
-      cp_async4(d, own + (cx + BSX * (cy + BSX * cz)));
+    float* d = tile + Tl::at(x, y, z);
+    if constexpr (F32) {
+      cp_async8(d, own + e);
+    } else {
+      const uint32_t v = *reinterpret_cast<const uint32_t*>(own + e);
+      *reinterpret_cast<float2*>(d) =
+          make_float2((float)(v & 0xffffu) * U16_SCALE, (float)(v >> 16) * U16_SCALE);
     }
   }
-  cp_async_wait_all();
-
-  __syncthreads();  // every thread's copies have landed (waited above)
-
-  // Column sweep with a 3-plane register window of the 5-point cross.
-  const int x = tid % BSX, y = tid / BSX;
-  const float* col = tile + (x + 1) + H * (y + 1);
-  float* out = pool + (size_t)slot0 * NV + x + BSX * y;
-  float cm = col[0], xmm = col[-1], xpm = col[1], ymm = col[-H], ypm = col[H];            // z-1
-  float c0 = col[H2], xm0 = col[H2 - 1], xp0 = col[H2 + 1], ym0 = col[H2 - H], yp0 = col[H2 + H];  // z
-#pragma unroll
-  for (int z = 0; z < BSX; z++) {
-    const float* p1 = col + H2 * (z + 2);
-    float cp = p1[0], xmp = p1[-1], xpp = p1[1], ymp = p1[-H], ypp = p1[H];  // z+1
-    const float* p0 = col + H2 * (z + 1);
-    float fpp = p0[1 + H], fpm = p0[1 - H], fmp = p0[-1 + H], fmm = p0[-1 - H];
-
-    float f0 = c0, f1 = xm0, f2 = xp0, f3 = ym0, f4 = yp0, f5 = cm, f6 = cp;
-    float fx = 0.5f * (f2 - f1), fy = 0.5f * (f4 - f3), fz = 0.5f * (f6 - f5);
-    float fxx = f1 + f2 - 2.f * f0, fyy = f3 + f4 - 2.f * f0, fzz = f5 + f6 - 2.f * f0;
-    float fy_right = (fpp - fpm) * 0.5f, fy_left = (fmp - fmm) * 0.5f;
-    float fz_right = (xpp - xpm) * 0.5f, fz_left = (xmp - xmm) * 0.5f;
-    float fz_up = (ypp - ypm) * 0.5f, fz_down = (ymp - ymm) * 0.5f;
-    float fyx = (fy_right - fy_left) * 0.5f;
-    float fzx = (fz_right - fz_left) * 0.5f;
-    float fzy = (fz_up - fz_down) * 0.5f;
-    float fx2 = fx * fx, fy2 = fy * fy, fz2 = fz * fz;
-    float H_ = (fy2 + fz2) * fxx + (fx2 + fz2) * fyy + (fx2 + fy2) * fzz -
-               2.0f * (fx * fy * fyx + fx * fz * fzx + fy * fz * fzy);
-    float g = fx2 + fy2 + fz2;
-    H_ = g > 1e-7f ? __fdividef(H_, g) : 0.0f;
-    float D = fminf(fmaxf(dt * H_, -0.1f), 0.1f);
-    float phi = f0 + D;
-    if (clamp01) phi = fminf(fmaxf(phi, 0.0f), 1.0f);
-    out[BSX * BSX * z] = phi;
-
-    cm = c0; xmm = xm0; xpm = xp0; ymm = ym0; ypm = yp0;
-    c0 = cp; xm0 = xmp; xp0 = xpp; ym0 = ymp; yp0 = ypp;
+  // shell voxels with x inside the block (z faces, y faces, x-direction
+  // edges): the ring of (y, z) around the block, one x pair each
+  constexpr int RING = 4 * BSX + 4;
+  for (int q = tid; q < RING * HP; q += NT) {
+    const int r = q / HP, x = 2 * (q % HP);
+    int y, z;
+    if (r < 2 * (BSX + 2)) {  // z = -1 and z = BSX, y in [-1, BSX]
+      z = r < BSX + 2 ? -1 : BSX;
+      y = (r % (BSX + 2)) - 1;
+    } else {  // y = -1 and y = BSX, z in [0, BSX)
+      const int r2 = r - 2 * (BSX + 2);
+      y = r2 < BSX ? -1 : BSX;
+      z = r2 % BSX;
+    }
+    int ck;
+    const T* src = halo_src<BSX, T>(pool, nbSlot, own, x, y, z, ck);
+    float* d = tile + Tl::at(x, y, z);
+    if (src) {
+      if constexpr (F32) {
+        cp_async8(d, src);
+      } else {
+        const uint32_t v = *reinterpret_cast<const uint32_t*>(src);
+        d[0] = (float)(v & 0xffffu) * U16_SCALE;
+        d[1] = (float)(v >> 16) * U16_SCALE;
+      }
+    } else {
+      const float v = ck == 1 ? emptyVal : fullVal;
+      d[0] = v;
+      d[1] = v;
+    }
+  }
+  // shell voxels with x = -1 or x = BSX (x faces, y- and z-direction edges):
+  // (y, z) in [-1, BSX]^2 without the four corners, one voxel each
+  constexpr int SIDE = (BSX + 2) * (BSX + 2);
+  for (int q = tid; q < 2 * SIDE; q += NT) {
+    const int side = q / SIDE, r = q % SIDE;
+    const int y = r % (BSX + 2) - 1, z = r / (BSX + 2) - 1;
+    if ((y < 0 || y >= BSX) && (z < 0 || z >= BSX)) continue;  // corner: not read
+    const int x = side ? BSX : -1;
+    int ck;
+    const T* src = halo_src<BSX, T>(pool, nbSlot, own, x, y, z, ck);
+    float* d = tile + Tl::at(x, y, z);
+    if (src) {
+      if constexpr (F32)
+        cp_async4(d, src);
+      else
+        *d = (float)(*src) * U16_SCALE;
+    } else {
+      *d = ck == 1 ? emptyVal : fullVal;
+    }
   }
 }
 
+// The 19-point update of one block from its tile, stored in place.
+template <int BSX, typename T>
+__device__ __forceinline__ void mcf_compute(const float* tile, T* __restrict__ block, float dt,
+                                            int clamp01, int tid) {
+  using Tl = McfTile<BSX>;
+  constexpr int RP = Tl::RP, PP = Tl::PP, HP = Tl::HP;
+  // Column march of the x pair (x0, x0 + 1) of row y.
+  const int x0 = 2 * (tid % HP), y = tid / HP;
+  const float* col = tile + Tl::at(x0, y, -1);  // plane z = -1
+  T* out = block + x0 + BSX * y;
+  const f2 m2 = pk(-2.f, -2.f), mh = pk(-0.5f, -0.5f);
+  // window: centre, x-1, x+1 pairs of row y; centre pairs of rows y-1, y+1
+  f2 Cm, XMm, XPm, YMm, YPm;  // plane z-1
+  f2 C0, XM0, XP0, YM0, YP0;  // plane z
+  {
+    const float* p = col;
+    const f2 a = ld2(p - 2), b = ld2(p), c = ld2(p + 2);
+    Cm = b; XMm = mid2(a, b); XPm = mid2(b, c);
+    YMm = ld2(p - RP); YPm = ld2(p + RP);
+    p += PP;
+    const f2 a1 = ld2(p - 2), b1 = ld2(p), c1 = ld2(p + 2);
+    C0 = b1; XM0 = mid2(a1, b1); XP0 = mid2(b1, c1);
+    YM0 = ld2(p - RP); YP0 = ld2(p + RP);
+  }
+#pragma unroll 4
+  for (int z = 0; z < BSX; z++) {
+    const float* p0 = col + PP * (z + 1);  // plane z
+    const float* p1 = p0 + PP;             // plane z+1
+    const f2 a = ld2(p1 - 2), b = ld2(p1), c = ld2(p1 + 2);
+    const f2 Cp = b, XMp = mid2(a, b), XPp = mid2(b, c);
+    const f2 YMp = ld2(p1 - RP), YPp = ld2(p1 + RP);
+    // x-1 and x+1 pairs of rows y-1 and y+1 in plane z (the xy diagonals)
+    const f2 XMYM = mid2(ld2(p0 - RP - 2), YM0), XPYM = mid2(YM0, ld2(p0 - RP + 2));
+    const f2 XMYP = mid2(ld2(p0 + RP - 2), YP0), XPYP = mid2(YP0, ld2(p0 + RP + 2));
+
+    const f2 dx = sub2(XP0, XM0), dy = sub2(YP0, YM0), dz = sub2(Cp, Cm);  // 2 f_x ...
+    const f2 fxx = fma2(m2, C0, add2(XM0, XP0));
+    const f2 fyy = fma2(m2, C0, add2(YM0, YP0));
+    const f2 fzz = fma2(m2, C0, add2(Cm, Cp));
+    const f2 sxy = sub2(sub2(XPYP, XPYM), sub2(XMYP, XMYM));  // 4 f_xy
+    const f2 sxz = sub2(sub2(XPp, XPm), sub2(XMp, XMm));      // 4 f_xz
+    const f2 syz = sub2(sub2(YPp, YPm), sub2(YMp, YMm));      // 4 f_yz
+    const f2 dx2 = mul2(dx, dx), dy2 = mul2(dy, dy), dz2 = mul2(dz, dz);
+    f2 n1 = mul2(add2(dy2, dz2), fxx);
+    n1 = fma2(add2(dx2, dz2), fyy, n1);
+    n1 = fma2(add2(dx2, dy2), fzz, n1);
+    f2 n2 = mul2(mul2(dx, dy), sxy);
+    n2 = fma2(mul2(dx, dz), sxz, n2);
+    n2 = fma2(mul2(dy, dz), syz, n2);
+    const f2 num = fma2(mh, n2, n1);
+    const f2 G = add2(add2(dx2, dy2), dz2);
+    float nl, nh, gl, gh, fl, fh;
+    upk(num, nl, nh);
+    upk(G, gl, gh);
+    upk(C0, fl, fh);
+    constexpr float GMIN = 4.0f * 1e-7f;  // |grad f|^2 > 1e-7 with d = 2 grad f
+    const float hl = gl > GMIN ? __fdividef(nl, gl) : 0.0f;
+    const float hh = gh > GMIN ? __fdividef(nh, gh) : 0.0f;
+    float pl = fl + fminf(fmaxf(dt * hl, -0.1f), 0.1f);
+    float ph = fh + fminf(fmaxf(dt * hh, -0.1f), 0.1f);
+    if (clamp01) {
+      pl = fminf(fmaxf(pl, 0.0f), 1.0f);
+      ph = fminf(fmaxf(ph, 0.0f), 1.0f);
+    }
+    if constexpr (std::is_same<T, float>::value) {
+      *reinterpret_cast<float2*>(out + BSX * BSX * z) = make_float2(pl, ph);
+    } else {  // round to nearest (even), as round_to_int under the default MXCSR
+      const uint32_t ql = (uint32_t)min(max(__float2int_rn(pl * 65535.0f), 0), 65535);
+      const uint32_t qh = (uint32_t)min(max(__float2int_rn(ph * 65535.0f), 0), 65535);
+      *reinterpret_cast<uint32_t*>(out + BSX * BSX * z) = ql | (qh << 16);
+    }
+
+    Cm = C0; XMm = XM0; XPm = XP0; YMm = YM0; YPm = YP0;
+    C0 = Cp; XM0 = XMp; XP0 = XPp; YM0 = YMp; YP0 = YPp;
+  }
+}
+
+// Tile stages per CTA: two (the next block's copies in flight while this one
+// is computed) where two tiles fit next to the other CTAs of an SM, one for
+// 32^3 blocks (a 166 KB tile).
 template <int BSX>
-cudaError_t launch_mcf_t(float* pool, const int* slotOf, const int* colourList,
+__host__ __device__ constexpr int mcf_stages() { return BSX <= 16 ? 2 : 1; }
+// CTAs per SM the launch plans for (persistent grid = SMs x this).
+template <int BSX>
+__host__ __device__ constexpr int mcf_ctas_per_sm() { return BSX == 8 ? 16 : BSX == 16 ? 4 : 1; }
+
+// One colour pass: the CTAs walk the pass's block list with a stride of
+// gridDim.x; with two stages the copies of block k + gridDim.x are issued
+// before block k is computed.
+template <int BSX, typename T>
+__global__ void __launch_bounds__(BSX* BSX / 2)
+    mcf_colour_kernel(T* __restrict__ pool, const int* __restrict__ slotOf,
+                      const int* __restrict__ list, int n, int nbx, int nby, int nbz,
+                      float emptyVal, float fullVal, float dt, int clamp01,
+                      int* __restrict__ errFlag) {
+  using Tl = McfTile<BSX>;
+  constexpr int ST = mcf_stages<BSX>();
+  constexpr int TILE = Tl::PP * (BSX + 2);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* tiles = reinterpret_cast<float*>(smem_raw);
+  __shared__ int nbSlot[2][27];
+  const int tid = threadIdx.x;
+  const int G = gridDim.x;
+  int k = blockIdx.x;
+  if (k >= n) return;
+  // the slots of the 27 blocks around list[kk] into nbSlot[s]
+  auto neighbours = [&](int kk, int s) {
+    if (tid < 27) {
+      const int bid = list[kk];
+      const int bx = bid % nbx, by = (bid / nbx) % nby, bz = bid / (nbx * nby);
+      const int dx = tid % 3 - 1, dy = (tid / 3) % 3 - 1, dz = tid / 9 - 1;
+      const int x = bx + dx, y = by + dy, z = bz + dz;
+      int sl = SLOT_OUT;
+      if (x >= 0 && y >= 0 && z >= 0 && x < nbx && y < nby && z < nbz)
+        sl = slotOf[x + nbx * (y + nby * z)];
+      nbSlot[s][tid] = sl;
+    }
+  };
+  // a listed block whose own slot is not a value block is skipped (uniform
+  // per CTA: every thread reads the same shared slot)
+  auto fill = [&](int s) {
+    if (nbSlot[s][13] >= 0)
+      mcf_fill<BSX, T>(tiles + s * TILE, pool, nbSlot[s], emptyVal, fullVal, tid);
+    cp_async_commit();
+  };
+  neighbours(k, 0);
+  __syncthreads();
+  fill(0);
+  for (int it = 0; k < n; it++, k += G) {
+    const int s = ST == 2 ? (it & 1) : 0;
+    const int kn = k + G;
+    if (ST == 2) {
+      if (kn < n) neighbours(kn, s ^ 1);
+      __syncthreads();  // nbSlot[s^1] written; stage s^1 is free since the last pass
+      if (kn < n) fill(s ^ 1);
+      else cp_async_commit();
+      cp_async_wait_group<1>();  // block k's copies have landed (the newest may fly)
+    } else {
+      cp_async_wait_group<0>();
+    }
+    __syncthreads();
+    const int slot0 = nbSlot[s][13];
+    if (slot0 < 0) {
+      if (tid == 0) atomicOr(errFlag, MCF_ERR_NOT_VALUE);
+    } else {
+      mcf_compute<BSX, T>(tiles + s * TILE, pool + (size_t)slot0 * Tl::NV, dt, clamp01, tid);
+    }
+    __syncthreads();  // stage s may be refilled
+    if (ST == 1 && kn < n) {
+      neighbours(kn, 0);
+      __syncthreads();
+      fill(0);
+    }
+  }
+}
+
+template <int BSX, typename T>
+cudaError_t launch_mcf_t(T* pool, const int* slotOf, const int* colourList,
                          const int* colourStart, int nbx, int nby, int nbz,
                          float emptyVal, float fullVal, int nIter, float dt,
                          int clamp01, int* errFlag, cudaStream_t stream) {
-  using T = McfTile<BSX>;
+  using Tl = McfTile<BSX>;
   // The shared-memory limit is an attribute of the kernel on each device:
   // set it once per device (bit per device; a race only repeats the call).
   static std::atomic<uint64_t> attrSet{0};
@@ -195,20 +395,50 @@ cudaError_t launch_mcf_t(float* pool, const int* slotOf, const int* colourList,
   if (e != cudaSuccess) return e;
   const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
   if (!bit || !(attrSet.load(std::memory_order_acquire) & bit)) {
-    e = cudaFuncSetAttribute(mcf_colour_kernel<BSX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)T::SMEM);
+    e = cudaFuncSetAttribute(mcf_colour_kernel<BSX, T>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(Tl::SMEM * mcf_stages<BSX>()));
     if (e != cudaSuccess) return e;
     attrSet.fetch_or(bit, std::memory_order_acq_rel);
   }
+  static int numSMs[64] = {0};
+  if (dev < 64 && !numSMs[dev]) {
+    int v = 0;
+    e = cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    numSMs[dev] = v;
+  }
+  const int maxGrid = (dev < 64 ? numSMs[dev] : 148) * mcf_ctas_per_sm<BSX>();
   for (int it = 0; it < nIter; it++)
     for (int c = 0; c < 8; c++) {
       int n = colourStart[c + 1] - colourStart[c];
       if (n <= 0) continue;
-      mcf_colour_kernel<BSX><<<n, T::NT, T::SMEM, stream>>>(
-          pool, slotOf, colourList + colourStart[c], nbx, nby, nbz, emptyVal, fullVal, dt,
+      const int grid = mcf_stages<BSX>() == 2 ? std::min(n, maxGrid) : n;
+      mcf_colour_kernel<BSX, T><<<grid, Tl::NT, Tl::SMEM * mcf_stages<BSX>(), stream>>>(
+          pool, slotOf, colourList + colourStart[c], n, nbx, nby, nbz, emptyVal, fullVal, dt,
           clamp01, errFlag);
     }
   return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_mcf_typed(T* pool, const int* slotOf, const int* colourList,
+                             const int* colourStart, int nbx, int nby, int nbz, int bsx,
+                             float emptyVal, float fullVal, int nIter, float dt, int clamp01,
+                             int* errFlag, cudaStream_t stream) {
+  switch (bsx) {
+    case 8:
+      return launch_mcf_t<8, T>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, emptyVal,
+                                fullVal, nIter, dt, clamp01, errFlag, stream);
+    case 16:
+      return launch_mcf_t<16, T>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, emptyVal,
+                                 fullVal, nIter, dt, clamp01, errFlag, stream);
+    case 32:
+      return launch_mcf_t<32, T>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, emptyVal,
+                                 fullVal, nIter, dt, clamp01, errFlag, stream);
+    default:
+      return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace
@@ -217,19 +447,18 @@ cudaError_t launch_mcf(float* pool, const int* slotOf, const int* colourList,
                        const int* colourStart, int nbx, int nby, int nbz, int bsx,
                        float emptyVal, float fullVal, int nIter, float dt, int clamp01,
                        int* errFlag, cudaStream_t stream) {
-  switch (bsx) {
-    case 8:
-      return launch_mcf_t<8>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, emptyVal,
-                             fullVal, nIter, dt, clamp01, errFlag, stream);
-    case 16:
-      return launch_mcf_t<16>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, emptyVal,
-                              fullVal, nIter, dt, clamp01, errFlag, stream);
-    case 32:
-      return launch_mcf_t<32>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, emptyVal,
-                              fullVal, nIter, dt, clamp01, errFlag, stream);
-    default:
-      return cudaErrorInvalidValue;
-  }
+  return launch_mcf_typed<float>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, bsx,
+                                 emptyVal, fullVal, nIter, dt, clamp01, errFlag, stream);
+}
+
+cudaError_t launch_mcf_u16(uint16_t* pool, const int* slotOf, const int* colourList,
+                           const int* colourStart, int nbx, int nby, int nbz, int bsx,
+                           uint16_t emptyVal, uint16_t fullVal, int nIter, float dt, int clamp01,
+                           int* errFlag, cudaStream_t stream) {
+  // const blocks read like stored values: q * (1/65535)
+  return launch_mcf_typed<uint16_t>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, bsx,
+                                    (float)emptyVal * U16_SCALE, (float)fullVal * U16_SCALE, nIter,
+                                    dt, clamp01, errFlag, stream);
 }
 
 }  // namespace msbg

@@ -67,6 +67,7 @@ extern "C" int msbg_gpu_pde_mcf_noalloc(float* pool, const int* slotOf, const in
                                         int clamp01, void* stream, int* timedOut) {
   if (!pool || !slotOf || (n > 0 && !blockList) || n < 0 || numIter < 0) return MSBG_EINVARG;
   if (n > MAXB) return MSBG_EINVARG;  // beyond the fixed scratch: see the header
+  if (reinterpret_cast<uintptr_t>(pool) % 8) return MSBG_EINVARG;  // voxel pairs are copied whole
   if (!(bsx == 8 || bsx == 16 || bsx == 32) || nbx <= 0 || nby <= 0 || nbz <= 0)
     return MSBG_EINVARG;
   const long long nb = (long long)nbx * nby * nbz;

@@ -206,7 +206,7 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
   std::string err;
   auto tp0 = std::chrono::steady_clock::now();
   rc = build_hierarchy(S.H, topo->sx, topo->sy, topo->sz, topo->bsx0, topo->nLevels,
-                       topo->blockLevel, cb, 512, &err);
+                       topo->blockLevel, topo->domainBc, cb, 512, &err);
   S.buildSeconds =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - tp0).count();
   if (rc) {

@@ -118,6 +118,8 @@ struct Hierarchy {
   int res = 0, bsx0 = 0, nLevels = 0, nb1x = 0, nb1y = 0, nb1z = 0;
   int sx = 0, sy = 0, sz = 0;
   std::vector<int> blockLevel;     // refinement map (MG level 0)
+  int domainBc[6] = {MSBG_DBC_OPEN, MSBG_DBC_OPEN, MSBG_DBC_OPEN,
+                     MSBG_DBC_OPEN, MSBG_DBC_OPEN, MSBG_DBC_OPEN};  // face = 2*dir + side
   std::vector<Level> levels;
   // coarsest-level dense inverse (FP64), fluid cell indices
   int nCoarse = 0;
@@ -127,8 +129,8 @@ struct Hierarchy {
 
 // Host construction (pressure_host.cpp).
 int build_hierarchy(Hierarchy& H, int sx, int sy, int sz, int bsx0, int nLevels,
-                    const int* blockLevel, const msbg_pressure_callbacks* cb,
-                    int maxCoarseCells, std::string* err);
+                    const int* blockLevel, const int* domainBc,
+                    const msbg_pressure_callbacks* cb, int maxCoarseCells, std::string* err);
 
 }  // namespace ps
 }  // namespace msbg

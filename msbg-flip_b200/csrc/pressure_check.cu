@@ -132,7 +132,7 @@ extern "C" int msbg_gpu_pressure_host_check(const msbg_topo_desc* topo,
   Hierarchy H;
   std::string err;
   int rc = build_hierarchy(H, topo->sx, topo->sy, topo->sz, topo->bsx0, topo->nLevels,
-                           topo->blockLevel, cb, 512, &err);
+                           topo->blockLevel, topo->domainBc, cb, 512, &err);
   if (rc) {
     fprintf(stderr, "msbg_gpu_pressure_host_check: %s\n", err.c_str());
     return rc;

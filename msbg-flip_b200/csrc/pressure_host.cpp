@@ -296,7 +296,11 @@ void sample_level0(const Ctx& C, Level& L, std::vector<uint8_t>& fluid) {
       if (side) q[dir] += 1;
       double c;
       if (onTileFace && !faceInside[dir][side]) {
-        c = h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
+        // the domain boundary: a wall has no coupling; open air is p = 0
+        // behind the face's own coefficient
+        c = C.H.domainBc[2 * dir + side] == MSBG_DBC_SOLID
+                ? 0.0
+                : h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
         if (side == 0) cdir[dir][ci] = (float)c;
         return c;
       }
@@ -641,9 +645,17 @@ bool dense_spd_inverse(std::vector<double>& A, int n, std::vector<double>& inv) 
 }  // namespace
 
 int build_hierarchy(Hierarchy& H, int sx, int sy, int sz, int bsx0, int nLevels,
-                    const int* blockLevel, const msbg_pressure_callbacks* cb,
-                    int maxCoarseCells, std::string* err) {
+                    const int* blockLevel, const int* domainBc,
+                    const msbg_pressure_callbacks* cb, int maxCoarseCells, std::string* err) {
   H = Hierarchy();
+  if (domainBc)
+    for (int f = 0; f < 6; f++) {
+      if (domainBc[f] != MSBG_DBC_OPEN && domainBc[f] != MSBG_DBC_SOLID) {
+        if (err) *err = "domainBc entries must be MSBG_DBC_OPEN or MSBG_DBC_SOLID";
+        return MSBG_EINVARG;
+      }
+      H.domainBc[f] = domainBc[f];
+    }
   H.sx = sx;
   H.sy = sy;
   H.sz = sz;

@@ -38,7 +38,10 @@ class MsbgError(RuntimeError):
 
 class TopoDesc(C.Structure):
     _fields_ = [("sx", C.c_int), ("sy", C.c_int), ("sz", C.c_int), ("bsx0", C.c_int),
-                ("nLevels", C.c_int), ("blockLevel", C.POINTER(C.c_int))]
+                ("nLevels", C.c_int), ("blockLevel", C.POINTER(C.c_int)),
+                ("domainBc", C.POINTER(C.c_int))]
+
+DBC_OPEN, DBC_SOLID = 0, 1
 
 
 def _p(a, ct):
@@ -65,6 +68,10 @@ def lib():
         "msbg_gpu_sync_topology": (i32, [vp, C.POINTER(TopoDesc)]),
         "msbg_gpu_upload_channel": (i32, [vp, i32, i32, pi8, C.POINTER(pf32), pf32, f32, f32]),
         "msbg_gpu_download_channel": (i32, [vp, i32, C.POINTER(pf32), pf32]),
+        "msbg_gpu_upload_channel_u16": (i32, [vp, i32, i32, pi8, C.POINTER(C.POINTER(C.c_uint16)),
+                                              C.POINTER(C.c_uint16), C.c_uint16, C.c_uint16]),
+        "msbg_gpu_download_channel_u16": (i32, [vp, i32, C.POINTER(C.POINTER(C.c_uint16)),
+                                                C.POINTER(C.c_uint16)]),
         "msbg_gpu_channel_num_value_blocks": (i32, [vp, i32, C.POINTER(C.c_int64)]),
         "msbg_gpu_channel_device_ptr": (i32, [vp, i32, C.POINTER(vp)]),
         "msbg_gpu_pde_mcf": (i32, [vp, i32, pi32, i32, i32, f32, i32]),
@@ -198,6 +205,21 @@ class Context:
     def download_channel(self, chan, out):
         self._check(self._L.msbg_gpu_download_channel(self._h, chan, None, _p(out, C.c_float)),
                     "download_channel")
+        return out
+
+    def upload_channel_u16(self, chan, level, kind, packed, empty_val=0, full_val=0):
+        """msbg_gpu_upload_channel_u16: a 16-bit render-density channel (raw values)."""
+        kind = np.ascontiguousarray(kind, np.int8)
+        packed = np.ascontiguousarray(packed, np.uint16)
+        self._check(self._L.msbg_gpu_upload_channel_u16(
+            self._h, chan, level, _p(kind, C.c_int8), None, _p(packed, C.c_uint16),
+            int(empty_val), int(full_val)), "upload_channel_u16")
+        self.sync()
+
+    def download_channel_u16(self, chan, out):
+        self._check(self._L.msbg_gpu_download_channel_u16(self._h, chan, None,
+                                                          _p(out, C.c_uint16)),
+                    "download_channel_u16")
         return out
 
     def num_value_blocks(self, chan):
@@ -343,11 +365,14 @@ def solve_params(**kw):
     return p
 
 
-def _ctx_pressure_prepare(self, scene):
+def _ctx_pressure_prepare(self, scene, domain_bc=None):
+    """msbg_gpu_pressure_prepare with the scene's callbacks; domain_bc: six
+    DBC_OPEN / DBC_SOLID values (-x, +x, -y, +y, -z, +z) or None."""
     _pressure_sigs(self._L)
     self._bl_p = np.ascontiguousarray(scene.block_levels, np.int32)
+    self._dbc_p = None if domain_bc is None else np.ascontiguousarray(domain_bc, np.int32)
     d = TopoDesc(scene.res, scene.res, scene.res, scene.bsx0, scene.n_levels,
-                 _p(self._bl_p, C.c_int))
+                 _p(self._bl_p, C.c_int), _p(self._dbc_p, C.c_int))
     cb = scene.callbacks()
     self._check(self._L.msbg_gpu_pressure_prepare(self._h, C.byref(d), C.byref(cb)),
                 "pressure_prepare")

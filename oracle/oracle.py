@@ -112,6 +112,32 @@ def mcf_reference(res3, bsx, kind, values, update, num_iter, dt, clamp01=False, 
     return v, secs.value
 
 
+def mcf_reference_u16(res3, bsx, kind, values, update, num_iter, dt, clamp01=True,
+                      empty_val=0, full_val=65535):
+    """Compiled reference applyChannelPdeFast<uint16_t> (16-bit render density,
+    the reference's RenderDensity); values are raw 16-bit integers.  Returns
+    (values, seconds)."""
+    L = ref()
+    if not hasattr(L, "_u16_sig"):
+        L.ref_mcf_u16.restype = C.c_int
+        L.ref_mcf_u16.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int8), C.c_uint16, C.c_uint16,
+                                                  C.POINTER(C.c_uint16), C.POINTER(C.c_int),
+                                                  C.c_int, C.c_int, C.c_float, C.c_int,
+                                                  C.POINTER(C.c_double)]
+        L._u16_sig = True
+    sx, sy, sz = res3
+    v = np.ascontiguousarray(values, np.uint16).copy()
+    kind = np.ascontiguousarray(kind, np.int8)
+    up = np.ascontiguousarray(update, np.int32)
+    secs = C.c_double(0)
+    rc = L.ref_mcf_u16(sx, sy, sz, bsx, _p(kind, C.c_int8), empty_val, full_val,
+                       _p(v, C.c_uint16), _p(up, C.c_int), len(up), num_iter, dt,
+                       int(bool(clamp01)), C.byref(secs))
+    if rc:
+        raise RuntimeError(f"ref_mcf_u16 rc={rc}")
+    return v, secs.value
+
+
 def pressure_oracle(scene, tol=1e-12, max_iter=20000):
     """FP64 CG solution of the pressure system of a msbg_gpu.PressureScene.
 

@@ -126,6 +126,68 @@ extern "C" int ref_mcf(int sx, int sy, int sz, int bsx, const int8_t* kind,
   return 0;
 }
 
+// Mean-curvature flow on the quantised render-density channel the reference
+// is built with (RSURF_16_BIT, src/msbgcell.h:67-68: RenderDensity = uint16_t),
+// as msbg_demo.cpp:297-298 and 716-727 run it: CH_UINT16_1, values stored as
+// round(phi * 65535) and read as q * (1/65535) (src/sbg.h:225-232, 360-368).
+// Same block kinds and packed layout as ref_mcf; values and the const
+// blocks' emptyVal / fullVal are raw 16-bit integers.
+extern "C" int ref_mcf_u16(int sx, int sy, int sz, int bsx, const int8_t* kind, uint16_t emptyVal,
+                           uint16_t fullVal, uint16_t* values, const int* update, int nUpdate,
+                           int numIter, float dt, int clamp01, double* seconds) {
+  MultiresSparseGrid* msbg = MultiresSparseGrid::create(
+      "REFQ", sx, sy, sz, bsx, -1, 0, -1,
+      MSBG::OPT_SINGLE_LEVEL | MSBG::OPT_SINGLE_CHANNEL_FLOAT);
+  if (!msbg) return 1;
+  const int nb = msbg->nBlocks();
+  {
+    std::vector<int> levels(nb, 0);
+    msbg->regularizeRefinementMap(levels.data());
+    msbg->setRefinementMap(levels.data(), NULL, -1, NULL, false);
+  }
+  const int chan = CH_UINT16_1;
+  SparseGrid<uint16_t>* sg = msbg->getUint16Channel(chan, 0);
+  if (!sg) {
+    MultiresSparseGrid::destroy(msbg);
+    return 2;
+  }
+  sg->reset();
+  sg->prepareDataAccess();
+  sg->setEmptyValue(emptyVal);
+  sg->setFullValue(fullVal);
+  const int nv = sg->nVoxelsInBlock();
+  size_t off = 0;
+  for (int bid = 0; bid < nb; bid++) {
+    switch (kind[bid]) {
+      case 1: {
+        uint16_t* d = sg->getBlockDataPtr(bid, 1, 0);
+        std::memcpy(d, values + off, sizeof(uint16_t) * nv);
+        off += nv;
+        break;
+      }
+      case 2: sg->setEmptyBlock(bid); break;
+      case 3: sg->setFullBlock(bid); break;
+      default: break;
+    }
+  }
+  std::vector<int> blockList(update, update + nUpdate);
+  auto t0 = std::chrono::steady_clock::now();
+  msbg->applyChannelPdeFast<uint16_t>(chan, CH_NULL, CH_NULL, &blockList,
+                                      -(PDE_MEAN_CURVATURE + OPT_8_COLOR_SCHEME), clamp01, 0, 0,
+                                      0, numIter, 1.0f, dt);
+  auto t1 = std::chrono::steady_clock::now();
+  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+  off = 0;
+  for (int bid = 0; bid < nb; bid++) {
+    if (kind[bid] != 1) continue;
+    const uint16_t* d = sg->getBlockDataPtr(bid);
+    std::memcpy(values + off, d, sizeof(uint16_t) * nv);
+    off += nv;
+  }
+  MultiresSparseGrid::destroy(msbg);
+  return 0;
+}
+
 // ---------------------------------------------------------------------------
 // FLIP pressure solver (src/msbg3.cpp:2467-3271) driven from arrays.
 //

@@ -64,3 +64,55 @@ def test_oracle_solution_satisfies_system():
     assert rr < 1e-11
     ax = oracle.pressure_apply_oracle(s, x)
     assert np.abs(ax - b).max() <= 1e-9 * np.abs(b).max()
+
+
+def test_domain_boundary_spec_sets_the_wall_faces():
+    """msbg_topo_desc.domainBc: a DBC_SOLID domain face has no coupling, a
+    DBC_OPEN one couples to p = 0 outside with the callback's coefficient
+    (setDomainBoundarySpec_, src/msbg.cpp:2462).  A pool (liquid below z = 12,
+    air above) whose face callback returns 1 everywhere, walls solid: opening
+    the -x face adds one coupling to each liquid cell at x = 0, so A x for
+    x = 1 differs by exactly 1 there and nowhere else."""
+    import ctypes as C
+
+    import numpy as np
+
+    import msbg_gpu
+    from refgrid import to_blocks
+
+    res, bsx0 = 16, 16
+    L = msbg_gpu.lib()
+    msbg_gpu._pressure_sigs(L)
+    ct = C.CFUNCTYPE(C.c_uint16, C.c_void_p, C.c_int, C.c_int, C.c_int)(
+        lambda u, x, y, z: 0 if z < 12 else 0x1000)
+    fc = C.CFUNCTYPE(C.c_float, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int)(
+        lambda u, d, x, y, z: 1.0)
+    rh = C.CFUNCTYPE(C.c_float, C.c_void_p, C.c_int, C.c_int, C.c_int)(lambda u, x, y, z: 1.0)
+    cb = msbg_gpu.PressureCallbacks(C.cast(ct, C.c_void_p).value, C.cast(fc, C.c_void_p).value,
+                                    C.cast(rh, C.c_void_p).value, None)
+    bl = np.zeros(1, np.int32)
+    x = np.ones(res ** 3, np.float32)
+    ys = []
+    for dbc in ([1, 1, 1, 1, 1, 1], [0, 1, 1, 1, 1, 1]):
+        d = np.array(dbc, np.int32)
+        topo = msbg_gpu.TopoDesc(res, res, res, bsx0, 2, bl.ctypes.data_as(C.POINTER(C.c_int)),
+                                 d.ctypes.data_as(C.POINTER(C.c_int)))
+        y = np.zeros(res ** 3, np.float64)
+        nm = C.c_int()
+        fluid = np.zeros(32, np.int64)
+        rc = L.msbg_gpu_pressure_host_check(C.byref(topo), C.byref(cb),
+                                            x.ctypes.data_as(C.POINTER(C.c_float)),
+                                            y.ctypes.data_as(C.POINTER(C.c_double)), C.byref(nm),
+                                            fluid.ctypes.data_as(C.POINTER(C.c_int64)), None)
+        assert rc == 0
+        ys.append(y)
+    zz, yy, xx = np.meshgrid(np.arange(res), np.arange(res), np.arange(res), indexing="ij")
+    face = to_blocks(((xx == 0) & (zz < 12)).astype(np.float32), bsx0) > 0
+    diff = ys[1] - ys[0]
+    assert np.allclose(diff[face], 1.0) and np.allclose(diff[~face], 0.0)
+    bad = np.array([0, 1, 1, 1, 1, 2], np.int32)  # not a DBC_* value
+    topo = msbg_gpu.TopoDesc(res, res, res, bsx0, 2, bl.ctypes.data_as(C.POINTER(C.c_int)),
+                             bad.ctypes.data_as(C.POINTER(C.c_int)))
+    nm = C.c_int()
+    assert L.msbg_gpu_pressure_host_check(C.byref(topo), C.byref(cb), None, None, C.byref(nm),
+                                          None, None) == 5

