@@ -75,9 +75,13 @@ C3_CFG = dict(PS_CFG, res=2048)
 # 4096^3, 3 levels, fine band of 48 voxels around a wavy free surface
 # z = (0.3 + 0.05 sum of 8 seeded sinusoids) * res plus 256 seeded spheres of
 # radius 20-60 voxels, no obstacles; FP16 storage with FP64 refinement and
-# the learned guess and correction, against plain FP32 on the same GPU
-C5_CFG = dict(PS_CFG, res=4096, n_levels=3, band=48.0, z_liquid=0.3, n_spheres=256,
-              r_min=20 / 4096, r_max=60 / 4096, n_cuboids=0, wave_amp=0.05, n_waves=8, seed=4096)
+# the learned guess and correction, against plain FP32 on the same GPU.  A
+# block is fine when its centre lies within 48 voxels of the surface: the
+# scene's band adds half a block diagonal (27.7 voxels for 32^3 blocks) to
+# the distance it is given, so it is given 48 - 27.7.
+C5_CFG = dict(PS_CFG, res=4096, n_levels=3, band=48.0 - 16 * 3 ** 0.5, z_liquid=0.3,
+              n_spheres=256, r_min=20 / 4096, r_max=60 / 4096, n_cuboids=0, wave_amp=0.05,
+              n_waves=8, seed=4096)
 
 
 def peaks():

@@ -14,8 +14,8 @@
 // pairs of x-adjacent voxels with the packed FP32 instructions of sm_100
 // (add/sub/mul/fma.rn.f32x2): one instruction updates both voxels of a pair,
 // and a pair arrives from shared memory in one 8-byte load.
-//   * CTA layout: one block per CTA, BSX*BSX/2 threads; thread (i, y) owns
-//     the x pair (2i, 2i+1) of row y and marches up z with a three-plane
+//   * CTA layout: BSX*BSX threads per block; thread (i, y, h) owns the x pair
+//     (2i, 2i+1) of row y and marches up one half h of z with a three-plane
 //     register window of the 5-point cross.
 //   * The padded tile holds x in [-2, BSX+1] (row pitch BSX+4, so every pair
 //     starts on an 8-byte boundary) and y, z in [-1, BSX].  The x-1 and x+1
@@ -116,7 +116,7 @@ struct McfTile {
   static constexpr int RP = BSX + 4;         // row pitch: x + 2 in [0, BSX + 4)
   static constexpr int PP = RP * (BSX + 2);  // plane pitch: y + 1 in [0, BSX + 2)
   static constexpr int NV = BSX * BSX * BSX;
-  static constexpr int NT = BSX * BSX / 2;   // one thread per x pair of a row
+  static constexpr int NT = BSX * BSX;       // one thread per x pair of a row and z half
   static constexpr int HP = BSX / 2;         // pairs per row
   static constexpr size_t SMEM = sizeof(float) * PP * (BSX + 2);
   __device__ static int at(int x, int y, int z) { return (x + 2) + RP * (y + 1) + PP * (z + 1); }
@@ -231,10 +231,11 @@ __device__ __forceinline__ void mcf_compute(const float* tile, T* __restrict__ b
                                             int clamp01, int tid) {
   using Tl = McfTile<BSX>;
   constexpr int RP = Tl::RP, PP = Tl::PP, HP = Tl::HP;
-  // Column march of the x pair (x0, x0 + 1) of row y.
-  const int x0 = 2 * (tid % HP), y = tid / HP;
-  const float* col = tile + Tl::at(x0, y, -1);  // plane z = -1
-  T* out = block + x0 + BSX * y;
+  // Column march of the x pair (x0, x0 + 1) of row y over one half of z.
+  constexpr int ZN = BSX / 2;
+  const int x0 = 2 * (tid % HP), y = (tid / HP) % BSX, zb = ZN * (tid / (HP * BSX));
+  const float* col = tile + Tl::at(x0, y, zb - 1);  // plane zb - 1
+  T* out = block + x0 + BSX * y + BSX * BSX * zb;
   const f2 m2 = pk(-2.f, -2.f), mh = pk(-0.5f, -0.5f);
   // window: centre, x-1, x+1 pairs of row y; centre pairs of rows y-1, y+1
   f2 Cm, XMm, XPm, YMm, YPm;  // plane z-1
@@ -250,8 +251,8 @@ __device__ __forceinline__ void mcf_compute(const float* tile, T* __restrict__ b
     YM0 = ld2(p - RP); YP0 = ld2(p + RP);
   }
 #pragma unroll 4
-  for (int z = 0; z < BSX; z++) {
-    const float* p0 = col + PP * (z + 1);  // plane z
+  for (int z = 0; z < ZN; z++) {
+    const float* p0 = col + PP * (z + 1);  // plane zb + z
     const float* p1 = p0 + PP;             // plane z+1
     const f2 a = ld2(p1 - 2), b = ld2(p1), c = ld2(p1 + 2);
     const f2 Cp = b, XMp = mid2(a, b), XPp = mid2(b, c);
@@ -315,7 +316,7 @@ __host__ __device__ constexpr int mcf_ctas_per_sm() { return BSX == 8 ? 16 : BSX
 // gridDim.x; with two stages the copies of block k + gridDim.x are issued
 // before block k is computed.
 template <int BSX, typename T>
-__global__ void __launch_bounds__(BSX* BSX / 2)
+__global__ void __launch_bounds__(BSX* BSX, BSX == 32 ? 1 : 1024 / (BSX * BSX))
     mcf_colour_kernel(T* __restrict__ pool, const int* __restrict__ slotOf,
                       const int* __restrict__ list, int n, int nbx, int nby, int nbz,
                       float emptyVal, float fullVal, float dt, int clamp01,
