@@ -88,6 +88,9 @@ int msbg_gpu_destroy(msbg_gpu_ctx* ctx);
 const char* msbg_gpu_last_error(const msbg_gpu_ctx* ctx);
 /* Waits for all work issued on the context's stream. */
 int msbg_gpu_sync(msbg_gpu_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t as void*), for callers that order
+ * their own work or timing events after the library's. */
+int msbg_gpu_stream(msbg_gpu_ctx* ctx, void** stream);
 
 /* Mirrors MultiresSparseGrid::create + setRefinementMap for the device side
  * (src/msbg.cpp:131, 1428): stores the block raster; drops all channels. */

@@ -89,6 +89,12 @@ extern "C" int msbg_gpu_sync(msbg_gpu_ctx* ctx) {
   return MSBG_OK;
 }
 
+extern "C" int msbg_gpu_stream(msbg_gpu_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return MSBG_EINVARG;
+  *stream = ctx->stream;
+  return MSBG_OK;
+}
+
 extern "C" int msbg_gpu_sync_topology(msbg_gpu_ctx* ctx, const msbg_topo_desc* d) {
   if (!ctx || !d) return MSBG_EINVARG;
   if (!(d->bsx0 == 8 || d->bsx0 == 16 || d->bsx0 == 32))
@@ -283,8 +289,7 @@ extern "C" int msbg_gpu_pde_mcf(msbg_gpu_ctx* ctx, int chan, const int* blockLis
   // Group the list by colour (src/msbg.h:642-646); the reference skips
   // blocks of other colours in each of its 8 passes (src/msbg4.cpp:456-462).
   int start[9] = {0};
-  std::vector<int>& lst = ctx->listHost;
-  lst.resize(n);
+  std::vector<int> lst(n);
   {
     int cnt[8] = {0};
     for (int i = 0; i < n; i++) {
@@ -303,22 +308,34 @@ extern "C" int msbg_gpu_pde_mcf(msbg_gpu_ctx* ctx, int chan, const int* blockLis
       lst[pos[(bx & 1) + 2 * (by & 1) + 4 * (bz & 1)]++] = b;
     }
   }
-  MSBG_CUDA_TRY(ctx, ctx->listBuf.ensure(sizeof(int) * std::max(n, 1)));
-  MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));  // listBuf may be in use
-  MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->listBuf.p, lst.data(), sizeof(int) * n,
-                                     cudaMemcpyHostToDevice, ctx->stream));
+  // The grouped list on the device is reused when a call repeats the last
+  // list (the usual time-step loop): no host synchronisation then.  A new
+  // list waits for the work that may still read the old one.
+  if (lst != ctx->listHost || !ctx->listBuf.p) {
+    MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));  // listBuf may be in use
+    MSBG_CUDA_TRY(ctx, ctx->listBuf.ensure(sizeof(int) * std::max(n, 1)));
+    ctx->listHost = lst;
+    MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->listBuf.p, ctx->listHost.data(), sizeof(int) * n,
+                                       cudaMemcpyHostToDevice, ctx->stream));
+  }
   const int nIter = numIter + (numIter & 1);  // src/msbg4.cpp:150-152
   int* ef = err_flag(ctx);
   if (!ef) return set_error(ctx, MSBG_ENOMEM, "error flag allocation failed");
+  // the face cache: each block's two x planes, contiguous, so the x halo of a
+  // neighbour is read in full sectors instead of one 4-byte value per row
+  const size_t esz = ch.dtype == MSBG_U16 ? 2 : 4;
+  MSBG_CUDA_TRY(ctx, ch.xfaces.ensure(esz * 2 * ch.bsx * ch.bsx * (size_t)std::max<int64_t>(
+                                                                      ch.nValue, 1)));
   if (ch.dtype == MSBG_U16)
     MSBG_CUDA_TRY(ctx, launch_mcf_u16(ch.pool.as<uint16_t>(), ch.slot.as<int>(),
                                       ctx->listBuf.as<int>(), start, ctx->nbx, ctx->nby, ctx->nbz,
                                       ch.bsx, ch.emptyQ, ch.fullQ, nIter, dt, clamp01, ef,
-                                      ctx->stream));
+                                      ctx->stream, ch.xfaces.p, ch.nValue));
   else
     MSBG_CUDA_TRY(ctx, launch_mcf(ch.pool.as<float>(), ch.slot.as<int>(), ctx->listBuf.as<int>(),
                                   start, ctx->nbx, ctx->nby, ctx->nbz, ch.bsx, ch.emptyVal,
-                                  ch.fullVal, nIter, dt, clamp01, ef, ctx->stream));
+                                  ch.fullVal, nIter, dt, clamp01, ef, ctx->stream, ch.xfaces.p,
+                                  ch.nValue));
   return MSBG_OK;
 }
 

@@ -63,6 +63,7 @@ struct Channel {
   std::vector<int> slotHost;   // [nb] slot or SLOT_* code
   std::vector<int8_t> kindHost;
   DeviceBuffer pool;           // [nValue][bsx^3] float or uint16_t
+  DeviceBuffer xfaces;         // [nValue][2][bsx^2]: the x = 0 and x = bsx-1 planes
   DeviceBuffer slot;           // [nb] int
 };
 
@@ -106,15 +107,20 @@ int set_error(msbg_gpu_ctx* ctx, int code, const char* fmt, ...);
 // Releases the pressure solver state of a context (pressure.cu).
 void pressure_release(msbg_gpu_ctx* ctx);
 
-// Launches of the 8-colour mean-curvature-flow passes (mcf.cu).
+// Launches of the 8-colour mean-curvature-flow passes (mcf.cu).  xfaces:
+// optional face cache of nSlots value blocks (2 * bsx^2 values each, the
+// pool's element type), refilled at the start of the call and kept current by
+// the passes; NULL reads the neighbours' x faces from the pool.
 cudaError_t launch_mcf(float* pool, const int* slotOf, const int* colourList,
                        const int* colourStart, int nbx, int nby, int nbz, int bsx,
                        float emptyVal, float fullVal, int nIter, float dt, int clamp01,
-                       int* errFlag, cudaStream_t stream);
+                       int* errFlag, cudaStream_t stream, void* xfaces = nullptr,
+                       int64_t nSlots = 0);
 // The same passes on a 16-bit render-density pool (const values raw).
 cudaError_t launch_mcf_u16(uint16_t* pool, const int* slotOf, const int* colourList,
                            const int* colourStart, int nbx, int nby, int nbz, int bsx,
                            uint16_t emptyVal, uint16_t fullVal, int nIter, float dt, int clamp01,
-                           int* errFlag, cudaStream_t stream);
+                           int* errFlag, cudaStream_t stream, void* xfaces = nullptr,
+                           int64_t nSlots = 0);
 
 }  // namespace msbg

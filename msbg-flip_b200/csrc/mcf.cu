@@ -149,10 +149,38 @@ constexpr float U16_SCALE = 1.0f / 65535.0f;  // RENDER_DENS_TO_FLOAT_UI16
 // Issue the copies of one block and its shell into a tile (FP32: asynchronous
 // copies, completed by the caller's cp.async wait; 16-bit: loads widened into
 // the tile on the spot).  nbSlot: the slots of the 27 blocks around it.
+// The x faces of a block's neighbours: with a face cache xf (per slot the
+// planes x = 0 and x = BSX-1 as [2][z][y], kept current by the kernel), one
+// contiguous 4-byte value per halo voxel; without it, a 4-byte value out of
+// a 64-byte row of the neighbour block.
+template <int BSX, typename T>
+__device__ __forceinline__ const T* xface_src(const T* pool, const T* xf, const int* nbSlot,
+                                              int x, int y, int z, int& constKind) {
+  if (!xf) {
+    const T* own = pool + (size_t)nbSlot[13] * (BSX * BSX * BSX);
+    return halo_src<BSX, T>(pool, nbSlot, own, x, y, z, constKind);
+  }
+  constexpr int M = BSX - 1, F = BSX * BSX;
+  const int dx = x < 0 ? -1 : 1;
+  const int dy = y < 0 ? -1 : (y > M ? 1 : 0);
+  const int dz = z < 0 ? -1 : (z > M ? 1 : 0);
+  const int s = nbSlot[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
+  constKind = 0;
+  if (s >= 0)  // the neighbour's plane that faces us: x = BSX-1 for dx < 0
+    return xf + ((size_t)s * 2 + (dx < 0 ? 1 : 0)) * F + (z & M) * BSX + (y & M);
+  if (s == SLOT_EMPTY || s == SLOT_FULL) {
+    constKind = s == SLOT_EMPTY ? 1 : 2;
+    return nullptr;
+  }
+  // NULL neighbour or outside the domain: our own boundary plane, clamped
+  const int cy = min(max(y, 0), M), cz = min(max(z, 0), M);
+  return xf + ((size_t)nbSlot[13] * 2 + (dx < 0 ? 0 : 1)) * F + cz * BSX + cy;
+}
+
 template <int BSX, typename T>
 __device__ __forceinline__ void mcf_fill(float* tile, const T* __restrict__ pool,
-                                         const int* nbSlot, float emptyVal, float fullVal,
-                                         int tid) {
+                                         const T* __restrict__ xf, const int* nbSlot,
+                                         float emptyVal, float fullVal, int tid) {
   using Tl = McfTile<BSX>;
   constexpr int NV = Tl::NV, NT = Tl::NT, HP = Tl::HP;
   constexpr bool F32 = std::is_same<T, float>::value;
@@ -212,7 +240,7 @@ __device__ __forceinline__ void mcf_fill(float* tile, const T* __restrict__ pool
     if ((y < 0 || y >= BSX) && (z < 0 || z >= BSX)) continue;  // corner: not read
     const int x = side ? BSX : -1;
     int ck;
-    const T* src = halo_src<BSX, T>(pool, nbSlot, own, x, y, z, ck);
+    const T* src = xface_src<BSX, T>(pool, xf, nbSlot, x, y, z, ck);
     float* d = tile + Tl::at(x, y, z);
     if (src) {
       if constexpr (F32)
@@ -227,8 +255,9 @@ __device__ __forceinline__ void mcf_fill(float* tile, const T* __restrict__ pool
 
 // The 19-point update of one block from its tile, stored in place.
 template <int BSX, typename T>
-__device__ __forceinline__ void mcf_compute(const float* tile, T* __restrict__ block, float dt,
-                                            int clamp01, int tid) {
+__device__ __forceinline__ void mcf_compute(const float* tile, T* __restrict__ block,
+                                            T* __restrict__ xfOwn, float dt, int clamp01,
+                                            int tid) {
   using Tl = McfTile<BSX>;
   constexpr int RP = Tl::RP, PP = Tl::PP, HP = Tl::HP;
   // Column march of the x pair (x0, x0 + 1) of row y over one half of z.
@@ -290,12 +319,21 @@ __device__ __forceinline__ void mcf_compute(const float* tile, T* __restrict__ b
       pl = fminf(fmaxf(pl, 0.0f), 1.0f);
       ph = fminf(fmaxf(ph, 0.0f), 1.0f);
     }
+    T vl, vh;
     if constexpr (std::is_same<T, float>::value) {
+      vl = pl;
+      vh = ph;
       *reinterpret_cast<float2*>(out + BSX * BSX * z) = make_float2(pl, ph);
     } else {  // round to nearest (even), as round_to_int under the default MXCSR
       const uint32_t ql = (uint32_t)min(max(__float2int_rn(pl * 65535.0f), 0), 65535);
       const uint32_t qh = (uint32_t)min(max(__float2int_rn(ph * 65535.0f), 0), 65535);
+      vl = (T)ql;
+      vh = (T)qh;
       *reinterpret_cast<uint32_t*>(out + BSX * BSX * z) = ql | (qh << 16);
+    }
+    if (xfOwn) {  // keep the face cache of this block current
+      if (x0 == 0) xfOwn[(zb + z) * BSX + y] = vl;
+      if (x0 + 1 == BSX - 1) xfOwn[BSX * BSX + (zb + z) * BSX + y] = vh;
     }
 
     Cm = C0; XMm = XM0; XPm = XP0; YMm = YM0; YPm = YP0;
@@ -317,7 +355,7 @@ __host__ __device__ constexpr int mcf_ctas_per_sm() { return BSX == 8 ? 16 : BSX
 // before block k is computed.
 template <int BSX, typename T>
 __global__ void __launch_bounds__(BSX* BSX, BSX == 32 ? 1 : 1024 / (BSX * BSX))
-    mcf_colour_kernel(T* __restrict__ pool, const int* __restrict__ slotOf,
+    mcf_colour_kernel(T* __restrict__ pool, T* __restrict__ xf, const int* __restrict__ slotOf,
                       const int* __restrict__ list, int n, int nbx, int nby, int nbz,
                       float emptyVal, float fullVal, float dt, int clamp01,
                       int* __restrict__ errFlag) {
@@ -348,7 +386,7 @@ __global__ void __launch_bounds__(BSX* BSX, BSX == 32 ? 1 : 1024 / (BSX * BSX))
   // per CTA: every thread reads the same shared slot)
   auto fill = [&](int s) {
     if (nbSlot[s][13] >= 0)
-      mcf_fill<BSX, T>(tiles + s * TILE, pool, nbSlot[s], emptyVal, fullVal, tid);
+      mcf_fill<BSX, T>(tiles + s * TILE, pool, xf, nbSlot[s], emptyVal, fullVal, tid);
     cp_async_commit();
   };
   neighbours(k, 0);
@@ -371,7 +409,8 @@ __global__ void __launch_bounds__(BSX* BSX, BSX == 32 ? 1 : 1024 / (BSX * BSX))
     if (slot0 < 0) {
       if (tid == 0) atomicOr(errFlag, MCF_ERR_NOT_VALUE);
     } else {
-      mcf_compute<BSX, T>(tiles + s * TILE, pool + (size_t)slot0 * Tl::NV, dt, clamp01, tid);
+      mcf_compute<BSX, T>(tiles + s * TILE, pool + (size_t)slot0 * Tl::NV,
+                          xf ? xf + (size_t)slot0 * 2 * BSX * BSX : nullptr, dt, clamp01, tid);
     }
     __syncthreads();  // stage s may be refilled
     if (ST == 1 && kn < n) {
@@ -382,10 +421,24 @@ __global__ void __launch_bounds__(BSX* BSX, BSX == 32 ? 1 : 1024 / (BSX * BSX))
   }
 }
 
+// Fills the face cache: the planes x = 0 and x = BSX-1 of every value block
+// (slots 0..nSlots-1), as [slot][2][z][y].
 template <int BSX, typename T>
-cudaError_t launch_mcf_t(T* pool, const int* slotOf, const int* colourList,
-                         const int* colourStart, int nbx, int nby, int nbz,
-                         float emptyVal, float fullVal, int nIter, float dt,
+__global__ void __launch_bounds__(256) k_mcf_xfaces(const T* __restrict__ pool, int64_t nSlots,
+                                                    T* __restrict__ xf) {
+  constexpr int F = BSX * BSX;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nSlots * 2 * F;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t sl = i / (2 * F);
+    const int r = (int)(i % (2 * F)), side = r / F, y = r % BSX, z = (r % F) / BSX;
+    xf[i] = pool[sl * (BSX * BSX * BSX) + (side ? BSX - 1 : 0) + BSX * (y + BSX * z)];
+  }
+}
+
+template <int BSX, typename T>
+cudaError_t launch_mcf_t(T* pool, T* xf, int64_t nSlots, const int* slotOf,
+                         const int* colourList, const int* colourStart, int nbx, int nby,
+                         int nbz, float emptyVal, float fullVal, int nIter, float dt,
                          int clamp01, int* errFlag, cudaStream_t stream) {
   using Tl = McfTile<BSX>;
   // The shared-memory limit is an attribute of the kernel on each device:
@@ -410,33 +463,36 @@ cudaError_t launch_mcf_t(T* pool, const int* slotOf, const int* colourList,
     numSMs[dev] = v;
   }
   const int maxGrid = (dev < 64 ? numSMs[dev] : 148) * mcf_ctas_per_sm<BSX>();
+  if (xf && nSlots > 0 && nIter > 0)
+    k_mcf_xfaces<BSX, T><<<(dev < 64 ? numSMs[dev] : 148) * 4, 256, 0, stream>>>(pool, nSlots,
+                                                                               xf);
   for (int it = 0; it < nIter; it++)
     for (int c = 0; c < 8; c++) {
       int n = colourStart[c + 1] - colourStart[c];
       if (n <= 0) continue;
       const int grid = mcf_stages<BSX>() == 2 ? std::min(n, maxGrid) : n;
       mcf_colour_kernel<BSX, T><<<grid, Tl::NT, Tl::SMEM * mcf_stages<BSX>(), stream>>>(
-          pool, slotOf, colourList + colourStart[c], n, nbx, nby, nbz, emptyVal, fullVal, dt,
+          pool, xf, slotOf, colourList + colourStart[c], n, nbx, nby, nbz, emptyVal, fullVal, dt,
           clamp01, errFlag);
     }
   return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t launch_mcf_typed(T* pool, const int* slotOf, const int* colourList,
-                             const int* colourStart, int nbx, int nby, int nbz, int bsx,
-                             float emptyVal, float fullVal, int nIter, float dt, int clamp01,
-                             int* errFlag, cudaStream_t stream) {
+cudaError_t launch_mcf_typed(T* pool, T* xf, int64_t nSlots, const int* slotOf,
+                             const int* colourList, const int* colourStart, int nbx, int nby,
+                             int nbz, int bsx, float emptyVal, float fullVal, int nIter, float dt,
+                             int clamp01, int* errFlag, cudaStream_t stream) {
   switch (bsx) {
     case 8:
-      return launch_mcf_t<8, T>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, emptyVal,
-                                fullVal, nIter, dt, clamp01, errFlag, stream);
+      return launch_mcf_t<8, T>(pool, xf, nSlots, slotOf, colourList, colourStart, nbx, nby, nbz,
+                                emptyVal, fullVal, nIter, dt, clamp01, errFlag, stream);
     case 16:
-      return launch_mcf_t<16, T>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, emptyVal,
-                                 fullVal, nIter, dt, clamp01, errFlag, stream);
+      return launch_mcf_t<16, T>(pool, xf, nSlots, slotOf, colourList, colourStart, nbx, nby,
+                                 nbz, emptyVal, fullVal, nIter, dt, clamp01, errFlag, stream);
     case 32:
-      return launch_mcf_t<32, T>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, emptyVal,
-                                 fullVal, nIter, dt, clamp01, errFlag, stream);
+      return launch_mcf_t<32, T>(pool, xf, nSlots, slotOf, colourList, colourStart, nbx, nby,
+                                 nbz, emptyVal, fullVal, nIter, dt, clamp01, errFlag, stream);
     default:
       return cudaErrorInvalidValue;
   }
@@ -447,17 +503,19 @@ cudaError_t launch_mcf_typed(T* pool, const int* slotOf, const int* colourList,
 cudaError_t launch_mcf(float* pool, const int* slotOf, const int* colourList,
                        const int* colourStart, int nbx, int nby, int nbz, int bsx,
                        float emptyVal, float fullVal, int nIter, float dt, int clamp01,
-                       int* errFlag, cudaStream_t stream) {
-  return launch_mcf_typed<float>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, bsx,
-                                 emptyVal, fullVal, nIter, dt, clamp01, errFlag, stream);
+                       int* errFlag, cudaStream_t stream, void* xfaces, int64_t nSlots) {
+  return launch_mcf_typed<float>(pool, static_cast<float*>(xfaces), nSlots, slotOf, colourList,
+                                 colourStart, nbx, nby, nbz, bsx, emptyVal, fullVal, nIter, dt,
+                                 clamp01, errFlag, stream);
 }
 
 cudaError_t launch_mcf_u16(uint16_t* pool, const int* slotOf, const int* colourList,
                            const int* colourStart, int nbx, int nby, int nbz, int bsx,
                            uint16_t emptyVal, uint16_t fullVal, int nIter, float dt, int clamp01,
-                           int* errFlag, cudaStream_t stream) {
+                           int* errFlag, cudaStream_t stream, void* xfaces, int64_t nSlots) {
   // const blocks read like stored values: q * (1/65535)
-  return launch_mcf_typed<uint16_t>(pool, slotOf, colourList, colourStart, nbx, nby, nbz, bsx,
+  return launch_mcf_typed<uint16_t>(pool, static_cast<uint16_t*>(xfaces), nSlots, slotOf,
+                                    colourList, colourStart, nbx, nby, nbz, bsx,
                                     (float)emptyVal * U16_SCALE, (float)fullVal * U16_SCALE, nIter,
                                     dt, clamp01, errFlag, stream);
 }

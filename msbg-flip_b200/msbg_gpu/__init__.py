@@ -65,6 +65,7 @@ def lib():
         "msbg_gpu_destroy": (i32, [vp]),
         "msbg_gpu_last_error": (C.c_char_p, [vp]),
         "msbg_gpu_sync": (i32, [vp]),
+        "msbg_gpu_stream": (i32, [vp, C.POINTER(vp)]),
         "msbg_gpu_sync_topology": (i32, [vp, C.POINTER(TopoDesc)]),
         "msbg_gpu_upload_channel": (i32, [vp, i32, i32, pi8, C.POINTER(pf32), pf32, f32, f32]),
         "msbg_gpu_download_channel": (i32, [vp, i32, C.POINTER(pf32), pf32]),
@@ -221,6 +222,13 @@ class Context:
                                                           _p(out, C.c_uint16)),
                     "download_channel_u16")
         return out
+
+    def stream(self):
+        """The context's CUDA stream handle (an int), e.g. for
+        torch.cuda.ExternalStream."""
+        p = C.c_void_p()
+        self._check(self._L.msbg_gpu_stream(self._h, C.byref(p)), "stream")
+        return p.value or 0
 
     def num_value_blocks(self, chan):
         n = C.c_int64()
