@@ -162,14 +162,16 @@ def dist_env():
     return ws, rank, local
 
 
-def init_dist(ws, backend="nccl"):
-    """Process group of the replicas (one per GPU; gloo for CPU tests)."""
+def init_dist(ws, backend="nccl", timeout_s=300):
+    """Process group of the replicas (one per GPU; gloo for CPU tests).  A
+    rank that fails or never arrives ends the others' next collective with an
+    error after timeout_s."""
     if ws <= 1:
         return None
     import datetime
 
     import torch.distributed as dist
-    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
     return dist
 
 

@@ -992,6 +992,10 @@ extern "C" int msbg_gpu_pressure_solve(msbg_gpu_ctx* ctx, const msbg_gpu_solve_p
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
+  // a pipelined kernel that gave up a bounded wait has set the context's
+  // error flag and left its tile unsmoothed: the solution is not delivered
+  rc = msbg_gpu_sync(ctx);
+  if (rc) return rc;
   if (info) {
     const Level& L0 = S.H.levels[0];
     info->iterations = o.iters;
