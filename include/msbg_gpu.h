@@ -69,11 +69,16 @@ typedef struct {
   int nLevels;           /* resolution levels (1..4) */
   const int* blockLevel; /* [nbx*nby*nbz] level per block, or NULL */
   /* Pressure boundary of the six domain faces (-x, +x, -y, +y, -z, +z), as
-   * setDomainBoundarySpec_ gives them (src/msbg.cpp:2462, flip_sim.cpp:1621):
-   * MSBG_DBC_OPEN (air outside: p = 0 with the face coefficient the callback
-   * returns for that face) or MSBG_DBC_SOLID (a wall: coefficient 0, the
-   * callback is not asked).  NULL: every domain face is OPEN, i.e. the
-   * callbacks alone decide. */
+   * setDomainBoundarySpec_ gives them (src/msbg.cpp:2462, flip_sim.cpp:1621).
+   * Outside the grid p = 0, behind a face coupling of
+   *   MSBG_DBC_SOLID: 0 (a wall; the callback is not asked);
+   *   MSBG_DBC_OPEN:  on a lower face (-x, -y, -z) the coefficient the
+   *                   callback returns for the cell's own lower face, on an
+   *                   upper face 1, the reference's open-face weight
+   *                   (constFaceCoeffAirBlock, src/msbg3.cpp:733-740).
+   * NULL: the reference's own FLIP operator, whose diagonal
+   * (computeDiagonalFLIP_, src/msbg3.cpp:2714-2722) ignores the spec: lower
+   * faces as OPEN, upper faces 0. */
   const int* domainBc;
 } msbg_topo_desc;
 

@@ -114,12 +114,21 @@ struct LevelDev {
   DeviceBuffer ctype;              // level 0: CT_* per cell
 };
 
+// Domain faces without a caller spec follow the reference's FLIP operator:
+// the lower faces (-x, -y, -z) couple to p = 0 outside with the coefficient
+// the callback returns for the cell's own lower face, the upper faces have no
+// coupling, because computeDiagonalFLIP_ reads the face channel past the
+// grid as its empty value 0 (src/msbg3.cpp:2714-2722, sbg.h:880-894).
+constexpr int DBC_REFERENCE = -1;
+
 struct Hierarchy {
   int res = 0, bsx0 = 0, nLevels = 0, nb1x = 0, nb1y = 0, nb1z = 0;
   int sx = 0, sy = 0, sz = 0;
   std::vector<int> blockLevel;     // refinement map (MG level 0)
-  int domainBc[6] = {MSBG_DBC_OPEN, MSBG_DBC_OPEN, MSBG_DBC_OPEN,
-                     MSBG_DBC_OPEN, MSBG_DBC_OPEN, MSBG_DBC_OPEN};  // face = 2*dir + side
+  // per domain face (2*dir + side): MSBG_DBC_OPEN, MSBG_DBC_SOLID, or
+  // DBC_REFERENCE when the caller gave no spec
+  int domainBc[6] = {DBC_REFERENCE, DBC_REFERENCE, DBC_REFERENCE,
+                     DBC_REFERENCE, DBC_REFERENCE, DBC_REFERENCE};
   std::vector<Level> levels;
   // coarsest-level dense inverse (FP64), fluid cell indices
   int nCoarse = 0;

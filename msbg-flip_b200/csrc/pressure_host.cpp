@@ -296,11 +296,18 @@ void sample_level0(const Ctx& C, Level& L, std::vector<uint8_t>& fluid) {
       if (side) q[dir] += 1;
       double c;
       if (onTileFace && !faceInside[dir][side]) {
-        // the domain boundary: a wall has no coupling; open air is p = 0
-        // behind the face's own coefficient
-        c = C.H.domainBc[2 * dir + side] == MSBG_DBC_SOLID
-                ? 0.0
-                : h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
+        // the domain boundary, p = 0 outside behind the coupling c: a wall
+        // has none; an open face has the callback's coefficient on the lower
+        // side and the constant 1 of the reference's open-face weights
+        // (constFaceCoeffAirBlock, src/msbg3.cpp:733-740) on the upper side;
+        // without a spec, the reference's operator (DBC_REFERENCE)
+        const int bc = C.H.domainBc[2 * dir + side];
+        if (bc == MSBG_DBC_SOLID || (bc == DBC_REFERENCE && side == 1))
+          c = 0.0;
+        else if (side == 1)
+          c = h;
+        else
+          c = h * cb->sampleFaceCoeff(cb->user, dir, q[0] << l, q[1] << l, q[2] << l);
         if (side == 0) cdir[dir][ci] = (float)c;
         return c;
       }

@@ -375,7 +375,9 @@ def solve_params(**kw):
 
 def _ctx_pressure_prepare(self, scene, domain_bc=None):
     """msbg_gpu_pressure_prepare with the scene's callbacks; domain_bc: six
-    DBC_OPEN / DBC_SOLID values (-x, +x, -y, +y, -z, +z) or None."""
+    DBC_OPEN / DBC_SOLID values (-x, +x, -y, +y, -z, +z), or None for the
+    reference's operator (lower domain faces open with the callback's
+    coefficient, upper faces closed)."""
     _pressure_sigs(self._L)
     self._bl_p = np.ascontiguousarray(scene.block_levels, np.int32)
     self._dbc_p = None if domain_bc is None else np.ascontiguousarray(domain_bc, np.int32)

@@ -46,15 +46,17 @@ int oracle_mcf(int nbx, int nby, int nbz, int bsx, const int8_t* kind,
 typedef unsigned short (*oracle_cell_type_fn)(void*, int, int, int);
 typedef float (*oracle_face_fn)(void*, int, int, int, int);
 typedef float (*oracle_rhs_fn)(void*, int, int, int);
+/* domainBc: six domain faces (-x, +x, -y, +y, -z, +z), 0 open, 1 solid, or
+ * NULL for the reference's rule (lower faces open, upper faces no coupling). */
 int oracle_pressure_solve(int sx, int sy, int sz, int bsx0, const int* blockLevel,
-                          oracle_cell_type_fn cellType, oracle_face_fn face, oracle_rhs_fn rhs,
-                          void* user, double tol, int maxIter, double* x, double* b,
-                          int* itersOut, double* relResOut);
+                          const int* domainBc, oracle_cell_type_fn cellType, oracle_face_fn face,
+                          oracle_rhs_fn rhs, void* user, double tol, int maxIter, double* x,
+                          double* b, int* itersOut, double* relResOut);
 
 /* y = A x for the same system (x, y in the block layout, FP64). */
 int oracle_pressure_apply(int sx, int sy, int sz, int bsx0, const int* blockLevel,
-                          oracle_cell_type_fn cellType, oracle_face_fn face, void* user,
-                          const double* x, double* y);
+                          const int* domainBc, oracle_cell_type_fn cellType, oracle_face_fn face,
+                          void* user, const double* x, double* y);
 
 /* Callbacks over per-cell arrays in the packed block layout of MG level 0:
  * flags, lower-face coefficient per direction, rhs (see

@@ -23,6 +23,7 @@
 typedef struct {
   int sx, sy, sz, bsx0, nbx, nby, nbz;
   const int* lev;
+  const int* dbc; /* six domain faces: 0 open, 1 solid; NULL: the reference's rule */
   int64_t* boff;
   oracle_cell_type_fn ct;
   oracle_face_fn fc;
@@ -67,7 +68,17 @@ static double cell_row(const Grid* g, int L, const int P[3], int64_t* cols, doub
       int q[3] = {P[0], P[1], P[2]};
       if (side) q[dir] += 1;
       if (!inside(g, fv)) {
-        diag += h * face_beta(g, L, dir, q);
+        /* p = 0 outside.  Solid: no coupling.  Open: the callback's lower
+         * face coefficient, 1 on an upper face.  No spec: the reference's
+         * diagonal (src/msbg3.cpp:2714-2722) reads faces past the grid as 0,
+         * so the lower faces count and the upper ones do not. */
+        const int bc = g->dbc ? g->dbc[2 * dir + side] : -1;
+        if (bc == 1 || (bc == -1 && side))
+          ;
+        else if (side)
+          diag += h;
+        else
+          diag += h * face_beta(g, L, dir, q);
         continue;
       }
       const int L2 = block_level(g, fv);
@@ -195,7 +206,7 @@ static double dot(const double* a, const double* b, int64_t n) {
   return s;
 }
 
-static int make_grid(Grid* g, int sx, int sy, int sz, int bsx0, const int* lev,
+static int make_grid(Grid* g, int sx, int sy, int sz, int bsx0, const int* lev, const int* dbc,
                      oracle_cell_type_fn ct, oracle_face_fn fc, void* user) {
   g->sx = sx;
   g->sy = sy;
@@ -205,6 +216,7 @@ static int make_grid(Grid* g, int sx, int sy, int sz, int bsx0, const int* lev,
   g->nby = sy / bsx0;
   g->nbz = sz / bsx0;
   g->lev = lev;
+  g->dbc = dbc;
   g->ct = ct;
   g->fc = fc;
   g->user = user;
@@ -220,11 +232,11 @@ static int make_grid(Grid* g, int sx, int sy, int sz, int bsx0, const int* lev,
 }
 
 int oracle_pressure_apply(int sx, int sy, int sz, int bsx0, const int* blockLevel,
-                          oracle_cell_type_fn cellType, oracle_face_fn face, void* user,
-                          const double* x, double* y) {
+                          const int* domainBc, oracle_cell_type_fn cellType, oracle_face_fn face,
+                          void* user, const double* x, double* y) {
   Grid g;
   Csr A;
-  if (make_grid(&g, sx, sy, sz, bsx0, blockLevel, cellType, face, user)) return 2;
+  if (make_grid(&g, sx, sy, sz, bsx0, blockLevel, domainBc, cellType, face, user)) return 2;
   int rc = assemble(&g, &A, NULL, NULL);
   if (!rc) spmv(&A, x, y);
   csr_free(&A);
@@ -233,13 +245,13 @@ int oracle_pressure_apply(int sx, int sy, int sz, int bsx0, const int* blockLeve
 }
 
 int oracle_pressure_solve(int sx, int sy, int sz, int bsx0, const int* blockLevel,
-                          oracle_cell_type_fn cellType, oracle_face_fn face, oracle_rhs_fn rhs,
-                          void* user, double tol, int maxIter, double* x, double* b,
-                          int* itersOut, double* relResOut) {
+                          const int* domainBc, oracle_cell_type_fn cellType, oracle_face_fn face,
+                          oracle_rhs_fn rhs, void* user, double tol, int maxIter, double* x,
+                          double* b, int* itersOut, double* relResOut) {
   Grid g;
   Csr A;
   if (sx % bsx0 || sy % bsx0 || sz % bsx0) return 5;
-  if (make_grid(&g, sx, sy, sz, bsx0, blockLevel, cellType, face, user)) return 2;
+  if (make_grid(&g, sx, sy, sz, bsx0, blockLevel, domainBc, cellType, face, user)) return 2;
   int rc = assemble(&g, &A, rhs, b);
   if (rc) return rc;
   const int64_t n = A.n;
@@ -300,6 +312,7 @@ int oracle_pressure_solve(int sx, int sy, int sz, int bsx0, const int* blockLeve
 typedef struct {
   int sx, sy, sz, bsx0, nbx, nby;
   const int* lev;
+  const int* dbc; /* six domain faces: 0 open, 1 solid; NULL: the reference's rule */
   int64_t* boff;
   const unsigned short* flags;
   const float* face[3];

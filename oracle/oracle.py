@@ -40,6 +40,9 @@ def build_ref(ref_root=REFERENCE_ROOT):
     if not os.path.isdir(os.path.join(ref_root, "src")):
         return False
     subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF_ROOT={ref_root}"], check=True)
+    # the INTEGRATION.md snippets compiled against the reference headers
+    # (needs msbg-flip_b200/libmsbg_gpu.so, built before the oracle)
+    subprocess.run(["make", "-s", "-C", HERE, "integ", f"REF_ROOT={ref_root}"], check=True)
     return True
 
 
@@ -59,6 +62,72 @@ def oracle():
 
 def ref_available():
     return os.path.exists(REF_SO)
+
+
+INTEG_SO = os.path.join(OUT, "libmsbg_integ.so")
+_integ = None
+
+
+def integ_available():
+    return os.path.exists(INTEG_SO)
+
+
+def integ():
+    """The INTEGRATION.md snippets compiled against the reference headers
+    (oracle/ref/integration_adapter.cpp)."""
+    global _integ
+    if _integ is None:
+        ref()  # the reference library first (ref_init, its thread pool)
+        L = C.CDLL(INTEG_SO)
+        i8, u16, f32 = C.POINTER(C.c_int8), C.POINTER(C.c_uint16), C.POINTER(C.c_float)
+        L.integ_mcf_u16.restype = C.c_int
+        L.integ_mcf_u16.argtypes = [C.c_int] * 4 + [i8, C.c_uint16, C.c_uint16, u16,
+                                                    C.POINTER(C.c_int), C.c_int, C.c_int, C.c_float]
+        L.integ_mcf_f32.restype = C.c_int
+        L.integ_mcf_f32.argtypes = [C.c_int] * 4 + [i8, C.c_float, C.c_float, f32,
+                                                    C.POINTER(C.c_int), C.c_int, C.c_int, C.c_float,
+                                                    C.c_int]
+        L.integ_pressure.restype = C.c_int
+        L.integ_pressure.argtypes = [C.c_void_p] * 5 + [C.c_float, C.c_int, C.POINTER(C.c_int),
+                                                        C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        _integ = L
+    return _integ
+
+
+def integ_mcf_u16(res3, bsx, kind, values, update, num_iter, dt, empty_val=0, full_val=65535):
+    """INTEGRATION.md's render-density snippet on a reference grid; returns
+    (status, values)."""
+    L = integ()
+    v = np.ascontiguousarray(values, np.uint16).copy()
+    k = np.ascontiguousarray(kind, np.int8)
+    u = np.ascontiguousarray(update, np.int32)
+    rc = L.integ_mcf_u16(*res3, bsx, _p(k, C.c_int8), empty_val, full_val, _p(v, C.c_uint16),
+                         _p(u, C.c_int), len(u), num_iter, dt)
+    return rc, v
+
+
+def integ_mcf_f32(res3, bsx, kind, values, update, num_iter, dt, clamp01=False, empty_val=4.0,
+                  full_val=-4.0):
+    """INTEGRATION.md's FP32 snippet on a reference grid; returns (status, values)."""
+    L = integ()
+    v = np.ascontiguousarray(values, np.float32).copy()
+    k = np.ascontiguousarray(kind, np.int8)
+    u = np.ascontiguousarray(update, np.int32)
+    rc = L.integ_mcf_f32(*res3, bsx, _p(k, C.c_int8), empty_val, full_val, _p(v, C.c_float),
+                         _p(u, C.c_int), len(u), num_iter, dt, int(bool(clamp01)))
+    return rc, v
+
+
+def integ_pressure(ref_handle, scene, tol, max_iter):
+    """INTEGRATION.md's pressure snippet on a grid the reference prepared
+    (ref_pressure.RefPressure.h); the solution lands in its CH_PRESSURE.
+    Returns (status code, solve status, iterations, relative residual)."""
+    L = integ()
+    cb = scene.callbacks()
+    st, it, rr = C.c_int(), C.c_int(), C.c_double()
+    rc = L.integ_pressure(ref_handle, cb.sampleCellType, cb.sampleFaceCoeff, cb.sampleRhs,
+                          cb.user, tol, max_iter, C.byref(st), C.byref(it), C.byref(rr))
+    return rc, st.value, it.value, rr.value
 
 
 def ref():
@@ -138,19 +207,20 @@ def mcf_reference_u16(res3, bsx, kind, values, update, num_iter, dt, clamp01=Tru
     return v, secs.value
 
 
-def pressure_oracle(scene, tol=1e-12, max_iter=20000):
+def pressure_oracle(scene, tol=1e-12, max_iter=20000, domain_bc=None):
     """FP64 CG solution of the pressure system of a msbg_gpu.PressureScene.
 
     Returns (x, b, iterations, true relative residual); x, b in the
-    reference block layout."""
+    reference block layout.  domain_bc: six DBC values (0 open, 1 solid) or
+    None for the reference's rule."""
     L = oracle()
     if not hasattr(L, "_ps_sig"):
         L.oracle_pressure_solve.restype = C.c_int
-        L.oracle_pressure_solve.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int)] + [C.c_void_p] * 4 + [
+        L.oracle_pressure_solve.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int)] * 2 + [C.c_void_p] * 4 + [
             C.c_double, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
             C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.oracle_pressure_apply.restype = C.c_int
-        L.oracle_pressure_apply.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int)] + [C.c_void_p] * 3 + [
+        L.oracle_pressure_apply.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int)] * 2 + [C.c_void_p] * 3 + [
             C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L._ps_sig = True
     n = scene.packed_size()
@@ -160,8 +230,9 @@ def pressure_oracle(scene, tol=1e-12, max_iter=20000):
     rr = C.c_double()
     cb = scene.callbacks()
     bl = np.ascontiguousarray(scene.block_levels, np.int32)
+    dbc = None if domain_bc is None else np.ascontiguousarray(domain_bc, np.int32)
     rc = L.oracle_pressure_solve(scene.res, scene.res, scene.res, scene.bsx0, _p(bl, C.c_int),
-                                 cb.sampleCellType, cb.sampleFaceCoeff, cb.sampleRhs, cb.user,
+                                 None if dbc is None else _p(dbc, C.c_int), cb.sampleCellType, cb.sampleFaceCoeff, cb.sampleRhs, cb.user,
                                  tol, max_iter, _p(x, C.c_double), _p(b, C.c_double),
                                  C.byref(it), C.byref(rr))
     if rc:
@@ -169,7 +240,7 @@ def pressure_oracle(scene, tol=1e-12, max_iter=20000):
     return x, b, it.value, rr.value
 
 
-def pressure_apply_oracle(scene, x):
+def pressure_apply_oracle(scene, x, domain_bc=None):
     L = oracle()
     pressure_oracle  # signatures are set on first solve
     if not hasattr(L, "_ps_sig"):
@@ -178,8 +249,9 @@ def pressure_apply_oracle(scene, x):
     bl = np.ascontiguousarray(scene.block_levels, np.int32)
     xx = np.ascontiguousarray(x, np.float64)
     y = np.zeros_like(xx)
+    dbc = None if domain_bc is None else np.ascontiguousarray(domain_bc, np.int32)
     rc = L.oracle_pressure_apply(scene.res, scene.res, scene.res, scene.bsx0, _p(bl, C.c_int),
-                                 cb.sampleCellType, cb.sampleFaceCoeff, cb.user,
+                                 None if dbc is None else _p(dbc, C.c_int), cb.sampleCellType, cb.sampleFaceCoeff, cb.user,
                                  _p(xx, C.c_double), _p(y, C.c_double))
     if rc:
         raise RuntimeError(f"oracle_pressure_apply rc={rc}")

@@ -25,6 +25,7 @@
 #include <mutex>
 #include <sstream>
 #include <string>
+#include <type_traits>
 #include <thread>
 #include <omp.h>
 #include "tbb/tbb.h"
@@ -68,124 +69,139 @@ extern "C" int ref_init(int nThreads) {
   return nMaxThreads;
 }
 
+// A single-level grid with one channel filled from the packed values, the
+// way the reference's demo builds its render-density grid
+// (src/msbg_demo.cpp:283-502): kind[nBlocks], values packed for kind==1 blocks
+// in ascending bid order.  T = float uses CH_FLOAT_1, T = uint16_t the
+// render-density channel CH_UINT16_1 (RenderDensity under RSURF_16_BIT,
+// src/msbgcell.h:67-68).
+namespace {
+
+template <typename T> SparseGrid<T>* mcf_channel(MultiresSparseGrid* m, int chan);
+template <> SparseGrid<float>* mcf_channel<float>(MultiresSparseGrid* m, int chan) {
+  return m->getFloatChannel(chan, 0);
+}
+template <> SparseGrid<uint16_t>* mcf_channel<uint16_t>(MultiresSparseGrid* m, int chan) {
+  return m->getUint16Channel(chan, 0);
+}
+template <typename T> constexpr int mcf_chan() {
+  return std::is_same<T, float>::value ? CH_FLOAT_1 : CH_UINT16_1;
+}
+
+template <typename T>
+MultiresSparseGrid* mcf_grid_create(int sx, int sy, int sz, int bsx, const int8_t* kind,
+                                    T emptyVal, T fullVal, const T* values) {
+  MultiresSparseGrid* msbg = MultiresSparseGrid::create(
+      "REF", sx, sy, sz, bsx, -1, 0, -1, MSBG::OPT_SINGLE_LEVEL | MSBG::OPT_SINGLE_CHANNEL_FLOAT);
+  if (!msbg) return nullptr;
+  const int nb = msbg->nBlocks();
+  {
+    std::vector<int> levels(nb, 0);
+    msbg->regularizeRefinementMap(levels.data());
+    msbg->setRefinementMap(levels.data(), NULL, -1, NULL, false);
+  }
+  SparseGrid<T>* sg = mcf_channel<T>(msbg, mcf_chan<T>());
+  if (!sg) {
+    MultiresSparseGrid::destroy(msbg);
+    return nullptr;
+  }
+  sg->reset();
+  sg->prepareDataAccess();
+  sg->setEmptyValue(emptyVal);
+  sg->setFullValue(fullVal);
+  const int nv = sg->nVoxelsInBlock();
+  size_t off = 0;
+  for (int bid = 0; bid < nb; bid++) {
+    switch (kind[bid]) {
+      case 1: {
+        T* d = sg->getBlockDataPtr(bid, 1, 0);
+        std::memcpy(d, values + off, sizeof(T) * nv);
+        off += nv;
+        break;
+      }
+      case 2: sg->setEmptyBlock(bid); break;
+      case 3: sg->setFullBlock(bid); break;
+      default: break;
+    }
+  }
+  return msbg;
+}
+
+template <typename T>
+void mcf_grid_read(MultiresSparseGrid* msbg, const int8_t* kind, T* values) {
+  SparseGrid<T>* sg = mcf_channel<T>(msbg, mcf_chan<T>());
+  const int nv = sg->nVoxelsInBlock();
+  size_t off = 0;
+  for (int bid = 0; bid < msbg->nBlocks(); bid++) {
+    if (kind[bid] != 1) continue;
+    std::memcpy(values + off, sg->getBlockDataPtr(bid), sizeof(T) * nv);
+    off += nv;
+  }
+}
+
+template <typename T>
+int mcf_run(int sx, int sy, int sz, int bsx, const int8_t* kind, T emptyVal, T fullVal,
+            T* values, const int* update, int nUpdate, int numIter, float dt, int clamp01,
+            double* seconds) {
+  MultiresSparseGrid* msbg = mcf_grid_create<T>(sx, sy, sz, bsx, kind, emptyVal, fullVal, values);
+  if (!msbg) return 1;
+  std::vector<int> blockList(update, update + nUpdate);
+  auto t0 = std::chrono::steady_clock::now();
+  msbg->applyChannelPdeFast<T>(mcf_chan<T>(), CH_NULL, CH_NULL, &blockList,
+                               -(PDE_MEAN_CURVATURE + OPT_8_COLOR_SCHEME), clamp01, 0, 0, 0,
+                               numIter, 1.0f, dt);
+  auto t1 = std::chrono::steady_clock::now();
+  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+  mcf_grid_read<T>(msbg, kind, values);
+  MultiresSparseGrid::destroy(msbg);
+  return 0;
+}
+
+}  // namespace
+
 // Mean-curvature flow, 8-colour in-place scheme, FP32 channel.
 // Mirrors msbg_demo.cpp:716-727 (applyChannelPdeFast with
 // -(PDE_MEAN_CURVATURE+OPT_8_COLOR_SCHEME)) on a single-level grid.
-//   kind[nBlocks], values packed for kind==1 blocks in ascending bid order.
 //   update[nUpdate] = block ids handed to the smoother as its block list.
 extern "C" int ref_mcf(int sx, int sy, int sz, int bsx, const int8_t* kind,
                        float emptyVal, float fullVal, float* values,
                        const int* update, int nUpdate, int numIter, float dt,
                        int clamp01, double* seconds) {
-  MultiresSparseGrid* msbg = MultiresSparseGrid::create(
-      "REF", sx, sy, sz, bsx, -1, 0, -1,
-      MSBG::OPT_SINGLE_LEVEL | MSBG::OPT_SINGLE_CHANNEL_FLOAT);
-  if (!msbg) return 1;
-  const int nb = msbg->nBlocks();
-  {
-    std::vector<int> levels(nb, 0);
-    msbg->regularizeRefinementMap(levels.data());
-    msbg->setRefinementMap(levels.data(), NULL, -1, NULL, false);
-  }
-  const int chan = CH_FLOAT_1;
-  SparseGrid<float>* sg = msbg->getFloatChannel(chan, 0);
-  sg->reset();
-  sg->prepareDataAccess();
-  sg->setEmptyValue(emptyVal);
-  sg->setFullValue(fullVal);
-  const int nv = sg->nVoxelsInBlock();
-  size_t off = 0;
-  for (int bid = 0; bid < nb; bid++) {
-    switch (kind[bid]) {
-      case 1: {
-        float* d = sg->getBlockDataPtr(bid, 1, 0);
-        std::memcpy(d, values + off, sizeof(float) * nv);
-        off += nv;
-        break;
-      }
-      case 2: sg->setEmptyBlock(bid); break;
-      case 3: sg->setFullBlock(bid); break;
-      default: break;
-    }
-  }
-  std::vector<int> blockList(update, update + nUpdate);
-  auto t0 = std::chrono::steady_clock::now();
-  msbg->applyChannelPdeFast<float>(chan, CH_NULL, CH_NULL, &blockList,
-                                   -(PDE_MEAN_CURVATURE + OPT_8_COLOR_SCHEME),
-                                   clamp01, 0, 0, 0, numIter, 1.0f, dt);
-  auto t1 = std::chrono::steady_clock::now();
-  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
-  off = 0;
-  for (int bid = 0; bid < nb; bid++) {
-    if (kind[bid] != 1) continue;
-    const float* d = sg->getBlockDataPtr(bid);
-    std::memcpy(values + off, d, sizeof(float) * nv);
-    off += nv;
-  }
-  MultiresSparseGrid::destroy(msbg);
-  return 0;
+  return mcf_run<float>(sx, sy, sz, bsx, kind, emptyVal, fullVal, values, update, nUpdate,
+                        numIter, dt, clamp01, seconds);
 }
 
 // Mean-curvature flow on the quantised render-density channel the reference
-// is built with (RSURF_16_BIT, src/msbgcell.h:67-68: RenderDensity = uint16_t),
-// as msbg_demo.cpp:297-298 and 716-727 run it: CH_UINT16_1, values stored as
-// round(phi * 65535) and read as q * (1/65535) (src/sbg.h:225-232, 360-368).
-// Same block kinds and packed layout as ref_mcf; values and the const
-// blocks' emptyVal / fullVal are raw 16-bit integers.
+// is built with, as msbg_demo.cpp:297-298 and 716-727 run it: values stored
+// as round(phi * 65535) and read as q * (1/65535) (src/sbg.h:225-232,
+// 360-368).  Values and the const blocks' emptyVal / fullVal are raw 16-bit
+// integers.
 extern "C" int ref_mcf_u16(int sx, int sy, int sz, int bsx, const int8_t* kind, uint16_t emptyVal,
                            uint16_t fullVal, uint16_t* values, const int* update, int nUpdate,
                            int numIter, float dt, int clamp01, double* seconds) {
-  MultiresSparseGrid* msbg = MultiresSparseGrid::create(
-      "REFQ", sx, sy, sz, bsx, -1, 0, -1,
-      MSBG::OPT_SINGLE_LEVEL | MSBG::OPT_SINGLE_CHANNEL_FLOAT);
-  if (!msbg) return 1;
-  const int nb = msbg->nBlocks();
-  {
-    std::vector<int> levels(nb, 0);
-    msbg->regularizeRefinementMap(levels.data());
-    msbg->setRefinementMap(levels.data(), NULL, -1, NULL, false);
-  }
-  const int chan = CH_UINT16_1;
-  SparseGrid<uint16_t>* sg = msbg->getUint16Channel(chan, 0);
-  if (!sg) {
-    MultiresSparseGrid::destroy(msbg);
-    return 2;
-  }
-  sg->reset();
-  sg->prepareDataAccess();
-  sg->setEmptyValue(emptyVal);
-  sg->setFullValue(fullVal);
-  const int nv = sg->nVoxelsInBlock();
-  size_t off = 0;
-  for (int bid = 0; bid < nb; bid++) {
-    switch (kind[bid]) {
-      case 1: {
-        uint16_t* d = sg->getBlockDataPtr(bid, 1, 0);
-        std::memcpy(d, values + off, sizeof(uint16_t) * nv);
-        off += nv;
-        break;
-      }
-      case 2: sg->setEmptyBlock(bid); break;
-      case 3: sg->setFullBlock(bid); break;
-      default: break;
-    }
-  }
-  std::vector<int> blockList(update, update + nUpdate);
-  auto t0 = std::chrono::steady_clock::now();
-  msbg->applyChannelPdeFast<uint16_t>(chan, CH_NULL, CH_NULL, &blockList,
-                                      -(PDE_MEAN_CURVATURE + OPT_8_COLOR_SCHEME), clamp01, 0, 0,
-                                      0, numIter, 1.0f, dt);
-  auto t1 = std::chrono::steady_clock::now();
-  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
-  off = 0;
-  for (int bid = 0; bid < nb; bid++) {
-    if (kind[bid] != 1) continue;
-    const uint16_t* d = sg->getBlockDataPtr(bid);
-    std::memcpy(values + off, d, sizeof(uint16_t) * nv);
-    off += nv;
-  }
-  MultiresSparseGrid::destroy(msbg);
-  return 0;
+  return mcf_run<uint16_t>(sx, sy, sz, bsx, kind, emptyVal, fullVal, values, update, nUpdate,
+                           numIter, dt, clamp01, seconds);
+}
+
+// The same grids for a caller that runs its own code on them (the
+// integration adapter): create, read the channel back, destroy.
+extern "C" void* ref_grid_create_f32(int sx, int sy, int sz, int bsx, const int8_t* kind,
+                                     float emptyVal, float fullVal, const float* values) {
+  return mcf_grid_create<float>(sx, sy, sz, bsx, kind, emptyVal, fullVal, values);
+}
+extern "C" void* ref_grid_create_u16(int sx, int sy, int sz, int bsx, const int8_t* kind,
+                                     uint16_t emptyVal, uint16_t fullVal, const uint16_t* values) {
+  return mcf_grid_create<uint16_t>(sx, sy, sz, bsx, kind, emptyVal, fullVal, values);
+}
+extern "C" void ref_grid_read_f32(void* m, const int8_t* kind, float* values) {
+  mcf_grid_read<float>((MultiresSparseGrid*)m, kind, values);
+}
+extern "C" void ref_grid_read_u16(void* m, const int8_t* kind, uint16_t* values) {
+  mcf_grid_read<uint16_t>((MultiresSparseGrid*)m, kind, values);
+}
+extern "C" void ref_grid_destroy(void* m) {
+  MultiresSparseGrid* g = (MultiresSparseGrid*)m;
+  MultiresSparseGrid::destroy(g);
 }
 
 // ---------------------------------------------------------------------------
@@ -245,6 +261,9 @@ extern "C" void ref_ps_destroy(void* hp) {
   MultiresSparseGrid::destroy(h->msbg);
   delete h;
 }
+
+// The prepared grid itself, for a caller that runs its own code on it.
+extern "C" void* ref_ps_grid(void* hp) { return ((PsHandle*)hp)->msbg; }
 
 extern "C" float ref_ps_omega(void* hp) { return ((PsHandle*)hp)->msbg->_mgSmOmega; }
 extern "C" int ref_ps_num_levels(void* hp) { return ((PsHandle*)hp)->msbg->getNumLevels(); }

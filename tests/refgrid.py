@@ -101,3 +101,34 @@ def box_problem(res=32, bsx0=16, z_liquid=20, seed=0):
     rng = np.random.default_rng(seed)
     rhs = (rng.standard_normal((res,) * 3) * (z < z_liquid)).astype(np.float32)
     return (to_blocks(flags, bsx0), [to_blocks(f, bsx0) for f in faces], to_blocks(rhs, bsx0))
+
+
+class OpenPool:
+    """A pool (liquid below z = z_liquid, air above) on a grid with every
+    block at level 0 whose face callback returns `face` for every face,
+    inside the grid or not, so that each domain-face rule shows in A x.  Has
+    the interface of msbg_gpu.PressureScene that the oracle functions and the
+    reference driver read."""
+
+    def __init__(self, res=16, bsx0=16, z_liquid=12, face=0.5):
+        import ctypes as C
+
+        import msbg_gpu
+
+        self.res, self.bsx0, self.n_levels = res, bsx0, 2
+        self.block_levels = np.zeros((res // bsx0) ** 3, np.int32)
+        self._ct = C.CFUNCTYPE(C.c_uint16, C.c_void_p, C.c_int, C.c_int, C.c_int)(
+            lambda u, x, y, z: 0 if z < z_liquid else 0x1000)
+        self._fc = C.CFUNCTYPE(C.c_float, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int)(
+            lambda u, d, x, y, z: face)
+        self._rh = C.CFUNCTYPE(C.c_float, C.c_void_p, C.c_int, C.c_int, C.c_int)(
+            lambda u, x, y, z: 1.0)
+        self._cb = msbg_gpu.PressureCallbacks(C.cast(self._ct, C.c_void_p).value,
+                                              C.cast(self._fc, C.c_void_p).value,
+                                              C.cast(self._rh, C.c_void_p).value, None)
+
+    def callbacks(self):
+        return self._cb
+
+    def packed_size(self):
+        return self.res ** 3

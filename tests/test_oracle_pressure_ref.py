@@ -66,3 +66,32 @@ def test_oracle_residual_equals_reference():
     r_ref = R.get(rp.CH_FLOAT_6)
     r = b - oracle.pressure_apply_oracle(scene, x.astype(np.float64))
     assert rel_max(r, r_ref, R.liquid()) <= 1e-6
+
+
+def test_domain_faces_follow_the_reference_operator():
+    """The reference's FLIP operator ignores setDomainBoundarySpec_: its
+    diagonal (computeDiagonalFLIP_, src/msbg3.cpp:2714-2722) takes the
+    callback's coefficient on the lower domain faces and reads the upper ones
+    past the grid as 0, whatever the spec.  With a face callback that is 0.5
+    everywhere, the oracle without a spec (the rule msbg_topo_desc.domainBc =
+    NULL selects) equals the reference's A x for every spec the reference is
+    given, including flip_sim's open top (src/flip_sim.cpp:1621)."""
+    import ref_pressure as rp
+    from refgrid import OpenPool
+
+    s = OpenPool(res=32, bsx0=16, z_liquid=20)
+    rng = np.random.default_rng(4)
+    for bc in ((rp.DBC_SOLID,) * 6, (rp.DBC_OPEN,) * 6, (1, 1, 1, 0, 1, 1)):
+        R = rp.RefPressure(s, dom_bc=bc)
+        try:
+            x = (rng.uniform(-1, 1, R.packed_size(0)) * R.liquid()).astype(np.float32)
+            R.set(rp.CH_FLOAT_3, x)
+            R.multiply(0, rp.CH_FLOAT_3, rp.CH_FLOAT_6)
+            y_ref = R.get(rp.CH_FLOAT_6)
+        finally:
+            R.close()
+        y = oracle.pressure_apply_oracle(s, x.astype(np.float64))
+        assert rel_max(y, y_ref) <= 1e-6, bc
+        # the lower faces do count: without them the two differ
+        y_solid = oracle.pressure_apply_oracle(s, x.astype(np.float64), domain_bc=[1] * 6)
+        assert rel_max(y_solid, y_ref) > 1e-2

@@ -66,53 +66,62 @@ def test_oracle_solution_satisfies_system():
     assert np.abs(ax - b).max() <= 1e-9 * np.abs(b).max()
 
 
-def test_domain_boundary_spec_sets_the_wall_faces():
-    """msbg_topo_desc.domainBc: a DBC_SOLID domain face has no coupling, a
-    DBC_OPEN one couples to p = 0 outside with the callback's coefficient
-    (setDomainBoundarySpec_, src/msbg.cpp:2462).  A pool (liquid below z = 12,
-    air above) whose face callback returns 1 everywhere, walls solid: opening
-    the -x face adds one coupling to each liquid cell at x = 0, so A x for
-    x = 1 differs by exactly 1 there and nowhere else."""
-    import ctypes as C
-
-    import numpy as np
-
-    import msbg_gpu
-    from refgrid import to_blocks
-
-    res, bsx0 = 16, 16
+def _host_apply(scene, x, dbc):
     L = msbg_gpu.lib()
     msbg_gpu._pressure_sigs(L)
-    ct = C.CFUNCTYPE(C.c_uint16, C.c_void_p, C.c_int, C.c_int, C.c_int)(
-        lambda u, x, y, z: 0 if z < 12 else 0x1000)
-    fc = C.CFUNCTYPE(C.c_float, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int)(
-        lambda u, d, x, y, z: 1.0)
-    rh = C.CFUNCTYPE(C.c_float, C.c_void_p, C.c_int, C.c_int, C.c_int)(lambda u, x, y, z: 1.0)
-    cb = msbg_gpu.PressureCallbacks(C.cast(ct, C.c_void_p).value, C.cast(fc, C.c_void_p).value,
-                                    C.cast(rh, C.c_void_p).value, None)
-    bl = np.zeros(1, np.int32)
-    x = np.ones(res ** 3, np.float32)
-    ys = []
-    for dbc in ([1, 1, 1, 1, 1, 1], [0, 1, 1, 1, 1, 1]):
-        d = np.array(dbc, np.int32)
-        topo = msbg_gpu.TopoDesc(res, res, res, bsx0, 2, bl.ctypes.data_as(C.POINTER(C.c_int)),
-                                 d.ctypes.data_as(C.POINTER(C.c_int)))
-        y = np.zeros(res ** 3, np.float64)
-        nm = C.c_int()
-        fluid = np.zeros(32, np.int64)
-        rc = L.msbg_gpu_pressure_host_check(C.byref(topo), C.byref(cb),
-                                            x.ctypes.data_as(C.POINTER(C.c_float)),
-                                            y.ctypes.data_as(C.POINTER(C.c_double)), C.byref(nm),
-                                            fluid.ctypes.data_as(C.POINTER(C.c_int64)), None)
-        assert rc == 0
-        ys.append(y)
-    zz, yy, xx = np.meshgrid(np.arange(res), np.arange(res), np.arange(res), indexing="ij")
-    face = to_blocks(((xx == 0) & (zz < 12)).astype(np.float32), bsx0) > 0
-    diff = ys[1] - ys[0]
-    assert np.allclose(diff[face], 1.0) and np.allclose(diff[~face], 0.0)
-    bad = np.array([0, 1, 1, 1, 1, 2], np.int32)  # not a DBC_* value
-    topo = msbg_gpu.TopoDesc(res, res, res, bsx0, 2, bl.ctypes.data_as(C.POINTER(C.c_int)),
-                             bad.ctypes.data_as(C.POINTER(C.c_int)))
+    bl = np.ascontiguousarray(scene.block_levels, np.int32)
+    d = None if dbc is None else np.array(dbc, np.int32)
+    topo = msbg_gpu.TopoDesc(scene.res, scene.res, scene.res, scene.bsx0, scene.n_levels,
+                             bl.ctypes.data_as(C.POINTER(C.c_int)),
+                             None if d is None else d.ctypes.data_as(C.POINTER(C.c_int)))
+    cb = scene.callbacks()
+    y = np.zeros(len(x), np.float64)
     nm = C.c_int()
-    assert L.msbg_gpu_pressure_host_check(C.byref(topo), C.byref(cb), None, None, C.byref(nm),
-                                          None, None) == 5
+    fluid = np.zeros(32, np.int64)
+    rc = L.msbg_gpu_pressure_host_check(C.byref(topo), C.byref(cb),
+                                        x.ctypes.data_as(C.POINTER(C.c_float)),
+                                        y.ctypes.data_as(C.POINTER(C.c_double)), C.byref(nm),
+                                        fluid.ctypes.data_as(C.POINTER(C.c_int64)), None)
+    return rc, y
+
+
+def test_domain_boundary_spec_sets_the_wall_faces():
+    """msbg_topo_desc.domainBc (setDomainBoundarySpec_, src/msbg.cpp:2462):
+    p = 0 outside the grid, behind a coupling of 0 (DBC_SOLID), of the
+    callback's coefficient on a lower face and 1 on an upper face (DBC_OPEN,
+    the reference's constFaceCoeffAirBlock, src/msbg3.cpp:733-740), and with
+    no spec the reference's own operator: lower faces as open, upper faces 0
+    (computeDiagonalFLIP_, src/msbg3.cpp:2714-2722).  For x = 1, A x is the
+    sum of the couplings to the outside and to air, so each rule shows as a
+    constant on the liquid cells of one domain face."""
+    from refgrid import OpenPool, to_blocks
+
+
+    s = OpenPool()
+    res = s.res
+    x = np.ones(res ** 3, np.float32)
+    zz, yy, xx = np.meshgrid(np.arange(res), np.arange(res), np.arange(res), indexing="ij")
+    liq = zz < 12
+    # couplings to air: the cells below the surface
+    air = np.where(liq & (zz == 11), 0.5, 0.0)
+
+    def expect(lo, hi):
+        """lo/hi: coupling through each lower/upper domain face (x, y, z)"""
+        e = air.copy()
+        for ax, c in enumerate((xx, yy, zz)):
+            e += np.where(liq & (c == 0), lo[ax], 0.0)
+            e += np.where(liq & (c == res - 1), hi[ax], 0.0)
+        return to_blocks(np.where(liq, e, 0.0), s.bsx0)
+
+    cases = [([1] * 6, (0, 0, 0), (0, 0, 0)),
+             ([0] * 6, (0.5, 0.5, 0.5), (1, 1, 1)),
+             ([1, 0, 0, 1, 1, 1], (0, 0.5, 0), (1, 0, 0)),
+             (None, (0.5, 0.5, 0.5), (0, 0, 0))]
+    for dbc, lo, hi in cases:
+        rc, y = _host_apply(s, x, dbc)
+        assert rc == 0
+        assert np.allclose(y, expect(lo, hi)), dbc
+        yo = oracle.pressure_apply_oracle(s, x.astype(np.float64), domain_bc=dbc)
+        assert np.abs(y - yo).max() <= 1e-6, dbc
+    bad = [0, 1, 1, 1, 1, 2]  # not a DBC_* value
+    assert _host_apply(s, x, bad)[0] == 5
