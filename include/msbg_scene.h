@@ -62,6 +62,13 @@ msbg_pressure_scene* msbg_scene_pressure_create_wavy(int res, int bsx0, int nLev
 void msbg_scene_pressure_destroy(msbg_pressure_scene* s);
 /* Refinement map (levels per base block, bid order). */
 int msbg_scene_pressure_block_levels(const msbg_pressure_scene* s, int* levels);
+/* The scene as per-cell arrays in the packed layout msbg_gpu_pressure_prepare_arrays
+ * takes: for every base block in bid order, (bsx0 >> level)^3 cells
+ * (vid = x + y*bs + z*bs*bs), each sampled by the callbacks below at the fine
+ * voxel of its lowest corner: cell type, lower-face coefficient per direction,
+ * rhs.  Each array holds the sum over blocks of (bsx0 >> level)^3 values. */
+int msbg_scene_pressure_arrays(const msbg_pressure_scene* s, uint16_t* flags, float* faceX,
+                               float* faceY, float* faceZ, float* rhs);
 uint16_t msbg_scene_cell_type(void* scene, int x, int y, int z);
 float msbg_scene_face_coeff(void* scene, int dir, int x, int y, int z);
 float msbg_scene_rhs(void* scene, int x, int y, int z);

@@ -107,6 +107,8 @@ def scene_lib():
                                                  i32, i32, f32, C.c_uint64]),
         "msbg_scene_pressure_destroy": (None, [vp]),
         "msbg_scene_pressure_block_levels": (i32, [vp, C.POINTER(C.c_int)]),
+        "msbg_scene_pressure_arrays": (i32, [vp, C.POINTER(C.c_uint16)] +
+                                       [C.POINTER(C.c_float)] * 4),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -350,6 +352,20 @@ class PressureScene:
 
     def packed_size(self):
         return int(sum((self.bsx0 >> int(l)) ** 3 for l in self.block_levels))
+
+    def arrays(self):
+        """The scene as the per-cell arrays of Context.pressure_prepare_arrays:
+        (flags uint16, [faceX, faceY, faceZ] float32, rhs float32)."""
+        n = self.packed_size()
+        flags = np.empty(n, np.uint16)
+        face = [np.empty(n, np.float32) for _ in range(3)]
+        rhs = np.empty(n, np.float32)
+        rc = self._L.msbg_scene_pressure_arrays(self.h, _p(flags, C.c_uint16),
+                                                *[_p(f, C.c_float) for f in face],
+                                                _p(rhs, C.c_float))
+        if rc:
+            raise MsbgError(rc, "scene arrays")
+        return flags, face, rhs
 
     def close(self):
         if self.h:

@@ -500,3 +500,36 @@ extern "C" float msbg_scene_face_coeff(void* p, int dir, int x, int y, int z) {
 extern "C" float msbg_scene_rhs(void* p, int x, int y, int z) {
   return static_cast<msbg_pressure_scene*>(p)->rhs(x, y, z);
 }
+
+// The scene sampled into the per-cell arrays of msbg_gpu_pressure_prepare_arrays:
+// for every base block in bid order, (bsx0 >> level)^3 cells in the block's
+// voxel order, each sampled at the fine voxel of its lowest corner.
+extern "C" int msbg_scene_pressure_arrays(const msbg_pressure_scene* s, uint16_t* flags,
+                                          float* faceX, float* faceY, float* faceZ,
+                                          float* rhs) {
+  if (!s || !flags || !faceX || !faceY || !faceZ || !rhs) return MSBG_EINVARG;
+  const int bs0 = s->bsx0, nbx = s->res / bs0;
+  const int64_t nb = (int64_t)nbx * nbx * nbx;
+  std::vector<int64_t> boff(nb + 1, 0);
+  for (int64_t b = 0; b < nb; b++) {
+    const int bs = bs0 >> s->levels[b];
+    boff[b + 1] = boff[b] + (int64_t)bs * bs * bs;
+  }
+  float* face[3] = {faceX, faceY, faceZ};
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t b = 0; b < nb; b++) {
+    const int l = s->levels[b], bs = bs0 >> l;
+    const int ox = (int)(b % nbx) * bs0, oy = (int)((b / nbx) % nbx) * bs0,
+              oz = (int)(b / ((int64_t)nbx * nbx)) * bs0;
+    int64_t c = boff[b];
+    for (int k = 0; k < bs; k++)
+      for (int j = 0; j < bs; j++)
+        for (int i = 0; i < bs; i++, c++) {
+          const int x = ox + (i << l), y = oy + (j << l), z = oz + (k << l);
+          flags[c] = s->cell_type(x, y, z);
+          for (int d = 0; d < 3; d++) face[d][c] = s->face(d, x, y, z);
+          rhs[c] = s->rhs(x, y, z);
+        }
+  }
+  return MSBG_OK;
+}
