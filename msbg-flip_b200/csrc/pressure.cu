@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -197,6 +198,11 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
                                          const msbg_pressure_callbacks* cb) {
   if (!ctx || !topo || !cb || !cb->sampleCellType || !cb->sampleFaceCoeff || !cb->sampleRhs)
     return MSBG_EINVARG;
+  return msbg::ps::pressure_prepare(ctx, topo, cb, nullptr);
+}
+
+int msbg::ps::pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
+                               const msbg_pressure_callbacks* cb, const ArrayInput* arr) {
   int rc = msbg_gpu_sync_topology(ctx, topo);
   if (rc) return rc;
   cudaSetDevice(ctx->device);
@@ -205,8 +211,18 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
   Solver& S = *sp;
   std::string err;
   auto tp0 = std::chrono::steady_clock::now();
-  rc = build_hierarchy(S.H, topo->sx, topo->sy, topo->sz, topo->bsx0, topo->nLevels,
-                       topo->blockLevel, topo->domainBc, cb, 512, &err);
+  // per-cell arrays: the per-cell work of the build runs on the GPU (set
+  // MSBG_PRESSURE_BUILD=host to build them on the host as the callbacks are)
+  const char* bsel = getenv("MSBG_PRESSURE_BUILD");
+  const bool onDevice = arr && !(bsel && std::strcmp(bsel, "host") == 0);
+  std::vector<std::unique_ptr<LevelDev>> built;
+  if (onDevice)
+    rc = build_hierarchy_device(S.H, built, S.rhs0, topo->sx, topo->sy, topo->sz, topo->bsx0,
+                                topo->nLevels, topo->blockLevel, topo->domainBc, *arr, 512,
+                                ctx->stream, &err);
+  else
+    rc = build_hierarchy(S.H, topo->sx, topo->sy, topo->sz, topo->bsx0, topo->nLevels,
+                         topo->blockLevel, topo->domainBc, cb, 512, &err, arr);
   S.buildSeconds =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - tp0).count();
   if (rc) {
@@ -233,25 +249,31 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
   int maxPartial = VEC_GRID;
   for (size_t m = 0; m < S.H.levels.size(); m++) {
     const Level& L = S.H.levels[m];
-    auto D = std::make_unique<LevelDev>();
+    // the operator of a device build is in place already
+    auto D = onDevice ? std::move(built[m]) : std::make_unique<LevelDev>();
     std::vector<int64_t> toff(L.tiles.size());
     for (size_t i = 0; i < L.tiles.size(); i++) toff[i] = L.tiles[i].off;
     MSBG_CUDA_TRY(ctx, upload(D->tileOff, toff, st));
     MSBG_CUDA_TRY(ctx, upload(D->face, L.face, st));
-    MSBG_CUDA_TRY(ctx, upload(D->ifOff, L.ifOff, st));
+    if (!onDevice) MSBG_CUDA_TRY(ctx, upload(D->ifOff, L.ifOff, st));
     MSBG_CUDA_TRY(ctx, upload(D->toCoarse, L.toCoarse, st));
     MSBG_CUDA_TRY(ctx, upload(D->passTiles, L.passTiles, st));
     MSBG_CUDA_TRY(ctx, upload(D->groupTiles, L.groupTiles, st));
-    MSBG_CUDA_TRY(ctx, upload(D->diag, L.diag, st));
-    if (m == 0) MSBG_CUDA_TRY(ctx, upload(D->ctype, L.ctype, st));
+    if (!onDevice) {
+      MSBG_CUDA_TRY(ctx, upload(D->diag, L.diag, st));
+      if (m == 0) MSBG_CUDA_TRY(ctx, upload(D->ctype, L.ctype, st));
+    }
     {
-      HostArray<float> inv;
-      inv.resize(L.diag.size());
-      const int64_t nInv = (int64_t)inv.size();
+      if (!onDevice) {
+        HostArray<float> inv;
+        inv.resize(L.diag.size());
+        const int64_t nInv = (int64_t)inv.size();
 #pragma omp parallel for schedule(static)
-      for (int64_t c = 0; c < nInv; c++)
-        inv[c] = L.diag[c] > 0.f ? (float)(1.0 / (double)L.diag[c]) : 0.f;
-      MSBG_CUDA_TRY(ctx, upload(D->invdiag, inv, st));
+        for (int64_t c = 0; c < nInv; c++)
+          inv[c] = L.diag[c] > 0.f ? (float)(1.0 / (double)L.diag[c]) : 0.f;
+        MSBG_CUDA_TRY(ctx, upload(D->invdiag, inv, st));
+        MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));  // inv is a temporary
+      }
       MSBG_CUDA_TRY(ctx, upload(D->tileRec, build_tile_records(L), st));
       // the hot-path kernels address passes as contiguous tile-id ranges
       for (size_t i = 0; i < L.passTiles.size(); i++)
@@ -259,10 +281,12 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
           return set_error(ctx, MSBG_EINTERNAL, "pass tiles are not contiguous");
       MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));  // host vectors above are temporaries
     }
-    MSBG_CUDA_TRY(ctx, upload(D->cx, L.cx, st));
-    MSBG_CUDA_TRY(ctx, upload(D->cy, L.cy, st));
-    MSBG_CUDA_TRY(ctx, upload(D->cz, L.cz, st));
-    MSBG_CUDA_TRY(ctx, upload(D->ifc, L.ifc, st));
+    if (!onDevice) {
+      MSBG_CUDA_TRY(ctx, upload(D->cx, L.cx, st));
+      MSBG_CUDA_TRY(ctx, upload(D->cy, L.cy, st));
+      MSBG_CUDA_TRY(ctx, upload(D->cz, L.cz, st));
+      MSBG_CUDA_TRY(ctx, upload(D->ifc, L.ifc, st));
+    }
     const size_t nb = sizeof(float) * std::max<int64_t>(L.nCells, 4);
     MSBG_CUDA_TRY(ctx, D->x.ensure(nb));
     MSBG_CUDA_TRY(ctx, D->b.ensure(nb));
@@ -307,7 +331,7 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
   }
   const Level& L0 = S.H.levels[0];
   const size_t n0 = sizeof(float) * L0.nCells;
-  MSBG_CUDA_TRY(ctx, upload(S.rhs0, L0.rhs, st));
+  if (!onDevice) MSBG_CUDA_TRY(ctx, upload(S.rhs0, L0.rhs, st));
   MSBG_CUDA_TRY(ctx, S.d0.ensure(n0));
   MSBG_CUDA_TRY(ctx, S.q0.ensure(n0));
   MSBG_CUDA_TRY(ctx, S.z0.ensure(n0));
@@ -322,9 +346,11 @@ extern "C" int msbg_gpu_pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc
   for (const auto& D : S.dev)
     S.h2dBytes += (int64_t)(D->tileOff.bytes + D->face.bytes + D->ifOff.bytes +
                             D->toCoarse.bytes + D->passTiles.bytes + D->groupTiles.bytes +
-                            D->diag.bytes + D->cx.bytes + D->cy.bytes + D->cz.bytes +
-                            D->ifc.bytes);
-  S.h2dBytes += (int64_t)(S.rhs0.bytes + S.dCoarseInv.bytes + S.dCoarseCells.bytes);
+                            (onDevice ? 0
+                                      : D->diag.bytes + D->cx.bytes + D->cy.bytes +
+                                            D->cz.bytes + D->ifc.bytes));
+  S.h2dBytes += (int64_t)(S.dCoarseInv.bytes + S.dCoarseCells.bytes) +
+                (onDevice ? S.H.deviceBuildH2D : (int64_t)S.rhs0.bytes);
   S.prepareSeconds =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - tp0).count();
   return MSBG_OK;

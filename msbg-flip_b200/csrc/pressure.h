@@ -9,6 +9,7 @@
 #include <map>
 #include <memory>
 #include <utility>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -112,6 +113,7 @@ struct LevelDev {
   DeviceBuffer tileRec;            // 256-byte per-tile records (smooth_pipe.cuh)
   DeviceBuffer x, b, r;            // FP32 work vectors of this level
   DeviceBuffer ctype;              // level 0: CT_* per cell
+  DeviceBuffer fluid;              // liquid flag per cell (device build only)
 };
 
 // Domain faces without a caller spec follow the reference's FLIP operator:
@@ -134,12 +136,36 @@ struct Hierarchy {
   int nCoarse = 0;
   std::vector<double> coarseInv;
   std::vector<int64_t> coarseCells;
+  int64_t deviceBuildH2D = 0;      // bytes a device build copied to the GPU
 };
 
-// Host construction (pressure_host.cpp).
+// Per-cell arrays of MG level 0 in the packed block layout (for every block
+// in bid order, (bsx0 >> level)^3 cells, vid = x + y*bs + z*bs*bs): cell
+// flags, lower-face coefficient per direction, right-hand side (may be NULL).
+// A level-l cell reads the entry of the cell holding its lowest fine voxel,
+// as the callbacks would be asked.
+struct ArrayInput {
+  const uint16_t* flags;
+  const float* face[3];
+  const float* rhs;
+};
+
+// Construction of the hierarchy from the arrays with the per-cell work on the
+// GPU (pressure_host.cpp, build_gpu.cu): H receives the topology of every
+// level (tiles, faces, restriction maps, passes) and the coarsest inverse;
+// dev[m] the operator of level m (diag, invdiag, cx, cy, cz, ifc, ifOff;
+// level 0 also ctype), rhs0 the right-hand side of level 0.
+int build_hierarchy_device(Hierarchy& H, std::vector<std::unique_ptr<LevelDev>>& dev,
+                           DeviceBuffer& rhs0, int sx, int sy, int sz, int bsx0, int nLevels,
+                           const int* blockLevel, const int* domainBc, const ArrayInput& arr,
+                           int maxCoarseCells, cudaStream_t st, std::string* err);
+
+// Host construction (pressure_host.cpp) from the callbacks cb, or from the
+// arrays arr when arr is given (cb is then not used).
 int build_hierarchy(Hierarchy& H, int sx, int sy, int sz, int bsx0, int nLevels,
                     const int* blockLevel, const int* domainBc,
-                    const msbg_pressure_callbacks* cb, int maxCoarseCells, std::string* err);
+                    const msbg_pressure_callbacks* cb, int maxCoarseCells, std::string* err,
+                    const ArrayInput* arr = nullptr);
 
 }  // namespace ps
 }  // namespace msbg

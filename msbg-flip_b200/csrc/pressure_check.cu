@@ -123,16 +123,13 @@ struct Packing {
 using namespace msbg;
 using namespace msbg::ps;
 
-extern "C" int msbg_gpu_pressure_host_check(const msbg_topo_desc* topo,
-                                            const msbg_pressure_callbacks* cb,
-                                            const float* xPacked, double* yPacked,
-                                            int* nMgLevels, int64_t* fluidPerLevel,
-                                            double* galerkinErr) {
-  if (!topo || !cb) return MSBG_EINVARG;
+static int host_check(const msbg_topo_desc* topo, const msbg_pressure_callbacks* cb,
+                      const ArrayInput* arr, const float* xPacked, double* yPacked,
+                      int* nMgLevels, int64_t* fluidPerLevel, double* galerkinErr) {
   Hierarchy H;
   std::string err;
   int rc = build_hierarchy(H, topo->sx, topo->sy, topo->sz, topo->bsx0, topo->nLevels,
-                           topo->blockLevel, topo->domainBc, cb, 512, &err);
+                           topo->blockLevel, topo->domainBc, cb, 512, &err, arr);
   if (rc) {
     fprintf(stderr, "msbg_gpu_pressure_host_check: %s\n", err.c_str());
     return rc;
@@ -194,4 +191,25 @@ extern "C" int msbg_gpu_pressure_host_check(const msbg_topo_desc* topo,
     }
   }
   return MSBG_OK;
+}
+
+extern "C" int msbg_gpu_pressure_host_check(const msbg_topo_desc* topo,
+                                            const msbg_pressure_callbacks* cb,
+                                            const float* xPacked, double* yPacked,
+                                            int* nMgLevels, int64_t* fluidPerLevel,
+                                            double* galerkinErr) {
+  if (!topo || !cb) return MSBG_EINVARG;
+  return host_check(topo, cb, nullptr, xPacked, yPacked, nMgLevels, fluidPerLevel, galerkinErr);
+}
+
+// The same from the per-cell arrays of msbg_gpu_pressure_prepare_arrays.
+extern "C" int msbg_gpu_pressure_host_check_arrays(const msbg_topo_desc* topo,
+                                                   const uint16_t* flags, const float* faceX,
+                                                   const float* faceY, const float* faceZ,
+                                                   const float* rhs, const float* xPacked,
+                                                   double* yPacked, int* nMgLevels,
+                                                   int64_t* fluidPerLevel, double* galerkinErr) {
+  if (!topo || !flags || !faceX || !faceY || !faceZ) return MSBG_EINVARG;
+  const ArrayInput A{flags, {faceX, faceY, faceZ}, rhs};
+  return host_check(topo, nullptr, &A, xPacked, yPacked, nMgLevels, fluidPerLevel, galerkinErr);
 }

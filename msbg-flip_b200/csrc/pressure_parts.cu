@@ -370,39 +370,6 @@ int relax_reference(msbg_gpu_ctx* ctx, Solver& S, int m, float* x, const float* 
 // ---------------------------------------------------------------------------
 // bulk-array prepare: callbacks that read the caller's arrays
 // ---------------------------------------------------------------------------
-struct ArrayScene {
-  int sx, sy, sz, bsx0, nbx, nby;
-  std::vector<int> level;
-  std::vector<int64_t> boff;
-  const uint16_t* flags;
-  const float* face[3];
-  const float* rhs;
-  // packed index of the cell holding fine voxel (x, y, z), or -1 outside
-  int64_t cell(int x, int y, int z) const {
-    if (x < 0 || y < 0 || z < 0 || x >= sx || y >= sy || z >= sz) return -1;
-    const int64_t b = (x / bsx0) + (int64_t)nbx * ((y / bsx0) + (int64_t)nby * (z / bsx0));
-    const int l = level[b], bs = bsx0 >> l;
-    const int vx = (x % bsx0) >> l, vy = (y % bsx0) >> l, vz = (z % bsx0) >> l;
-    return boff[b] + vx + (int64_t)bs * (vy + (int64_t)bs * vz);
-  }
-};
-
-uint16_t array_cell_type(void* u, int x, int y, int z) {
-  const ArrayScene* A = static_cast<const ArrayScene*>(u);
-  const int64_t c = A->cell(x, y, z);
-  return c < 0 ? (uint16_t)0x1 : A->flags[c];  // outside the domain: solid
-}
-float array_face(void* u, int dir, int x, int y, int z) {
-  const ArrayScene* A = static_cast<const ArrayScene*>(u);
-  const int64_t c = A->cell(x, y, z);
-  return c < 0 ? 0.f : A->face[dir][c];  // no face outside the domain
-}
-float array_rhs(void* u, int x, int y, int z) {
-  const ArrayScene* A = static_cast<const ArrayScene*>(u);
-  const int64_t c = A->cell(x, y, z);
-  return c < 0 || !A->rhs ? 0.f : A->rhs[c];
-}
-
 }  // namespace
 }  // namespace ps
 }  // namespace msbg
@@ -603,31 +570,13 @@ extern "C" int msbg_gpu_pressure_prepare_arrays(msbg_gpu_ctx* ctx, const msbg_to
       topo->sy <= 0 || topo->sz <= 0 || topo->sx % topo->bsx0 || topo->sy % topo->bsx0 ||
       topo->sz % topo->bsx0 || topo->nLevels < 1 || topo->nLevels > 4)
     return msbg_gpu_sync_topology(ctx, topo);  // reports the invalid field
-  ArrayScene A;
-  A.sx = topo->sx;
-  A.sy = topo->sy;
-  A.sz = topo->sz;
-  A.bsx0 = topo->bsx0;
-  A.nbx = topo->sx / topo->bsx0;
-  A.nby = topo->sy / topo->bsx0;
-  const int64_t nb = (int64_t)A.nbx * A.nby * (topo->sz / topo->bsx0);
-  A.level.assign(nb, 0);
-  A.boff.resize(nb);
-  int64_t c = 0;
-  for (int64_t b = 0; b < nb; b++) {
-    const int l = topo->blockLevel ? topo->blockLevel[b] : 0;
+  const int64_t nb =
+      (int64_t)(topo->sx / topo->bsx0) * (topo->sy / topo->bsx0) * (topo->sz / topo->bsx0);
+  for (int64_t b = 0; topo->blockLevel && b < nb; b++) {
+    const int l = topo->blockLevel[b];
     if (l < 0 || l >= topo->nLevels)
       return set_error(ctx, MSBG_EINVARG, "blockLevel[%lld]=%d out of range", (long long)b, l);
-    A.level[b] = l;
-    A.boff[b] = c;
-    const int bs = topo->bsx0 >> l;
-    c += (int64_t)bs * bs * bs;
   }
-  A.flags = flags;
-  A.face[0] = faceX;
-  A.face[1] = faceY;
-  A.face[2] = faceZ;
-  A.rhs = rhs;
-  msbg_pressure_callbacks cb{array_cell_type, array_face, array_rhs, &A};
-  return msbg_gpu_pressure_prepare(ctx, topo, &cb);
+  ArrayInput A{flags, {faceX, faceY, faceZ}, rhs};
+  return pressure_prepare(ctx, topo, nullptr, &A);
 }

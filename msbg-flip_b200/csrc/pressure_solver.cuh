@@ -205,6 +205,11 @@ struct Runner {
 // The prepared solver of a context (nullptr before msbg_gpu_pressure_prepare).
 Solver* find_solver(msbg_gpu_ctx* ctx);
 
+// msbg_gpu_pressure_prepare from the callbacks cb, or from the per-cell arrays
+// arr (msbg_gpu_pressure_prepare_arrays) when arr is given (pressure.cu).
+int pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
+                     const msbg_pressure_callbacks* cb, const ArrayInput* arr);
+
 // Host <-> device copies through pinned staging buffers (pressure.cu).
 cudaError_t copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t st);
 cudaError_t copy_d2h(void* dst, const void* src, size_t bytes, cudaStream_t st);

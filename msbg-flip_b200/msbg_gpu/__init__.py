@@ -456,12 +456,15 @@ def _f32(a):
     return np.ascontiguousarray(a, np.float32)
 
 
-def _ctx_pressure_prepare_arrays(self, res, bsx0, n_levels, block_levels, flags, face, rhs=None):
+def _ctx_pressure_prepare_arrays(self, res, bsx0, n_levels, block_levels, flags, face, rhs=None,
+                                 domain_bc=None):
     """msbg_gpu_pressure_prepare_arrays: per-cell flags, lower-face coefficients
-    face[3] and rhs in the packed block layout of MG level 0."""
+    face[3] and rhs in the packed block layout of MG level 0; domain_bc as in
+    pressure_prepare."""
     _pressure_sigs(self._L)
     self._bl_p = np.ascontiguousarray(block_levels, np.int32)
-    d = TopoDesc(res, res, res, bsx0, n_levels, _p(self._bl_p, C.c_int))
+    self._dbc_p = None if domain_bc is None else np.ascontiguousarray(domain_bc, np.int32)
+    d = TopoDesc(res, res, res, bsx0, n_levels, _p(self._bl_p, C.c_int), _p(self._dbc_p, C.c_int))
     fl = np.ascontiguousarray(flags, np.uint16)
     fx, fy, fz = (_f32(f) for f in face)
     rh = None if rhs is None else _f32(rhs)

@@ -125,3 +125,35 @@ def test_domain_boundary_spec_sets_the_wall_faces():
         assert np.abs(y - yo).max() <= 1e-6, dbc
     bad = [0, 1, 1, 1, 1, 2]  # not a DBC_* value
     assert _host_apply(s, x, bad)[0] == 5
+
+
+@pytest.mark.parametrize("res,bsx0,nl,band", SCENES)
+def test_array_build_equals_callback_build(res, bsx0, nl, band):
+    """The bulk prepare's arrays (msbg_scene_pressure_arrays samples each cell
+    at its lowest fine voxel, as the callbacks are asked) build the callback
+    build's level-0 operator: bit-identical where no face reads a coarser
+    block at another fine voxel of its cell, and the same liquid cells on
+    every level."""
+    from refgrid import interface_mask
+
+    s = msbg_gpu.PressureScene(res, bsx0, nl, band=band, seed=5)
+    flags, face, rhs = s.arrays()
+    x = np.random.default_rng(2).standard_normal(s.packed_size()).astype(np.float32)
+    y_cb, nm_cb, fl_cb, _ = host_check(s, x)
+    L = msbg_gpu.lib()
+    fn = L.msbg_gpu_pressure_host_check_arrays
+    fn.restype = C.c_int
+    bl = np.ascontiguousarray(s.block_levels, np.int32)
+    d = msbg_gpu.TopoDesc(res, res, res, bsx0, nl, bl.ctypes.data_as(C.POINTER(C.c_int)))
+    P = lambda a, t: a.ctypes.data_as(C.POINTER(t))
+    y = np.zeros(len(x))
+    nm = C.c_int()
+    fluid = np.zeros(32, np.int64)
+    rc = fn(C.byref(d), P(flags, C.c_uint16), P(face[0], C.c_float), P(face[1], C.c_float),
+            P(face[2], C.c_float), P(rhs, C.c_float), P(x, C.c_float), P(y, C.c_double),
+            C.byref(nm), P(fluid, C.c_int64), None)
+    assert rc == 0
+    assert nm.value == nm_cb and (fluid[:nm.value] == fl_cb).all()
+    iface = interface_mask(s.block_levels, res, bsx0)
+    assert np.array_equal(y[~iface], y_cb[~iface])
+    assert np.abs(y - y_cb).max() <= 1e-6 * np.abs(y_cb).max()
