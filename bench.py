@@ -300,7 +300,7 @@ LEARN_CFG = dict(res=512, seeds=(100, 101, 102, 103), pairs_per_instance=500, ep
                  batch=64, lr=2e-3)
 
 
-def learned_variants(ctx, c, scene, fluid, steps):
+def learned_variants(ctx, c, scene, fluid, steps, prepare=None):
     """Train the guess and correction networks on the GPU, then time the
     learned solves of the bench problem (FP64 refinement to 1e-6), one
     warm-up and `steps` timed calls each."""
@@ -327,7 +327,10 @@ def learned_variants(ctx, c, scene, fluid, steps):
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     rel = lambda ls, T, M: (ls[-1] / float((T * T * M).sum() / M.sum())) ** 0.5
-    ctx.pressure_prepare(scene)
+    if prepare:
+        prepare()
+    else:
+        ctx.pressure_prepare(scene)
     ctx.pressure_set_cnn(net)
     ctx.pressure_set_correction_cnn(corr)
     out = {"pairs": int(G[0].shape[0]), "correction_pairs": int(K[0].shape[0]),
@@ -391,7 +394,15 @@ def bench_mgpcg(args):
         c["band"] = PS_CFG["band"] * args.res / PS_CFG["res"]
     ctx = msbg_gpu.Context(local)
     scene = ps_scene(c)
-    ctx.pressure_prepare(scene)
+    # the caller's per-cell arrays (flags, lower-face coefficients, rhs):
+    # input generation, outside every timed region
+    arrays = scene.arrays()
+
+    def prepare_arrays():
+        ctx.pressure_prepare_arrays(c["res"], c["bsx0"], c["n_levels"], scene.block_levels,
+                                    *arrays)
+
+    prepare_arrays()
     st = ps_stats(ctx)
     fluid = int(st.fluid[0])
     # the step: MGPCG to a true FP64 residual of 1e-6, FP32 level-0 vectors
@@ -416,27 +427,37 @@ def bench_mgpcg(args):
     if args.profile:
         ctx.close()
         return
-    # end to end through the C ABI: prepare from the host callbacks (host
-    # sampling + hierarchy build + upload), the same solve, download of the
-    # pressure; averaged over 3 calls
+    # end to end through the C ABI from host buffers: the bulk prepare from the
+    # per-cell arrays (copy to the GPU, hierarchy built there), the same
+    # solve, download of the pressure; averaged over 3 calls
     n_e2e = 3
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     e2e_iters = 0
     for _ in range(n_e2e):
-        ctx.pressure_prepare(scene)
+        prepare_arrays()
         inf = ctx.pressure_solve(params)
         e2e_iters += inf.iterations
         out = ctx.pressure_download()
     e2e_s = max_over_ranks(dist, (time.perf_counter() - t0) / n_e2e, dev)
     e2e_rate = fluid * (e2e_iters / n_e2e) / e2e_s / 1e9 * ws
     st2 = ps_stats(ctx)
+    # the same through the callbacks (the reference's preparePressureSolveFLIP
+    # interface): host sampling and hierarchy build, upload, solve, download
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    ctx.pressure_prepare(scene)
+    inf_cb = ctx.pressure_solve(params)
+    ctx.pressure_download()
+    e2e_cb_s = max_over_ranks(dist, time.perf_counter() - t0, dev)
+    st_cb = ps_stats(ctx)
     extras = {}
     roof = None
     cb = None
     if ws == 1 and not args.quick:
-        extras, roof, cb = mgpcg_extras(args, ctx, c, scene, st, fluid)
+        extras, roof, cb = mgpcg_extras(args, ctx, c, scene, st, fluid, prepare_arrays)
     if rank == 0:
         line = {"metric": METRIC, "value": rate, "unit": "Gvoxel/s/iter", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -452,7 +473,7 @@ def bench_mgpcg(args):
                            "refinements": infos[-1].refinements,
                            "liquid_cells": fluid, "stored_cells_level0": int(st.cells[0]),
                            "mg_levels": int(st.nMgLevels),
-                           "prepare_s": st.prepareSeconds, "host_build_s": st.buildSeconds,
+                           "prepare_s": st.prepareSeconds, "build_s": st.buildSeconds,
                            "l2": "inputs larger than L2 (%.1f GB operator+vectors)" %
                                  (st.deviceBytesUsed / 1e9),
                            "parallelism": f"replicas{ws}", **extras},
@@ -462,7 +483,16 @@ def bench_mgpcg(args):
                         "h2d_bytes_per_step": int(st2.h2dBytes),
                         "d2h_bytes_per_step": int(out.nbytes),
                         "seconds_per_step": e2e_s, "calls": n_e2e,
-                        "host_build_s": st2.buildSeconds},
+                        "path": "msbg_gpu_pressure_prepare_arrays (host arrays; hierarchy "
+                                "built on the GPU) + msbg_gpu_pressure_solve + "
+                                "msbg_gpu_pressure_download",
+                        "prepare_s": st2.prepareSeconds, "build_s": st2.buildSeconds,
+                        "callbacks": {"value": fluid * inf_cb.iterations / e2e_cb_s / 1e9 * ws,
+                                      "seconds_per_step": e2e_cb_s,
+                                      "h2d_bytes_per_step": int(st_cb.h2dBytes),
+                                      "host_build_s": st_cb.buildSeconds,
+                                      "path": "msbg_gpu_pressure_prepare (host callbacks, "
+                                              "host build) + solve + download"}},
                 "cpu_baseline": cb}
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -471,7 +501,7 @@ def bench_mgpcg(args):
         dist.destroy_process_group()
 
 
-def mgpcg_extras(args, ctx, c, scene, st, fluid):
+def mgpcg_extras(args, ctx, c, scene, st, fluid, prepare=None):
     """Sub-figures of the default line (one GPU): roofline of the dominant
     kernel, the other solve variants, the learned variants, the reference's
     analogue, the error against the FP64 oracle and the smoother workload."""
@@ -500,7 +530,7 @@ def mgpcg_extras(args, ctx, c, scene, st, fluid):
         variants[name] = summarize(timed_solves(ctx, solve_params(c, **kw), 1, K), fluid)
     x["variants"] = variants
     if not args.no_learned:
-        x["learned"] = learned_variants(ctx, c, scene, fluid, K)
+        x["learned"] = learned_variants(ctx, c, scene, fluid, K, prepare)
     # the reference's runnable analogue (16^3 base blocks), GPU and CPU
     s = dict(PS_SAME_CFG, res=c["res"], band=c["band"])
     ctx.pressure_prepare(ps_scene(s))
@@ -521,8 +551,8 @@ def mgpcg_extras(args, ctx, c, scene, st, fluid):
 
 
 def bench_large(args):
-    """The 2048^3 (c3) and 4096^3 (c5) configurations on one GPU: the host
-    build of the hierarchy, the smoother's level-0 sweep rate (Gvoxel/s per
+    """The 2048^3 (c3) and 4096^3 (c5) configurations on one GPU: the bulk
+    prepare (hierarchy built on the GPU), the smoother's level-0 sweep rate (Gvoxel/s per
     smoother iteration) and the time to a true FP64 residual of 1e-6 of each
     variant, one warm-up and --steps timed calls each."""
     import torch
@@ -535,8 +565,12 @@ def bench_large(args):
     ctx = msbg_gpu.Context(0)
     scene = ps_scene(c)
     t0 = time.perf_counter()
-    ctx.pressure_prepare(scene)
+    arrays = scene.arrays()  # the caller's per-cell arrays (input generation)
+    arrays_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ctx.pressure_prepare_arrays(c["res"], c["bsx0"], c["n_levels"], scene.block_levels, *arrays)
     prep_s = time.perf_counter() - t0
+    del arrays
     st = ps_stats(ctx)
     fluid = int(st.fluid[0])
     free, total = torch.cuda.mem_get_info(0)
@@ -544,7 +578,9 @@ def bench_large(args):
            "liquid_cells_level0": fluid,
            "active_cells_all_levels": int(sum(st.fluid[m] for m in range(st.nMgLevels))),
            "stored_cells_level0": int(st.cells[0]), "mg_levels": int(st.nMgLevels),
-           "prepare_s": prep_s, "host_build_s": st.buildSeconds,
+           "scene_arrays_s": arrays_s,
+           "prepare_s": prep_s, "build_s": st.buildSeconds,
+           "prepare_path": "msbg_gpu_pressure_prepare_arrays (hierarchy built on the GPU)",
            "device_bytes_used": int(st.deviceBytesUsed), "device_free_after_prepare": int(free)}
     hbm, _, _ = peaks()
     for name, storage in (("f32", msbg_gpu.F32), ("f16", msbg_gpu.F16), ("bf16", msbg_gpu.BF16)):
@@ -559,7 +595,12 @@ def bench_large(args):
     for name, kw in variants:
         out[name] = summarize(timed_solves(ctx, solve_params(c, **kw), 1, args.steps), fluid)
     if args.workload == "c5" and not args.no_learned:
-        out["learned"] = learned_variants(ctx, c, scene, fluid, args.steps)
+        def reprepare():
+            a = scene.arrays()
+            ctx.pressure_prepare_arrays(c["res"], c["bsx0"], c["n_levels"], scene.block_levels,
+                                        *a)
+
+        out["learned"] = learned_variants(ctx, c, scene, fluid, args.steps, reprepare)
     print(json.dumps(out), flush=True)
     ctx.close()
 
