@@ -36,7 +36,9 @@
 // A listed block whose slot is not a value block (NULL, const, or a caller's
 // slot map that disagrees with the list) is skipped and reported through
 // errFlag (MCF_ERR_NOT_VALUE).  The kernel has no waits that could time out.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <atomic>
@@ -111,15 +113,21 @@ __device__ __forceinline__ f2 mid2(f2 a, f2 b) {
   return pk(a1, b0);
 }
 
-template <int BSX>
+// The padded tile: x in [-XOFF, BSX + XOFF) (row pitch BSX + 2 XOFF, so every
+// x pair starts on an 8-byte boundary), y and z in [-1, BSX].  XOFF = 2 for
+// the copies issued by threads; XOFF = 4 when the block arrives as one tensor
+// box, whose x origin must sit on a 16-byte boundary (x = -4).
+template <int BSX, int XOFF = 2>
 struct McfTile {
-  static constexpr int RP = BSX + 4;         // row pitch: x + 2 in [0, BSX + 4)
+  static constexpr int RP = BSX + 2 * XOFF;  // row pitch
   static constexpr int PP = RP * (BSX + 2);  // plane pitch: y + 1 in [0, BSX + 2)
   static constexpr int NV = BSX * BSX * BSX;
   static constexpr int NT = BSX * BSX;       // one thread per x pair of a row and z half
   static constexpr int HP = BSX / 2;         // pairs per row
   static constexpr size_t SMEM = sizeof(float) * PP * (BSX + 2);
-  __device__ static int at(int x, int y, int z) { return (x + 2) + RP * (y + 1) + PP * (z + 1); }
+  __host__ __device__ static constexpr int at(int x, int y, int z) {
+    return (x + XOFF) + RP * (y + 1) + PP * (z + 1);
+  }
 };
 
 // Where halo voxel (x, y, z) (block coordinates, some outside [0, BSX)) comes
@@ -254,11 +262,11 @@ __device__ __forceinline__ void mcf_fill(float* tile, const T* __restrict__ pool
 }
 
 // The 19-point update of one block from its tile, stored in place.
-template <int BSX, typename T>
+template <int BSX, typename T, int XOFF = 2>
 __device__ __forceinline__ void mcf_compute(const float* tile, T* __restrict__ block,
                                             T* __restrict__ xfOwn, float dt, int clamp01,
                                             int tid) {
-  using Tl = McfTile<BSX>;
+  using Tl = McfTile<BSX, XOFF>;
   constexpr int RP = Tl::RP, PP = Tl::PP, HP = Tl::HP;
   // Column march of the x pair (x0, x0 + 1) of row y over one half of z.
   constexpr int ZN = BSX / 2;
@@ -425,6 +433,254 @@ __global__ void __launch_bounds__(BSX* BSX, mcf_ctas_per_sm<BSX>())
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP32 16^3 blocks of a context pool: the block arrives as one tensor box
+// ---------------------------------------------------------------------------
+// The pool is a 4-D tensor (x, y, z, slot) of 16^3 FP32 blocks.  One box of
+// 24 x 18 x 16 voxels at (-4, -1, 0, slot) lands as planes 1..16 of the padded
+// tile (XOFF = 4: row pitch 24, plane pitch 432), x and y outside the block
+// filled with zeros by the copy.  What the stencil reads there - the x faces,
+// the y faces and the four edges along z - is loaded into registers while the
+// previous block is computed and stored once the box has landed; the z = -1
+// and z = 16 planes (faces and the edges in them) arrive by 8- and 4-byte
+// asynchronous copies, which no box overlaps.  One mbarrier per tile stage
+// counts the box's bytes; its waits are bounded.
+namespace tma {
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Bounded wait on the given phase parity; false if the copy never landed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done = 0;
+  for (int i = 0; i < (1 << 24); i++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// One box of the 4-D tensor map into shared memory (no multicast).
+__device__ __forceinline__ void box_g2s(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                        int w, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+      : "memory");
+}
+
+constexpr int BS = 16, XO = 4;
+using Tl = McfTile<BS, XO>;
+constexpr int TILE = Tl::PP * (BS + 2);                      // floats per stage
+constexpr uint32_t BOX_BYTES = sizeof(float) * Tl::RP * (BS + 2) * BS;
+// the box lands at plane 1 of a stage: the stages start where that plane is
+// 128-byte aligned (TILE floats keep the second stage aligned too)
+static_assert((TILE * 4) % 128 == 0 && (Tl::PP * 4) % 16 == 0, "stage alignment");
+constexpr size_t SMEM = 2 * sizeof(float) * TILE + 128;
+
+// Register-staged halo of one block: thread t holds one y-face pair, two
+// x-face values and (t < 64) one edge along z.
+struct Halo {
+  float y0, y1, x0, x1, e;
+};
+
+__device__ __forceinline__ float const_val(int ck, float emptyVal, float fullVal) {
+  return ck == 1 ? emptyVal : fullVal;
+}
+
+__device__ __forceinline__ void halo_load(Halo& h, const float* __restrict__ pool,
+                                          const float* __restrict__ xf, const int* nbSlot,
+                                          float emptyVal, float fullVal, int tid) {
+  const float* own = pool + (size_t)nbSlot[13] * Tl::NV;
+  {  // y faces: y = -1 / 16, z in [0, 16), one x pair
+    const int side = tid >> 7, r = tid & 127, z = r >> 3, x = 2 * (r & 7);
+    int ck;
+    const float* src = halo_src<BS, float>(pool, nbSlot, own, x, side ? BS : -1, z, ck);
+    if (src) {
+      const float2 v = *reinterpret_cast<const float2*>(src);
+      h.y0 = v.x;
+      h.y1 = v.y;
+    } else {
+      h.y0 = h.y1 = const_val(ck, emptyVal, fullVal);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 2; q++) {  // x faces: x = -1 / 16, (y, z) in [0, 16)^2
+    const int g = tid + 256 * q, side = g >> 8, y = g & 15, z = (g >> 4) & 15;
+    int ck;
+    const float* src = xface_src<BS, float>(pool, xf, nbSlot, side ? BS : -1, y, z, ck);
+    const float v = src ? *src : const_val(ck, emptyVal, fullVal);
+    if (q == 0) h.x0 = v; else h.x1 = v;
+  }
+  if (tid < 64) {  // edges along z: (x, y) in {-1, 16}^2
+    const int c = tid >> 4, z = tid & 15;
+    const int x = (c & 1) ? BS : -1, y = (c & 2) ? BS : -1;
+    int ck;
+    const float* src = halo_src<BS, float>(pool, nbSlot, own, x, y, z, ck);
+    h.e = src ? *src : const_val(ck, emptyVal, fullVal);
+  }
+}
+
+__device__ __forceinline__ void halo_store(const Halo& h, float* tile, int tid) {
+  {
+    const int side = tid >> 7, r = tid & 127, z = r >> 3, x = 2 * (r & 7);
+    float* d = tile + Tl::at(x, side ? BS : -1, z);
+    *reinterpret_cast<float2*>(d) = make_float2(h.y0, h.y1);
+  }
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int g = tid + 256 * q, side = g >> 8, y = g & 15, z = (g >> 4) & 15;
+    tile[Tl::at(side ? BS : -1, y, z)] = q == 0 ? h.x0 : h.x1;
+  }
+  if (tid < 64) {
+    const int c = tid >> 4, z = tid & 15;
+    tile[Tl::at((c & 1) ? BS : -1, (c & 2) ? BS : -1, z)] = h.e;
+  }
+}
+
+// The z = -1 and z = 16 planes: faces (x pairs, y in [-1, 16]) and the edges
+// along y (x = -1 / 16, y in [0, 16)), by asynchronous copies.
+__device__ __forceinline__ void zplanes_fill(float* tile, const float* __restrict__ pool,
+                                             const float* __restrict__ xf, const int* nbSlot,
+                                             float emptyVal, float fullVal, int tid) {
+  const float* own = pool + (size_t)nbSlot[13] * Tl::NV;
+  constexpr int ROWS = BS + 2, PAIRS = 2 * ROWS * (BS / 2);  // 288
+  for (int q = tid; q < PAIRS; q += Tl::NT) {
+    const int side = q / (ROWS * (BS / 2)), r = q % (ROWS * (BS / 2));
+    const int y = r / (BS / 2) - 1, x = 2 * (r % (BS / 2)), z = side ? BS : -1;
+    int ck;
+    const float* src = halo_src<BS, float>(pool, nbSlot, own, x, y, z, ck);
+    float* d = tile + Tl::at(x, y, z);
+    if (src) {
+      cp_async8(d, src);
+    } else {
+      const float v = const_val(ck, emptyVal, fullVal);
+      d[0] = v;
+      d[1] = v;
+    }
+  }
+  if (tid < 64) {
+    const int side = tid >> 5, xs = (tid >> 4) & 1, y = tid & 15;
+    const int z = side ? BS : -1, x = xs ? BS : -1;
+    int ck;
+    const float* src = xface_src<BS, float>(pool, xf, nbSlot, x, y, z, ck);
+    float* d = tile + Tl::at(x, y, z);
+    if (src)
+      cp_async4(d, src);
+    else
+      *d = const_val(ck, emptyVal, fullVal);
+  }
+}
+
+}  // namespace tma
+
+__global__ void __launch_bounds__(256, 3)
+    mcf_colour_kernel_tma(const __grid_constant__ CUtensorMap map, float* __restrict__ pool,
+                          float* __restrict__ xf, const int* __restrict__ slotOf,
+                          const int* __restrict__ list, int n, int nbx, int nby, int nbz,
+                          float emptyVal, float fullVal, float dt, int clamp01,
+                          int* __restrict__ errFlag) {
+  using namespace tma;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const uint32_t pad = (128u - ((smem_u32(smem_raw) + Tl::PP * 4u) & 127u)) & 127u;
+  float* tiles = reinterpret_cast<float*>(smem_raw + pad);
+  __shared__ int nbSlot[2][27];
+  __shared__ __align__(8) uint64_t bar[2];
+  const int tid = threadIdx.x;
+  const int G = gridDim.x;
+  int k = blockIdx.x;
+  if (k >= n) return;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  auto neighbours = [&](int kk, int s) {
+    if (tid < 27) {
+      const int bid = list[kk];
+      const int bx = bid % nbx, by = (bid / nbx) % nby, bz = bid / (nbx * nby);
+      const int dx = tid % 3 - 1, dy = (tid / 3) % 3 - 1, dz = tid / 9 - 1;
+      const int x = bx + dx, y = by + dy, z = bz + dz;
+      int sl = SLOT_OUT;
+      if (x >= 0 && y >= 0 && z >= 0 && x < nbx && y < nby && z < nbz)
+        sl = slotOf[x + nbx * (y + nby * z)];
+      nbSlot[s][tid] = sl;
+    }
+  };
+  Halo h{0.f, 0.f, 0.f, 0.f, 0.f};
+  // per stage (bit s): a box is in flight / the parity of its next phase
+  // (uniform: every thread reads the same shared slot)
+  uint32_t issued = 0u, phase = 0u;
+  // block kk into stage s: the box (one thread), the z planes, the halo loads
+  auto issue = [&](int s) {
+    const int slot = nbSlot[s][13];
+    if (slot < 0) {
+      issued &= ~(1u << s);
+      cp_async_commit();
+      return;
+    }
+    issued |= 1u << s;
+    float* tile = tiles + s * TILE;
+    if (tid == 0) {
+      fence_proxy_async();  // the stage was last written by ordinary stores
+      mbar_expect_tx(&bar[s], BOX_BYTES);
+      box_g2s(tile + Tl::PP, &map, -XO, -1, 0, slot, &bar[s]);
+    }
+    zplanes_fill(tile, pool, xf, nbSlot[s], emptyVal, fullVal, tid);
+    cp_async_commit();
+    halo_load(h, pool, xf, nbSlot[s], emptyVal, fullVal, tid);
+  };
+  __syncthreads();  // barriers initialised
+  neighbours(k, 0);
+  __syncthreads();
+  issue(0);
+  for (int it = 0; k < n; it++, k += G) {
+    const int s = it & 1;
+    const int kn = k + G;
+    // the block's box has landed: its register halo into the tile
+    if ((issued >> s) & 1u) {
+      const uint32_t par = (phase >> s) & 1u;
+      const bool ok = __syncthreads_and(mbar_wait(&bar[s], par));
+      if (!ok) {
+        if (tid == 0) atomicOr(errFlag, ERR_WAIT_TIMEOUT);
+        mbar_wait(&bar[s], par);  // bounded: the box in flight
+        cp_async_wait_group<0>();
+        return;
+      }
+      phase ^= 1u << s;
+      halo_store(h, tiles + s * TILE, tid);
+    }
+    cp_async_wait_group<0>();
+    if (kn < n) neighbours(kn, s ^ 1);
+    __syncthreads();  // stage s complete, nbSlot[s ^ 1] written
+    if (kn < n) issue(s ^ 1);
+    const int slot0 = nbSlot[s][13];
+    if (slot0 < 0) {
+      if (tid == 0) atomicOr(errFlag, MCF_ERR_NOT_VALUE);
+    } else {
+      mcf_compute<BS, float, XO>(tiles + s * TILE, pool + (size_t)slot0 * Tl::NV,
+                                 xf + (size_t)slot0 * 2 * BS * BS, dt, clamp01, tid);
+    }
+    __syncthreads();  // stage s may be refilled
+  }
+}
+
 // Fills the face cache: the planes x = 0 and x = BSX-1 of every value block
 // (slots 0..nSlots-1), as [slot][2][z][y].
 template <int BSX, typename T>
@@ -437,6 +693,35 @@ __global__ void __launch_bounds__(256) k_mcf_xfaces(const T* __restrict__ pool, 
     const int r = (int)(i % (2 * F)), side = r / F, y = r % BSX, z = (r % F) / BSX;
     xf[i] = pool[sl * (BSX * BSX * BSX) + (side ? BSX - 1 : 0) + BSX * (y + BSX * z)];
   }
+}
+
+// The tensor map of an FP32 16^3 pool of nSlots blocks (see
+// mcf_colour_kernel_tma); false if the driver's encoder is not available or
+// refuses the pool, and the copies issued by threads are used instead.
+bool mcf_tensor_map(CUtensorMap* map, float* pool, int64_t nSlots) {
+  static std::atomic<PFN_cuTensorMapEncodeTiled_v12000> encode{nullptr};
+  PFN_cuTensorMapEncodeTiled_v12000 fn = encode.load(std::memory_order_acquire);
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !f)
+      return false;
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    encode.store(fn, std::memory_order_release);
+  }
+  if ((reinterpret_cast<uintptr_t>(pool) & 15) != 0 || nSlots <= 0) return false;
+  constexpr int B = tma::BS;
+  const cuuint64_t dim[4] = {B, B, B, (cuuint64_t)nSlots};
+  const cuuint64_t stride[3] = {sizeof(float) * B, sizeof(float) * B * B,
+                                sizeof(float) * B * B * B};
+  const cuuint32_t box[4] = {(cuuint32_t)tma::Tl::RP, B + 2, B, 1};
+  const cuuint32_t estride[4] = {1, 1, 1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, pool, dim, stride, box, estride,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 template <int BSX, typename T>
@@ -470,6 +755,28 @@ cudaError_t launch_mcf_t(T* pool, T* xf, int64_t nSlots, const int* slotOf,
   if (xf && nSlots > 0 && nIter > 0)
     k_mcf_xfaces<BSX, T><<<(dev < 64 ? numSMs[dev] : 148) * 4, 256, 0, stream>>>(pool, nSlots,
                                                                                xf);
+  // FP32 16^3 blocks of a context pool: the block arrives as one tensor box
+  if constexpr (BSX == 16 && std::is_same<T, float>::value) {
+    CUtensorMap map;
+    if (xf && nSlots > 0 && mcf_tensor_map(&map, pool, nSlots)) {
+      static std::atomic<uint64_t> tmaAttr{0};
+      if (!bit || !(tmaAttr.load(std::memory_order_acquire) & bit)) {
+        e = cudaFuncSetAttribute(mcf_colour_kernel_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tma::SMEM);
+        if (e != cudaSuccess) return e;
+        tmaAttr.fetch_or(bit, std::memory_order_acq_rel);
+      }
+      for (int it = 0; it < nIter; it++)
+        for (int c = 0; c < 8; c++) {
+          const int n = colourStart[c + 1] - colourStart[c];
+          if (n <= 0) continue;
+          mcf_colour_kernel_tma<<<std::min(n, maxGrid), tma::Tl::NT, tma::SMEM, stream>>>(
+              map, pool, xf, slotOf, colourList + colourStart[c], n, nbx, nby, nbz, emptyVal,
+              fullVal, dt, clamp01, errFlag);
+        }
+      return cudaGetLastError();
+    }
+  }
   for (int it = 0; it < nIter; it++)
     for (int c = 0; c < 8; c++) {
       int n = colourStart[c + 1] - colourStart[c];

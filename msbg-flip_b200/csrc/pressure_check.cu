@@ -182,8 +182,9 @@ static int host_check(const msbg_topo_desc* topo, const msbg_pressure_callbacks*
       host_restrict(F, G, yf, ptApf);
       host_apply(G, xc, yc);
       double emax = 0, ymax = 0;
+      // every coarse cell: one that P^T A P reaches but A_c leaves empty
+      // (a liquid cell built without its children) shows here too
       for (int64_t c = 0; c < G.nCells; c++) {
-        if (!(G.diag[c] > 0)) continue;
         emax = std::max(emax, std::fabs(ptApf[c] - yc[c]));
         ymax = std::max(ymax, std::fabs(ptApf[c]));
       }

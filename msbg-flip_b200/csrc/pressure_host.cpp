@@ -547,11 +547,19 @@ void galerkin(const Ctx& C, const Level& F, const std::vector<uint8_t>& fineFlui
     const int lc = t.level, ts = t.ts;
     zero_tile(G, ti, false);
     float* cdir[3] = {&G.cx[t.off], &G.cy[t.off], &G.cz[t.off]};
-    // Fast path of an aggregated tile (the tile lies in one block, so all its
-    // cells aggregate or none do): its children fill a fine region of
-    // (2 ts)^3 cells at level lc-1 covered by whole fine tiles, resolved once.
-    const int P0[3] = {t.ox, t.oy, t.oz};
-    const bool aggT = aggregated(lc, P0);
+    // Fast path of a tile whose cells all aggregate: its children fill a
+    // fine region of (2 ts)^3 cells at level lc-1 covered by whole fine tiles,
+    // resolved once.  A tile of a uniform level spans several blocks, which
+    // may aggregate or not; such a tile takes the per-cell path.
+    bool aggT = true;
+    {
+      const int ext = t.ts << lc, o[3] = {t.ox << lc, t.oy << lc, t.oz << lc};
+      const int step = std::min(ext, C.H.bsx0);
+      for (int z = o[2]; z < o[2] + ext && aggT; z += step)
+        for (int y = o[1]; y < o[1] + ext && aggT; y += step)
+          for (int x = o[0]; x < o[0] + ext && aggT; x += step)
+            aggT = C.level_at(F.m, x, y, z) == lc - 1;
+    }
     const int tsf = aggT ? F.tsOf[lc - 1] : 0;
     const int nsub = aggT && tsf > 0 ? (2 * ts) / tsf : 0;
     int64_t subOff[64];

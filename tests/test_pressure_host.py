@@ -157,3 +157,16 @@ def test_array_build_equals_callback_build(res, bsx0, nl, band):
     iface = interface_mask(s.block_levels, res, bsx0)
     assert np.array_equal(y[~iface], y_cb[~iface])
     assert np.abs(y - y_cb).max() <= 1e-6 * np.abs(y_cb).max()
+
+
+def test_galerkin_levels_of_a_three_level_grid_are_exact():
+    """A tile of a uniform coarse level spans several blocks, some of whose
+    cells aggregate at that level and some not (a 3-level grid around a wavy
+    surface): every coarse level is still P^T A P on every cell."""
+    s = msbg_gpu.PressureScene(512, 32, 3, z_liquid=0.3, n_spheres=32, r_min=20 / 4096,
+                               r_max=60 / 4096, n_cuboids=0, band=(48.0 - 16 * 3 ** 0.5) / 8,
+                               seed=4096, wave_amp=0.05, n_waves=8)
+    x = np.zeros(s.packed_size(), np.float32)
+    _, nmg, _, gerr = host_check(s, x)
+    assert nmg >= 5
+    assert gerr.max() < 1e-6, gerr
