@@ -736,11 +736,12 @@ def mcf_line(args, ctx, dist=None, dev=None, ws=1, local=0):
     hbm, _, pk_kind = peaks()
     alg = 8.0 * nvox * c["iters"]
     achieved = alg / (ms_step * 1e-3) / 1e9
-    dpc = read_profile_value("mcf_colour_kernel_512_b16.txt", "dram_bytes_per_cell")
+    dpc = read_profile_value("mcf_colour_kernel_tma_512_b16.txt", "dram_bytes_per_cell")
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "peak_kind": pk_kind,
             "traffic": dpc * nvox / 8.0 if dpc else None,
-            "alg_bytes_per_launch": 8.0 * nvox / 8.0, "kernel": "mcf_colour_kernel<16>"}
+            "alg_bytes_per_launch": 8.0 * nvox / 8.0,
+            "kernel": "mcf_colour_kernel_tma (16^3 FP32 blocks, tensor-box staging)"}
     ctx.set_topology(c["res"], c["res"], c["res"], c["bsx"])  # the C-ABI path needs the raster
     host_in = torch.from_numpy(vals).pin_memory()
     host_out = torch.empty_like(host_in).pin_memory()

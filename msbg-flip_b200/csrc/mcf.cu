@@ -22,7 +22,9 @@
 //     pairs are rebuilt in registers from three aligned pairs.
 //   * The block and its 1-voxel shell (faces and edges; the 19-point stencil
 //     reads no corner) arrive by asynchronous copies straight into the tile:
-//     8-byte copies for x pairs, 4-byte copies for the x faces.
+//     for FP32 16^3 blocks of a context channel the block is one tensor box
+//     (cp.async.bulk.tensor, mcf_colour_kernel_tma), otherwise 8-byte copies
+//     for x pairs; 4-byte copies for the x faces.
 //   * The curvature is evaluated with the central differences left unscaled:
 //     with d = f(+1) - f(-1) (= 2 f_x) and s = the mixed second difference
 //     (= 4 f_xy) the reference's H = [...] / |grad f|^2 becomes
