@@ -254,10 +254,28 @@ def ref_pressure_rate(cfg, max_seconds=40.0):
         iters.append(it)
         if time.perf_counter() - t0 > max_seconds * 0.5 or len(times) >= 3:
             break
+    # its two hot routines, one call each after a warm-up call: the level-0
+    # operator (multiplyLaplacianMatrixOpt) and the smoother (relax: one
+    # red-black block sweep of 5 inner sweeps, src/msbg3.cpp:2245-2369)
+    comp = {}
+    x0 = (np.random.default_rng(1).uniform(-1, 1, r.packed_size(0)) * r.liquid()).astype(
+        np.float32)
+    r.set(ref_pressure.CH_FLOAT_3, x0)
+    r.set(ref_pressure.CH_FLOAT_2, x0)
+    for name, fn in (("matvec", lambda: r.multiply(0, ref_pressure.CH_FLOAT_3,
+                                                   ref_pressure.CH_FLOAT_6)),
+                     ("relax_sweep", lambda: r.relax(0, ref_pressure.CH_FLOAT_3,
+                                                     ref_pressure.CH_FLOAT_2,
+                                                     ref_pressure.CH_FLOAT_6, 1))):
+        fn()
+        t1 = time.perf_counter()
+        fn()
+        dt1 = time.perf_counter() - t1
+        comp[name] = {"ms": dt1 * 1e3, "gvoxel_s": nfl / dt1 / 1e9}
     prep = r.prep_seconds
     r.close()
     return {"value": nfl * sum(iters) / sum(times) / 1e9, "unit": "Gvoxel/s/iter",
-            "cores": cores, "kind": "reference", "liquid_cells": nfl,
+            "cores": cores, "kind": "reference", "liquid_cells": nfl, "components": comp,
             "sample": (f"reference solvePressureFLIP (V(2,2)-PCG, src/msbg3.cpp:3098) on "
                        f"{workload_name(cfg)}: {len(times)} calls of {REF_ITERS} PCG "
                        f"iterations after a 1-iteration warm-up; {nfl} liquid cells (its own "
@@ -535,7 +553,15 @@ def mgpcg_extras(args, ctx, c, scene, st, fluid, prepare=None):
     s = dict(PS_SAME_CFG, res=c["res"], band=c["band"])
     ctx.pressure_prepare(ps_scene(s))
     st_s = ps_stats(ctx)
+    ms_sw, _ = ctx.pressure_profile(0, 5, c["inner"])
+    ms_mv, _ = ctx.pressure_profile(1, 5, c["inner"])
+    fl_s = int(st_s.fluid[0])
     same = {"workload": workload_name(s),
+            "gpu_components": {
+                "matvec": {"ms": ms_mv, "gvoxel_s": fl_s / (ms_mv * 1e-3) / 1e9},
+                "smooth_sweep": {"ms": ms_sw, "gvoxel_s": fl_s / (ms_sw * 1e-3) / 1e9,
+                                 "note": f"one red-black tile sweep of {c['inner']} inner "
+                                         "sweeps (the reference's: 5 inner block sweeps)"}},
             "gpu": summarize(timed_solves(ctx, solve_params(s, maxRefine=30), 1, K),
                              int(st_s.fluid[0])),
             "gpu_plain_recursive_residual": summarize(
