@@ -399,6 +399,60 @@ def error_vs_oracle(ctx, c):
     return out
 
 
+FLIP_CFG = dict(res=256, bsx=16, z_liquid=0.4, ppv=8, air_ppv=1, air_band=8, seed=7, dt=0.02,
+                gravity=-9.8, alpha=0.95)
+
+
+def flip_line(args, ctx):
+    """The FLIP transfers either side of the pressure solve on a 256^3
+    single-level grid (16^3 blocks): seeded particles (8 liquid per cell below
+    z = 0.4 res, 1 air per cell in the 8 cells above), one step of P2G,
+    gravity, the pressure-gradient update (with a seeded pressure field) and
+    G2P through the C ABI from host arrays, each timed over --steps calls;
+    the CPU restatement of the same steps times a sample of the particles."""
+    import msbg_gpu
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    c = FLIP_CFG
+    res, bsx = c["res"], c["bsx"]
+    n = res ** 3
+    ctx.set_topology(res, res, res, bsx)
+    p = msbg_gpu.flip_particles(res, bsx, c["z_liquid"], c["ppv"], c["air_ppv"], c["air_band"],
+                                c["seed"])
+    pres = np.random.default_rng(1).standard_normal(n).astype(np.float32)
+    steps = max(args.steps, 1)
+    out = {"grid": f"{res}^3, {bsx}^3 blocks, single level", "particles": int(len(p))}
+    q = p.copy()
+    for name, fn in (("p2g", lambda: ctx.flip_p2g(p)),
+                     ("gravity", lambda: ctx.flip_gravity(c["gravity"], c["dt"])),
+                     ("pressure_gradient", lambda: ctx.flip_pressure_gradient(pres, c["dt"])),
+                     ("g2p", lambda: ctx.flip_g2p(q, c["alpha"]))):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            fn()
+        dt = (time.perf_counter() - t0) / steps
+        per = len(p) if name in ("p2g", "g2p") else n
+        out[name] = {"ms": dt * 1e3, ("mparticles_s" if per == len(p) else "mvoxels_s"):
+                     per / dt / 1e6}
+    out["path"] = "C ABI from host arrays (particle and pressure copies inside each call)"
+    if not args.no_cpu:
+        sample = p[:: max(1, len(p) // 2_000_000)]
+        t0 = time.perf_counter()
+        oracle.flip_p2g(res, bsx, sample)
+        t_p2g = time.perf_counter() - t0
+        vel, mass, beta, _ = oracle.flip_p2g(res, bsx, p[:1])
+        t0 = time.perf_counter()
+        oracle.flip_g2p(res, bsx, sample, vel, vel, c["alpha"])
+        t_g2p = time.perf_counter() - t0
+        out["cpu_port"] = {"kind": "port", "cores": 1,
+                           "sample": f"{len(sample)} of the particles, CPU restatement "
+                                     "(oracle/msbg_oracle_flip.c), one thread",
+                           "p2g_mparticles_s": len(sample) / t_p2g / 1e6,
+                           "g2p_mparticles_s": len(sample) / t_g2p / 1e6}
+    return out
+
+
 def bench_mgpcg(args):
     import torch
     import msbg_gpu
@@ -449,6 +503,8 @@ def bench_mgpcg(args):
     # per-cell arrays (copy to the GPU, hierarchy built there), the same
     # solve, download of the pressure; averaged over 3 calls
     n_e2e = 3
+    # the caller's pressure array (written in place, as CH_PRESSURE is)
+    out = np.zeros_like(ctx.pressure_download())
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
@@ -457,7 +513,7 @@ def bench_mgpcg(args):
         prepare_arrays()
         inf = ctx.pressure_solve(params)
         e2e_iters += inf.iterations
-        out = ctx.pressure_download()
+        ctx.pressure_download(out=out)
     e2e_s = max_over_ranks(dist, (time.perf_counter() - t0) / n_e2e, dev)
     e2e_rate = fluid * (e2e_iters / n_e2e) / e2e_s / 1e9 * ws
     st2 = ps_stats(ctx)
@@ -468,7 +524,7 @@ def bench_mgpcg(args):
     t0 = time.perf_counter()
     ctx.pressure_prepare(scene)
     inf_cb = ctx.pressure_solve(params)
-    ctx.pressure_download()
+    ctx.pressure_download(out=out)
     e2e_cb_s = max_over_ranks(dist, time.perf_counter() - t0, dev)
     st_cb = ps_stats(ctx)
     extras = {}
@@ -573,6 +629,7 @@ def mgpcg_extras(args, ctx, c, scene, st, fluid, prepare=None):
     x["same_config"] = same
     x["max_err_vs_fp64_oracle"] = error_vs_oracle(ctx, c)
     x["mcf_512_b16"] = mcf_line(args, ctx)
+    x["flip_transfers_256_b16"] = flip_line(args, ctx)
     return x, roof, cb
 
 

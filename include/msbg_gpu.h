@@ -1,11 +1,14 @@
 /*
  * msbg_gpu.h — C ABI of the B200 sparse block-grid PDE solver.
  *
- * Drop-in GPU path for two MSBG entry points (reference = AkirA-fx/MSBG-Flip):
+ * Drop-in GPU path for MSBG entry points (reference = AkirA-fx/MSBG-Flip):
  *   - MultiresSparseGrid::applyChannelPdeFast<float>(..., -(PDE_MEAN_CURVATURE +
  *     OPT_8_COLOR_SCHEME), ...)                          src/msbg4.cpp:59-957
- *   - MultiresSparseGrid::preparePressureSolveFLIP / solvePressureFLIP
- *                                                       src/msbg3.cpp:3041-3271
+ *   - MultiresSparseGrid::preparePressureSolveFLIP / solvePressureFLIP and
+ *     their pieces                                      src/msbg3.cpp:3041-3271
+ *   - the FLIP transfers either side of the solve (particleToGrid,
+ *     applyGravity, the pressure-gradient update, gridToParticle) on
+ *     single-level grids                                src/flip_sim.cpp
  *
  * The host keeps owning the MSBG block pool; this library owns device pools and
  * moves data only on explicit upload/download calls.  Every function returns an
@@ -405,6 +408,57 @@ int msbg_gpu_relax(msbg_gpu_ctx* ctx, int levelMg, float* x, const float* b, int
  * V-cycle reduces to the pre- and post-smoothing of level 0. */
 int msbg_gpu_vcycle(msbg_gpu_ctx* ctx, const float* r, float* z, int64_t n, int nPre, int nPost,
                     int innerIter, float coarseScale);
+
+/* ---- FLIP transfers around the pressure solve -------------------------
+ * On the context's single-level grid (msbg_gpu_sync_topology with every block
+ * at level 0, the reference's flip_sim grids), with device-resident grid
+ * channels in the block layout (blocks in bid order, bsx^3 voxels, vid =
+ * x + y*bsx + z*bsx^2).  The vector channels hold per voxel the MAC values
+ * (u, v, w) of its lower x, y and z faces. */
+
+/* FlipParticle (src/flip_sim.h:48): position and velocity in voxel units,
+ * phase 0 liquid / 1 air; 28 bytes, the reference's layout. */
+typedef struct {
+  float pos[3], vel[3];
+  int phase;
+} msbg_flip_particle;
+
+/* The FlipConfig fields the transfers read (src/flip_sim.h:29-45). */
+typedef struct {
+  float rhoL, rhoG, massEps, betaMin, alphaPhi;
+  int particlesPerVoxel;
+} msbg_flip_params;
+
+enum { MSBG_FLIP_VEL = 0, MSBG_FLIP_VEL_OLD = 1, MSBG_FLIP_BETA = 2, MSBG_FLIP_MASS = 3 };
+
+/* Replaces FlipSimulation::particleToGrid (src/flip_sim.cpp:579-831): the
+ * particles' cell mass and trilinear face weights, the face velocities
+ * normalised by their weights (0 where the weight is <= massEps), the face
+ * coefficients beta = max(1/rho, betaMin) of the two-phase density with the
+ * interface clamp.  activeBlocks / nActive (either may be NULL) receive the
+ * ids of the blocks holding a cell with mass > massEps, ascending. */
+int msbg_gpu_flip_p2g(msbg_gpu_ctx* ctx, const msbg_flip_particle* particles, int64_t np,
+                      const msbg_flip_params* params, int* activeBlocks, int64_t* nActive);
+/* Replaces FlipSimulation::applyGravity (src/flip_sim.cpp:832-857): the
+ * velocity is kept as MSBG_FLIP_VEL_OLD, gravity*dt is added to the v faces
+ * next to liquid, and the reference's wall faces are set to 0. */
+int msbg_gpu_flip_gravity(msbg_gpu_ctx* ctx, float gravity, float dt, float massEps);
+/* Replaces the pressure-gradient update of FlipSimulation::pressureProjection
+ * (src/flip_sim.cpp:1316-1349): u -= dt * beta * (p_b - p_a) on every face
+ * with liquid on a side (p = 0 in a cell without), 0 on faces without liquid
+ * and on the lower domain faces.  pressure: host array in the block layout
+ * (msbg_gpu_pressure_download of a grid whose blocks are all at level 0). */
+int msbg_gpu_flip_pressure_gradient(msbg_gpu_ctx* ctx, const float* pressure, float dt,
+                                    float massEps);
+/* Replaces FlipSimulation::gridToParticle (src/flip_sim.cpp:1526-1545) with
+ * the level-0 branch of interpVec3MSBG (src/flip_sim.cpp:1354-1395):
+ * vel = (1 - alpha) pic + alpha (vel + pic - old), pic and old trilinear in
+ * MSBG_FLIP_VEL and MSBG_FLIP_VEL_OLD.  Updates the particles in place. */
+int msbg_gpu_flip_g2p(msbg_gpu_ctx* ctx, msbg_flip_particle* particles, int64_t np,
+                      float flipAlpha);
+/* Copies a channel out (get = 1) or in (get = 0); n = 3 * voxels for the
+ * vector channels, voxels for MSBG_FLIP_MASS. */
+int msbg_gpu_flip_channel(msbg_gpu_ctx* ctx, int which, float* data, int64_t n, int get);
 
 /* Diagnostics without a GPU (no counterpart in the reference): builds the
  * multigrid hierarchy as msbg_gpu_pressure_prepare does, then on the host

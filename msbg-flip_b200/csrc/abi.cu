@@ -58,6 +58,7 @@ extern "C" int msbg_gpu_destroy(msbg_gpu_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   pressure_release(ctx);
+  flip_release(ctx);
   ctx->channels.clear();
   ctx->listBuf.release();
   ctx->errBuf.release();

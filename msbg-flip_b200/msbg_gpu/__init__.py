@@ -181,6 +181,7 @@ class Context:
             bl = _p(self._bl, C.c_int)
         d = TopoDesc(sx, sy, sz, bsx0, n_levels, bl)
         self._check(self._L.msbg_gpu_sync_topology(self._h, C.byref(d)), "sync_topology")
+        self.n_blocks = (sx // bsx0) * (sy // bsx0) * (sz // bsx0)
 
     def upload_channel(self, chan, level, kind, packed, empty_val=0.0, full_val=0.0):
         kind = np.ascontiguousarray(kind, np.int8)
@@ -438,7 +439,9 @@ def count_liquid_cells(scene):
     return int(fluid[0])
 
 
-def _ctx_pressure_download(self, rhs=False, fp64=False):
+def _ctx_pressure_download(self, rhs=False, fp64=False, out=None):
+    """The pressure (or the rhs) in the block layout; out: a float32 array of
+    the packed size to fill instead of a new one."""
     n = C.c_int64()
     self._check(self._L.msbg_gpu_pressure_packed_size(self._h, C.byref(n)), "packed_size")
     if fp64:
@@ -446,7 +449,10 @@ def _ctx_pressure_download(self, rhs=False, fp64=False):
         self._check(self._L.msbg_gpu_pressure_download64(self._h, _p(out, C.c_double), n.value),
                     "pressure_download64")
         return out
-    out = np.zeros(n.value, np.float32)
+    if out is None:
+        out = np.zeros(n.value, np.float32)
+    elif out.dtype != np.float32 or out.size != n.value or not out.flags.c_contiguous:
+        raise ValueError("out: contiguous float32 array of the packed size")
     fn = self._L.msbg_gpu_pressure_download_rhs if rhs else self._L.msbg_gpu_pressure_download
     self._check(fn(self._h, _p(out, C.c_float), n.value), "pressure_download")
     return out
@@ -552,3 +558,121 @@ Context.last_solve_launches = lambda self: getattr(self, "_last_launches", None)
 
 
 from .learned import Cnn, collect_correction_pairs, collect_training_pairs, train_cnn  # noqa: E402,F401
+
+
+# ---------------------------------------------------------------------------
+# FLIP transfers around the pressure solve (single-level grids)
+# ---------------------------------------------------------------------------
+FLIP_VEL, FLIP_VEL_OLD, FLIP_BETA, FLIP_MASS = 0, 1, 2, 3
+# msbg_flip_particle = FlipParticle (src/flip_sim.h:48): 28 bytes
+FLIP_PARTICLE = np.dtype([("pos", "<f4", (3,)), ("vel", "<f4", (3,)), ("phase", "<i4")])
+assert FLIP_PARTICLE.itemsize == 28
+
+
+class FlipParams(C.Structure):
+    _fields_ = [("rhoL", C.c_float), ("rhoG", C.c_float), ("massEps", C.c_float),
+                ("betaMin", C.c_float), ("alphaPhi", C.c_float), ("particlesPerVoxel", C.c_int)]
+
+
+def flip_params(rhoL=1000.0, rhoG=1.0, massEps=1e-5, betaMin=1e-6, alphaPhi=1.0,
+                particlesPerVoxel=8):
+    """FlipConfig's defaults (src/flip_sim.h:29-45)."""
+    return FlipParams(rhoL, rhoG, massEps, betaMin, alphaPhi, particlesPerVoxel)
+
+
+def _flip_sigs(L):
+    if getattr(L, "_flip_sig", False):
+        return
+    vp, i32, f32 = C.c_void_p, C.c_int, C.c_float
+    sig = {
+        "msbg_gpu_flip_p2g": (i32, [vp, vp, C.c_int64, C.POINTER(FlipParams),
+                                    C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
+        "msbg_gpu_flip_gravity": (i32, [vp, f32, f32, f32]),
+        "msbg_gpu_flip_pressure_gradient": (i32, [vp, C.POINTER(C.c_float), f32, f32]),
+        "msbg_gpu_flip_g2p": (i32, [vp, vp, C.c_int64, f32]),
+        "msbg_gpu_flip_channel": (i32, [vp, i32, C.POINTER(C.c_float), C.c_int64, i32]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    L._flip_sig = True
+
+
+def _ctx_flip_p2g(self, particles, params=None):
+    """msbg_gpu_flip_p2g after set_topology; returns the active block ids."""
+    _flip_sigs(self._L)
+    p = np.ascontiguousarray(particles, FLIP_PARTICLE)
+    prm = params or flip_params()
+    act = np.zeros(max(getattr(self, "n_blocks", 0), 1), np.int32)
+    nb = C.c_int64()
+    self._check(self._L.msbg_gpu_flip_p2g(self._h, p.ctypes.data, len(p), C.byref(prm),
+                                          _p(act, C.c_int), C.byref(nb)), "flip_p2g")
+    return act[:nb.value]
+
+
+def _ctx_flip_gravity(self, gravity, dt, mass_eps=1e-5):
+    _flip_sigs(self._L)
+    self._check(self._L.msbg_gpu_flip_gravity(self._h, gravity, dt, mass_eps), "flip_gravity")
+
+
+def _ctx_flip_pressure_gradient(self, pressure, dt, mass_eps=1e-5):
+    _flip_sigs(self._L)
+    p = _f32(pressure)
+    self._check(self._L.msbg_gpu_flip_pressure_gradient(self._h, _p(p, C.c_float), dt,
+                                                        mass_eps), "flip_pressure_gradient")
+
+
+def _ctx_flip_g2p(self, particles, alpha=0.95):
+    """msbg_gpu_flip_g2p on a FLIP_PARTICLE array, in place."""
+    _flip_sigs(self._L)
+    if not (particles.flags.c_contiguous and particles.dtype == FLIP_PARTICLE):
+        raise ValueError("particles: contiguous FLIP_PARTICLE array")
+    self._check(self._L.msbg_gpu_flip_g2p(self._h, particles.ctypes.data, len(particles), alpha),
+                "flip_g2p")
+
+
+def _ctx_flip_channel(self, which, n_voxels, data=None):
+    """Get (data None) or set a FLIP channel: 3 floats per voxel, 1 for the mass."""
+    _flip_sigs(self._L)
+    comps = 1 if which == FLIP_MASS else 3
+    if data is None:
+        out = np.empty(comps * n_voxels, np.float32)
+        self._check(self._L.msbg_gpu_flip_channel(self._h, which, _p(out, C.c_float), len(out),
+                                                  1), "flip_channel")
+        return out
+    d = _f32(data).reshape(-1)
+    self._check(self._L.msbg_gpu_flip_channel(self._h, which, _p(d, C.c_float), len(d), 0),
+                "flip_channel")
+
+
+Context.flip_p2g = _ctx_flip_p2g
+Context.flip_gravity = _ctx_flip_gravity
+Context.flip_pressure_gradient = _ctx_flip_pressure_gradient
+Context.flip_g2p = _ctx_flip_g2p
+Context.flip_channel = _ctx_flip_channel
+
+
+def flip_particles(res, bsx, z_liquid=0.4, ppv=8, air_ppv=1, air_band=8, seed=7, vel_scale=1.0):
+    """Seeded FLIP particles on a res^3 grid: ppv liquid particles jittered in
+    every cell below z_liquid * res, air_ppv air particles in the air_band
+    cells above it; velocities from three seeded sinusoids.  Returns a
+    FLIP_PARTICLE array."""
+    rng = np.random.default_rng(seed)
+    zl = int(z_liquid * res)
+    out = []
+    for zlo, zhi, n, phase in ((0, zl, ppv, 0), (zl, min(res, zl + air_band), air_ppv, 1)):
+        if zhi <= zlo or n <= 0:
+            continue
+        cz, cy, cx = np.meshgrid(np.arange(zlo, zhi), np.arange(res), np.arange(res),
+                                 indexing="ij")
+        cells = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], 1).astype(np.float32)
+        pos = np.repeat(cells, n, 0) + rng.random((len(cells) * n, 3), dtype=np.float32)
+        a = rng.standard_normal((3, 3)).astype(np.float32)
+        vel = np.stack([np.sin(2 * np.pi * (pos @ a[i]) / res) for i in range(3)], 1) * vel_scale
+        p = np.empty(len(pos), FLIP_PARTICLE)
+        p["pos"] = pos
+        p["vel"] = vel.astype(np.float32)
+        p["phase"] = phase
+        out.append(p)
+    return np.concatenate(out)

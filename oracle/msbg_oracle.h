@@ -70,6 +70,29 @@ unsigned short oracle_array_cell_type(void* scene, int x, int y, int z);
 float oracle_array_face(void* scene, int dir, int x, int y, int z);
 float oracle_array_rhs(void* scene, int x, int y, int z);
 
+/* ---- FLIP transfers (msbg_oracle_flip.c, src/flip_sim.cpp) ---- */
+/* FlipParticle (src/flip_sim.h:48) */
+typedef struct {
+  float pos[3], vel[3];
+  int phase; /* 0 liquid, 1 air */
+} oracle_flip_particle;
+/* the FlipConfig fields the transfers read (src/flip_sim.h:29-45) */
+typedef struct {
+  float rhoL, rhoG, massEps, betaMin, alphaPhi;
+  int particlesPerVoxel;
+} oracle_flip_params;
+/* vel, beta: 3 floats per voxel (lower-face u, v, w); mass: 1; block layout;
+ * activeBlock[nBlocks]: 1 where a voxel has mass > massEps. */
+int oracle_flip_p2g(int sx, int sy, int sz, int bsx, const oracle_flip_particle* p, int64_t np,
+                    const oracle_flip_params* c, float* vel, float* mass, float* beta,
+                    uint8_t* activeBlock);
+void oracle_flip_gravity(int sx, int sy, int sz, int bsx, float* vel, float* velOld,
+                         const float* mass, float gravity, float dt, float massEps);
+void oracle_flip_gradient(int sx, int sy, int sz, int bsx, float* vel, const float* mass,
+                          const float* beta, const float* pressure, float dt, float massEps);
+void oracle_flip_g2p(int sx, int sy, int sz, int bsx, oracle_flip_particle* p, int64_t np,
+                     const float* vel, const float* velOld, float alpha);
+
 #ifdef __cplusplus
 }
 #endif

@@ -311,3 +311,75 @@ class ArrayScene:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# FLIP transfers (oracle/msbg_oracle_flip.c)
+# ---------------------------------------------------------------------------
+class _FlipParams(C.Structure):
+    _fields_ = [("rhoL", C.c_float), ("rhoG", C.c_float), ("massEps", C.c_float),
+                ("betaMin", C.c_float), ("alphaPhi", C.c_float), ("particlesPerVoxel", C.c_int)]
+
+
+def _flip_lib():
+    L = oracle()
+    if not hasattr(L, "_flip_sig"):
+        vp, i32, f32 = C.c_void_p, C.c_int, C.c_float
+        L.oracle_flip_p2g.restype = i32
+        L.oracle_flip_p2g.argtypes = [i32] * 4 + [vp, C.c_int64, C.POINTER(_FlipParams), vp, vp,
+                                                 vp, vp]
+        L.oracle_flip_gravity.argtypes = [i32] * 4 + [vp, vp, vp, f32, f32, f32]
+        L.oracle_flip_gradient.argtypes = [i32] * 4 + [vp, vp, vp, vp, f32, f32]
+        L.oracle_flip_g2p.argtypes = [i32] * 4 + [vp, C.c_int64, vp, vp, f32]
+        L._flip_sig = True
+    return L
+
+
+def flip_p2g(res, bsx, particles, rhoL=1000.0, rhoG=1.0, massEps=1e-5, betaMin=1e-6,
+             alphaPhi=1.0, ppv=8):
+    """FlipSimulation::particleToGrid restated on the CPU: (vel[3n], mass[n],
+    beta[3n], active block flags)."""
+    L = _flip_lib()
+    n = res ** 3
+    vel = np.zeros(3 * n, np.float32)
+    mass = np.zeros(n, np.float32)
+    beta = np.zeros(3 * n, np.float32)
+    act = np.zeros((res // bsx) ** 3, np.uint8)
+    prm = _FlipParams(rhoL, rhoG, massEps, betaMin, alphaPhi, ppv)
+    p = np.ascontiguousarray(particles)
+    rc = L.oracle_flip_p2g(res, res, res, bsx, p.ctypes.data, len(p), C.byref(prm),
+                           vel.ctypes.data, mass.ctypes.data, beta.ctypes.data, act.ctypes.data)
+    if rc:
+        raise RuntimeError(f"oracle_flip_p2g rc={rc}")
+    return vel, mass, beta, act
+
+
+def flip_gravity(res, bsx, vel, mass, gravity, dt, massEps=1e-5):
+    """applyGravity restated: (vel, velOld)."""
+    L = _flip_lib()
+    v = np.array(vel, np.float32)
+    old = np.zeros_like(v)
+    m = np.ascontiguousarray(mass, np.float32)
+    L.oracle_flip_gravity(res, res, res, bsx, v.ctypes.data, old.ctypes.data, m.ctypes.data,
+                          gravity, dt, massEps)
+    return v, old
+
+
+def flip_gradient(res, bsx, vel, mass, beta, pressure, dt, massEps=1e-5):
+    """The pressure-gradient update restated: the new vel."""
+    L = _flip_lib()
+    v = np.array(vel, np.float32)
+    args = [np.ascontiguousarray(a, np.float32) for a in (mass, beta, pressure)]
+    L.oracle_flip_gradient(res, res, res, bsx, v.ctypes.data, *[a.ctypes.data for a in args],
+                           dt, massEps)
+    return v
+
+
+def flip_g2p(res, bsx, particles, vel, velOld, alpha):
+    """gridToParticle restated (level-0 interpolation): updated particles."""
+    L = _flip_lib()
+    p = np.array(particles)
+    v, o = np.ascontiguousarray(vel, np.float32), np.ascontiguousarray(velOld, np.float32)
+    L.oracle_flip_g2p(res, res, res, bsx, p.ctypes.data, len(p), v.ctypes.data, o.ctypes.data,
+                      alpha)
+    return p
