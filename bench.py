@@ -436,6 +436,20 @@ def flip_line(args, ctx):
         out[name] = {"ms": dt * 1e3, ("mparticles_s" if per == len(p) else "mvoxels_s"):
                      per / dt / 1e6}
     out["path"] = "C ABI from host arrays (particle and pressure copies inside each call)"
+    # the same on particles resident in device memory (no particle copies)
+    import torch
+    dpart = torch.from_numpy(p.view(np.uint8).copy()).to(f"cuda:{ctx.device}")
+    torch.cuda.synchronize()
+    for name, fn in (("p2g", lambda: ctx.flip_p2g_device(dpart.data_ptr(), len(p))),
+                     ("g2p", lambda: ctx.flip_g2p_device(dpart.data_ptr(), len(p),
+                                                          c["alpha"]))):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            fn()
+        dt = (time.perf_counter() - t0) / steps
+        out[name + "_device_particles"] = {"ms": dt * 1e3, "mparticles_s": len(p) / dt / 1e6}
+    del dpart
     if not args.no_cpu:
         sample = p[:: max(1, len(p) // 2_000_000)]
         t0 = time.perf_counter()

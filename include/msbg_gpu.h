@@ -456,6 +456,12 @@ int msbg_gpu_flip_pressure_gradient(msbg_gpu_ctx* ctx, const float* pressure, fl
  * MSBG_FLIP_VEL and MSBG_FLIP_VEL_OLD.  Updates the particles in place. */
 int msbg_gpu_flip_g2p(msbg_gpu_ctx* ctx, msbg_flip_particle* particles, int64_t np,
                       float flipAlpha);
+/* The same two transfers on particles that stay in device memory (a
+ * cudaMalloc'd array the caller owns), ordered on the context's stream. */
+int msbg_gpu_flip_p2g_device(msbg_gpu_ctx* ctx, const msbg_flip_particle* particles, int64_t np,
+                             const msbg_flip_params* params, int* activeBlocks, int64_t* nActive);
+int msbg_gpu_flip_g2p_device(msbg_gpu_ctx* ctx, msbg_flip_particle* particles, int64_t np,
+                             float flipAlpha);
 /* Copies a channel out (get = 1) or in (get = 0); n = 3 * voxels for the
  * vector channels, voxels for MSBG_FLIP_MASS. */
 int msbg_gpu_flip_channel(msbg_gpu_ctx* ctx, int which, float* data, int64_t n, int get);

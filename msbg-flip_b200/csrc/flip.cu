@@ -287,9 +287,10 @@ void flip_release(msbg_gpu_ctx* ctx) { states().erase(ctx); }
 
 using namespace msbg;
 
-extern "C" int msbg_gpu_flip_p2g(msbg_gpu_ctx* ctx, const msbg_flip_particle* particles,
-                                 int64_t np, const msbg_flip_params* prm, int* activeBlocks,
-                                 int64_t* nActive) {
+namespace {
+
+int flip_p2g(msbg_gpu_ctx* ctx, const msbg_flip_particle* particles, int64_t np,
+             const msbg_flip_params* prm, int* activeBlocks, int64_t* nActive, bool onDevice) {
   if (!ctx || (!particles && np) || np < 0 || !prm) return MSBG_EINVARG;
   if (!(prm->rhoL > 0.f) || !(prm->rhoG > 0.f) || prm->particlesPerVoxel <= 0 ||
       !(prm->alphaPhi > 0.f))
@@ -307,14 +308,17 @@ extern "C" int msbg_gpu_flip_p2g(msbg_gpu_ctx* ctx, const msbg_flip_particle* pa
   MSBG_CUDA_TRY(ctx, cudaMemsetAsync(S->mass.p, 0, 4 * (size_t)n, st));
   MSBG_CUDA_TRY(ctx, cudaMemsetAsync(S->liq.p, 0, 4 * (size_t)n, st));
   MSBG_CUDA_TRY(ctx, cudaMemsetAsync(S->active.p, 0, S->active.bytes, st));
-  if (np) {
+  const msbg_flip_particle* dp = particles;
+  if (np && !onDevice) {
     MSBG_CUDA_TRY(ctx, S->parts.ensure(sizeof(msbg_flip_particle) * (size_t)np));
     MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(S->parts.p, particles, sizeof(msbg_flip_particle) * np,
                                        cudaMemcpyHostToDevice, st));
-    k_p2g_scatter<<<grid_blocks(np), 256, 0, st>>>(S->parts.as<msbg_flip_particle>(), np, g, n,
-                                                   prm->rhoL, prm->rhoG, S->acc.as<float>(),
-                                                   S->mass.as<float>(), S->liq.as<int>());
+    dp = S->parts.as<msbg_flip_particle>();
   }
+  if (np)
+    k_p2g_scatter<<<grid_blocks(np), 256, 0, st>>>(dp, np, g, n, prm->rhoL, prm->rhoG,
+                                                   S->acc.as<float>(), S->mass.as<float>(),
+                                                   S->liq.as<int>());
   P2GConst c;
   c.massEps = prm->massEps;
   c.rhoL = prm->rhoL;
@@ -341,6 +345,46 @@ extern "C" int msbg_gpu_flip_p2g(msbg_gpu_ctx* ctx, const msbg_flip_particle* pa
     if (nActive) *nActive = k;
   }
   return msbg_gpu_sync(ctx);
+}
+
+int flip_g2p(msbg_gpu_ctx* ctx, msbg_flip_particle* particles, int64_t np, float flipAlpha,
+             bool onDevice) {
+  if (!ctx || (!particles && np) || np < 0) return MSBG_EINVARG;
+  cudaSetDevice(ctx->device);
+  FlipState* S = nullptr;
+  GridF g;
+  int rc = state_of(ctx, &S, g);
+  if (rc) return rc;
+  if (!np) return MSBG_OK;
+  cudaStream_t st = ctx->stream;
+  msbg_flip_particle* dp = particles;
+  if (!onDevice) {
+    MSBG_CUDA_TRY(ctx, S->parts.ensure(sizeof(msbg_flip_particle) * (size_t)np));
+    MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(S->parts.p, particles, sizeof(msbg_flip_particle) * np,
+                                       cudaMemcpyHostToDevice, st));
+    dp = S->parts.as<msbg_flip_particle>();
+  }
+  k_g2p<<<grid_blocks(np), 256, 0, st>>>(dp, np, g, S->vel.as<float>(), S->velOld.as<float>(),
+                                         flipAlpha);
+  MSBG_CUDA_TRY(ctx, cudaGetLastError());
+  if (!onDevice)
+    MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(particles, dp, sizeof(msbg_flip_particle) * np,
+                                       cudaMemcpyDeviceToHost, st));
+  return msbg_gpu_sync(ctx);
+}
+
+}  // namespace
+
+extern "C" int msbg_gpu_flip_p2g(msbg_gpu_ctx* ctx, const msbg_flip_particle* particles,
+                                 int64_t np, const msbg_flip_params* prm, int* activeBlocks,
+                                 int64_t* nActive) {
+  return flip_p2g(ctx, particles, np, prm, activeBlocks, nActive, false);
+}
+
+extern "C" int msbg_gpu_flip_p2g_device(msbg_gpu_ctx* ctx, const msbg_flip_particle* particles,
+                                        int64_t np, const msbg_flip_params* prm,
+                                        int* activeBlocks, int64_t* nActive) {
+  return flip_p2g(ctx, particles, np, prm, activeBlocks, nActive, true);
 }
 
 extern "C" int msbg_gpu_flip_gravity(msbg_gpu_ctx* ctx, float gravity, float dt, float massEps) {
@@ -379,23 +423,12 @@ extern "C" int msbg_gpu_flip_pressure_gradient(msbg_gpu_ctx* ctx, const float* p
 
 extern "C" int msbg_gpu_flip_g2p(msbg_gpu_ctx* ctx, msbg_flip_particle* particles, int64_t np,
                                  float flipAlpha) {
-  if (!ctx || (!particles && np) || np < 0) return MSBG_EINVARG;
-  cudaSetDevice(ctx->device);
-  FlipState* S = nullptr;
-  GridF g;
-  int rc = state_of(ctx, &S, g);
-  if (rc) return rc;
-  if (!np) return MSBG_OK;
-  cudaStream_t st = ctx->stream;
-  MSBG_CUDA_TRY(ctx, S->parts.ensure(sizeof(msbg_flip_particle) * (size_t)np));
-  MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(S->parts.p, particles, sizeof(msbg_flip_particle) * np,
-                                     cudaMemcpyHostToDevice, st));
-  k_g2p<<<grid_blocks(np), 256, 0, st>>>(S->parts.as<msbg_flip_particle>(), np, g,
-                                         S->vel.as<float>(), S->velOld.as<float>(), flipAlpha);
-  MSBG_CUDA_TRY(ctx, cudaGetLastError());
-  MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(particles, S->parts.p, sizeof(msbg_flip_particle) * np,
-                                     cudaMemcpyDeviceToHost, st));
-  return msbg_gpu_sync(ctx);
+  return flip_g2p(ctx, particles, np, flipAlpha, false);
+}
+
+extern "C" int msbg_gpu_flip_g2p_device(msbg_gpu_ctx* ctx, msbg_flip_particle* particles,
+                                        int64_t np, float flipAlpha) {
+  return flip_g2p(ctx, particles, np, flipAlpha, true);
 }
 
 namespace {

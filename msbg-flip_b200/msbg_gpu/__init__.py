@@ -591,6 +591,9 @@ def _flip_sigs(L):
         "msbg_gpu_flip_pressure_gradient": (i32, [vp, C.POINTER(C.c_float), f32, f32]),
         "msbg_gpu_flip_g2p": (i32, [vp, vp, C.c_int64, f32]),
         "msbg_gpu_flip_channel": (i32, [vp, i32, C.POINTER(C.c_float), C.c_int64, i32]),
+        "msbg_gpu_flip_p2g_device": (i32, [vp, vp, C.c_int64, C.POINTER(FlipParams),
+                                           C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
+        "msbg_gpu_flip_g2p_device": (i32, [vp, vp, C.c_int64, f32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -646,6 +649,24 @@ def _ctx_flip_channel(self, which, n_voxels, data=None):
                 "flip_channel")
 
 
+def _ctx_flip_p2g_device(self, dev_ptr, n_particles, params=None):
+    """msbg_gpu_flip_p2g_device on particles at device address dev_ptr."""
+    _flip_sigs(self._L)
+    prm = params or flip_params()
+    nb = C.c_int64()
+    self._check(self._L.msbg_gpu_flip_p2g_device(self._h, dev_ptr, n_particles, C.byref(prm),
+                                                 None, C.byref(nb)), "flip_p2g_device")
+    return nb.value
+
+
+def _ctx_flip_g2p_device(self, dev_ptr, n_particles, alpha=0.95):
+    _flip_sigs(self._L)
+    self._check(self._L.msbg_gpu_flip_g2p_device(self._h, dev_ptr, n_particles, alpha),
+                "flip_g2p_device")
+
+
+Context.flip_p2g_device = _ctx_flip_p2g_device
+Context.flip_g2p_device = _ctx_flip_g2p_device
 Context.flip_p2g = _ctx_flip_p2g
 Context.flip_gravity = _ctx_flip_gravity
 Context.flip_pressure_gradient = _ctx_flip_pressure_gradient

@@ -81,3 +81,26 @@ def test_multilevel_topology_is_refused(setup):
             c2.flip_p2g(p)
     finally:
         c2.close()
+
+
+def test_device_resident_particles_give_the_same_grid(setup):
+    import torch
+
+    ctx, p = setup
+    n = RES ** 3
+    ctx.flip_p2g(p)
+    ref_vel = ctx.flip_channel(msbg_gpu.FLIP_VEL, n)
+    ref_mass = ctx.flip_channel(msbg_gpu.FLIP_MASS, n)
+    d = torch.from_numpy(p.view(np.uint8).copy()).cuda()
+    torch.cuda.synchronize()
+    nact = ctx.flip_p2g_device(d.data_ptr(), len(p))
+    assert nact > 0
+    assert np.array_equal(ctx.flip_channel(msbg_gpu.FLIP_MASS, n), ref_mass)
+    assert np.abs(ctx.flip_channel(msbg_gpu.FLIP_VEL, n) - ref_vel).max() <= 1e-5
+    ctx.flip_gravity(-9.8, 0.02)
+    q = p.copy()
+    ctx.flip_g2p(q, 0.9)
+    ctx.flip_g2p_device(d.data_ptr(), len(p), 0.9)
+    torch.cuda.synchronize()
+    qd = d.cpu().numpy().view(msbg_gpu.FLIP_PARTICLE)
+    assert np.array_equal(qd["vel"], q["vel"])
