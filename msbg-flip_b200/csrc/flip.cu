@@ -70,6 +70,8 @@ __global__ void k_p2g_scatter(const msbg_flip_particle* __restrict__ p, int64_t 
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < np;
        k += (int64_t)gridDim.x * blockDim.x) {
     const msbg_flip_particle q = p[k];
+    // a particle without a finite position reaches no cell
+    if (!isfinite(q.pos[0]) || !isfinite(q.pos[1]) || !isfinite(q.pos[2])) continue;
     const float mp = q.phase == 0 ? rhoL : rhoG;
     const int64_t ci = g.idx((int)floorf(q.pos[0]), (int)floorf(q.pos[1]), (int)floorf(q.pos[2]));
     if (ci >= 0) {
@@ -202,6 +204,7 @@ __global__ void k_gradient(GridF g, int64_t n, float* __restrict__ vel,
 
 __device__ __forceinline__ float interp_comp(const GridF& g, const float* __restrict__ v,
                                              const float pos[3], int d) {
+  if (!isfinite(pos[0]) || !isfinite(pos[1]) || !isfinite(pos[2])) return 0.f;  // no cell
   const float gx = __fsub_rn(pos[0], kOff[d][0]), gy = __fsub_rn(pos[1], kOff[d][1]),
               gz = __fsub_rn(pos[2], kOff[d][2]);
   const int ix0 = (int)floorf(gx), iy0 = (int)floorf(gy), iz0 = (int)floorf(gz);

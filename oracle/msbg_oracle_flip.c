@@ -81,6 +81,9 @@ int oracle_flip_p2g(int sx, int sy, int sz, int bsx, const oracle_flip_particle*
   static const float OFF[3][3] = {{0.f, 0.5f, 0.5f}, {0.5f, 0.f, 0.5f}, {0.5f, 0.5f, 0.f}};
   for (int64_t k = 0; k < np; k++) {
     const oracle_flip_particle* q = &p[k];
+    /* a particle without a finite position reaches no cell (the reference's
+     * float-to-int conversion of it is undefined) */
+    if (!isfinite(q->pos[0]) || !isfinite(q->pos[1]) || !isfinite(q->pos[2])) continue;
     const float mp = q->phase == 0 ? c->rhoL : c->rhoG;
     const int64_t ci =
         fidx(&g, (int)floorf(q->pos[0]), (int)floorf(q->pos[1]), (int)floorf(q->pos[2]));
@@ -203,6 +206,7 @@ void oracle_flip_gradient(int sx, int sy, int sz, int bsx, float* vel, const flo
 
 static float interp_comp(const FGrid* g, const float* vel, const float pos[3], const float off[3],
                          int comp) {
+  if (!isfinite(pos[0]) || !isfinite(pos[1]) || !isfinite(pos[2])) return 0.f; /* no cell */
   const float gx = pos[0] - off[0], gy = pos[1] - off[1], gz = pos[2] - off[2];
   const int ix0 = (int)floorf(gx), iy0 = (int)floorf(gy), iz0 = (int)floorf(gz);
   const float fx = gx - ix0, fy = gy - iy0, fz = gz - iz0;

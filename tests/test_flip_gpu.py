@@ -104,3 +104,26 @@ def test_device_resident_particles_give_the_same_grid(setup):
     torch.cuda.synchronize()
     qd = d.cpu().numpy().view(msbg_gpu.FLIP_PARTICLE)
     assert np.array_equal(qd["vel"], q["vel"])
+
+
+def test_particles_outside_or_not_finite(setup):
+    """Particles outside the grid or with a non-finite position reach no
+    cell, on the GPU as in the restatement."""
+    ctx, p = setup
+    n = RES ** 3
+    q = p[:20000].copy()
+    q["pos"][:50] = [-3.0, 5.0, 5.0]
+    q["pos"][50:60] = [RES + 0.5, 1.0, 1.0]
+    q["pos"][60:70] = [np.nan, 1.0, 1.0]
+    q["pos"][70:80] = [np.inf, 2.0, 2.0]
+    ctx.flip_p2g(q)
+    _, mass_o, _, _ = oracle.flip_p2g(RES, BSX, q)
+    assert np.array_equal(ctx.flip_channel(msbg_gpu.FLIP_MASS, n), mass_o)
+    assert mass_o.sum() == len(q) - 80
+    ctx.flip_gravity(-9.8, 0.02)
+    vel = ctx.flip_channel(msbg_gpu.FLIP_VEL, n)
+    old = ctx.flip_channel(msbg_gpu.FLIP_VEL_OLD, n)
+    r = q.copy()
+    ctx.flip_g2p(r, 0.95)
+    r_o = oracle.flip_g2p(RES, BSX, q, vel, old, 0.95)
+    assert np.array_equal(r["vel"], r_o["vel"])
