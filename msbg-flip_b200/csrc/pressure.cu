@@ -214,13 +214,20 @@ int msbg::ps::pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
   // per-cell arrays: the per-cell work of the build runs on the GPU (set
   // MSBG_PRESSURE_BUILD=host to build them on the host as the callbacks are)
   const char* bsel = getenv("MSBG_PRESSURE_BUILD");
-  const bool onDevice = arr && !(bsel && std::strcmp(bsel, "host") == 0);
+  const bool onDeviceReq = arr && !(bsel && std::strcmp(bsel, "host") == 0);
   std::vector<std::unique_ptr<LevelDev>> built;
-  if (onDevice)
+  bool onDevice = onDeviceReq;
+  if (onDevice) {
     rc = build_hierarchy_device(S.H, built, S.rhs0, topo->sx, topo->sy, topo->sz, topo->bsx0,
                                 topo->nLevels, topo->blockLevel, topo->domainBc, *arr, 512,
                                 ctx->stream, &err);
-  else
+    if (rc == MSBG_ENOTIMPL) {  // no staging for this device on this thread: host build
+      onDevice = false;
+      built.clear();
+      err.clear();
+    }
+  }
+  if (!onDevice)
     rc = build_hierarchy(S.H, topo->sx, topo->sy, topo->sz, topo->bsx0, topo->nLevels,
                          topo->blockLevel, topo->domainBc, cb, 512, &err, arr);
   S.buildSeconds =

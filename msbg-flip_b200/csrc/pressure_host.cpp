@@ -1143,9 +1143,10 @@ struct BuildStaging {
   bool ready(int dev) {
     if (device == dev) return true;
     if (device >= 0) return false;
+    // (a partial earlier attempt keeps what it got; nothing is allocated twice)
     for (int i = 0; i < 2; i++)
-      if (cudaMallocHost(&buf[i], BYTES) != cudaSuccess ||
-          cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess ||
+      if ((!buf[i] && cudaMallocHost(&buf[i], BYTES) != cudaSuccess) ||
+          (!ev[i] && cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) ||
           raw[i].ensure(BYTES) != cudaSuccess)
         return false;
     device = dev;
@@ -1249,7 +1250,9 @@ int build_hierarchy_device(Hierarchy& H, std::vector<std::unique_ptr<LevelDev>>&
   DB_TRY(dScal.ensure(sizeof(scal0)));
   DB_TRY(cudaMemcpyAsync(dScal.p, scal0, sizeof(scal0), cudaMemcpyHostToDevice, st));
   BuildStaging& stg = build_staging();
-  if (!stg.ready(device)) return fail(MSBG_ENOMEM, "pinned staging of the array prepare");
+  // (the staging of a host thread serves one device; the caller then builds
+  // on the host)
+  if (!stg.ready(device)) return fail(MSBG_ENOTIMPL, "no pinned staging for this device");
   for (int k = 0; k < 2; k++)
     if (stg.used[k]) DB_TRY(cudaEventSynchronize(stg.ev[k]));
   stg.used[0] = stg.used[1] = false;
