@@ -466,6 +466,45 @@ int msbg_gpu_flip_g2p_device(msbg_gpu_ctx* ctx, msbg_flip_particle* particles, i
  * vector channels, voxels for MSBG_FLIP_MASS. */
 int msbg_gpu_flip_channel(msbg_gpu_ctx* ctx, int which, float* data, int64_t n, int get);
 
+/* ---- particle splatting -------------------------------------------------- */
+
+/* The splat parameters of the reference's demo (src/msbg_demo.cpp:235-236,
+ * rParticle 2, nbDist 2): particles reach rScan = rParticle + nbDist voxels;
+ * rScan + 1 must not exceed the base block size. */
+typedef struct {
+  float rParticle, nbDist;
+  int flags; /* MSBG_SPLAT_RAW: leave the quantised squared distances */
+} msbg_splat_params;
+
+enum { MSBG_SPLAT_RAW = 1 };
+
+/* Replaces the particle splatting of the reference's demo (msbg_test_sparse,
+ * src/msbg_demo.cpp:339-684) on the context's level-0 block raster:
+ *   pos[3n]  particle positions in voxel units (x, y, z); particles outside
+ *            [1e-4, s - 1e-4] on an axis, or not finite, are dropped
+ *            (isInDomainRange + inRange, src/msbg_demo.cpp:358-360)
+ *   kind     NULL: every block within rScan of a kept particle becomes a
+ *            value block, the others const empty blocks (the demo's marking
+ *            and refinement map, src/msbg_demo.cpp:366-500); else the caller's
+ *            MSBG_BLOCK_* per block
+ *   kindOut  optional [nBlocks]: the kinds used
+ * Creates 16-bit channel `chan` (msbg_gpu_upload_channel_u16 layout, const
+ * empty 0, full 65535): every value voxel at 65535, lowered by each particle
+ * to round(d^2 / rScan^2 * 65535) over the voxels of its scan box within
+ * rScan (a particle whose scan meets a block without values stops there, as
+ * the reference's goto does), then finalised to
+ * round((1 - linstep(-rParticle, rParticle + nbDist, d - rParticle)) * 65535)
+ * for d^2 < 0.999 rScan^2, else 0 (src/msbg_demo.cpp:661-675).  The channel
+ * is the smoother's input: msbg_gpu_pde_mcf runs on it directly.  Returns
+ * when the channel is complete. */
+int msbg_gpu_splat_particles(msbg_gpu_ctx* ctx, int chan, const float* pos, int64_t n,
+                             const msbg_splat_params* params, const int8_t* kind,
+                             int8_t* kindOut);
+/* The same with `pos` in device memory (read on the context's stream). */
+int msbg_gpu_splat_particles_device(msbg_gpu_ctx* ctx, int chan, const float* pos, int64_t n,
+                                    const msbg_splat_params* params, const int8_t* kind,
+                                    int8_t* kindOut);
+
 /* Diagnostics without a GPU (no counterpart in the reference): builds the
  * multigrid hierarchy as msbg_gpu_pressure_prepare does, then on the host
  *   yPacked = A xPacked on MG level 0 (block layout; both may be NULL),

@@ -59,6 +59,7 @@ extern "C" int msbg_gpu_destroy(msbg_gpu_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   pressure_release(ctx);
   flip_release(ctx);
+  splat_release(ctx);
   ctx->channels.clear();
   ctx->listBuf.release();
   ctx->errBuf.release();

@@ -108,6 +108,8 @@ int set_error(msbg_gpu_ctx* ctx, int code, const char* fmt, ...);
 void pressure_release(msbg_gpu_ctx* ctx);
 // Releases the FLIP transfer channels of a context (flip.cu).
 void flip_release(msbg_gpu_ctx* ctx);
+// Releases the particle-splatting buffers of a context (splat.cu).
+void splat_release(msbg_gpu_ctx* ctx);
 
 // Launches of the 8-colour mean-curvature-flow passes (mcf.cu).  xfaces:
 // optional face cache of nSlots value blocks (2 * bsx^2 values each, the

@@ -697,3 +697,78 @@ def flip_particles(res, bsx, z_liquid=0.4, ppv=8, air_ppv=1, air_band=8, seed=7,
         p["phase"] = phase
         out.append(p)
     return np.concatenate(out)
+
+
+# ---------------------------------------------------------------------------
+# Particle splatting into a 16-bit render-density channel
+# ---------------------------------------------------------------------------
+SPLAT_RAW = 1
+
+
+class SplatParams(C.Structure):
+    _fields_ = [("rParticle", C.c_float), ("nbDist", C.c_float), ("flags", C.c_int)]
+
+
+def _splat_sigs(L):
+    if getattr(L, "_splat_sig", False):
+        return
+    vp, i32 = C.c_void_p, C.c_int
+    for name in ("msbg_gpu_splat_particles", "msbg_gpu_splat_particles_device"):
+        fn = getattr(L, name)
+        fn.restype = i32
+        fn.argtypes = [vp, i32, vp, C.c_int64, C.POINTER(SplatParams), vp, vp]
+    L._splat_sig = True
+
+
+def _ctx_splat(self, chan, pos, r_particle=2.0, nb_dist=2.0, kind=None, raw=False):
+    """msbg_gpu_splat_particles after set_topology: creates 16-bit channel
+    `chan` from particle positions [n, 3]; returns the block kinds used."""
+    _splat_sigs(self._L)
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    prm = SplatParams(r_particle, nb_dist, SPLAT_RAW if raw else 0)
+    kout = np.zeros(max(getattr(self, "n_blocks", 0), 1), np.int8)
+    k = None if kind is None else np.ascontiguousarray(kind, np.int8)
+    self._check(self._L.msbg_gpu_splat_particles(self._h, chan, p.ctypes.data, len(p),
+                                                 C.byref(prm),
+                                                 None if k is None else k.ctypes.data,
+                                                 kout.ctypes.data), "splat_particles")
+    return kout
+
+
+def _ctx_splat_device(self, chan, dev_ptr, n_particles, r_particle=2.0, nb_dist=2.0, kind=None,
+                      raw=False):
+    """msbg_gpu_splat_particles_device on positions at device address dev_ptr."""
+    _splat_sigs(self._L)
+    prm = SplatParams(r_particle, nb_dist, SPLAT_RAW if raw else 0)
+    kout = np.zeros(max(getattr(self, "n_blocks", 0), 1), np.int8)
+    k = None if kind is None else np.ascontiguousarray(kind, np.int8)
+    self._check(self._L.msbg_gpu_splat_particles_device(self._h, chan, dev_ptr, n_particles,
+                                                        C.byref(prm),
+                                                        None if k is None else k.ctypes.data,
+                                                        kout.ctypes.data), "splat_particles")
+    return kout
+
+
+Context.splat = _ctx_splat
+Context.splat_device = _ctx_splat_device
+
+
+def splat_demo_particles(res3, n_base, seed=11, test_case=1):
+    """Seeded particles built the way the reference's demo builds its
+    bunny-of-bunnies (src/msbg_demo.cpp:339-385): n_base instances of a base
+    cloud of n_base points (a seeded stand-in for the PLY model: points near
+    an ellipsoid surface), instance i at 0.2 * sMax + 0.6 * sMax * b_i and
+    scaled by 0.01 * sMin (0.005 for test case 2), b the base cloud
+    normalised by its bounding box.  Returns float32 [n_base^2, 3]."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(n_base, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    v = (v * np.array([1.0, 0.7, 0.5]) + 0.05 * rng.normal(size=(n_base, 3))).astype(np.float32)
+    bmin = v.min(0)
+    span = (v.max(0) - bmin).max()
+    b = ((v - bmin) * np.float32(1.0 / span)).astype(np.float32)
+    smax, smin = max(res3), min(res3)
+    scale = np.float32(smin * (0.005 if test_case == 2 else 0.01))
+    centres = (np.float32(smax * 0.2) + np.float32(0.6) * (np.float32(smax) * b)).astype(np.float32)
+    pos = centres[:, None, :] + scale * b[None, :, :]
+    return pos.reshape(-1, 3).astype(np.float32)

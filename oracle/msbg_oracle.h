@@ -93,6 +93,17 @@ void oracle_flip_gradient(int sx, int sy, int sz, int bsx, float* vel, const flo
 void oracle_flip_g2p(int sx, int sy, int sz, int bsx, oracle_flip_particle* p, int64_t np,
                      const float* vel, const float* velOld, float alpha);
 
+/* ---- particle splatting (msbg_oracle_splat.c, src/msbg_demo.cpp) ---- */
+/* pos: 3 floats per particle; kind/active: one byte per block (1 = value);
+ * out: the value blocks packed in bid order, 16-bit render density
+ * (finalize = 0: the quantised squared distances before finalisation). */
+void oracle_splat_domain(int sx, int sy, int sz, float lo[3], float hi[3]);
+int oracle_splat_mark(int sx, int sy, int sz, int bsx, const float* pos, int64_t n,
+                      float rParticle, float nbDist, int8_t* active);
+int oracle_splat(int sx, int sy, int sz, int bsx, const int8_t* kind, const float* pos,
+                 int64_t n, float rParticle, float nbDist, int finalize, uint16_t* out);
+uint16_t oracle_splat_finalize_value(uint16_t q, float rParticle, float nbDist);
+
 #ifdef __cplusplus
 }
 #endif

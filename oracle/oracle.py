@@ -40,6 +40,8 @@ def build_ref(ref_root=REFERENCE_ROOT):
     if not os.path.isdir(os.path.join(ref_root, "src")):
         return False
     subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF_ROOT={ref_root}"], check=True)
+    # the reference's particle-splatting demo with its capture hooks
+    subprocess.run(["make", "-s", "-C", HERE, "splat", f"REF_ROOT={ref_root}"], check=True)
     # the INTEGRATION.md snippets compiled against the reference headers
     # (needs msbg-flip_b200/libmsbg_gpu.so, built before the oracle)
     subprocess.run(["make", "-s", "-C", HERE, "integ", f"REF_ROOT={ref_root}"], check=True)
@@ -383,3 +385,133 @@ def flip_g2p(res, bsx, particles, vel, velOld, alpha):
     L.oracle_flip_g2p(res, res, res, bsx, p.ctypes.data, len(p), v.ctypes.data, o.ctypes.data,
                       alpha)
     return p
+
+
+# ---- particle splatting (msbg_oracle_splat.c; src/msbg_demo.cpp) ----
+
+def _splat_lib():
+    L = oracle()
+    if not hasattr(L, "_splat_sig"):
+        vp, i32, f32 = C.c_void_p, C.c_int, C.c_float
+        L.oracle_splat_domain.argtypes = [i32] * 3 + [vp, vp]
+        L.oracle_splat_mark.restype = i32
+        L.oracle_splat_mark.argtypes = [i32] * 4 + [vp, C.c_int64, f32, f32, vp]
+        L.oracle_splat.restype = i32
+        L.oracle_splat.argtypes = [i32] * 4 + [vp, vp, C.c_int64, f32, f32, i32, vp]
+        L.oracle_splat_finalize_value.restype = C.c_uint16
+        L.oracle_splat_finalize_value.argtypes = [C.c_uint16, f32, f32]
+        L._splat_sig = True
+    return L
+
+
+def splat_domain(res3):
+    """The demo's particle domain bounds (lo[3], hi[3]) restated."""
+    L = _splat_lib()
+    lo = np.zeros(3, np.float32)
+    hi = np.zeros(3, np.float32)
+    L.oracle_splat_domain(*res3, lo.ctypes.data, hi.ctypes.data)
+    return lo, hi
+
+
+def splat_mark(res3, bsx, pos, r_particle=2.0, nb_dist=2.0):
+    """Active-block marking restated: one byte per block (1 = active)."""
+    L = _splat_lib()
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    nb = (res3[0] // bsx) * (res3[1] // bsx) * (res3[2] // bsx)
+    act = np.zeros(nb, np.int8)
+    rc = L.oracle_splat_mark(*res3, bsx, p.ctypes.data, len(p), r_particle, nb_dist,
+                             act.ctypes.data)
+    if rc:
+        raise RuntimeError(f"oracle_splat_mark rc={rc}")
+    return act
+
+
+def splat(res3, bsx, kind, pos, r_particle=2.0, nb_dist=2.0, finalize=True):
+    """The splat restated: the value blocks (kind == 1) packed in bid order."""
+    L = _splat_lib()
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    k = np.ascontiguousarray(kind, np.int8)
+    out = np.zeros(int((k == 1).sum()) * bsx ** 3, np.uint16)
+    rc = L.oracle_splat(*res3, bsx, k.ctypes.data, p.ctypes.data, len(p), r_particle, nb_dist,
+                        1 if finalize else 0, out.ctypes.data)
+    if rc:
+        raise RuntimeError(f"oracle_splat rc={rc}")
+    return out
+
+
+def splat_finalize_table(r_particle=2.0, nb_dist=2.0):
+    """The finalisation of every 16-bit squared distance (65536 entries)."""
+    L = _splat_lib()
+    return np.array([L.oracle_splat_finalize_value(q, r_particle, nb_dist) for q in range(65536)],
+                    np.uint16)
+
+
+SPLAT_REF_SO = os.path.join(OUT, "libmsbg_splatref.so")
+_splat_ref = None
+
+
+def splat_reference_available():
+    return os.path.exists(SPLAT_REF_SO) and os.path.exists(REF_SO)
+
+
+def _splat_ref_lib():
+    global _splat_ref
+    if _splat_ref is None:
+        ref()  # the reference library first (ref_init, its thread pool)
+        L = C.CDLL(SPLAT_REF_SO)
+        L.ref_splat_demo.restype = C.c_int
+        L.ref_splat_demo.argtypes = [C.c_int, C.c_char_p] + [C.c_int] * 4
+        L.ref_splat_sizes.argtypes = [C.c_void_p]
+        L.ref_splat_copy.argtypes = [C.c_void_p] * 5
+        L.ref_splat_times.argtypes = [C.c_void_p]
+        L.ref_splat_in_domain.restype = C.c_int
+        L.ref_splat_in_domain.argtypes = [C.c_int] * 4 + [C.c_void_p, C.c_int64, C.c_void_p]
+        _splat_ref = L
+    return _splat_ref
+
+
+def write_ply(path, points):
+    """An ASCII PLY with the vertices the demo's reader takes
+    (readVerticesFromPLY, src/msbg_demo.cpp:72-120)."""
+    with open(path, "w") as f:
+        f.write("ply\nformat ascii 1.0\nelement vertex %d\n" % len(points))
+        f.write("property float x\nproperty float y\nproperty float z\nend_header\n")
+        for p in points:
+            f.write("%.6f %.6f %.6f\n" % (p[0], p[1], p[2]))
+
+
+def splat_reference_demo(ply_path, test_case, bsx, res3):
+    """Runs the reference's msbg_test_sparse on a PLY file up to its
+    smoothing call (oracle/ref/splat_harness.cpp) and returns what it
+    splatted: particle positions, the value blocks, the quantised squared
+    distances after the splat loop, the render density after finalisation,
+    and the phase times."""
+    L = _splat_ref_lib()
+    rc = L.ref_splat_demo(test_case, ply_path.encode(), bsx, *res3)
+    if rc:
+        raise RuntimeError(f"ref_splat_demo rc={rc}")
+    sz = np.zeros(5, np.int64)
+    L.ref_splat_sizes(sz.ctypes.data)
+    n, nr, nf, b, _ = (int(v) for v in sz)
+    pos = np.zeros((n, 3), np.float32)
+    rb = np.zeros(nr, np.int32)
+    raw = np.zeros(nr * b ** 3, np.uint16)
+    fb = np.zeros(nf, np.int32)
+    fv = np.zeros(nr * b ** 3, np.uint16)
+    L.ref_splat_copy(pos.ctypes.data, rb.ctypes.data, raw.ctypes.data, fb.ctypes.data,
+                     fv.ctypes.data)
+    t = np.zeros(3, np.float64)
+    L.ref_splat_times(t.ctypes.data)
+    return {"pos": pos, "blocks": rb, "raw": raw, "active": fb, "final": fv, "bsx": b,
+            "t_marked": t[0], "t_splat": t[1], "t_final": t[2]}
+
+
+def splat_reference_in_domain(res3, bsx, pts):
+    """The demo's particle test run by the reference on a grid it creates."""
+    L = _splat_ref_lib()
+    p = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+    out = np.zeros(len(p), np.int32)
+    rc = L.ref_splat_in_domain(*res3, bsx, p.ctypes.data, len(p), out.ctypes.data)
+    if rc:
+        raise RuntimeError(f"ref_splat_in_domain rc={rc}")
+    return out
