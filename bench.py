@@ -28,7 +28,12 @@ calls after one warm-up:
     64 seeded spheres, 20 iterations, dt 0.1) with its roofline and the
     reference's CPU smoother on the same input.
 
-``--workload mcf`` benches only the smoother; ``--workload c3`` / ``c5`` the
+  - the particle splatting that produces the smoother's input in the
+    reference's demo (1024^3, 16^3 blocks, 4096 instances of a 4096-point
+    seeded cloud), next to the reference's own demo code on 1024 instances.
+
+``--workload mcf`` benches only the smoother, ``--workload splat`` only the
+splatting; ``--workload c3`` / ``c5`` the
 2048^3 mixed-precision and 4096^3 three-level configurations (one JSON line
 of figures each, see bench_large).
 ``--impl reference`` times the reference's own CPU implementation (compiled
@@ -289,6 +294,24 @@ def bench_reference(args):
         return
     if args.workload == "mcf":
         return bench_reference_mcf(args)
+    if args.workload == "splat":
+        cb = splat_reference_rate()
+        if cb is None:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "oracle/_ref/libmsbg_splatref.so was not built"}), flush=True)
+            return
+        print(json.dumps({
+            "metric": "particle splat rate (16-bit render density, the smoother's input)",
+            "value": cb["value"], "unit": "Mparticles/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded point cloud, the demo's instance construction)",
+            "impl": "reference", "config": {"workload": splat_workload_name(),
+                                            "parallelism": "cpu"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "Mparticles/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
     c = dict(PS_SAME_CFG)
     cb = ref_pressure_rate(c, max_seconds=60.0)
     kind, vals, upd = mcf_scene()
@@ -302,7 +325,8 @@ def bench_reference(args):
                                 f"{workload_name(PS_CFG)}: same scene with 16^3 base blocks "
                                 "(its smoother aborts for 32^3 blocks)"),
                        "time_to_1e-6": "not reached (the reference MGPCG stalls)",
-                       "mcf_512_b16": mcf, "parallelism": "cpu"},
+                       "mcf_512_b16": mcf, splat_workload_name(): splat_reference_rate(),
+                       "parallelism": "cpu"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "Gvoxel/s/iter", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -465,6 +489,107 @@ def flip_line(args, ctx):
                            "p2g_mparticles_s": len(sample) / t_p2g / 1e6,
                            "g2p_mparticles_s": len(sample) / t_g2p / 1e6}
     return out
+
+
+# the demo's particle splatting (src/msbg_demo.cpp:339-684): rParticle 2,
+# nbDist 2, n_base instances of an n_base-point cloud; the reference's demo is
+# timed on the first ref_n_base points of the same cloud (ref_n_base^2
+# particles)
+SPLAT_CFG = dict(res=1024, bsx=16, n_base=4096, test_case=1, seed=11, ref_n_base=1024)
+
+
+def splat_workload_name(c=SPLAT_CFG):
+    return f"splat_{c['res']}_b{c['bsx']}_demo{c['n_base']}x{c['n_base']}"
+
+
+def splat_reference_rate(c=SPLAT_CFG):
+    """The reference's demo code (msbg_test_sparse, compiled from
+    src/msbg_demo.cpp with oracle/ref/splat_harness.cpp observing it) on
+    ref_n_base instances of the first ref_n_base points of the cloud, all
+    host threads: particles / (block allocation + splat + finalisation)."""
+    import msbg_gpu
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.splat_reference_available():
+        return None
+    base = msbg_gpu.splat_base_cloud(c["n_base"], c["seed"])[: c["ref_n_base"]]
+    with tempfile.TemporaryDirectory() as d:
+        ply = os.path.join(d, "base.ply")
+        oracle.write_ply(ply, base)
+        r = oracle.splat_reference_demo(ply, c["test_case"], c["bsx"], (c["res"],) * 3)
+    n = len(r["pos"])
+    t_splat = r["t_final"] - r["t_marked"]
+    return {"value": n / t_splat / 1e6, "unit": "Mparticles/s", "cores": os.cpu_count(),
+            "kind": "reference",
+            "sample": (f"reference msbg_test_sparse (src/msbg_demo.cpp:228-684) on "
+                       f"{c['ref_n_base']} instances of the first {c['ref_n_base']} cloud "
+                       f"points ({n} particles, {len(r['blocks'])} value blocks), "
+                       f"{c['res']}^3, {c['bsx']}^3 blocks: value = particles / (block "
+                       f"allocation + splat + finalisation) = {t_splat:.3f} s; marking and "
+                       f"particle construction {r['t_marked']:.3f} s")}
+
+
+def splat_line(args, ctx):
+    """The demo's particle splatting on the GPU: positions resident in device
+    memory (value) and through the C ABI from host positions with the
+    channel downloaded (e2e), each over --steps calls after one warm-up."""
+    import torch
+    import msbg_gpu
+    c = dict(SPLAT_CFG)
+    if args.workload == "splat" and args.res:
+        c["res"] = args.res
+    if args.workload == "splat" and args.splat_base:
+        c["n_base"] = args.splat_base
+    res3, bsx = (c["res"],) * 3, c["bsx"]
+    pos = msbg_gpu.splat_demo_particles(res3, c["n_base"], c["seed"], c["test_case"])
+    ctx.set_topology(*res3, bsx)
+    steps = max(args.steps, 1)
+    dpos = torch.from_numpy(pos).to(f"cuda:{ctx.device}")
+    torch.cuda.synchronize()
+    kind = ctx.splat_device(7, dpos.data_ptr(), len(pos))
+    nval = int((kind == 1).sum())
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ctx.splat_device(7, dpos.data_ptr(), len(pos))
+    dt_dev = (time.perf_counter() - t0) / steps
+    del dpos
+    out = np.empty(nval * bsx ** 3, np.uint16)
+    ctx.splat(7, pos)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ctx.splat(7, pos)
+        ctx.download_channel_u16(7, out)
+    dt_e2e = (time.perf_counter() - t0) / steps
+    line = {"workload": splat_workload_name(c), "particles": int(len(pos)),
+            "value_blocks": nval, "unit": "Mparticles/s",
+            "value": len(pos) / dt_dev / 1e6, "ms_per_call": dt_dev * 1e3,
+            "path": "msbg_gpu_splat_particles_device (positions in device memory; marking, "
+                    "block kinds, binning, splat and finalisation in each call)",
+            "e2e": {"value": len(pos) / dt_e2e / 1e6, "unit": "Mparticles/s",
+                    "ms_per_call": dt_e2e * 1e3, "h2d_bytes_per_step": int(pos.nbytes),
+                    "d2h_bytes_per_step": int(out.nbytes)}}
+    if not args.no_cpu:
+        line["cpu_baseline"] = splat_reference_rate(c)
+    return line
+
+
+def bench_splat(args):
+    import torch
+    import msbg_gpu
+    torch.cuda.set_device(0)
+    ctx = msbg_gpu.Context(0)
+    with Clocks(0) as clk:
+        s = splat_line(args, ctx)
+    ctx.close()
+    cb = s.pop("cpu_baseline", None)
+    e2e = s.pop("e2e")
+    line = {"metric": "particle splat rate (16-bit render density, the smoother's input)",
+            "value": s["value"], "unit": "Mparticles/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": s["ms_per_call"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded point cloud, the demo's instance construction)",
+            "config": s, "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cb}
+    print(json.dumps(line), flush=True)
 
 
 def bench_mgpcg(args):
@@ -644,6 +769,7 @@ def mgpcg_extras(args, ctx, c, scene, st, fluid, prepare=None):
     x["max_err_vs_fp64_oracle"] = error_vs_oracle(ctx, c)
     x["mcf_512_b16"] = mcf_line(args, ctx)
     x["flip_transfers_256_b16"] = flip_line(args, ctx)
+    x[splat_workload_name()] = splat_line(args, ctx)
     return x, roof, cb
 
 
@@ -940,8 +1066,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mgpcg", choices=["mgpcg", "mcf", "c3", "c5"])
+    ap.add_argument("--workload", default="mgpcg",
+                    choices=["mgpcg", "mcf", "splat", "c3", "c5"])
     ap.add_argument("--res", type=int, default=0, help="override the pressure resolution")
+    ap.add_argument("--splat-base", type=int, default=0,
+                    help="points of the splat workload's cloud (n^2 particles)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline legs")
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned guess")
     ap.add_argument("--quick", action="store_true",
@@ -960,6 +1089,8 @@ def main():
         bench_reference(args)
     elif args.workload == "mcf":
         bench_mcf(args)
+    elif args.workload == "splat":
+        bench_splat(args)
     elif args.workload in ("c3", "c5"):
         bench_large(args)
     else:

@@ -302,6 +302,21 @@ int msbg::ps::pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
     MSBG_CUDA_TRY(ctx, cudaMemsetAsync(D->x.p, 0, nb, st));
     MSBG_CUDA_TRY(ctx, cudaMemsetAsync(D->b.p, 0, nb, st));
     maxPartial = std::max(maxPartial, (int)L.tiles.size());
+    // packed x faces on levels with 16^3 passes: the x = 0 plane of cx,
+    // gathered once, and room for the faces of the V-cycle's x
+    bool has16 = false;
+    for (const auto& P : L.passes) has16 |= P.ts == 16 && P.count > 0;
+    if (has16 && m + 1 < S.H.levels.size()) {
+      const size_t nf = (size_t)xface_len(L.nCells);
+      MSBG_CUDA_TRY(ctx, D->cxf.ensure(sizeof(float) * (nf / 2 + 256)));
+      MSBG_CUDA_TRY(ctx, D->xf.ensure(sizeof(float) * nf));
+      MSBG_CUDA_TRY(ctx, cudaMemsetAsync(D->xf.p, 0, sizeof(float) * nf, st));
+      for (const auto& P : L.passes)
+        if (P.ts == 16 && P.count > 0)
+          k_pack_cx_plane<16><<<P.count, 256, 0, st>>>(D->tileOff.as<int64_t>(), P.start,
+                                                   D->cx.as<float>(), D->cxf.as<float>());
+      MSBG_CUDA_TRY(ctx, cudaGetLastError());
+    }
     LevelView v;
     v.tileOff = D->tileOff.as<int64_t>();
     v.face = D->face.as<int>();
@@ -314,6 +329,7 @@ int msbg::ps::pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
     v.cy = D->cy.as<float>();
     v.cz = D->cz.as<float>();
     v.ifc = D->ifc.as<float>();
+    v.cxf = D->cxf.p ? D->cxf.as<float>() : nullptr;
     S.views.push_back(v);
     if (m == 0) {
       // tiles the learned network runs on: the 16^3 tiles of level 0
@@ -1233,6 +1249,8 @@ int profile_typed(msbg_gpu_ctx* ctx, Solver& S, int what, int reps, int innerIte
   // and writes x; the matvec reads d, a_ii, cx, cy, cz and writes q
   const double v = sizeof(VT);
   const double smooth0 = 16.0 + 3 * v, smoothC = 28.0, mvB = 16.0 + 2 * v;
+  // the sweep keeps the packed x faces of x, as inside a V-cycle
+  VT* xf0 = R.template faces<VT>(0);
   auto vcycle_bytes = [&]() {
     double s = 0;
     for (size_t m = 0; m + 1 < S.H.levels.size(); m++) {
@@ -1248,7 +1266,7 @@ int profile_typed(msbg_gpu_ctx* ctx, Solver& S, int what, int reps, int innerIte
   double bytes = 0;
   auto body = [&]() {
     switch (what) {
-      case 0: R.smooth(0, x, (const VT*)b, false); break;
+      case 0: R.smooth(0, x, (const VT*)b, false, xf0); break;
       case 3: R.usePipe = false; R.smooth(0, x, (const VT*)b, false); R.usePipe = true; break;
       case 1: R.matvec_dot(x, S.q0.as<VT>(), part); break;
       case 2: R.vcycle(0, S.z0.as<VT>(), (const VT*)b); break;
@@ -1263,6 +1281,7 @@ int profile_typed(msbg_gpu_ctx* ctx, Solver& S, int what, int reps, int innerIte
     default: return set_error(ctx, MSBG_EINVARG, "profile target %d", what);
   }
   MSBG_CUDA_TRY(ctx, cudaMemsetAsync(x, 0, sizeof(VT) * L0.nCells, st));
+  if (xf0) MSBG_CUDA_TRY(ctx, cudaMemsetAsync(xf0, 0, sizeof(VT) * xface_len(L0.nCells), st));
   body();  // warm-up
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);

@@ -114,6 +114,9 @@ struct LevelDev {
   DeviceBuffer x, b, r;            // FP32 work vectors of this level
   DeviceBuffer ctype;              // level 0: CT_* per cell
   DeviceBuffer fluid;              // liquid flag per cell (device build only)
+  // packed x = 0 plane of cx per 16^3 tile, and the packed x faces of the
+  // V-cycle's x on this level (pressure_kernels.cuh: xface_slot)
+  DeviceBuffer cxf, xf;
 };
 
 // Domain faces without a caller spec follow the reference's FLIP operator:

@@ -28,7 +28,20 @@ struct LevelView {
   const float* cy;
   const float* cz;
   const float* ifc;
+  // the x = 0 plane of cx of every 16^3 tile, packed: 256 floats at tile
+  // offset / 16 (the coupling across a tile's upper x face, read as one
+  // contiguous run instead of 256 values 64 bytes apart); nullptr if absent
+  const float* cxf = nullptr;
 };
+
+// Packed x faces of a level vector on 16^3 tiles: the x = 0 plane at
+// tile offset / 8 and the x = 15 plane 256 further, each face cell (y, z) at
+// y + 16 z.  Kernels that write such a vector also write its faces, so the
+// x-face halo of a neighbour is read in full 128-byte lines.
+__host__ __device__ __forceinline__ int64_t xface_slot(int64_t off, int side, int y, int z) {
+  return (off >> 3) + (side ? 256 : 0) + y + 16 * z;
+}
+__host__ __device__ __forceinline__ int64_t xface_len(int64_t nCells) { return nCells / 8 + 512; }
 
 __host__ __device__ __forceinline__ int tidx(int ts, int i, int j, int k) { return i + ts * (j + ts * k); }
 

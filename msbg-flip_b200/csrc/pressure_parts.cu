@@ -313,7 +313,7 @@ void launch_matvec(Solver& S, int m, const float* x, float* q, cudaStream_t st, 
       const int grid = std::min(P.count, S.numSMs);
       k_apply_pipe16<APPLY_MATVEC, float, float, pipe::NT_APPLY>
           <<<grid, pipe::NT_APPLY, pipe::SMEM, st>>>(S.views[m], P.start, P.count, x, nullptr, q,
-                                                     nullptr, nullptr, nullptr, err);
+                                                     nullptr, nullptr, nullptr, err, nullptr);
     } else {
       const int* lst = S.dev[m]->passTiles.as<int>() + P.start;
       TS_DISPATCH(P.ts, (k_matvec_dot<T, float><<<P.count, T * T, 0, st>>>(S.views[m], lst, x, q,
@@ -473,7 +473,7 @@ extern "C" int msbg_gpu_restrict(msbg_gpu_ctx* ctx, int levelMgCoarse, const flo
       k_apply_pipe16<APPLY_RESIDUAL, float, float, pipe::NT_APPLY>
           <<<grid, pipe::NT_APPLY, pipe::SMEM, st>>>(S->views[mf], Pp.start, Pp.count,
                                                      dx.as<float>(), db.as<float>(), nullptr,
-                                                     dc.as<float>(), coff, nullptr, err);
+                                                     dc.as<float>(), coff, nullptr, err, nullptr);
     } else {
       const int* lst = S->dev[mf]->passTiles.as<int>() + Pp.start;
       TS_DISPATCH(Pp.ts, (k_residual_restrict<T, float, float><<<Pp.count, T * T, 0, st>>>(
@@ -508,7 +508,7 @@ extern "C" int msbg_gpu_prolongate(msbg_gpu_ctx* ctx, int levelMgFine, const flo
     const int* lst = S->dev[levelMgFine]->groupTiles.as<int>() + g.start;
     TS_DISPATCH(g.ts, (k_prolong<T, float, float><<<g.count, T * T, 0, st>>>(
                           S->views[levelMgFine], lst, dfine.as<float>(), dc.as<float>(), coff,
-                          scale)));
+                          scale, nullptr)));
   }
   MSBG_CUDA_TRY(ctx, cudaGetLastError());
   if ((rc = PF.pack(dfine, fine))) return rc;

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -79,6 +80,13 @@ void set_kernel_attrs() {
                        cudaFuncAttributeMaxDynamicSharedMemorySize, pipeSmem);
 }
 
+// MSBG_PRESSURE_FACES=0 turns the packed x faces off (the halo then reads
+// the neighbours' strided x planes); the results are the same bits.
+inline bool packed_faces_enabled() {
+  const char* e = std::getenv("MSBG_PRESSURE_FACES");
+  return !(e && std::strcmp(e, "0") == 0);
+}
+
 #define TS_DISPATCH(ts, CALL)        \
   switch (ts) {                      \
     case 16: { constexpr int T = 16; CALL; } break; \
@@ -101,7 +109,16 @@ struct Runner {
   int* err = nullptr;     // device flag set by kernels whose bounded wait gave up
   int numSMs = 148;
   bool usePipe = true;
+  // the V-cycle keeps packed x faces of its x on every level that has them
+  // (LevelDev::xf); callers that smooth a vector outside a V-cycle pass none
+  bool useFaces = packed_faces_enabled();
   int64_t launches = 0;  // kernels launched through this runner
+
+  template <typename V>
+  V* faces(int m) {
+    LevelDev& D = *S.dev[m];
+    return useFaces && usePipe && D.xf.p && S.views[m].cxf ? D.xf.template as<V>() : nullptr;
+  }
 
   const int* passList(int m) { return S.dev[m]->passTiles.template as<int>(); }
   const int* groupList(int m) { return S.dev[m]->groupTiles.template as<int>(); }
@@ -109,7 +126,7 @@ struct Runner {
   // One smoothing sweep of MG level m: the (level, colour) passes in order
   // (pre) or in reverse order with the adjoint colour order inside (post).
   template <typename V>
-  void smooth(int m, V* x, const V* b, bool post) {
+  void smooth(int m, V* x, const V* b, bool post, V* xf = nullptr) {
     const Level& L = S.H.levels[m];
     const int np = (int)L.passes.size();
     for (int pi = 0; pi < np; pi++) {
@@ -120,7 +137,7 @@ struct Runner {
         const int grid = std::min(P.count, numSMs);
         // passes are contiguous tile-id ranges (register_tiles sorts by pass)
         k_smooth_pipe16<V, pipe::NT_SMOOTH><<<grid, pipe::NT_SMOOTH, pipe::SMEM_SMOOTH, st>>>(
-            S.views[m], P.start, P.count, x, b, inner, post ? 1 : 0, err);
+            S.views[m], P.start, P.count, x, b, inner, post ? 1 : 0, err, xf);
       } else {
         TS_DISPATCH(P.ts, (k_smooth<T, V><<<P.count, T * T, smooth_smem<T>(), st>>>(
                                S.views[m], lst, x, b, inner, post ? 1 : 0)));
@@ -134,25 +151,27 @@ struct Runner {
     const int last = (int)S.H.levels.size() - 1;
     const Level& L = S.H.levels[m];
     cudaMemsetAsync(x, 0, sizeof(V) * L.nCells, st);
+    V* xf = m == last ? nullptr : faces<V>(m);
+    if (xf) cudaMemsetAsync(xf, 0, sizeof(V) * xface_len(L.nCells), st);
     if (m == last) {
       k_coarse_solve<V><<<1, 512, 0, st>>>(S.dCoarseInv.template as<double>(), S.H.nCoarse,
                                            S.dCoarseCells.template as<int64_t>(), b, x);
       launches++;
       return;
     }
-    for (int s = 0; s < nPre; s++) smooth(m, x, b, false);
+    for (int s = 0; s < nPre; s++) smooth(m, x, b, false, xf);
     LevelDev& C = *S.dev[m + 1];
-    residual_restrict(m, x, b);
+    residual_restrict(m, x, b, xf);
     float* xc = C.x.template as<float>();
     vcycle<float>(m + 1, xc, C.b.template as<float>());
     for (const auto& g : L.groups) {
       const int* lst = groupList(m) + g.start;
       TS_DISPATCH(g.ts, (k_prolong<T, V, float><<<g.count, T * T, 0, st>>>(
                             S.views[m], lst, x, xc, C.tileOff.template as<int64_t>(),
-                            coarseScale)));
+                            coarseScale, xf)));
       launches++;
     }
-    for (int s = 0; s < nPost; s++) smooth(m, x, b, true);
+    for (int s = 0; s < nPost; s++) smooth(m, x, b, true, xf);
   }
 
   // q = A d with partial d.q (level 0); returns the number of partials.
@@ -166,7 +185,8 @@ struct Runner {
       if (P.ts == 16 && usePipe) {
         const int grid = std::min(P.count, numSMs);
         k_apply_pipe16<APPLY_MATVEC, VT, VT, pipe::NT_APPLY><<<grid, pipe::NT_APPLY, pipe::SMEM, st>>>(
-            S.views[0], P.start, P.count, d, nullptr, q, nullptr, nullptr, partial + off, err);
+            S.views[0], P.start, P.count, d, nullptr, q, nullptr, nullptr, partial + off, err,
+            nullptr);
         off += grid;
       } else {
         const int* lst = passList(0) + P.start;
@@ -181,7 +201,7 @@ struct Runner {
 
   // r = b - A x on MG level m, restricted into the (FP32) right-hand side of m+1.
   template <typename V>
-  void residual_restrict(int m, const V* x, const V* b) {
+  void residual_restrict(int m, const V* x, const V* b, const V* xf = nullptr) {
     const Level& L = S.H.levels[m];
     LevelDev& C = *S.dev[m + 1];
     float* bc = C.b.template as<float>();
@@ -191,7 +211,7 @@ struct Runner {
       if (P.ts == 16 && usePipe) {
         const int grid = std::min(P.count, numSMs);
         k_apply_pipe16<APPLY_RESIDUAL, V, float, pipe::NT_APPLY><<<grid, pipe::NT_APPLY, pipe::SMEM, st>>>(
-            S.views[m], P.start, P.count, x, b, nullptr, bc, coff, nullptr, err);
+            S.views[m], P.start, P.count, x, b, nullptr, bc, coff, nullptr, err, xf);
       } else {
         const int* lst = passList(m) + P.start;
         TS_DISPATCH(P.ts, (k_residual_restrict<T, V, float><<<P.count, T * T, 0, st>>>(

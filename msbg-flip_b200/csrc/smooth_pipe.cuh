@@ -92,17 +92,23 @@ constexpr size_t SMEM = sizeof(float) * ZERO_FLOATS + 3 * sizeof(TileRec) + 3 * 
 // lower-face coupling of a SAME face is taken later from shared memory).
 // The branches only choose the addresses: each value is one load straight
 // into its register, raw, so nothing waits for it before it is used (faces
-// without these values load a harmless word and ignore it).
+// without these values load a harmless word and ignore it).  With the packed
+// x faces xf of x (and L.cxf), an x face reads the neighbour's packed plane.
 template <typename VT>
 __device__ __forceinline__ void halo_load(const LevelView& L, const VT* __restrict__ x,
-                                          const FaceRes& r, int dir, int side, int a, int b,
-                                          VT& xv, float& cv) {
+                                          const VT* __restrict__ xf, const FaceRes& r, int dir,
+                                          int side, int a, int b, VT& xv, float& cv) {
   const float* cd = dir == 0 ? L.cx : dir == 1 ? L.cy : L.cz;
   const VT* px = x;
   const float* pc = cd;
   if (r.kind == FACE_SAME) {
-    px = x + r.nOff + plane_idx(TS, dir, side ? 0 : TS - 1, a, b);
-    if (side) pc = cd + r.nOff + plane_idx(TS, dir, 0, a, b);
+    if (dir == 0 && xf) {
+      px = xf + xface_slot(r.nOff, side ? 0 : 1, a, b);
+      if (side) pc = L.cxf + (r.nOff >> 4) + a + TS * b;
+    } else {
+      px = x + r.nOff + plane_idx(TS, dir, side ? 0 : TS - 1, a, b);
+      if (side) pc = cd + r.nOff + plane_idx(TS, dir, 0, a, b);
+    }
   } else if (r.kind == FACE_COARSER) {
     px = x + r.nOff + plane_idx(r.nts, dir, side ? 0 : r.nts - 1, r.oa + (a >> 1), r.ob + (b >> 1));
     pc = L.ifc + r.ifOwn + a + TS * b;
@@ -169,7 +175,8 @@ __device__ __forceinline__ VT* sraw_b(float* st) {
 template <typename VT, int NTH>
 __global__ void __launch_bounds__(NTH, 1)
     k_smooth_pipe16(LevelView L, int tileBase, int count, VT* __restrict__ x,
-                    const VT* __restrict__ b, int inner, int reverse, int* __restrict__ err) {
+                    const VT* __restrict__ b, int inner, int reverse, int* __restrict__ err,
+                    VT* __restrict__ xf) {
   using namespace pipe;
   static_assert(NTH == 1024, "the z-pair thread map covers a 16^3 tile with 1024 threads");
   constexpr int NHALO = 6 * TS * TS;           // halo cells of a tile
@@ -240,12 +247,14 @@ __global__ void __launch_bounds__(NTH, 1)
   };
   VT hx[HQ];
   float hc[HQ];
+  // packed x faces only with the packed upper-face couplings
+  const VT* xfr = L.cxf ? xf : nullptr;
   auto halo_issue = [&](const TileRec& r) {
 #pragma unroll
     for (int q = 0; q < HQ; q++) {
       const int g = tid + NTH * q, f = g >> 8, c = g & 255;
       if (NHALO % NTH == 0 || g < NHALO)
-        halo_load(L, x, r.f[f], f >> 1, f & 1, c & 15, c >> 4, hx[q], hc[q]);
+        halo_load(L, x, xfr, r.f[f], f >> 1, f & 1, c & 15, c >> 4, hx[q], hc[q]);
     }
   };
   auto halo_combine = [&](const TileRec& r, int ti, int u) {
@@ -430,6 +439,9 @@ __global__ void __launch_bounds__(NTH, 1)
         const bool c1lo = dxof(1, sl) == 0;  // colour 1 holds the even cell
         const float lo = c1lo ? xv[1][sl] : xv[0][sl], hi = c1lo ? xv[0][sl] : xv[1][sl];
         store2(xg + TS * TS * sl, lo, hi);
+        // the tile's own x faces: x = 0 from ip = 0, x = 15 from ip = 7
+        if (xf && (ip == 0 || ip == 7))
+          xf[xface_slot(rc.off, ip == 7, jj, 2 * kp + sl)] = from_f<VT>(ip == 0 ? lo : hi);
       }
     }
     // 5: next tile's arrays landed -> its halo sums
@@ -484,7 +496,8 @@ __global__ void __launch_bounds__(NTH, 1)
     k_apply_pipe16(LevelView L, int tileBase, int count, const VT* __restrict__ x,
                    const VT* __restrict__ b, VT* __restrict__ y,
                    VC* __restrict__ bc, const int64_t* __restrict__ coarseOff,
-                   double* __restrict__ partial, int* __restrict__ err) {
+                   double* __restrict__ partial, int* __restrict__ err,
+                   const VT* __restrict__ xf) {
   using namespace pipe;
   constexpr int ZC = TS / (NTH / (TS * TS));  // cells of a thread's z column
   constexpr int NHALO = 6 * TS * TS;
@@ -541,12 +554,13 @@ __global__ void __launch_bounds__(NTH, 1)
     };
     VT hx[HQ];
     float hc[HQ];
+    const VT* xfr = L.cxf ? xf : nullptr;
     auto halo_issue = [&](const TileRec& r, int ti, int u) {
 #pragma unroll
       for (int q = 0; q < HQ; q++) {
         const int g = tid + NTH * q, f = g >> 8, c = g & 255;
         if (NHALO % NTH == 0 || g < NHALO)
-          halo_load(L, x, r.f[f], f >> 1, f & 1, c & 15, c >> 4, hx[q], hc[q]);
+          halo_load(L, x, xfr, r.f[f], f >> 1, f & 1, c & 15, c >> 4, hx[q], hc[q]);
       }
       if (MODE == APPLY_RESIDUAL && tid < 6) cmap[u][tid] = L.toCoarse[(size_t)ti * 6 + tid];
     };

@@ -257,11 +257,15 @@ __global__ void k_splat_scatter(const float* __restrict__ pos, int64_t n, SplatG
   }
 }
 
-// One CTA per value block: the minimum of the quantised squared distances of
-// the particles binned in its 27-block neighbourhood, in shared memory, then
-// finalised (or left raw) into the channel's pool.
+// One CTA per value block: the minimum squared distance of the particles
+// binned in its 27-block neighbourhood, in shared memory, then quantised and
+// finalised (or left raw) into the channel's pool.  The quantisation
+// round(d^2 / rScan^2 * 65535) is monotonic in d^2, so quantising the minimum
+// equals the reference's minimum of quantised values; the tile holds the
+// FP32 bits of d^2 (non-negative floats order like their bit patterns), +inf
+// where no particle reaches.
 template <int BSX>
-__global__ void __launch_bounds__(256) k_splat_blocks(SplatGeom g, const int* __restrict__ slot,
+__global__ void __launch_bounds__(256, 4) k_splat_blocks(SplatGeom g, const int* __restrict__ slot,
                                                       const int* __restrict__ vbid,
                                                       const int64_t* __restrict__ start,
                                                       const float4* __restrict__ sorted,
@@ -273,7 +277,8 @@ __global__ void __launch_bounds__(256) k_splat_blocks(SplatGeom g, const int* __
   const int bx = bid % g.nb[0], by = (bid / g.nb[0]) % g.nb[1],
             bz = bid / (g.nb[0] * g.nb[1]);
   const int B0[3] = {bx * BSX, by * BSX, bz * BSX};
-  for (int v = threadIdx.x; v < NV; v += blockDim.x) tile[v] = 65535u;
+  constexpr uint32_t FAR = 0x7f800000u;  // +inf
+  for (int v = threadIdx.x; v < NV; v += blockDim.x) tile[v] = FAR;
   __syncthreads();
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
@@ -316,21 +321,27 @@ __global__ void __launch_bounds__(256) k_splat_blocks(SplatGeom g, const int* __
                              __fsub_rn(p[2], 0.5f)};
         const int wx = c2[0] - c1[0] + 1, wy = c2[1] - c1[1] + 1;
         const int fx = i2[0] - i1[0] + 1, fy = i2[1] - i1[1] + 1;
-        // lanes over the (x, y) columns of the clipped box, each marching z
+        // lanes over the (x, y) columns of the clipped box, each marching the
+        // z range that can lie within rScan (a bound one voxel wider than
+        // the sphere's chord; the exact test decides inside it)
         for (int t = lane; t < wx * wy; t += 32) {
           const int ly = t / wx, ix = c1[0] + (t - ly * wx), iy = c1[1] + ly;
           const float dx = __fsub_rn((float)ix, p0[0]), dy = __fsub_rn((float)iy, p0[1]);
+          const float zr2 = g.distSqMax - (dx * dx + dy * dy);
+          if (zr2 < -0.5f) continue;
+          const float h = sqrtf(fmaxf(zr2, 0.f)) + 1.f;
+          const int z1 = max(c1[2], (int)ceilf(p0[2] - h)), z2 = min(c2[2], (int)floorf(p0[2] + h));
           uint32_t* col = tile + (ix - B0[0]) + BSX * (iy - B0[1]);
-          for (int iz = c1[2]; iz <= c2[2]; iz++) {
+          for (int iz = z1; iz <= z2; iz++) {
             const float dz = __fsub_rn((float)iz, p0[2]);
             const float distSq = splat_dist_sq(dx, dy, dz);
             if (distSq > g.distSqMax) continue;
             if (abortIdx != INT_MAX &&
                 ((iz - i1[2]) * fy + (iy - i1[1])) * fx + (ix - i1[0]) >= abortIdx)
               continue;
-            const uint32_t qv = splat_quantise(g, distSq);
             uint32_t* cell = col + BSX * BSX * (iz - B0[2]);
-            if (qv < *cell) atomicMin(cell, qv);
+            const uint32_t bits = __float_as_uint(distSq);
+            if (bits < *cell) atomicMin(cell, bits);
           }
         }
       }
@@ -339,7 +350,9 @@ __global__ void __launch_bounds__(256) k_splat_blocks(SplatGeom g, const int* __
   __syncthreads();
   uint32_t* out = reinterpret_cast<uint32_t*>(pool + (int64_t)s * NV);
   for (int v = threadIdx.x; v < NV / 2; v += blockDim.x) {
-    const uint32_t a = tile[2 * v], b = tile[2 * v + 1];
+    const uint32_t ta = tile[2 * v], tb = tile[2 * v + 1];
+    const uint32_t a = ta == FAR ? 65535u : splat_quantise(g, __uint_as_float(ta));
+    const uint32_t b = tb == FAR ? 65535u : splat_quantise(g, __uint_as_float(tb));
     const uint32_t lo = raw ? a : splat_finalise(g, a), hi = raw ? b : splat_finalise(g, b);
     out[v] = lo | (hi << 16);
   }

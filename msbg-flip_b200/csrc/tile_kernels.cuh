@@ -293,13 +293,26 @@ __global__ void __launch_bounds__(TS* TS) k_residual_restrict(LevelView L,
   }
 }
 
-// x += scale * P xc (liquid cells only; vectors VT, coarse vectors VC).
+// The x = 0 plane of cx of the TS^3 tiles tileBase, tileBase+1, ... (one CTA
+// per tile) into the packed layout of LevelView::cxf.
+template <int TS = 16>
+__global__ void __launch_bounds__(TS* TS) k_pack_cx_plane(const int64_t* __restrict__ tileOff,
+                                                          int tileBase,
+                                                          const float* __restrict__ cx,
+                                                          float* __restrict__ cxf) {
+  const int64_t off = tileOff[tileBase + blockIdx.x];
+  const int c = threadIdx.x;  // y + TS z
+  cxf[(off >> 4) + c] = cx[off + TS * c];
+}
+
+// x += scale * P xc (liquid cells only; vectors VT, coarse vectors VC).  On
+// 16^3 tiles the packed x faces xf (if given) are written too.
 template <int TS, typename VT, typename VC>
 __global__ void __launch_bounds__(TS* TS) k_prolong(LevelView L, const int* __restrict__ tiles,
                                                     VT* __restrict__ x,
                                                     const VC* __restrict__ xc,
                                                     const int64_t* __restrict__ coarseOff,
-                                                    float scale) {
+                                                    float scale, VT* __restrict__ xf) {
   constexpr int N = TS * TS * TS, NT = TS * TS;
   const int ti = tiles[blockIdx.x];
   const int64_t off = L.tileOff[ti];
@@ -336,6 +349,11 @@ __global__ void __launch_bounds__(TS* TS) k_prolong(LevelView L, const int* __re
       if (dv[p].z > 0.f) o.z = to_f(from_f<VT>(xv[p].z + scale * cv[p].z));
       if (dv[p].w > 0.f) o.w = to_f(from_f<VT>(xv[p].w + scale * cv[p].w));
       store4(x + off + e, o);
+      if (TS == 16 && xf) {
+        const int i = e % TS, j = (e / TS) % TS, k = e / (TS * TS);
+        if (i == 0) xf[xface_slot(off, 0, j, k)] = from_f<VT>(o.x);
+        if (i == TS - 4) xf[xface_slot(off, 1, j, k)] = from_f<VT>(o.w);
+      }
     }
   } else {
     for (int e = threadIdx.x; e < N; e += NT) {

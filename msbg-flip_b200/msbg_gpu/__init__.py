@@ -753,17 +753,23 @@ Context.splat = _ctx_splat
 Context.splat_device = _ctx_splat_device
 
 
-def splat_demo_particles(res3, n_base, seed=11, test_case=1):
-    """Seeded particles built the way the reference's demo builds its
-    bunny-of-bunnies (src/msbg_demo.cpp:339-385): n_base instances of a base
-    cloud of n_base points (a seeded stand-in for the PLY model: points near
-    an ellipsoid surface), instance i at 0.2 * sMax + 0.6 * sMax * b_i and
-    scaled by 0.01 * sMin (0.005 for test case 2), b the base cloud
-    normalised by its bounding box.  Returns float32 [n_base^2, 3]."""
+def splat_base_cloud(n_base, seed=11):
+    """A seeded stand-in for the demo's PLY model: n_base points near an
+    ellipsoid surface, float32 [n_base, 3]."""
     rng = np.random.default_rng(seed)
     v = rng.normal(size=(n_base, 3))
     v /= np.linalg.norm(v, axis=1, keepdims=True)
-    v = (v * np.array([1.0, 0.7, 0.5]) + 0.05 * rng.normal(size=(n_base, 3))).astype(np.float32)
+    return (v * np.array([1.0, 0.7, 0.5]) + 0.05 * rng.normal(size=(n_base, 3))).astype(np.float32)
+
+
+def splat_demo_particles(res3, n_base, seed=11, test_case=1, base=None):
+    """Seeded particles built the way the reference's demo builds its
+    bunny-of-bunnies (src/msbg_demo.cpp:339-385): n_base instances of a base
+    cloud of n_base points (splat_base_cloud, or `base`), instance i at
+    0.2 * sMax + 0.6 * sMax * b_i and scaled by 0.01 * sMin (0.005 for test
+    case 2), b the base cloud normalised by its bounding box.  Returns
+    float32 [n_base^2, 3]."""
+    v = splat_base_cloud(n_base, seed) if base is None else np.asarray(base, np.float32)
     bmin = v.min(0)
     span = (v.max(0) - bmin).max()
     b = ((v - bmin) * np.float32(1.0 / span)).astype(np.float32)
