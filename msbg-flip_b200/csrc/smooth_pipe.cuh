@@ -439,9 +439,13 @@ __global__ void __launch_bounds__(NTH, 1)
         const bool c1lo = dxof(1, sl) == 0;  // colour 1 holds the even cell
         const float lo = c1lo ? xv[1][sl] : xv[0][sl], hi = c1lo ? xv[0][sl] : xv[1][sl];
         store2(xg + TS * TS * sl, lo, hi);
-        // the tile's own x faces: x = 0 from ip = 0, x = 15 from ip = 7
-        if (xf && (ip == 0 || ip == 7))
-          xf[xface_slot(rc.off, ip == 7, jj, 2 * kp + sl)] = from_f<VT>(ip == 0 ? lo : hi);
+      }
+      // the tile's own x faces, read back from the stage (final after the
+      // last half sweep's barrier) so each warp writes whole lines
+      if (xf && tid < 2 * TS * TS) {
+        const int side = tid >> 8, c = tid & 255;
+        xf[xface_slot(rc.off, side, 0, 0) + c] =
+            from_f<VT>(X[xpad(side * (TS - 1) + TS * c)]);
       }
     }
     // 5: next tile's arrays landed -> its halo sums
