@@ -307,7 +307,7 @@ int msbg::ps::pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
     bool has16 = false;
     for (const auto& P : L.passes) has16 |= P.ts == 16 && P.count > 0;
     if (has16 && m + 1 < S.H.levels.size()) {
-      const size_t nf = (size_t)xface_len(L.nCells);
+      const size_t nf = (size_t)xface_words(L.nCells);
       MSBG_CUDA_TRY(ctx, D->cxf.ensure(sizeof(float) * (nf / 2 + 256)));
       MSBG_CUDA_TRY(ctx, D->xf.ensure(sizeof(float) * nf));
       MSBG_CUDA_TRY(ctx, cudaMemsetAsync(D->xf.p, 0, sizeof(float) * nf, st));
@@ -410,10 +410,17 @@ int run_pcg(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const VT* bin, double t
   cudaMemcpyAsync(r, bin, sizeof(VT) * n, cudaMemcpyDeviceToDevice, st);
   k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(bin, bin, n, part);
   k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_BB);
+  // packed x faces of the direction d, kept by the same updates as d from
+  // the faces of z that the V-cycle leaves (d = z, then d = z + beta d)
+  VT* zf = R.template faces<VT>(0);
+  const int64_t nf = xface_words(n);
+  if (zf) MSBG_CUDA_TRY(ctx, S.df.ensure(sizeof(float) * nf));
+  VT* df = zf ? S.df.as<VT>() : nullptr;
   R.vcycle(0, z, r);
   k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
   k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHO);
   cudaMemcpyAsync(d, z, sizeof(VT) * n, cudaMemcpyDeviceToDevice, st);
+  if (df) cudaMemcpyAsync(df, zf, sizeof(VT) * nf, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
   R.launches += 4;
   MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
@@ -429,7 +436,7 @@ int run_pcg(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const VT* bin, double t
   }
   auto iteration = [&]() {
     R.launches += 6;  // finalize x3, axpy_norm, dot, update_d
-    int nt = R.matvec_dot(d, q, part);
+    int nt = R.matvec_dot(d, q, part, df);
     k_finalize<<<1, 1024, 0, st>>>(part, nt, sc, FIN_DQ_ALPHA);
     k_axpy_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x, r, d, q, n, sc, part);
     k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
@@ -437,6 +444,10 @@ int run_pcg(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const VT* bin, double t
     k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
     k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHONEW_BETA);
     k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, n, sc);
+    if (df) {
+      k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(df, zf, nf, sc);
+      R.launches++;
+    }
     cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
   };
   if (useGraph && !exec) {

@@ -42,6 +42,10 @@ __host__ __device__ __forceinline__ int64_t xface_slot(int64_t off, int side, in
   return (off >> 3) + (side ? 256 : 0) + y + 16 * z;
 }
 __host__ __device__ __forceinline__ int64_t xface_len(int64_t nCells) { return nCells / 8 + 512; }
+// the same rounded up to whole groups of 4 (the vector kernels' unit)
+__host__ __device__ __forceinline__ int64_t xface_words(int64_t nCells) {
+  return (xface_len(nCells) + 3) & ~(int64_t)3;
+}
 
 __host__ __device__ __forceinline__ int tidx(int ts, int i, int j, int k) { return i + ts * (j + ts * k); }
 

@@ -58,6 +58,7 @@ struct Solver {
   int cnnChunk = 0;
   bool haveX64 = false;  // x64 holds the solution of the last refined solve
   DeviceBuffer packTiles, packBuf;  // device-side packing into the block layout
+  DeviceBuffer df;                  // packed x faces of the PCG direction d0
 };
 
 // Dynamic shared-memory limits of the kernels a level-0 vector type needs
@@ -177,7 +178,8 @@ struct Runner {
   // q = A d with partial d.q (level 0); returns the number of partials.
   // Passes are contiguous tile ranges of one tile size; 16^3 passes go
   // through the pipelined kernel, the others through the per-tile kernel.
-  int matvec_dot(const VT* d, VT* q, double* partial) {
+  // df: packed x faces of d (nullptr: strided halo reads).
+  int matvec_dot(const VT* d, VT* q, double* partial, const VT* df = nullptr) {
     const Level& L = S.H.levels[0];
     int off = 0;
     for (const auto& P : L.passes) {
@@ -186,7 +188,7 @@ struct Runner {
         const int grid = std::min(P.count, numSMs);
         k_apply_pipe16<APPLY_MATVEC, VT, VT, pipe::NT_APPLY><<<grid, pipe::NT_APPLY, pipe::SMEM, st>>>(
             S.views[0], P.start, P.count, d, nullptr, q, nullptr, nullptr, partial + off, err,
-            nullptr);
+            S.views[0].cxf ? df : nullptr);
         off += grid;
       } else {
         const int* lst = passList(0) + P.start;
