@@ -495,7 +495,7 @@ int residual64(msbg_gpu_ctx* ctx, Solver& S, Runner<VT>& R, const float* b, floa
   int off = 0;
   for (const auto& g : L.groups) {
     const int* lst = S.dev[0]->groupTiles.as<int>() + g.start;
-    TS_DISPATCH(g.ts, (k_residual64<T><<<g.count, T * T, 0, st>>>(
+    TS_DISPATCH(g.ts, (k_residual64<T><<<g.count, T * T * res64_split<T>(), 0, st>>>(
                           S.views[0], lst, S.x64.as<double>(), b, r32, part + off)));
     off += g.count;
     R.launches++;

@@ -7,29 +7,34 @@
 // correction to x in FP64.  This is what lets the true residual reach 1e-6
 // where an FP32 iterate cannot represent it.
 
-// r32 = b - A x64 on MG level 0 (one CTA per tile, thread (i,j) owns the z
-// column), per-CTA partial |r|^2 in FP64.
+// r32 = b - A x64 on MG level 0 (one CTA per tile; thread (i,j,h) owns the
+// h-th part of the z column (i,j): 16^3 tiles in two halves, so a CTA has
+// 512 threads and more loads in flight), per-CTA partial |r|^2 in FP64.
 template <int TS>
-__global__ void __launch_bounds__(TS* TS) k_residual64(LevelView L, const int* __restrict__ tiles,
-                                                       const double* __restrict__ x,
-                                                       const float* __restrict__ b,
-                                                       float* __restrict__ r,
-                                                       double* __restrict__ partial) {
-  constexpr int N = TS * TS * TS, NT = TS * TS;
+__host__ __device__ constexpr int res64_split() { return TS == 16 ? 2 : 1; }
+template <int TS>
+__global__ void __launch_bounds__(TS* TS* res64_split<TS>())
+    k_residual64(LevelView L, const int* __restrict__ tiles, const double* __restrict__ x,
+                 const float* __restrict__ b, float* __restrict__ r,
+                 double* __restrict__ partial) {
+  constexpr int N = TS * TS * TS, NF = TS * TS, SPLIT = res64_split<TS>(), NT = NF * SPLIT;
+  constexpr int ZC = TS / SPLIT;  // cells of a thread's z column part
   __shared__ double xs[N];
-  __shared__ double gs[6][NT];
+  __shared__ double gs[6][NF];
   const int ti = tiles[blockIdx.x];
   const int64_t off = L.tileOff[ti];
-  const int t = threadIdx.x, i = t % TS, j = t / TS;
+  const int t = threadIdx.x, i = t % TS, j = (t / TS) % TS, h = t / NF;
   for (int e = t; e < N; e += NT) xs[e] = x[off + e];
-#pragma unroll
-  for (int f = 0; f < 6; f++) gs[f][t] = ghost_sum<double, double>(L, x, ti, TS, f >> 1, f & 1, i, j);
+  for (int q = t; q < 6 * NF; q += NT) {
+    const int f = q / NF, c = q % NF;
+    gs[f][c] = ghost_sum<double, double>(L, x, ti, TS, f >> 1, f & 1, c % TS, c / TS);
+  }
   __syncthreads();
   const float* cx = L.cx + off;
   const float* cy = L.cy + off;
   const float* cz = L.cz + off;
   double acc = 0;
-  for (int k = 0; k < TS; k++) {
+  for (int k = h * ZC; k < (h + 1) * ZC; k++) {
     const int e = tidx(TS, i, j, k);
     const double dg = L.diag[off + e];
     double rv = 0;
