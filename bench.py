@@ -605,9 +605,9 @@ def bench_mgpcg(args):
         c["band"] = PS_CFG["band"] * args.res / PS_CFG["res"]
     ctx = msbg_gpu.Context(local)
     scene = ps_scene(c)
-    # the caller's per-cell arrays (flags, lower-face coefficients, rhs):
-    # input generation, outside every timed region
-    arrays = scene.arrays()
+    # the caller's per-cell arrays (flags, lower-face coefficients, rhs) in
+    # page-locked host memory: input generation, outside every timed region
+    arrays = scene.arrays(pinned=True)
 
     def prepare_arrays():
         ctx.pressure_prepare_arrays(c["res"], c["bsx0"], c["n_levels"], scene.block_levels,
@@ -642,8 +642,9 @@ def bench_mgpcg(args):
     # per-cell arrays (copy to the GPU, hierarchy built there), the same
     # solve, download of the pressure; averaged over 3 calls
     n_e2e = 3
-    # the caller's pressure array (written in place, as CH_PRESSURE is)
-    out = np.zeros_like(ctx.pressure_download())
+    # the caller's pressure array (written in place, as CH_PRESSURE is), in
+    # page-locked host memory like the inputs
+    out = msbg_gpu.pinned_empty(ctx.pressure_download().shape, np.float32)
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
@@ -696,8 +697,8 @@ def bench_mgpcg(args):
                         "h2d_bytes_per_step": int(st2.h2dBytes),
                         "d2h_bytes_per_step": int(out.nbytes),
                         "seconds_per_step": e2e_s, "calls": n_e2e,
-                        "path": "msbg_gpu_pressure_prepare_arrays (host arrays; hierarchy "
-                                "built on the GPU) + msbg_gpu_pressure_solve + "
+                        "path": "msbg_gpu_pressure_prepare_arrays (pinned host arrays; "
+                                "hierarchy built on the GPU) + msbg_gpu_pressure_solve + "
                                 "msbg_gpu_pressure_download",
                         "prepare_s": st2.prepareSeconds, "build_s": st2.buildSeconds,
                         "callbacks": {"value": fluid * inf_cb.iterations / e2e_cb_s / 1e9 * ws,

@@ -89,11 +89,23 @@ PinnedStaging& staging() {
   return stg;
 }
 
+// True when p points into page-locked host memory (cudaMallocHost,
+// cudaHostRegister, a pinned torch tensor): the DMA then reads or writes it
+// directly, with no staging copy.
+bool host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // pageable memory may report an error on older drivers
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 cudaError_t copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
   PinnedStaging& stg = staging();
   int dev = 0;
   cudaGetDevice(&dev);
-  if (bytes < (8u << 20) || !stg.ready(dev))
+  if (bytes < (8u << 20) || host_pinned(src) || !stg.ready(dev))
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
   for (size_t o = 0, c = 0; o < bytes; o += PinnedStaging::CH, c++) {
     const int k = (int)(c & 1);
@@ -126,7 +138,7 @@ cudaError_t copy_d2h(void* dst, const void* src, size_t bytes, cudaStream_t st) 
   PinnedStaging& stg = staging();
   int dev = 0;
   cudaGetDevice(&dev);
-  if (bytes < (8u << 20) || !stg.ready(dev)) {
+  if (bytes < (8u << 20) || host_pinned(dst) || !stg.ready(dev)) {
     cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
     return e != cudaSuccess ? e : cudaStreamSynchronize(st);
   }

@@ -232,7 +232,11 @@ Solver* find_solver(msbg_gpu_ctx* ctx);
 int pressure_prepare(msbg_gpu_ctx* ctx, const msbg_topo_desc* topo,
                      const msbg_pressure_callbacks* cb, const ArrayInput* arr);
 
-// Host <-> device copies through pinned staging buffers (pressure.cu).
+// True when p points into page-locked host memory (pressure.cu).
+bool host_pinned(const void* p);
+
+// Host <-> device copies through pinned staging buffers (pressure.cu); a
+// page-locked host side is copied directly.
 cudaError_t copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t st);
 cudaError_t copy_d2h(void* dst, const void* src, size_t bytes, cudaStream_t st);
 

@@ -354,13 +354,16 @@ class PressureScene:
     def packed_size(self):
         return int(sum((self.bsx0 >> int(l)) ** 3 for l in self.block_levels))
 
-    def arrays(self):
+    def arrays(self, pinned=False):
         """The scene as the per-cell arrays of Context.pressure_prepare_arrays:
-        (flags uint16, [faceX, faceY, faceZ] float32, rhs float32)."""
+        (flags uint16, [faceX, faceY, faceZ] float32, rhs float32); pinned:
+        in page-locked host memory (the prepare then copies them to the GPU
+        by DMA straight from there)."""
         n = self.packed_size()
-        flags = np.empty(n, np.uint16)
-        face = [np.empty(n, np.float32) for _ in range(3)]
-        rhs = np.empty(n, np.float32)
+        alloc = pinned_empty if pinned else np.empty
+        flags = alloc(n, np.uint16)
+        face = [alloc(n, np.float32) for _ in range(3)]
+        rhs = alloc(n, np.float32)
         rc = self._L.msbg_scene_pressure_arrays(self.h, _p(flags, C.c_uint16),
                                                 *[_p(f, C.c_float) for f in face],
                                                 _p(rhs, C.c_float))
@@ -778,3 +781,13 @@ def splat_demo_particles(res3, n_base, seed=11, test_case=1, base=None):
     centres = (np.float32(smax * 0.2) + np.float32(0.6) * (np.float32(smax) * b)).astype(np.float32)
     pos = centres[:, None, :] + scale * b[None, :, :]
     return pos.reshape(-1, 3).astype(np.float32)
+
+
+def pinned_empty(shape, dtype):
+    """An uninitialised numpy array in page-locked host memory (a pinned torch
+    tensor's storage; the array keeps the tensor alive)."""
+    import torch
+    dt = np.dtype(dtype)
+    t = torch.empty(int(np.prod(shape)) * dt.itemsize, dtype=torch.uint8, pin_memory=True)
+    a = t.numpy().view(dt).reshape(shape)
+    return a

@@ -97,3 +97,29 @@ def test_device_build_reports_an_isolated_liquid_cell():
         assert ctx.pressure_solve(tol=1e-6, maxRefine=30).status == 0
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("res,bsx0,nl,band,dbc", CASES[:2] + CASES[3:])
+def test_pinned_arrays_build_the_same_bits(res, bsx0, nl, band, dbc):
+    """The caller's arrays in page-locked host memory (the e2e bench keeps
+    them there) give the same operator and solve as pageable ones, bit for
+    bit, and a pinned output buffer receives the same pressure."""
+    scene = msbg_gpu.PressureScene(res, bsx0, nl, band=band, seed=9)
+    out = []
+    for pinned in (False, True):
+        arrays = scene.arrays(pinned=pinned)
+        ctx = msbg_gpu.Context(0)
+        try:
+            prepared(ctx, scene, arrays, False, dbc)
+            info = ctx.pressure_solve(tol=1e-6, maxRefine=30)
+            p = (msbg_gpu.pinned_empty(ctx.pressure_download().shape, np.float32)
+                 if pinned else None)
+            out.append((level_count(ctx), ctx.diagonal(0), ctx.pressure_download(rhs=True),
+                        info.iterations, ctx.pressure_download(fp64=True),
+                        ctx.pressure_download(out=p)))
+        finally:
+            ctx.close()
+    a, b = out
+    assert a[0] == b[0] and a[3] == b[3]
+    for u, v in zip(a[1:3] + a[4:], b[1:3] + b[4:]):
+        assert np.array_equal(u, v)
