@@ -164,6 +164,17 @@ int upload_channel_t(msbg_gpu_ctx* ctx, int chan, int level, const int8_t* kind,
     }
   }
   ch->nValue = s;
+  {
+    // an earlier channel of this id hands over its allocations (the stream
+    // may still read them: it finishes first); it is gone from here on, so a
+    // failure below leaves no channel behind
+    auto old = ctx->channels.find(chan);
+    if (old != ctx->channels.end()) {
+      MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+      ch->reuse(*old->second);
+      ctx->channels.erase(old);
+    }
+  }
   const size_t nv = (size_t)ch->bsx * ch->bsx * ch->bsx;
   const size_t bytes = sizeof(T) * nv * (size_t)s;
   MSBG_CUDA_TRY(ctx, ch->pool.ensure(bytes));

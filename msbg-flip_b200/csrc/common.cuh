@@ -49,6 +49,15 @@ struct DeviceBuffer {
   }
   template <typename T>
   T* as() const { return reinterpret_cast<T*>(p); }
+  // takes over o's allocation (o is left empty)
+  void adopt(DeviceBuffer& o) {
+    if (&o == this) return;
+    release();
+    p = o.p;
+    bytes = o.bytes;
+    o.p = nullptr;
+    o.bytes = 0;
+  }
 };
 
 // One uploaded channel at one resolution level: FP32 or 16-bit render
@@ -65,6 +74,13 @@ struct Channel {
   DeviceBuffer pool;           // [nValue][bsx^3] float or uint16_t
   DeviceBuffer xfaces;         // [nValue][2][bsx^2]: the x = 0 and x = bsx-1 planes
   DeviceBuffer slot;           // [nb] int
+  // a channel that replaces an earlier one of the same id keeps its device
+  // allocations (no cudaMalloc / cudaFree per upload when the sizes fit)
+  void reuse(Channel& old) {
+    pool.adopt(old.pool);
+    xfaces.adopt(old.xfaces);
+    slot.adopt(old.slot);
+  }
 };
 
 }  // namespace msbg

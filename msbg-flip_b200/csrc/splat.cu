@@ -488,6 +488,14 @@ int splat_run(msbg_gpu_ctx* ctx, int chan, const float* pos, int64_t n,
 
   // the channel: value blocks at level 0, const blocks at 0 (empty) / 65535
   auto ch = std::make_unique<Channel>();
+  {
+    auto old = ctx->channels.find(chan);
+    if (old != ctx->channels.end()) {  // its allocations are reused; it is gone
+      MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+      ch->reuse(*old->second);
+      ctx->channels.erase(old);
+    }
+  }
   ch->level = 0;
   ch->bsx = bsx;
   ch->dtype = MSBG_U16;

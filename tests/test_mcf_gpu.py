@@ -124,3 +124,27 @@ def test_gpu_constant_field_is_fixed_point(gpu_ctx):
     (out,) = run_gpu(gpu_ctx, (res,) * 3, bsx, kind, vals, np.arange(8, dtype=np.int32), 6,
                      ev=1.25, fv=1.25)
     np.testing.assert_array_equal(out, vals)
+
+
+def test_reupload_reuses_and_resizes_the_channel(gpu_ctx):
+    """A channel uploaded again under the same id takes over the earlier
+    allocations (growing them when the new one is larger) and holds exactly
+    the new data; an upload rejected for its arguments leaves the earlier
+    channel as it was."""
+    res, bsx = 128, 16
+    gpu_ctx.set_topology(res, res, res, bsx)
+    for n_spheres, seed in ((2, 1), (12, 2), (1, 3)):  # small, larger, smaller
+        kind, vals = msbg_gpu.sphere_sdf_scene(res, bsx, n_spheres=n_spheres, rmin=6, rmax=24,
+                                               seed=seed)
+        upd = np.nonzero(kind == 1)[0].astype(np.int32)
+        gpu_ctx.upload_channel(3, 0, kind, vals, 4.0, -4.0)
+        assert np.array_equal(gpu_ctx.download_channel(3, np.empty_like(vals)), vals)
+        gpu_ctx.apply_channel_pde_mcf(3, upd, 2, 0.1)
+        got = gpu_ctx.download_channel(3, np.empty_like(vals))
+        ref = oracle.mcf_oracle((res // bsx,) * 3, bsx, kind, vals, upd, 2, 0.1)
+        ok, err = tol_ok(got, ref)
+        assert ok, err
+    bad = np.full(len(kind), 9, np.int8)
+    with pytest.raises(msbg_gpu.MsbgError):
+        gpu_ctx.upload_channel(3, 0, bad, vals, 4.0, -4.0)
+    assert np.array_equal(gpu_ctx.download_channel(3, np.empty_like(got)), got)
