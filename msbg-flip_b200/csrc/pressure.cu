@@ -823,12 +823,19 @@ int solve_reliable(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gp
     R.launches += 6;
     return MSBG_OK;
   };
+  // packed x faces of d, kept from the V-cycle's faces of z (not with the
+  // correction, which changes z after the V-cycle)
+  float* zf = corr ? nullptr : R.template faces<float>(0);
+  const int64_t nf = xface_words(n);
+  if (zf) MSBG_CUDA_TRY(ctx, S.df.ensure(sizeof(float) * nf));
+  float* df = zf ? S.df.as<float>() : nullptr;
   // z = B r, rho = r.z, d = z
   rc = precond(false);
   if (rc) return rc;
   k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
   k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHO);
   cudaMemcpyAsync(d, z, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+  if (df) cudaMemcpyAsync(df, zf, sizeof(float) * nf, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(S.hScal, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
   R.launches += 4;
   MSBG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
@@ -845,7 +852,7 @@ int solve_reliable(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gp
   }
   auto part1 = [&]() {
     R.launches += 3;
-    const int nt = R.matvec_dot(d, q, part);
+    const int nt = R.matvec_dot(d, q, part, df);
     k_finalize<<<1, 1024, 0, st>>>(part, nt, sc, corr ? FIN_FCG_DQ_ALPHA : FIN_DQ_ALPHA);
     k_axpy64_norm<<<VEC_GRID, VEC_BLOCK, 0, st>>>(x64, r, d, q, n, sc, part);
     k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RR);
@@ -860,6 +867,10 @@ int solve_reliable(msbg_gpu_ctx* ctx, Solver& S, Runner<float>& R, const msbg_gp
       k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(r, z, n, part);
       k_finalize<<<1, 1024, 0, st>>>(part, VEC_GRID, sc, FIN_RHONEW_BETA);
       k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(d, z, n, sc);
+      if (df) {
+        k_update_d<<<VEC_GRID, VEC_BLOCK, 0, st>>>(df, zf, nf, sc);
+        R.launches++;
+      }
     } else {
       // beta = -(z.q)/(d.q); d = z + beta d; rho = d.r for the next alpha
       k_dot<<<VEC_GRID, VEC_BLOCK, 0, st>>>(z, q, n, part);
