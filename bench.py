@@ -553,11 +553,14 @@ def splat_line(args, ctx):
         ctx.splat_device(7, dpos.data_ptr(), len(pos))
     dt_dev = (time.perf_counter() - t0) / steps
     del dpos
-    out = np.empty(nval * bsx ** 3, np.uint16)
-    ctx.splat(7, pos)
+    # end to end: positions in, the channel out, both in page-locked host memory
+    hpos = msbg_gpu.pinned_empty(pos.shape, np.float32)
+    hpos[:] = pos
+    out = msbg_gpu.pinned_empty((nval * bsx ** 3,), np.uint16)
+    ctx.splat(7, hpos)
     t0 = time.perf_counter()
     for _ in range(steps):
-        ctx.splat(7, pos)
+        ctx.splat(7, hpos)
         ctx.download_channel_u16(7, out)
     dt_e2e = (time.perf_counter() - t0) / steps
     line = {"workload": splat_workload_name(c), "particles": int(len(pos)),

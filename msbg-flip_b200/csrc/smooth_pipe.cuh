@@ -625,8 +625,6 @@ __global__ void __launch_bounds__(NTH, 1)
       const float* CY = X + 4 * N;
       const float* CZ = X + 5 * N;
       const float(*gs)[TS * TS] = gsb[s];
-      float* Y = X + 2 * N;  // results overwrite the a_ii array in place (each
-                             // thread reads its own a_ii before writing it)
       const int k0 = ZC * kh;
       float xm = k0 > 0 ? X[tidx(TS, i, j, k0 - 1)] : 0.f;
       float xc = X[tidx(TS, i, j, k0)];
@@ -660,30 +658,36 @@ __global__ void __launch_bounds__(NTH, 1)
 #pragma unroll
         for (int kk = 0; kk < ZC; kk++) y[rc.off + tidx(TS, i, j, k0 + kk)] = from_f<VT>(yv[kk]);
       } else {
-        __syncthreads();  // every thread has read its D / neighbours before Y is written
-#pragma unroll
-        for (int kk = 0; kk < ZC; kk++) Y[tidx(TS, i, j, k0 + kk)] = yv[kk];
-        __syncthreads();
+        // the restriction from the registers: a warp holds rows j, j+1 of 16
+        // cells, so the x and y partners of a 2 x 2 x 2 group are lanes ^1
+        // and ^16, and the z partner the thread's next value; the sum keeps
+        // the order x, then y, then z of the group's eight cells
+        static_assert(ZC % 2 == 0 && NTH / (TS * TS) * ZC == TS, "z pairs inside a thread");
         const int* tc = cmap[s];
         const int ct = tc[0];
         if (ct >= 0) {
           VC* dst = bc + coarseOff[ct];
           const int ox = tc[1], oy = tc[2], oz = tc[3], cts = tc[5];
           if (tc[4]) {
-            constexpr int H = TS / 2;
-            for (int c = tid; c < H * H * H; c += NTH) {  // 512 coarse cells
-            const int ci = c % H, cj = (c / H) % H, ck = c / (H * H);
-            const int e = tidx(TS, 2 * ci, 2 * cj, 2 * ck);
-            const float sum = Y[e] + Y[e + 1] + Y[e + TS] + Y[e + TS + 1] + Y[e + TS * TS] +
-                              Y[e + TS * TS + 1] + Y[e + TS * TS + TS] +
-                              Y[e + TS * TS + TS + 1];
-            dst[tidx(cts, ox + ci, oy + cj, oz + ck)] = from_f<VC>(sum);
+#pragma unroll
+            for (int zz = 0; zz < ZC; zz += 2) {
+              const float a000 = yv[zz], a001 = yv[zz + 1];
+              const float a100 = __shfl_xor_sync(0xffffffffu, a000, 1);
+              const float a101 = __shfl_xor_sync(0xffffffffu, a001, 1);
+              const float a010 = __shfl_xor_sync(0xffffffffu, a000, 16);
+              const float a011 = __shfl_xor_sync(0xffffffffu, a001, 16);
+              const float a110 = __shfl_xor_sync(0xffffffffu, a100, 16);
+              const float a111 = __shfl_xor_sync(0xffffffffu, a101, 16);
+              if (!(i & 1) && !(j & 1)) {
+                const float sum = a000 + a100 + a010 + a110 + a001 + a101 + a011 + a111;
+                dst[tidx(cts, ox + (i >> 1), oy + (j >> 1), oz + ((k0 + zz) >> 1))] =
+                    from_f<VC>(sum);
+              }
             }
           } else {
-            for (int e = tid; e < N; e += NTH) {
-              const int ii = e % TS, jj = (e / TS) % TS, kk = e / (TS * TS);
-              dst[tidx(cts, ox + ii, oy + jj, oz + kk)] = from_f<VC>(Y[e]);
-            }
+#pragma unroll
+            for (int kk = 0; kk < ZC; kk++)
+              dst[tidx(cts, ox + i, oy + j, oz + k0 + kk)] = from_f<VC>(yv[kk]);
           }
         }
       }
