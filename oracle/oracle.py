@@ -89,6 +89,9 @@ def integ():
         L.integ_mcf_f32.argtypes = [C.c_int] * 4 + [i8, C.c_float, C.c_float, f32,
                                                     C.POINTER(C.c_int), C.c_int, C.c_int, C.c_float,
                                                     C.c_int]
+        L.integ_splat.restype = C.c_int
+        L.integ_splat.argtypes = [C.c_int] * 4 + [C.c_void_p, C.c_int64, C.c_int, C.c_float,
+                                                  C.c_void_p, C.c_void_p]
         L.integ_pressure.restype = C.c_int
         L.integ_pressure.argtypes = [C.c_void_p] * 5 + [C.c_float, C.c_int, C.POINTER(C.c_int),
                                                         C.POINTER(C.c_int), C.POINTER(C.c_double)]
@@ -118,6 +121,19 @@ def integ_mcf_f32(res3, bsx, kind, values, update, num_iter, dt, clamp01=False, 
     rc = L.integ_mcf_f32(*res3, bsx, _p(k, C.c_int8), empty_val, full_val, _p(v, C.c_float),
                          _p(u, C.c_int), len(u), num_iter, dt, int(bool(clamp01)))
     return rc, v
+
+
+def integ_splat(res3, bsx, pos, num_iter, dt):
+    """INTEGRATION.md's splat snippet on a reference grid without blocks;
+    returns (status, active block flags, values of the active blocks)."""
+    L = integ()
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    nb = (res3[0] // bsx) * (res3[1] // bsx) * (res3[2] // bsx)
+    act = np.zeros(nb, np.int8)
+    vals = np.zeros(nb * bsx ** 3, np.uint16)
+    rc = L.integ_splat(*res3, bsx, p.ctypes.data, len(p), num_iter, dt, act.ctypes.data,
+                       vals.ctypes.data)
+    return rc, act, vals[: int(act.sum()) * bsx ** 3]
 
 
 def integ_pressure(ref_handle, scene, tol, max_iter):

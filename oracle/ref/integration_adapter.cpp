@@ -57,6 +57,15 @@ int run_pressure(MultiresSparseGrid* msbg, const FlipPressureCallbacks& cb,
   return rc;
 }
 
+// INTEGRATION.md "splat": the demo's splat and smoothing from particle
+// positions into the render-density channel; the active blocks out.
+int run_splat(MultiresSparseGrid* msbg, int chan, const std::vector<float>& pos, int nIterPde,
+              float dt, std::vector<int>& activeOut) {
+#include "integration_splat.inc"
+  activeOut = activeBlocks;
+  return rc;
+}
+
 }  // namespace
 
 // The demo's call on a single-level render-density grid: kind / values as in
@@ -106,5 +115,25 @@ extern "C" int integ_pressure(void* refHandle, CellFlags (*cellType)(void*, int,
   if (status) *status = info.status;
   if (iterations) *iterations = info.iterations;
   if (relRes) *relRes = info.relResidual;
+  return rc;
+}
+
+// The splat snippet on a single-level grid of sx*sy*sz voxels in bsx^3 blocks
+// with no blocks yet: active[nBlocks] receives 1 for the blocks it made value
+// blocks, values their voxels after the smoothing (packed in bid order, room
+// for every block).  Returns the snippet's status.
+extern "C" int integ_splat(int sx, int sy, int sz, int bsx, const float* pos, int64_t n,
+                           int nIterPde, float dt, int8_t* active, uint16_t* values) {
+  const int nb = (sx / bsx) * (sy / bsx) * (sz / bsx);
+  std::vector<int8_t> none(nb, 0);
+  void* m = ref_grid_create_u16(sx, sy, sz, bsx, none.data(), 0, 65535, nullptr);
+  if (!m) return -1;
+  std::vector<float> p(pos, pos + 3 * n);
+  std::vector<int> act;
+  const int rc = run_splat((MultiresSparseGrid*)m, CH_UINT16_1, p, nIterPde, dt, act);
+  std::memset(active, 0, nb);
+  for (int b : act) active[b] = 1;
+  ref_grid_read_u16(m, active, values);
+  ref_grid_destroy(m);
   return rc;
 }

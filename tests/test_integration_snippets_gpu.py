@@ -6,6 +6,8 @@ objects and compared with the reference routines they replace:
     test_mcf_u16_gpu (at most 2 quanta, at most 0.2 % of the voxels differ);
   - "mcf_f32": against applyChannelPdeFast<float>, |gpu - ref| <= 1e-5
     max(1, |ref|) per voxel;
+  - "splat": the demo's splat and smoothing from particle positions,
+    against the reference demo's splat smoothed by the reference;
   - "pressure": on a grid the reference prepared (every block at level 0,
     where the two operators coincide), the snippet's solution in CH_PRESSURE
     leaves a relative residual <= 1e-5 in the reference's own operator and
@@ -68,3 +70,25 @@ def test_pressure_snippet_solves_the_reference_system():
         R.close()
     xo, _, _, _ = oracle.pressure_oracle(scene, tol=1e-12)
     assert np.linalg.norm(p - xo) <= 1e-5 * np.linalg.norm(xo)
+
+
+def test_splat_snippet_matches_reference_demo():
+    """"splat": the demo's particle splatting and smoothing through the
+    snippet, on a reference grid without blocks, against the reference demo's
+    own output (tests/golden/splat_demo_b16.npz) smoothed by the reference's
+    applyChannelPdeFast<uint16_t> with the demo's arguments (5 iterations, dt
+    0.05, the [0, 1] clamp)."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "splat_demo_b16.npz"))
+    res3, bsx = tuple(int(v) for v in g["res"]), int(g["bsx"])
+    nb = (res3[0] // bsx) * (res3[1] // bsx) * (res3[2] // bsx)
+    kind = np.full(nb, 2, np.int8)
+    kind[g["blocks"]] = 1
+    ref, _ = oracle.mcf_reference_u16(res3, bsx, kind, g["final"], g["blocks"], 5, 0.05,
+                                      clamp01=True, empty_val=0, full_val=65535)
+    rc, act, got = oracle.integ_splat(res3, bsx, g["pos"], 5, 0.05)
+    assert rc == 0
+    assert np.array_equal(np.nonzero(act)[0], g["blocks"])
+    d = np.abs(got.astype(np.int64) - ref.astype(np.int64))
+    assert (ref != g["final"]).any()
+    assert d.max() <= 2 and (d > 0).mean() <= 2e-3, (int(d.max()), float((d > 0).mean()))
