@@ -491,6 +491,79 @@ def flip_line(args, ctx):
     return out
 
 
+def flip_mr_line(args, ctx):
+    """G2P on a 512^3 grid of 16^3 blocks with 3 levels (level 0 within 7
+    blocks of a seeded centre, level 1 within 12, level 2 beyond), seeded MAC
+    velocity channels and 16 M seeded particles spread over the grid: the
+    interpolation of interpVec3MSBG with its fine/coarse blend, timed over
+    --steps calls through the C ABI from host arrays and on particles resident
+    in device memory (CUDA events on the context's stream); the CPU
+    restatement times a sample of the particles."""
+    import msbg_gpu
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    res, bsx, nl, n_part, alpha = 512, 16, 3, 16_000_000, 0.95
+    nb = res // bsx
+    b = np.arange(nb ** 3)
+    bx, by, bz = b % nb, (b // nb) % nb, b // (nb * nb)
+    r = np.sqrt((bx - 12.5) ** 2 + (by - 15.5) ** 2 + (bz - 17.5) ** 2)
+    lev = np.where(r < 7, 0, np.where(r < 12, 1, 2)).astype(np.int32)
+    ctx.set_topology(res, res, res, bsx, nl, lev)
+    n = msbg_gpu.packed_voxels(bsx, lev)
+    rng = np.random.default_rng(21)
+    vel = rng.standard_normal(3 * n).astype(np.float32)
+    old = rng.standard_normal(3 * n).astype(np.float32)
+    ctx.flip_mr_channel(msbg_gpu.FLIP_VEL, vel)
+    ctx.flip_mr_channel(msbg_gpu.FLIP_VEL_OLD, old)
+    p = np.zeros(n_part, msbg_gpu.FLIP_PARTICLE)
+    p["pos"] = rng.uniform(0, res, (n_part, 3)).astype(np.float32)
+    p["vel"] = rng.standard_normal((n_part, 3)).astype(np.float32)
+    steps = max(args.steps, 1)
+    out = {"grid": f"{res}^3, {bsx}^3 blocks, {nl} levels ({np.bincount(lev).tolist()} blocks "
+                   "per level)", "particles": n_part, "packed_voxels": n}
+    q = p.copy()
+    ctx.flip_g2p_mr(q, alpha)  # builds the distance channel once
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ctx.flip_g2p_mr(q, alpha)
+    dt = (time.perf_counter() - t0) / steps
+    out["g2p_host_particles"] = {"ms": dt * 1e3, "mparticles_s": n_part / dt / 1e6,
+                                 "h2d_bytes": 28 * n_part, "d2h_bytes": 28 * n_part}
+    dev = torch.from_numpy(p.view(np.uint8).copy()).to(f"cuda:{ctx.device}")
+    st = torch.cuda.ExternalStream(ctx.stream(), device=f"cuda:{ctx.device}")
+    ctx.flip_g2p_mr_device(dev.data_ptr(), n_part, alpha)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        ctx.flip_g2p_mr_device(dev.data_ptr(), n_part, alpha)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    hbm, _, _ = peaks()
+    part_bytes = 28 * n_part + 12 * n_part  # particle read + velocity write
+    out["g2p_device_particles"] = {
+        "ms": ms, "mparticles_s": n_part / (ms * 1e-3) / 1e6,
+        "particle_stream_gbs": part_bytes / (ms * 1e-3) / 1e9,
+        "particle_stream_frac": part_bytes / (ms * 1e-3) / 1e9 / hbm,
+        "note": "a gather: per particle and component 8 level-0, 8 level-L and 8 distance "
+                "reads from the grid channels (L2-resident at this size) besides the "
+                "particle's own 28 B read and 12 B write"}
+    del dev
+    if not args.no_cpu:
+        sample = p[:: max(1, n_part // 1_000_000)]
+        d, k = oracle.mr_dist([nb] * 3, bsx, lev, nl)
+        t0 = time.perf_counter()
+        oracle.mr_g2p((res,) * 3, bsx, lev, sample, vel, old, d, k, alpha)
+        t = time.perf_counter() - t0
+        out["cpu_port"] = {"kind": "port", "cores": 1,
+                           "sample": f"{len(sample)} of the particles, CPU restatement "
+                                     "(oracle/msbg_oracle_flip_mr.c), one thread",
+                           "mparticles_s": len(sample) / t / 1e6}
+    return out
+
+
 # the demo's particle splatting (src/msbg_demo.cpp:339-684): rParticle 2,
 # nbDist 2, n_base instances of an n_base-point cloud; the reference's demo is
 # timed on the first ref_n_base points of the same cloud (ref_n_base^2
@@ -773,6 +846,7 @@ def mgpcg_extras(args, ctx, c, scene, st, fluid, prepare=None):
     x["max_err_vs_fp64_oracle"] = error_vs_oracle(ctx, c)
     x["mcf_512_b16"] = mcf_line(args, ctx)
     x["flip_transfers_256_b16"] = flip_line(args, ctx)
+    x["g2p_multires_512_b16_3lvl"] = flip_mr_line(args, ctx)
     x[splat_workload_name()] = splat_line(args, ctx)
     return x, roof, cb
 

@@ -466,6 +466,45 @@ int msbg_gpu_flip_g2p_device(msbg_gpu_ctx* ctx, msbg_flip_particle* particles, i
  * vector channels, voxels for MSBG_FLIP_MASS. */
 int msbg_gpu_flip_channel(msbg_gpu_ctx* ctx, int which, float* data, int64_t n, int get);
 
+/* ---- G2P on mixed-resolution grids --------------------------------------
+ * On the context's topology (msbg_gpu_sync_topology; blocks whose 26
+ * neighbours differ from them by at most one level, as the reference
+ * asserts), with channels in the packed layout of the pressure channels: for
+ * every block in ascending bid, its (bsx0>>level)^3 voxels at its own level
+ * (vid = x + y*bs + z*bs^2).  A voxel of a level's grid that lies in a block
+ * of another level reads 0, as a NULL block of that level's sparse grid. */
+
+/* Builds the fine/coarse distance channel CH_DIST_FINECOARSE of every level
+ * as setRefinementMap does (src/msbg.cpp:1700-1723, 1887-1960, 1994-2029) and,
+ * where dist / kind are not NULL, copies it out: dist (n = packed voxels)
+ * holds the distances (uint16, voxels of the block's level times 1024) of the
+ * blocks with a coarser neighbour, 0 elsewhere; kind[l*nBlocks + b] (nk =
+ * nLevels * nBlocks) is block b's kind in the channel of level l: 0 empty,
+ * 1 value block, 2 full block of value 6*1024 (dTransRes is 6,
+ * src/msbg.cpp:201).  msbg_gpu_flip_g2p_mr builds it by itself. */
+int msbg_gpu_flip_mr_dist(msbg_gpu_ctx* ctx, uint16_t* dist, int64_t n, int8_t* kind,
+                          int64_t nk);
+/* Copies the mixed-resolution velocity channel MSBG_FLIP_VEL or
+ * MSBG_FLIP_VEL_OLD out (get = 1) or in (get = 0): per voxel the lower-face
+ * MAC values (u, v, w) at the voxel's level, n = 3 * packed voxels.  These
+ * are the reference's getVecChannel(CH_VEC3_4 / CH_VEC3_2, level, 0) of every
+ * level, merged block by block. */
+int msbg_gpu_flip_mr_channel(msbg_gpu_ctx* ctx, int which, float* data, int64_t n, int get);
+/* Replaces FlipSimulation::gridToParticle (src/flip_sim.cpp:1526-1545) on a
+ * grid with several levels: vel = (1 - alpha) pic + alpha (vel + pic - old),
+ * pic and old from interpVec3MSBG / interpCompMSBG (src/flip_sim.cpp:
+ * 1354-1525): in a level-0 block the trilinear MAC interpolation of the
+ * level-0 channel; in a block of level L > 0 that of the level-L channel at
+ * the position scaled by 2^-L, blended with the level-0 interpolation by
+ * MtLinstep(1.01 sqrt3, 0.99 (dTransRes + 2) / sqrt3, d), d the level-L
+ * distance channel interpolated there / 1024.  Updates the particles in
+ * place; the _device form takes particles in device memory (a cudaMalloc'd
+ * array the caller owns), ordered on the context's stream. */
+int msbg_gpu_flip_g2p_mr(msbg_gpu_ctx* ctx, msbg_flip_particle* particles, int64_t np,
+                         float flipAlpha);
+int msbg_gpu_flip_g2p_mr_device(msbg_gpu_ctx* ctx, msbg_flip_particle* particles, int64_t np,
+                                float flipAlpha);
+
 /* ---- particle splatting -------------------------------------------------- */
 
 /* The splat parameters of the reference's demo (src/msbg_demo.cpp:235-236,

@@ -60,6 +60,7 @@ extern "C" int msbg_gpu_destroy(msbg_gpu_ctx* ctx) {
   pressure_release(ctx);
   flip_release(ctx);
   splat_release(ctx);
+  flip_mr_release(ctx);
   ctx->channels.clear();
   ctx->listBuf.release();
   ctx->errBuf.release();

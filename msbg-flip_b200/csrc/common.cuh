@@ -126,6 +126,8 @@ void pressure_release(msbg_gpu_ctx* ctx);
 void flip_release(msbg_gpu_ctx* ctx);
 // Releases the particle-splatting buffers of a context (splat.cu).
 void splat_release(msbg_gpu_ctx* ctx);
+// Releases the mixed-resolution G2P state of a context (flip_mr.cu).
+void flip_mr_release(msbg_gpu_ctx* ctx);
 
 // Launches of the 8-colour mean-curvature-flow passes (mcf.cu).  xfaces:
 // optional face cache of nSlots value blocks (2 * bsx^2 values each, the

@@ -182,6 +182,9 @@ class Context:
         d = TopoDesc(sx, sy, sz, bsx0, n_levels, bl)
         self._check(self._L.msbg_gpu_sync_topology(self._h, C.byref(d)), "sync_topology")
         self.n_blocks = (sx // bsx0) * (sy // bsx0) * (sz // bsx0)
+        self._bsx0 = bsx0
+        self._levels = (np.array(self._bl) if block_level is not None
+                        else np.zeros(self.n_blocks, np.int32))
 
     def upload_channel(self, chan, level, kind, packed, empty_val=0.0, full_val=0.0):
         kind = np.ascontiguousarray(kind, np.int8)
@@ -668,6 +671,74 @@ def _ctx_flip_g2p_device(self, dev_ptr, n_particles, alpha=0.95):
                 "flip_g2p_device")
 
 
+def _mr_sigs(L):
+    if getattr(L, "_mr_sig", False):
+        return
+    vp, i32, f32 = C.c_void_p, C.c_int, C.c_float
+    sig = {
+        "msbg_gpu_flip_mr_dist": (i32, [vp, vp, C.c_int64, vp, C.c_int64]),
+        "msbg_gpu_flip_mr_channel": (i32, [vp, i32, C.POINTER(C.c_float), C.c_int64, i32]),
+        "msbg_gpu_flip_g2p_mr": (i32, [vp, vp, C.c_int64, f32]),
+        "msbg_gpu_flip_g2p_mr_device": (i32, [vp, vp, C.c_int64, f32]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    L._mr_sig = True
+
+
+def packed_voxels(bsx0, block_level):
+    """Voxels of the packed layout: (bsx0 >> level)^3 per block."""
+    bl = np.asarray(block_level, np.int64)
+    return int(((bsx0 >> bl) ** 3).sum())
+
+
+def _ctx_flip_mr_dist(self, n_levels):
+    """msbg_gpu_flip_mr_dist: (packed uint16 distances, kinds [n_levels, nBlocks])."""
+    _mr_sigs(self._L)
+    n = packed_voxels(self._bsx0, self._levels)
+    dist = np.zeros(n, np.uint16)
+    kind = np.zeros((n_levels, len(self._levels)), np.int8)
+    self._check(self._L.msbg_gpu_flip_mr_dist(self._h, dist.ctypes.data, n, kind.ctypes.data,
+                                              kind.size), "flip_mr_dist")
+    return dist, kind
+
+
+def _ctx_flip_mr_channel(self, which, data=None):
+    """Get (data None) or set a mixed-resolution velocity channel (3 floats per
+    packed voxel)."""
+    _mr_sigs(self._L)
+    n = 3 * packed_voxels(self._bsx0, self._levels)
+    if data is None:
+        out = np.empty(n, np.float32)
+        self._check(self._L.msbg_gpu_flip_mr_channel(self._h, which, _p(out, C.c_float), n, 1),
+                    "flip_mr_channel")
+        return out
+    d = _f32(data).reshape(-1)
+    self._check(self._L.msbg_gpu_flip_mr_channel(self._h, which, _p(d, C.c_float), len(d), 0),
+                "flip_mr_channel")
+
+
+def _ctx_flip_g2p_mr(self, particles, alpha=0.95):
+    """msbg_gpu_flip_g2p_mr on a FLIP_PARTICLE array, in place."""
+    _mr_sigs(self._L)
+    if not (particles.flags.c_contiguous and particles.dtype == FLIP_PARTICLE):
+        raise ValueError("particles: contiguous FLIP_PARTICLE array")
+    self._check(self._L.msbg_gpu_flip_g2p_mr(self._h, particles.ctypes.data, len(particles),
+                                             alpha), "flip_g2p_mr")
+
+
+def _ctx_flip_g2p_mr_device(self, dev_ptr, n_particles, alpha=0.95):
+    _mr_sigs(self._L)
+    self._check(self._L.msbg_gpu_flip_g2p_mr_device(self._h, dev_ptr, n_particles, alpha),
+                "flip_g2p_mr_device")
+
+
+Context.flip_mr_dist = _ctx_flip_mr_dist
+Context.flip_mr_channel = _ctx_flip_mr_channel
+Context.flip_g2p_mr = _ctx_flip_g2p_mr
+Context.flip_g2p_mr_device = _ctx_flip_g2p_mr_device
 Context.flip_p2g_device = _ctx_flip_p2g_device
 Context.flip_g2p_device = _ctx_flip_g2p_device
 Context.flip_p2g = _ctx_flip_p2g

@@ -93,6 +93,24 @@ void oracle_flip_gradient(int sx, int sy, int sz, int bsx, float* vel, const flo
 void oracle_flip_g2p(int sx, int sy, int sz, int bsx, oracle_flip_particle* p, int64_t np,
                      const float* vel, const float* velOld, float alpha);
 
+/* ---- mixed-resolution G2P interpolation (msbg_oracle_flip_mr.c,
+ * src/flip_sim.cpp:1354-1545, src/msbg.cpp:1887-1960, src/sbg.h:3111-3420) ----
+ * level[b]: resolution level of block b; packed layout: per block in bid
+ * order its (bsx0>>level)^3 voxels at its level, off[b] its first voxel
+ * (oracle_mr_layout returns the total).  dist: the value blocks of
+ * CH_DIST_FINECOARSE, packed; kind[l*nBlocks + b]: block b's kind in the
+ * channel of level l (0 empty, 1 value, 2 full = dTransRes*1024). */
+int64_t oracle_mr_layout(int nbx, int nby, int nbz, int bsx0, const int* level, int64_t* off);
+void oracle_mr_dist(int nbx, int nby, int nbz, int bsx0, const int* level, int nLevels,
+                    int dTransRes, uint16_t* dist, int8_t* kind);
+void oracle_mr_dist_interp(int sx, int sy, int sz, int bsx0, int nbx, int nby, int nbz,
+                           const int* level, const int64_t* off, const uint16_t* dist,
+                           const int8_t* kind, int dTransRes, int lv, const float* pos,
+                           int64_t n, float* out);
+void oracle_mr_g2p(int sx, int sy, int sz, int bsx0, const int* level, int dTransRes,
+                   oracle_flip_particle* p, int64_t np, const float* vel, const float* velOld,
+                   const uint16_t* dist, const int8_t* kind, float alpha);
+
 /* ---- particle splatting (msbg_oracle_splat.c, src/msbg_demo.cpp) ---- */
 /* pos: 3 floats per particle; kind/active: one byte per block (1 = value);
  * out: the value blocks packed in bid order, 16-bit render density

@@ -531,3 +531,130 @@ def splat_reference_in_domain(res3, bsx, pts):
     if rc:
         raise RuntimeError(f"ref_splat_in_domain rc={rc}")
     return out
+
+
+# ---- mixed-resolution G2P interpolation (msbg_oracle_flip_mr.c) ----
+
+def _mr_lib():
+    L = oracle()
+    if not hasattr(L, "_mr_sig"):
+        vp, i32, f32 = C.c_void_p, C.c_int, C.c_float
+        L.oracle_mr_layout.restype = C.c_int64
+        L.oracle_mr_layout.argtypes = [i32] * 4 + [vp, vp]
+        L.oracle_mr_dist.argtypes = [i32] * 4 + [vp, i32, i32, vp, vp]
+        L.oracle_mr_dist_interp.argtypes = [i32] * 7 + [vp, vp, vp, vp, i32, i32, vp, C.c_int64,
+                                                        vp]
+        L.oracle_mr_g2p.argtypes = [i32] * 4 + [vp, i32, vp, C.c_int64, vp, vp, vp, vp, f32]
+        L._mr_sig = True
+    return L
+
+
+def mr_layout(nb3, bsx0, level):
+    """Packed layout of a mixed-resolution grid: (first voxel per block, total)."""
+    L = _mr_lib()
+    lv = np.ascontiguousarray(level, np.int32)
+    off = np.zeros(lv.size, np.int64)
+    n = L.oracle_mr_layout(nb3[0], nb3[1], nb3[2], bsx0, lv.ctypes.data, off.ctypes.data)
+    return off, int(n)
+
+
+def mr_dist(nb3, bsx0, level, n_levels, dtrans=6):
+    """CH_DIST_FINECOARSE restated: (packed uint16 distances of the value
+    blocks, block kinds per level [n_levels, nBlocks]: 0 empty, 1 value, 2 full)."""
+    L = _mr_lib()
+    lv = np.ascontiguousarray(level, np.int32)
+    _, n = mr_layout(nb3, bsx0, lv)
+    dist = np.zeros(n, np.uint16)
+    kind = np.zeros((n_levels, lv.size), np.int8)
+    L.oracle_mr_dist(nb3[0], nb3[1], nb3[2], bsx0, lv.ctypes.data, n_levels, dtrans,
+                     dist.ctypes.data, kind.ctypes.data)
+    return dist, kind
+
+
+def mr_dist_interp(res3, bsx0, level, dist, kind, lv, pos, dtrans=6):
+    """The distance channel of level lv interpolated at pos (level units, n x 3)."""
+    L = _mr_lib()
+    nb3 = [r // bsx0 for r in res3]
+    lev = np.ascontiguousarray(level, np.int32)
+    off, _ = mr_layout(nb3, bsx0, lev)
+    p = np.ascontiguousarray(pos, np.float32)
+    out = np.zeros(len(p), np.float32)
+    L.oracle_mr_dist_interp(res3[0], res3[1], res3[2], bsx0, *nb3, lev.ctypes.data,
+                            off.ctypes.data, np.ascontiguousarray(dist, np.uint16).ctypes.data,
+                            np.ascontiguousarray(kind, np.int8).ctypes.data, dtrans, lv,
+                            p.ctypes.data, len(p), out.ctypes.data)
+    return out
+
+
+def mr_g2p(res3, bsx0, level, particles, vel, velOld, dist, kind, alpha, dtrans=6):
+    """gridToParticle through interpVec3MSBG restated: updated particles."""
+    L = _mr_lib()
+    lev = np.ascontiguousarray(level, np.int32)
+    p = np.array(particles)
+    v, o = np.ascontiguousarray(vel, np.float32), np.ascontiguousarray(velOld, np.float32)
+    d = np.ascontiguousarray(dist, np.uint16)
+    k = np.ascontiguousarray(kind, np.int8)
+    L.oracle_mr_g2p(res3[0], res3[1], res3[2], bsx0, lev.ctypes.data, dtrans, p.ctypes.data,
+                    len(p), v.ctypes.data, o.ctypes.data, d.ctypes.data, k.ctypes.data, alpha)
+    return p
+
+
+def _ref_mr():
+    L = ref()
+    if not hasattr(L, "_mr_sig"):
+        vp = C.c_void_p
+        L.ref_mr_create.restype = vp
+        L.ref_mr_create.argtypes = [C.c_int] * 5 + [vp]
+        L.ref_mr_destroy.argtypes = [vp]
+        L.ref_mr_dtransres.restype = C.c_int
+        L.ref_mr_dtransres.argtypes = [vp]
+        L.ref_mr_block_info.argtypes = [vp, vp, vp]
+        L.ref_mr_dist.restype = C.c_longlong
+        L.ref_mr_dist.argtypes = [vp, vp, vp]
+        L.ref_mr_dist_interp.argtypes = [vp, C.c_int, vp, C.c_longlong, vp]
+        L._mr_sig = True
+    return L
+
+
+class RefMultires:
+    """A reference MultiresSparseGrid with the given block levels, set up by its
+    own setRefinementMap (which builds the fine/coarse distance channel)."""
+
+    def __init__(self, res3, bsx0, n_levels, level):
+        self.L = _ref_mr()
+        self.level = np.ascontiguousarray(level, np.int32)
+        self.h = self.L.ref_mr_create(res3[0], res3[1], res3[2], bsx0, n_levels,
+                                      self.level.ctypes.data)
+        if not self.h:
+            raise RuntimeError("ref_mr_create failed")
+        self.nb3 = [r // bsx0 for r in res3]
+        self.bsx0 = bsx0
+
+    def dtrans(self):
+        return self.L.ref_mr_dtransres(self.h)
+
+    def block_info(self):
+        lv = np.zeros(self.level.size, np.int32)
+        fl = np.zeros(self.level.size, np.int32)
+        self.L.ref_mr_block_info(self.h, lv.ctypes.data, fl.ctypes.data)
+        return lv, fl
+
+    def dist(self, n_levels):
+        _, n = mr_layout(self.nb3, self.bsx0, self.level)
+        out = np.zeros(n, np.uint16)
+        kind = np.zeros((n_levels, self.level.size), np.int8)
+        got = self.L.ref_mr_dist(self.h, out.ctypes.data, kind.ctypes.data)
+        if got != n:
+            raise RuntimeError(f"ref_mr_dist returned {got}, packed size {n}")
+        return out, kind
+
+    def dist_interp(self, lv, pos):
+        p = np.ascontiguousarray(pos, np.float32)
+        out = np.zeros(len(p), np.float32)
+        self.L.ref_mr_dist_interp(self.h, lv, p.ctypes.data, len(p), out.ctypes.data)
+        return out
+
+    def close(self):
+        if self.h:
+            self.L.ref_mr_destroy(self.h)
+            self.h = None

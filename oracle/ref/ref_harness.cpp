@@ -375,3 +375,85 @@ extern "C" int ref_ps_solve(void* hp, int nPre, int nPost, int nCoarse, int maxI
   if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
   return it;
 }
+
+// ---------------------------------------------------------------------------
+// Mixed-resolution grids for the velocity interpolation of G2P.
+//
+// A MultiresSparseGrid with the given block levels, set up by the
+// reference's own setRefinementMap (src/msbg.cpp:1428), which flags the blocks
+// with a coarser neighbour (BLK_FINE_COARSE, src/msbg.cpp:1700-1723) and fills
+// their fine/coarse distance channel (CH_DIST_FINECOARSE,
+// src/msbg.cpp:1887-1960).  Channel data move in the packed layout: for every
+// block id in ascending order, the block's (bsx0>>level)^3 values at its level.
+// ---------------------------------------------------------------------------
+extern "C" void* ref_mr_create(int sx, int sy, int sz, int bsx0, int nLevels,
+                               const int* blockLevel) {
+  MultiresSparseGrid* m = MultiresSparseGrid::create("MR", sx, sy, sz, bsx0, -1, 0, -1, 0,
+                                                     NULL, NULL, nLevels);
+  if (!m) return nullptr;
+  std::vector<int> levels(blockLevel, blockLevel + m->nBlocks());
+  m->setRefinementMap(levels.data(), NULL, -1, NULL, false, true);
+  return m;
+}
+
+extern "C" void ref_mr_destroy(void* mp) {
+  MultiresSparseGrid* m = (MultiresSparseGrid*)mp;
+  MultiresSparseGrid::destroy(m);
+}
+
+extern "C" int ref_mr_dtransres(void* m) { return ((MultiresSparseGrid*)m)->dTransRes(); }
+
+// Block levels and flags (BLK_*) at MG level 0, as the grid holds them.
+extern "C" void ref_mr_block_info(void* mp, int* level, int* flags) {
+  auto* m = (MultiresSparseGrid*)mp;
+  for (int b = 0; b < m->nBlocks(); b++) {
+    level[b] = m->getBlockInfo(b, 0)->level;
+    flags[b] = m->getBlockInfo(b, 0)->flags;
+  }
+}
+
+// The distance channel of every level: kind[l*nBlocks + b] is block b's kind
+// in the channel of level l (0 = no block or empty, 1 = value block, 2 = full
+// block of value dTransRes*1024, src/msbg.cpp:1994-2029); value blocks (only
+// ever at their own level, src/msbg.cpp:1887-1960) land in `out` in the packed
+// layout, every other packed voxel reads 0, the channel's empty value
+// (src/sbg.cpp:348).  Returns the packed size, or -1 for a value block at a
+// level other than its own.
+extern "C" long long ref_mr_dist(void* mp, uint16_t* out, int8_t* kind) {
+  auto* m = (MultiresSparseGrid*)mp;
+  const int bsx0 = m->sg0()->bsx(), nb = m->nBlocks(), nl = m->getNumLevels();
+  for (int l = 0; l < nl; l++) {
+    SparseGrid<uint16_t>* sg = m->getDistFineCoarseChannel(l);
+    for (int b = 0; b < nb; b++) {
+      int k = 0;
+      if (sg && sg->isValueBlock(b)) k = 1;
+      else if (sg && sg->isFullBlock(b)) k = 2;
+      kind[(size_t)l * nb + b] = (int8_t)k;
+      if (k == 1 && m->getBlockInfo(b, 0)->level != l) return -1;
+    }
+  }
+  long long off = 0;
+  for (int b = 0; b < nb; b++) {
+    const int l = m->getBlockInfo(b, 0)->level;
+    const int bs = bsx0 >> l, nv = bs * bs * bs;
+    SparseGrid<uint16_t>* sg = m->getDistFineCoarseChannel(l);
+    const uint16_t* d = (sg && sg->isValueBlock(b)) ? sg->getBlockDataPtr(b) : nullptr;
+    for (int i = 0; i < nv; i++) out[off + i] = d ? d[i] : 0;
+    off += nv;
+  }
+  return off;
+}
+
+// The reference's own linear interpolation of the distance channel of level
+// `level` with Neumann borders, at n positions in that level's voxel units:
+// the call interpVec3MSBG makes (src/flip_sim.cpp:1430-1432), without the
+// division by 1024.
+extern "C" void ref_mr_dist_interp(void* mp, int level, const float* pos, long long n,
+                                   float* out) {
+  auto* m = (MultiresSparseGrid*)mp;
+  SparseGrid<uint16_t>* sg = m->getDistFineCoarseChannel(level);
+  for (long long i = 0; i < n; i++) {
+    float p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    out[i] = sg ? sg->interpolateToFloat<IP_LINEAR>(p, OPT_IPBC_NEUMAN) : 0.f;
+  }
+}
