@@ -8,7 +8,8 @@
  *     their pieces                                      src/msbg3.cpp:3041-3271
  *   - the FLIP transfers either side of the solve (particleToGrid,
  *     applyGravity, the pressure-gradient update, gridToParticle) on
- *     single-level grids                                src/flip_sim.cpp
+ *     single-level grids, and gridToParticle through interpVec3MSBG on
+ *     mixed-resolution grids                            src/flip_sim.cpp
  *
  * The host keeps owning the MSBG block pool; this library owns device pools and
  * moves data only on explicit upload/download calls.  Every function returns an
