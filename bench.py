@@ -551,6 +551,19 @@ def flip_mr_line(args, ctx):
                 "reads from the grid channels (L2-resident at this size) besides the "
                 "particle's own 28 B read and 12 B write"}
     del dev
+    # downsampleVelocity from MG level 0 to 1 on the same grid (no solid or
+    # void cells), through the C ABI from host arrays
+    lv1 = np.maximum(lev, 1)
+    n1 = int(((bsx >> lv1.astype(np.int64)) ** 3).sum())
+    flags1 = np.zeros(n1, np.uint16)
+    ctx.flip_downsample_velocity(1, flags1, vel)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ctx.flip_downsample_velocity(1, flags1, vel)
+    dt = (time.perf_counter() - t0) / steps
+    out["downsample_velocity_mg1"] = {"ms": dt * 1e3, "mvoxels_s": n1 / dt / 1e6,
+                                      "h2d_bytes": 12 * n + 2 * n1, "d2h_bytes": 12 * n1,
+                                      "path": "C ABI from host arrays (copies inside)"}
     if not args.no_cpu:
         sample = p[:: max(1, n_part // 1_000_000)]
         d, k = oracle.mr_dist([nb] * 3, bsx, lev, nl)

@@ -506,6 +506,20 @@ int msbg_gpu_flip_g2p_mr(msbg_gpu_ctx* ctx, msbg_flip_particle* particles, int64
 int msbg_gpu_flip_g2p_mr_device(msbg_gpu_ctx* ctx, msbg_flip_particle* particles, int64_t np,
                                 float flipAlpha);
 
+/* Replaces MultiresSparseGrid::downsampleVelocity(levelMg, chSrc, chDst)
+ * (src/msbg4.cpp:2035-2270): the velocity of MG level levelMg - 1 restricted
+ * to MG level levelMg (1 <= levelMg < nLevels, the sparse MG levels).  At MG
+ * level m a block sits at level max(its level, m) (getBlockLevel,
+ * src/msbg.h:3574-3590); src (nSrc = 3 * packed voxels of MG level m-1) and
+ * dst (nDst = 3 * those of MG level m) use the packed layout at those levels,
+ * 3 floats per voxel; flags are the CellFlags of MG level m, packed (the
+ * reference's CH_CELL_FLAGS after preparePressureSolveFLIP).  A block already
+ * at level >= m is copied (0 in CELL_SOLID or CELL_VOID cells); a coarsened
+ * block takes the 4x4x4 (1,3,3,1)^3/512 filter of the finer cells, 0 in
+ * CELL_SOLID cells.  Host arrays; the copies are inside the call. */
+int msbg_gpu_flip_downsample_velocity(msbg_gpu_ctx* ctx, int levelMg, const uint16_t* flags,
+                                      const float* src, int64_t nSrc, float* dst, int64_t nDst);
+
 /* ---- particle splatting -------------------------------------------------- */
 
 /* The splat parameters of the reference's demo (src/msbg_demo.cpp:235-236,

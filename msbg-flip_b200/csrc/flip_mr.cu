@@ -6,6 +6,8 @@
 //   msbg_gpu_flip_mr_dist        the distance channel, built on the GPU
 //   msbg_gpu_flip_mr_channel     the velocity channels in/out
 //   msbg_gpu_flip_g2p_mr(_device) the particle update
+//   msbg_gpu_flip_downsample_velocity  downsampleVelocity (src/msbg4.cpp:2035),
+//                                the velocity restricted to the next MG level
 //
 // Layout (the packed layout of the pressure channels): for every block in
 // ascending bid, its (bsx0 >> level)^3 voxels at its own level, vid = x +
@@ -41,6 +43,7 @@ struct MrState {
   int64_t n = 0;  // packed voxels
   bool distBuilt = false;
   DeviceBuffer level, off, fc, kind, dist, vel, velOld, parts;
+  DeviceBuffer dsOffA, dsOffB, dsFlags, dsSrc, dsDst;  // downsampleVelocity
 };
 
 std::map<msbg_gpu_ctx*, std::unique_ptr<MrState>>& states() {
@@ -290,6 +293,78 @@ __global__ void k_g2p_mr(msbg_flip_particle* __restrict__ p, int64_t np, MrGrid 
   }
 }
 
+// downsampleVelocity (src/msbg4.cpp:2035-2270), MG level m-1 -> m, one CTA
+// per block (grid-stride), its threads over the block's voxels.  Block b sits
+// at level max(level0[b], m - 1) at MG level m-1 (offA) and max(level0[b], m)
+// at MG level m (offB).  A block already at level >= m is copied (0 in SOLID
+// or VOID cells); a block coarsened at this MG level takes per non-SOLID cell
+// the 4x4x4 (1,3,3,1)^3/512 sum over the level-(m-1) cells 2x-1 .. 2x+2
+// clamped to that level's grid, each from the level-(m-1) block where it is
+// one at MG level m-1, else the level-m value at (x2/2, y2/2, z2/2), summed in
+// the reference's order k, j, i without contraction.
+__global__ void __launch_bounds__(256)
+    k_downsample_velocity(int sx, int sy, int sz, int sh0, int nbx, int nby, int nbz, int m,
+                          const int8_t* __restrict__ level0, const int64_t* __restrict__ offA,
+                          const int64_t* __restrict__ offB, const uint16_t* __restrict__ flags,
+                          const float* __restrict__ src, float* __restrict__ dst) {
+  const int64_t nb = (int64_t)nbx * nby * nbz;
+  const int fs = m - 1, nsx = sx >> fs, nsy = sy >> fs, nsz = sz >> fs, shA = sh0 - fs;
+  for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
+    const int l0 = level0[b], lv = max(l0, m), sh = sh0 - lv, bs = 1 << sh;
+    const int bx = (int)(b % nbx), by = (int)((b / nbx) % nby), bz = (int)(b / ((int64_t)nbx * nby));
+    const int nv = bs * bs * bs;
+    for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+      const uint16_t fl = flags[offB[b] + v];
+      float* out = dst + 3 * (offB[b] + v);
+      if (l0 >= m) {
+        const float* in = src + 3 * (offA[b] + v);
+        const bool zero = (fl & (0x1 | 0x1000)) != 0;  // CELL_SOLID | CELL_VOID
+        out[0] = zero ? 0.f : in[0];
+        out[1] = zero ? 0.f : in[1];
+        out[2] = zero ? 0.f : in[2];
+        continue;
+      }
+      float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+      if (!(fl & 0x1)) {
+        const int x = bx * bs + (v & (bs - 1)), y = by * bs + ((v >> sh) & (bs - 1)),
+                  z = bz * bs + (v >> (2 * sh));
+        for (int k = 0; k < 4; k++) {
+          const int z2 = min(max(2 * z - 1 + k, 0), nsz - 1);
+          for (int j = 0; j < 4; j++) {
+            const int y2 = min(max(2 * y - 1 + j, 0), nsy - 1);
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              const int x2 = min(max(2 * x - 1 + i, 0), nsx - 1);
+              const int64_t b2 = (x2 >> shA) + (int64_t)nbx * ((y2 >> shA) + (int64_t)nby * (z2 >> shA));
+              const int l2 = max((int)level0[b2], fs);  // its level at MG level m-1
+              int64_t q = -1;
+              if (l2 == fs) {
+                const int mk = (1 << shA) - 1;
+                q = offA[b2] + (x2 & mk) + ((int64_t)(y2 & mk) << shA) +
+                    ((int64_t)(z2 & mk) << (2 * shA));
+              } else if (l2 == fs + 1) {
+                const int s2 = shA - 1, mk = (1 << s2) - 1;
+                q = offA[b2] + ((x2 >> 1) & mk) + ((int64_t)((y2 >> 1) & mk) << s2) +
+                    ((int64_t)((z2 >> 1) & mk) << (2 * s2));
+              }
+              const float w = (float)((i == 0 || i == 3 ? 1 : 3) * (j == 0 || j == 3 ? 1 : 3) *
+                                      (k == 0 || k == 3 ? 1 : 3)) * (1.0f / 512.0f);
+              const float f0 = q < 0 ? 0.f : src[3 * q], f1 = q < 0 ? 0.f : src[3 * q + 1],
+                          f2 = q < 0 ? 0.f : src[3 * q + 2];
+              v0 = __fadd_rn(v0, __fmul_rn(f0, w));
+              v1 = __fadd_rn(v1, __fmul_rn(f1, w));
+              v2 = __fadd_rn(v2, __fmul_rn(f2, w));
+            }
+          }
+        }
+      }
+      out[0] = v0;
+      out[1] = v1;
+      out[2] = v2;
+    }
+  }
+}
+
 int grid_blocks(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 32); }
 
 // The state of a context for its current topology (rebuilt when it changed).
@@ -471,4 +546,52 @@ extern "C" int msbg_gpu_flip_g2p_mr(msbg_gpu_ctx* ctx, msbg_flip_particle* parti
 extern "C" int msbg_gpu_flip_g2p_mr_device(msbg_gpu_ctx* ctx, msbg_flip_particle* particles,
                                            int64_t np, float flipAlpha) {
   return flip_g2p_mr(ctx, particles, np, flipAlpha, true);
+}
+
+extern "C" int msbg_gpu_flip_downsample_velocity(msbg_gpu_ctx* ctx, int levelMg,
+                                                 const uint16_t* flags, const float* src,
+                                                 int64_t nSrc, float* dst, int64_t nDst) {
+  if (!ctx || !flags || !src || !dst) return MSBG_EINVARG;
+  cudaSetDevice(ctx->device);
+  MrState* S = nullptr;
+  MrGrid g;
+  int rc = mr_state(ctx, &S, g);
+  if (rc) return rc;
+  if (levelMg < 1 || levelMg >= ctx->nLevels)
+    return set_error(ctx, MSBG_EINVARG, "levelMg=%d: the sparse MG levels are 1..%d", levelMg,
+                     ctx->nLevels - 1);
+  const int64_t nb = ctx->nb();
+  std::vector<int64_t> offA(nb), offB(nb);
+  int64_t nA = 0, nB = 0;
+  for (int64_t b = 0; b < nb; b++) {
+    const int l0 = ctx->blockLevel[b];
+    const int64_t bsA = ctx->bsx0 >> std::max(l0, levelMg - 1), bsB = ctx->bsx0 >> std::max(l0, levelMg);
+    offA[b] = nA;
+    offB[b] = nB;
+    nA += bsA * bsA * bsA;
+    nB += bsB * bsB * bsB;
+  }
+  if (nSrc != 3 * nA || nDst != 3 * nB)
+    return set_error(ctx, MSBG_EINVARG,
+                     "MG levels %d / %d hold %lld / %lld floats, not %lld / %lld", levelMg - 1,
+                     levelMg, (long long)(3 * nA), (long long)(3 * nB), (long long)nSrc,
+                     (long long)nDst);
+  cudaStream_t st = ctx->stream;
+  MSBG_CUDA_TRY(ctx, S->dsOffA.ensure(8 * nb));
+  MSBG_CUDA_TRY(ctx, S->dsOffB.ensure(8 * nb));
+  MSBG_CUDA_TRY(ctx, S->dsFlags.ensure(2 * (size_t)nB));
+  MSBG_CUDA_TRY(ctx, S->dsSrc.ensure(12 * (size_t)nA));
+  MSBG_CUDA_TRY(ctx, S->dsDst.ensure(12 * (size_t)nB));
+  MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(S->dsOffA.p, offA.data(), 8 * nb, cudaMemcpyHostToDevice, st));
+  MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(S->dsOffB.p, offB.data(), 8 * nb, cudaMemcpyHostToDevice, st));
+  MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(S->dsFlags.p, flags, 2 * nB, cudaMemcpyHostToDevice, st));
+  MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(S->dsSrc.p, src, 12 * nA, cudaMemcpyHostToDevice, st));
+  k_downsample_velocity<<<(int)std::min<int64_t>(nb, 148 * 16), 256, 0, st>>>(
+      ctx->sx, ctx->sy, ctx->sz, g.sh0, ctx->nbx, ctx->nby, ctx->nbz, levelMg,
+      S->level.as<int8_t>(), S->dsOffA.as<int64_t>(), S->dsOffB.as<int64_t>(),
+      S->dsFlags.as<uint16_t>(), S->dsSrc.as<float>(), S->dsDst.as<float>());
+  MSBG_CUDA_TRY(ctx, cudaGetLastError());
+  MSBG_CUDA_TRY(ctx, cudaMemcpyAsync(dst, S->dsDst.p, 12 * nB, cudaMemcpyDeviceToHost, st));
+  // the offset vectors are read by the copies above before they go out of scope
+  return msbg_gpu_sync(ctx);
 }

@@ -680,6 +680,7 @@ def _mr_sigs(L):
         "msbg_gpu_flip_mr_channel": (i32, [vp, i32, C.POINTER(C.c_float), C.c_int64, i32]),
         "msbg_gpu_flip_g2p_mr": (i32, [vp, vp, C.c_int64, f32]),
         "msbg_gpu_flip_g2p_mr_device": (i32, [vp, vp, C.c_int64, f32]),
+        "msbg_gpu_flip_downsample_velocity": (i32, [vp, i32, vp, vp, C.c_int64, vp, C.c_int64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -735,6 +736,22 @@ def _ctx_flip_g2p_mr_device(self, dev_ptr, n_particles, alpha=0.95):
                 "flip_g2p_mr_device")
 
 
+def _ctx_flip_downsample_velocity(self, level_mg, flags, src):
+    """msbg_gpu_flip_downsample_velocity: MG level level_mg - 1 (src) to
+    level_mg, with that level's cell flags; returns dst."""
+    _mr_sigs(self._L)
+    lv = np.maximum(np.asarray(self._levels, np.int64), level_mg)
+    n = int(((self._bsx0 >> lv) ** 3).sum())
+    fl = np.ascontiguousarray(flags, np.uint16)
+    s = _f32(src).reshape(-1)
+    dst = np.empty(3 * n, np.float32)
+    self._check(self._L.msbg_gpu_flip_downsample_velocity(self._h, level_mg, fl.ctypes.data,
+                                                          s.ctypes.data, len(s), dst.ctypes.data,
+                                                          len(dst)), "flip_downsample_velocity")
+    return dst
+
+
+Context.flip_downsample_velocity = _ctx_flip_downsample_velocity
 Context.flip_mr_dist = _ctx_flip_mr_dist
 Context.flip_mr_channel = _ctx_flip_mr_channel
 Context.flip_g2p_mr = _ctx_flip_g2p_mr

@@ -111,6 +111,11 @@ void oracle_mr_g2p(int sx, int sy, int sz, int bsx0, const int* level, int dTran
                    oracle_flip_particle* p, int64_t np, const float* vel, const float* velOld,
                    const uint16_t* dist, const int8_t* kind, float alpha);
 
+/* downsampleVelocity (src/msbg4.cpp:2035-2270), MG level m-1 -> m: src/dst
+ * packed at those MG levels (3 floats per voxel), flags packed at MG level m. */
+void oracle_mr_downsample_velocity(int sx, int sy, int sz, int bsx0, const int* level0, int m,
+                                   const uint16_t* flags, const float* src, float* dst);
+
 /* ---- particle splatting (msbg_oracle_splat.c, src/msbg_demo.cpp) ---- */
 /* pos: 3 floats per particle; kind/active: one byte per block (1 = value);
  * out: the value blocks packed in bid order, 16-bit render density

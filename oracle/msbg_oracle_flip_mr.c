@@ -263,3 +263,80 @@ void oracle_mr_g2p(int sx, int sy, int sz, int bsx0, const int* level, int dTran
   }
   free(off);
 }
+
+/* downsampleVelocity (src/msbg4.cpp:2035-2270): the velocity of MG level m-1
+ * restricted to MG level m (1 <= m < nLevels, the sparse MG levels).  At MG
+ * level m block b sits at level max(level0[b], m) (getBlockLevel,
+ * src/msbg.h:3574-3590); src and dst are packed at MG levels m-1 and m, 3
+ * floats per voxel; flags (CellFlags) packed at MG level m.
+ *   level0[b] >= m: a copy of the block, 0 in SOLID or VOID cells;
+ *   level0[b] <  m: per non-SOLID cell (x, y, z) of level m, the 4x4x4 sum of
+ *     w_ijk * f over the level-(m-1) cells (2x-1+i, 2y-1+j, 2z-1+k) clamped to
+ *     that level's grid, w = (1,3,3,1)^3 / 512 (G3D_GetGausslikeKernel4x4x4,
+ *     src/grid.c:30-75), f from the level-(m-1) block where it exists at MG
+ *     level m-1, else the level-m value at (x2/2, y2/2, z2/2); SOLID cells 0.
+ * Accumulated in float in the order k, j, i. */
+void oracle_mr_downsample_velocity(int sx, int sy, int sz, int bsx0, const int* level0, int m,
+                                   const uint16_t* flags, const float* src, float* dst) {
+  const int nbx = sx / bsx0, nby = sy / bsx0, nbz = sz / bsx0;
+  const int64_t nb = (int64_t)nbx * nby * nbz;
+  int* lvA = (int*)malloc(sizeof(int) * (size_t)nb); /* levels at MG m-1 */
+  int* lvB = (int*)malloc(sizeof(int) * (size_t)nb); /* levels at MG m */
+  int64_t* offA = (int64_t*)malloc(sizeof(int64_t) * (size_t)nb);
+  int64_t* offB = (int64_t*)malloc(sizeof(int64_t) * (size_t)nb);
+  for (int64_t b = 0; b < nb; b++) {
+    lvA[b] = level0[b] > m - 1 ? level0[b] : m - 1;
+    lvB[b] = level0[b] > m ? level0[b] : m;
+  }
+  oracle_mr_layout(nbx, nby, nbz, bsx0, lvA, offA);
+  oracle_mr_layout(nbx, nby, nbz, bsx0, lvB, offB);
+  const float k1[4] = {1.f, 3.f, 3.f, 1.f};
+  float krn[64];
+  for (int k = 0; k < 4; k++)
+    for (int j = 0; j < 4; j++)
+      for (int i = 0; i < 4; i++) krn[i + 4 * j + 16 * k] = (float)((double)(k1[i] * k1[j] * k1[k]) / 512.0);
+  MRGrid gA = {sx, sy, sz, bsx0, nbx, nby, nbz, lvA, offA};
+  const int fs = m - 1; /* the finer source level */
+  const int nsx = sx >> fs, nsy = sy >> fs, nsz = sz >> fs;
+  for (int64_t b = 0; b < nb; b++) {
+    const int lv = lvB[b], bs = bsx0 >> lv;
+    const int bx = (int)(b % nbx), by = (int)((b / nbx) % nby), bz = (int)(b / ((int64_t)nbx * nby));
+    const int64_t nv = (int64_t)bs * bs * bs;
+    for (int64_t v = 0; v < nv; v++) {
+      const uint16_t fl = flags[offB[b] + v];
+      float* out = dst + 3 * (offB[b] + v);
+      if (level0[b] >= m) {
+        const float* in = src + 3 * (offA[b] + v);
+        const int zero = (fl & (0x1 | 0x1000)) != 0; /* CELL_SOLID | CELL_VOID */
+        for (int c = 0; c < 3; c++) out[c] = zero ? 0.f : in[c];
+        continue;
+      }
+      float val[3] = {0.f, 0.f, 0.f};
+      if (!(fl & 0x1)) {
+        const int x = bx * bs + (int)(v % bs), y = by * bs + (int)((v / bs) % bs),
+                  z = bz * bs + (int)(v / ((int64_t)bs * bs));
+        for (int k = 0; k < 4; k++) {
+          int z2 = 2 * z - 1 + k;
+          z2 = z2 < 0 ? 0 : z2 >= nsz ? nsz - 1 : z2;
+          for (int j = 0; j < 4; j++) {
+            int y2 = 2 * y - 1 + j;
+            y2 = y2 < 0 ? 0 : y2 >= nsy ? nsy - 1 : y2;
+            for (int i = 0; i < 4; i++) {
+              int x2 = 2 * x - 1 + i;
+              x2 = x2 < 0 ? 0 : x2 >= nsx ? nsx - 1 : x2;
+              int64_t q = mr_idx(&gA, fs, x2, y2, z2);
+              if (q < 0) q = mr_idx(&gA, fs + 1, x2 / 2, y2 / 2, z2 / 2);
+              const float w = krn[i + 4 * j + 16 * k];
+              for (int c = 0; c < 3; c++) val[c] += (q < 0 ? 0.f : src[3 * q + c]) * w;
+            }
+          }
+        }
+      }
+      for (int c = 0; c < 3; c++) out[c] = val[c];
+    }
+  }
+  free(lvA);
+  free(lvB);
+  free(offA);
+  free(offB);
+}

@@ -545,6 +545,7 @@ def _mr_lib():
         L.oracle_mr_dist_interp.argtypes = [i32] * 7 + [vp, vp, vp, vp, i32, i32, vp, C.c_int64,
                                                         vp]
         L.oracle_mr_g2p.argtypes = [i32] * 4 + [vp, i32, vp, C.c_int64, vp, vp, vp, vp, f32]
+        L.oracle_mr_downsample_velocity.argtypes = [i32] * 4 + [vp, i32, vp, vp, vp]
         L._mr_sig = True
     return L
 
@@ -597,6 +598,25 @@ def mr_g2p(res3, bsx0, level, particles, vel, velOld, dist, kind, alpha, dtrans=
     L.oracle_mr_g2p(res3[0], res3[1], res3[2], bsx0, lev.ctypes.data, dtrans, p.ctypes.data,
                     len(p), v.ctypes.data, o.ctypes.data, d.ctypes.data, k.ctypes.data, alpha)
     return p
+
+
+def mg_levels(level0, m):
+    """Block levels at MG level m: max(level0, m) (src/msbg.h:3574-3590)."""
+    return np.maximum(np.asarray(level0, np.int32), m).astype(np.int32)
+
+
+def mr_downsample_velocity(res3, bsx0, level0, m, flags, src):
+    """downsampleVelocity restated: MG level m-1 (src, packed, 3 floats per
+    voxel) to MG level m, with the MG-level-m cell flags; returns dst."""
+    L = _mr_lib()
+    lev = np.ascontiguousarray(level0, np.int32)
+    _, n = mr_layout([r // bsx0 for r in res3], bsx0, mg_levels(lev, m))
+    dst = np.zeros(3 * n, np.float32)
+    L.oracle_mr_downsample_velocity(res3[0], res3[1], res3[2], bsx0, lev.ctypes.data, m,
+                                    np.ascontiguousarray(flags, np.uint16).ctypes.data,
+                                    np.ascontiguousarray(src, np.float32).ctypes.data,
+                                    dst.ctypes.data)
+    return dst
 
 
 def _ref_mr():

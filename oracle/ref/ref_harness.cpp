@@ -457,3 +457,57 @@ extern "C" void ref_mr_dist_interp(void* mp, int level, const float* pos, long l
     out[i] = sg ? sg->interpolateToFloat<IP_LINEAR>(p, OPT_IPBC_NEUMAN) : 0.f;
   }
 }
+
+namespace {
+// The reference allocates a sparse grid's block map on first data access
+// (SparseGrid::prepareDataAccess, src/sbg.cpp:702-720; its FLIP driver does
+// it per channel); the vector channels of every (level, MG level) pair.
+void ps_prepare_vec(MultiresSparseGrid* m, int ch) {
+  for (int l = 0; l < m->getNumLevels(); l++)
+    for (int lMg = 0; lMg <= l; lMg++) {
+      SparseGrid<Vec3Float>* sg = m->getVecChannel(ch, l, lMg);
+      if (sg && !sg->hasData()) sg->prepareDataAccess();
+    }
+}
+}  // namespace
+
+// Vector channel ch (CH_VEC3_*) of MG level levelMg in the packed layout, 3
+// floats per voxel; -1 where the reference has no such channel at a block's
+// level.  Missing blocks read 0 and are skipped on write (written with
+// allocation when alloc != 0).
+extern "C" int ref_ps_vec_channel(void* hp, int ch, int levelMg, float* data, int get,
+                                  int alloc) {
+  auto* m = ((PsHandle*)hp)->msbg;
+  ps_prepare_vec(m, ch);
+  const int bsx0 = m->sg0()->bsx();
+  size_t off = 0;
+  for (int b = 0; b < m->nBlocks(); b++) {
+    const int l = m->getBlockInfo(b, levelMg)->level;
+    const int bs = bsx0 >> l, nv = bs * bs * bs;
+    SparseGrid<Vec3Float>* sg = m->getVecChannel(ch, l, levelMg);
+    if (!sg) return -1;
+    Vec3Float* d = sg->getBlockDataPtr(b, (!get && alloc) ? 1 : 0, 0);
+    for (int i = 0; i < nv; i++) {
+      if (get) {
+        data[3 * (off + i)] = d ? d[i].x : 0.f;
+        data[3 * (off + i) + 1] = d ? d[i].y : 0.f;
+        data[3 * (off + i) + 2] = d ? d[i].z : 0.f;
+      } else if (d) {
+        d[i] = Vec3Float(data[3 * (off + i)], data[3 * (off + i) + 1], data[3 * (off + i) + 2]);
+      }
+    }
+    off += nv;
+  }
+  return 0;
+}
+
+// downsampleVelocity(levelMg, chSrc, chDst) (src/msbg4.cpp:2035-2270): the
+// velocity of MG level levelMg - 1 restricted to MG level levelMg.
+extern "C" int ref_ps_downsample_velocity(void* hp, int levelMg, int chSrc, int chDst) {
+  auto* m = ((PsHandle*)hp)->msbg;
+  if (levelMg < 1 || levelMg >= m->getNumLevels()) return -1;
+  ps_prepare_vec(m, chSrc);
+  ps_prepare_vec(m, chDst);
+  m->downsampleVelocity(levelMg, chSrc, chDst);
+  return 0;
+}

@@ -18,6 +18,7 @@ CH_FLOAT_1, CH_DIVERGENCE, CH_PRESSURE, CH_FLOAT_2, CH_FLOAT_3, CH_DIAGONAL, CH_
     1, 2, 3, 6, 7, 13, 36)
 CH_FACE = (-1, -2, -3)  # CH_FACE_AREA dir 0, 1, 2
 CH_FLAGS = -10          # CH_CELL_FLAGS
+CH_VEC3_2, CH_VEC3_4 = 21, 23  # vector channels (src/msbg.h:302-305)
 CELL_SOLID, CELL_FIXED, CELL_VOID = 0x1, 0x2, 0x1000
 
 
@@ -42,6 +43,11 @@ def _lib():
         L.ref_ps_downsample.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.ref_ps_prolongate.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.ref_ps_vcycle.argtypes = [vp] + [C.c_int] * 7
+        L.ref_ps_vec_channel.restype = C.c_int
+        L.ref_ps_vec_channel.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_float), C.c_int,
+                                         C.c_int]
+        L.ref_ps_downsample_velocity.restype = C.c_int
+        L.ref_ps_downsample_velocity.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.ref_ps_solve.restype = C.c_int
         L.ref_ps_solve.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                    C.POINTER(C.c_float), C.POINTER(C.c_double)]
@@ -121,6 +127,30 @@ class RefPressure:
 
     def prolongate(self, level_mg_fine, ch_src, ch_dst):
         self._L.ref_ps_prolongate(self.h, level_mg_fine, ch_src, ch_dst)
+
+    def get_vec(self, ch, level_mg=0):
+        """Vector channel ch (CH_VEC3_*) of MG level level_mg, packed, 3 floats
+        per voxel."""
+        out = np.zeros(3 * self.packed_size(level_mg), np.float32)
+        rc = self._L.ref_ps_vec_channel(self.h, ch, level_mg,
+                                        out.ctypes.data_as(C.POINTER(C.c_float)), 1, 0)
+        if rc:
+            raise RuntimeError(f"ref_ps_vec_channel rc={rc}")
+        return out
+
+    def set_vec(self, ch, data, level_mg=0):
+        d = np.ascontiguousarray(data, np.float32)
+        assert len(d) == 3 * self.packed_size(level_mg)
+        rc = self._L.ref_ps_vec_channel(self.h, ch, level_mg,
+                                        d.ctypes.data_as(C.POINTER(C.c_float)), 0, 1)
+        if rc:
+            raise RuntimeError(f"ref_ps_vec_channel rc={rc}")
+
+    def downsample_velocity(self, level_mg, ch_src, ch_dst):
+        """downsampleVelocity (src/msbg4.cpp:2035): MG level level_mg - 1 to level_mg."""
+        rc = self._L.ref_ps_downsample_velocity(self.h, level_mg, ch_src, ch_dst)
+        if rc:
+            raise RuntimeError(f"ref_ps_downsample_velocity rc={rc}")
 
     def level0_arrays(self):
         """The reference's prepared level-0 inputs (preparePressureSolveFLIPLevel0_,

@@ -166,3 +166,46 @@ def test_large_grid_sampled_against_restatement():
         assert (q["vel"][idx].view(np.uint32) == e["vel"].view(np.uint32)).all()
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("cfg", [(64, 16, 2, 12), (128, 16, 3, 8), (128, 8, 3, 8),
+                                 (128, 32, 2, 16)])
+def test_downsample_velocity_bit_identical(cfg):
+    """msbg_gpu_flip_downsample_velocity against the restatement (pinned bit
+    for bit to the reference's downsampleVelocity on the CPU), MG level by MG
+    level, with the cell flags of the reference's own prepare where the
+    compiled reference is present, else SOLID/VOID flags of a seeded mix."""
+    res, bsx, nl, band = cfg
+    scene = msbg_gpu.PressureScene(res, bsx, nl, band=band, seed=5)
+    lev0 = np.ascontiguousarray(scene.block_levels, np.int32)
+    ref = None
+    if os.path.exists(oracle.REF_SO):
+        import ref_pressure as rp
+        ref = rp.RefPressure(scene)
+    ctx = msbg_gpu.Context(0)
+    try:
+        ctx.set_topology(res, res, res, bsx, nl, lev0)
+        rng = np.random.default_rng(2)
+        _, n0 = oracle.mr_layout([res // bsx] * 3, bsx, lev0)
+        src = rng.standard_normal(3 * n0).astype(np.float32)
+        if ref is not None:
+            ref.set_vec(rp.CH_VEC3_4, src, 0)
+        for m in range(1, nl):
+            _, nm = oracle.mr_layout([res // bsx] * 3, bsx, oracle.mg_levels(lev0, m))
+            if ref is not None:
+                flags = ref.get(rp.CH_FLAGS, m).astype(np.uint16)
+            else:
+                flags = rng.choice(np.array([0, 0, 0, 1, 0x1000], np.uint16), nm)
+            got = ctx.flip_downsample_velocity(m, flags, src)
+            exp = oracle.mr_downsample_velocity((res,) * 3, bsx, lev0, m, flags, src)
+            assert (got.view(np.uint32) == exp.view(np.uint32)).all(), m
+            if ref is not None:
+                ref.downsample_velocity(m, rp.CH_VEC3_4, rp.CH_VEC3_4)
+                assert (got.view(np.uint32) == ref.get_vec(rp.CH_VEC3_4, m).view(np.uint32)).all()
+            src = got
+        with pytest.raises(msbg_gpu.MsbgError):  # MG level 0 has no finer source
+            ctx.flip_downsample_velocity(0, np.zeros(n0, np.uint16), src)
+    finally:
+        ctx.close()
+        if ref is not None:
+            ref.close()

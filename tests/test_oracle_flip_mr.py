@@ -90,3 +90,37 @@ def test_layout_offsets():
     sizes = (bsx >> lev.astype(np.int64)) ** 3
     assert n == sizes.sum()
     assert (off == np.concatenate([[0], np.cumsum(sizes)[:-1]])).all()
+
+
+# PressureScene configurations (res, bsx0, nLevels, band): single-level and
+# adaptive grids of 8^3, 16^3 and 32^3 blocks
+DOWNSAMPLE_CFGS = [(64, 16, 2, 12), (128, 16, 3, 8), (128, 8, 3, 8), (128, 32, 2, 16)]
+
+
+@needs_ref
+@pytest.mark.parametrize("cfg", DOWNSAMPLE_CFGS)
+def test_downsample_velocity_equals_reference(cfg):
+    """downsampleVelocity restated, bit for bit against the reference on the
+    grid its own preparePressureSolveFLIP set up, MG level by MG level."""
+    import msbg_gpu
+    import ref_pressure as rp
+
+    res, bsx, nl, band = cfg
+    R = rp.RefPressure(msbg_gpu.PressureScene(res, bsx, nl, band=band, seed=5))
+    try:
+        lev0, _ = R.block_levels(0)
+        src = np.random.default_rng(1).standard_normal(3 * R.packed_size(0)).astype(np.float32)
+        R.set_vec(rp.CH_VEC3_4, src, 0)
+        for m in range(1, R.num_levels()):
+            lv, _ = R.block_levels(m)
+            assert (lv == oracle.mg_levels(lev0, m)).all()
+            R.downsample_velocity(m, rp.CH_VEC3_4, rp.CH_VEC3_4)
+            ref = R.get_vec(rp.CH_VEC3_4, m)
+            flags = R.get(rp.CH_FLAGS, m)
+            assert (flags >= 0).all()
+            got = oracle.mr_downsample_velocity((res,) * 3, bsx, lev0, m, flags.astype(np.uint16),
+                                                src)
+            assert (got.view(np.uint32) == ref.view(np.uint32)).all(), m
+            src = ref
+    finally:
+        R.close()
