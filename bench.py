@@ -33,7 +33,7 @@ calls after one warm-up:
     seeded cloud), next to the reference's own demo code on 1024 instances.
 
 ``--workload mcf`` benches only the smoother, ``--workload splat`` only the
-splatting; ``--workload c3`` / ``c5`` the
+splatting, ``--workload g2p_mr`` only G2P on the 3-level grid; ``--workload c3`` / ``c5`` the
 2048^3 mixed-precision and 4096^3 three-level configurations (one JSON line
 of figures each, see bench_large).
 ``--impl reference`` times the reference's own CPU implementation (compiled
@@ -294,6 +294,42 @@ def bench_reference(args):
         return
     if args.workload == "mcf":
         return bench_reference_mcf(args)
+    if args.workload == "g2p_mr":
+        # the reference's G2P (src/flip_sim.cpp) does not compile here: the CPU
+        # restatement of it is timed in its place
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        res, bsx, nl, n_part = 512, 16, 3, 1_000_000
+        nb = res // bsx
+        b = np.arange(nb ** 3)
+        r = np.sqrt((b % nb - 12.5) ** 2 + ((b // nb) % nb - 15.5) ** 2 + (b // (nb * nb) - 17.5) ** 2)
+        lev = np.where(r < 7, 0, np.where(r < 12, 1, 2)).astype(np.int32)
+        _, n = oracle.mr_layout([nb] * 3, bsx, lev)
+        rng = np.random.default_rng(21)
+        vel = rng.standard_normal(3 * n).astype(np.float32)
+        d, k = oracle.mr_dist([nb] * 3, bsx, lev, nl)
+        p = np.zeros(n_part, [("pos", "<f4", 3), ("vel", "<f4", 3), ("phase", "<i4")])
+        p["pos"] = rng.uniform(0, res, (n_part, 3)).astype(np.float32)
+        times = []
+        for _ in range(max(args.steps, 1)):
+            t0 = time.perf_counter()
+            oracle.mr_g2p((res,) * 3, bsx, lev, p, vel, vel, d, k, 0.95)
+            times.append(time.perf_counter() - t0)
+        v = n_part / float(np.median(times)) / 1e6
+        cb = {"value": v, "unit": "Mparticles/s", "cores": 1, "kind": "port",
+              "sample": f"{n_part} particles of g2p_multires_512_b16_3lvl, CPU restatement "
+                        "(oracle/msbg_oracle_flip_mr.c), one thread, median of "
+                        f"{len(times)} calls"}
+        print(json.dumps({"metric": "G2P rate on a 3-level grid (interpVec3MSBG blend)",
+                          "value": v, "unit": "Mparticles/s", "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": 0, "ms_per_step": n_part / v / 1e3,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f32", "data": "synthetic",
+                          "config": {"workload": "g2p_multires_512_b16_3lvl"},
+                          "impl": "reference", "cpu_baseline": cb,
+                          "e2e": {"value": v, "unit": "Mparticles/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
     if args.workload == "splat":
         cb = splat_reference_rate()
         if cb is None:
@@ -678,6 +714,28 @@ def bench_splat(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded point cloud, the demo's instance construction)",
             "config": s, "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cb}
+    print(json.dumps(line), flush=True)
+
+
+def bench_g2p_mr(args):
+    """--workload g2p_mr: G2P on the 3-level 512^3 grid alone (one JSON line)."""
+    import torch
+    import msbg_gpu
+    torch.cuda.set_device(0)
+    ctx = msbg_gpu.Context(0)
+    with Clocks(0) as clk:
+        s = flip_mr_line(args, ctx)
+    ctx.close()
+    d, h = s["g2p_device_particles"], s["g2p_host_particles"]
+    line = {"metric": "G2P rate on a 3-level grid (interpVec3MSBG blend)",
+            "value": d["mparticles_s"], "unit": "Mparticles/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": 1, "ms_per_step": d["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded velocity channels, uniformly random particles)",
+            "config": dict(s, workload="g2p_multires_512_b16_3lvl"), "clocks": clk.summary(),
+            "e2e": {"value": h["mparticles_s"], "unit": "Mparticles/s",
+                    "h2d_bytes_per_step": h["h2d_bytes"], "d2h_bytes_per_step": h["d2h_bytes"]},
+            "cpu_baseline": s.get("cpu_port")}
     print(json.dumps(line), flush=True)
 
 
@@ -1158,7 +1216,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mgpcg",
-                    choices=["mgpcg", "mcf", "splat", "c3", "c5"])
+                    choices=["mgpcg", "mcf", "splat", "c3", "c5", "g2p_mr"])
     ap.add_argument("--res", type=int, default=0, help="override the pressure resolution")
     ap.add_argument("--splat-base", type=int, default=0,
                     help="points of the splat workload's cloud (n^2 particles)")
@@ -1182,6 +1240,8 @@ def main():
         bench_mcf(args)
     elif args.workload == "splat":
         bench_splat(args)
+    elif args.workload == "g2p_mr":
+        bench_g2p_mr(args)
     elif args.workload in ("c3", "c5"):
         bench_large(args)
     else:
