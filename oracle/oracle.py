@@ -89,6 +89,8 @@ def integ():
         L.integ_mcf_f32.argtypes = [C.c_int] * 4 + [i8, C.c_float, C.c_float, f32,
                                                     C.POINTER(C.c_int), C.c_int, C.c_int, C.c_float,
                                                     C.c_int]
+        L.integ_g2p_mr.restype = C.c_int
+        L.integ_g2p_mr.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_float]
         L.integ_splat.restype = C.c_int
         L.integ_splat.argtypes = [C.c_int] * 4 + [C.c_void_p, C.c_int64, C.c_int, C.c_float,
                                                   C.c_void_p, C.c_void_p]
@@ -632,6 +634,8 @@ def _ref_mr():
         L.ref_mr_dist.restype = C.c_longlong
         L.ref_mr_dist.argtypes = [vp, vp, vp]
         L.ref_mr_dist_interp.argtypes = [vp, C.c_int, vp, C.c_longlong, vp]
+        L.ref_mr_set_vec.restype = C.c_int
+        L.ref_mr_set_vec.argtypes = [vp, C.c_int, vp]
         L._mr_sig = True
     return L
 
@@ -673,6 +677,12 @@ class RefMultires:
         out = np.zeros(len(p), np.float32)
         self.L.ref_mr_dist_interp(self.h, lv, p.ctypes.data, len(p), out.ctypes.data)
         return out
+
+    def set_vec(self, ch, packed):
+        """Fills vector channel ch of every level from the packed layout."""
+        d = np.ascontiguousarray(packed, np.float32)
+        if self.L.ref_mr_set_vec(self.h, ch, d.ctypes.data):
+            raise RuntimeError("ref_mr_set_vec failed")
 
     def close(self):
         if self.h:

@@ -7,7 +7,7 @@
 // (oracle/ref/ref_harness.cpp), so the tests can compare the drop-in's
 // results with the reference routines the snippets replace.  Each function
 // declares the variables its snippet expects from the reference call site
-// (src/msbg_demo.cpp:716-727, src/flip_sim.cpp:1289-1304).
+// (src/msbg_demo.cpp:716-727, src/flip_sim.cpp:1289-1304, 1526-1545).
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -66,7 +66,27 @@ int run_splat(MultiresSparseGrid* msbg, int chan, const std::vector<float>& pos,
   return rc;
 }
 
+// The FlipConfig field the G2P snippet reads (src/flip_sim.h:29-45).
+struct G2pConfig {
+  float flipAlpha;
+};
+
+// INTEGRATION.md "g2p_mr": gridToParticle on a mixed-resolution grid.
+int run_g2p_mr(MultiresSparseGrid* msbg, msbg_flip_particle* P, int64_t np,
+               const G2pConfig& cfg_) {
+#include "integration_g2p_mr.inc"
+  return rc;
+}
+
 }  // namespace
+
+// The G2P snippet on a grid made by ref_mr_create whose CH_VEC3_4 / CH_VEC3_2
+// channels were filled with ref_mr_set_vec; the particles are updated in place.
+extern "C" int integ_g2p_mr(void* mrGrid, msbg_flip_particle* particles, int64_t np,
+                            float flipAlpha) {
+  G2pConfig cfg = {flipAlpha};
+  return run_g2p_mr((MultiresSparseGrid*)mrGrid, particles, np, cfg);
+}
 
 // The demo's call on a single-level render-density grid: kind / values as in
 // ref_mcf_u16; values are overwritten with the result.  Returns the snippet's

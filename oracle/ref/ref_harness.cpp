@@ -511,3 +511,29 @@ extern "C" int ref_ps_downsample_velocity(void* hp, int levelMg, int chSrc, int 
   m->downsampleVelocity(levelMg, chSrc, chDst);
   return 0;
 }
+
+// Fills vector channel ch (CH_VEC3_*) of a grid made by ref_mr_create from the
+// packed layout (3 floats per voxel, each block at its own level), as the
+// reference's FLIP driver holds its velocity: getVecChannel(ch, level, 0) of
+// every level, block maps prepared first (SparseGrid::prepareDataAccess,
+// src/sbg.cpp:702-720).
+extern "C" int ref_mr_set_vec(void* mp, int ch, const float* data) {
+  auto* m = (MultiresSparseGrid*)mp;
+  const int bsx0 = m->sg0()->bsx();
+  for (int l = 0; l < m->getNumLevels(); l++) {
+    SparseGrid<Vec3Float>* sg = m->getVecChannel(ch, l, 0);
+    if (!sg) return -1;
+    if (!sg->hasData()) sg->prepareDataAccess();
+  }
+  size_t off = 0;
+  for (int b = 0; b < m->nBlocks(); b++) {
+    const int l = m->getBlockInfo(b, 0)->level;
+    const int bs = bsx0 >> l, nv = bs * bs * bs;
+    Vec3Float* d = m->getVecChannel(ch, l, 0)->getBlockDataPtr(b, 1, 0);
+    if (!d) return -1;
+    for (int i = 0; i < nv; i++)
+      d[i] = Vec3Float(data[3 * (off + i)], data[3 * (off + i) + 1], data[3 * (off + i) + 2]);
+    off += nv;
+  }
+  return 0;
+}

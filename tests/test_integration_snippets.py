@@ -22,7 +22,7 @@ def test_marked_blocks_are_the_compiled_ones():
     import extract_snippets
 
     blocks = extract_snippets.snippets(open(os.path.join(ROOT, "INTEGRATION.md")).read())
-    assert set(blocks) == {"header", "mcf_u16", "mcf_f32", "pressure", "splat"}
+    assert set(blocks) == {"header", "mcf_u16", "mcf_f32", "pressure", "splat", "g2p_mr"}
     for name, code in blocks.items():
         path = os.path.join(oracle.OUT, f"integration_{name}.inc")
         assert open(path).read() == code, f"{path} is older than INTEGRATION.md"
@@ -30,5 +30,6 @@ def test_marked_blocks_are_the_compiled_ones():
 
 def test_adapter_exports_the_snippet_runners():
     L = oracle.integ()
-    for sym in ("integ_mcf_u16", "integ_mcf_f32", "integ_pressure", "integ_splat"):
+    for sym in ("integ_mcf_u16", "integ_mcf_f32", "integ_pressure", "integ_splat",
+                "integ_g2p_mr"):
         assert hasattr(L, sym)

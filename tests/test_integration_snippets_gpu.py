@@ -12,7 +12,9 @@ objects and compared with the reference routines they replace:
     where the two operators coincide), the snippet's solution in CH_PRESSURE
     leaves a relative residual <= 1e-5 in the reference's own operator and
     right-hand side (multiplyLaplacianMatrixOpt with OPT_CALC_RESIDUAL), and
-    is within 1e-5 of the FP64 oracle."""
+    is within 1e-5 of the FP64 oracle;
+  - "g2p_mr": G2P from the velocity channels of a mixed-resolution grid the
+    reference set up, bit for bit against the restatement of gridToParticle."""
 import numpy as np
 import pytest
 
@@ -92,3 +94,35 @@ def test_splat_snippet_matches_reference_demo():
     d = np.abs(got.astype(np.int64) - ref.astype(np.int64))
     assert (ref != g["final"]).any()
     assert d.max() <= 2 and (d > 0).mean() <= 2e-3, (int(d.max()), float((d > 0).mean()))
+
+
+@pytest.mark.parametrize("name", ["z3_b16", "sphere3_b16"])
+def test_g2p_mr_snippet_on_a_reference_grid(name):
+    """The "g2p_mr" snippet reads the velocity channels of a MultiresSparseGrid
+    the reference set up (its own setRefinementMap, CH_VEC3_4 / CH_VEC3_2 of
+    every level) and updates the particles bit for bit as the restatement of
+    gridToParticle does on the same channels."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from mr_grids import grid_levels, particles_for
+
+    res, bsx, nl, lev = grid_levels(name)
+    ref = oracle.RefMultires((res,) * 3, bsx, nl, lev)
+    try:
+        _, n = oracle.mr_layout([res // bsx] * 3, bsx, lev)
+        rng = np.random.default_rng(31)
+        vel = rng.standard_normal(3 * n).astype(np.float32)
+        old = rng.standard_normal(3 * n).astype(np.float32)
+        ref.set_vec(23, vel)  # CH_VEC3_4 (src/msbg.h:305)
+        ref.set_vec(21, old)  # CH_VEC3_2
+        p = particles_for(res, 100_000, 32)
+        q = p.copy()
+        rc = oracle.integ().integ_g2p_mr(ref.h, q.ctypes.data, len(q), 0.95)
+        assert rc == 0
+        d, k = oracle.mr_dist([res // bsx] * 3, bsx, lev, nl)
+        e = oracle.mr_g2p((res,) * 3, bsx, lev, p, vel, old, d, k, 0.95)
+        assert (q["vel"].view(np.uint32) == e["vel"].view(np.uint32)).all()
+    finally:
+        ref.close()
